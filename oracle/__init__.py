@@ -1,0 +1,317 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+The oracle restates the reference's per-step particle hot path in plain C
+(``ctc_oracle.c``).  Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` use it -- as the checker, never as the product.
+
+Particle arrays are the reference's AoS layout ``Particle {float r[3], v[3]}``
+(src/inc/type.h:6-8) as numpy ``float32`` arrays of shape ``(n, 6)``.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libctc_oracle.so")
+_lib = None
+
+f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+
+
+class Dpd(C.Structure):
+    """``PairDPD {a, g, s, spow}`` (src/pair/type.h:7-9)."""
+    _fields_ = [("a", C.c_float), ("g", C.c_float), ("s", C.c_float), ("spow", C.c_float)]
+
+
+class RbcParams(C.Structure):
+    """``RbcParams_v`` (src/rbc/params/imp.h:3-9)."""
+    _fields_ = [(k, C.c_float) for k in
+                ("gammaC", "gammaT", "kBT", "kb", "phi", "ks", "x0", "mpow", "ka", "kd", "kv",
+                 "totArea", "totVolume")]
+
+
+def build():
+    """Compile the oracle with its Makefile (gcc, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        sig = {
+            "orc_kiss_ini": (None, [u32p, C.c_int, C.c_int, C.c_int, C.c_int]),
+            "orc_kiss_get": (C.c_float, [u32p]),
+            "orc_mean0var1ii": (C.c_float, [C.c_float, C.c_int, C.c_int]),
+            "orc_mean0var1uu": (C.c_float, [C.c_float, C.c_uint32, C.c_uint32]),
+            "orc_set_rng_contraction": (None, [C.c_int]),
+            "orc_get_rng_contraction": (C.c_int, []),
+            "orc_pair_force": (None, [C.c_float] * 4 + [f32p, f32p, C.c_float, f32p]),
+            "orc_clist_build": (C.c_int, [C.c_int] * 4 + [f32p, C.c_int, i32p, i32p, i32p, f32p]),
+            "orc_dpd_bulk": (None, [C.c_int] * 4 + [f32p, i32p, Dpd, C.c_float, f32p]),
+            "orc_dpd_bulk_f64": (None, [C.c_int] * 4 + [f32p, i32p, Dpd, C.c_float, f64p]),
+            "orc_dpd_bulk_parallel": (None, [C.c_int] * 4 + [f32p, i32p, Dpd, C.c_float, f32p]),
+            "orc_dpd_halo": (None, [C.c_int] * 4 + [f32p, i32p, i32p, Dpd, f32p, f32p]),
+            "orc_dpd_halo_f64": (None, [C.c_int] * 4 + [f32p, i32p, i32p, Dpd, f32p, f64p]),
+            "orc_halo_masks": (None, [i32p]),
+            "orc_halo_trunk_ini": (None, [C.c_int, u32p]),
+            "orc_frag_i2d": (C.c_int, [C.c_int, C.c_int]),
+            "orc_frag_d2i": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+            "orc_frag_anti": (C.c_int, [C.c_int]),
+            "orc_fsi_bulk": (None, [C.c_int] * 4 + [f32p, C.c_int, f32p, i32p, Dpd, C.c_float, f32p, f32p]),
+            "orc_fsi_halo": (None, [C.c_int] * 4 + [f32p, C.c_int, f32p, i32p, Dpd, C.c_float, f32p, f32p]),
+            "orc_fsi_halo_images": (C.c_int, [C.c_int] * 4 + [f32p, C.c_void_p, C.c_void_p]),
+            "orc_mesh_md": (C.c_int, [C.c_int, C.c_int, i32p]),
+            "orc_adj_build": (C.c_int, [C.c_int] * 3 + [i32p, i32p, i32p]),
+            "orc_area_volume": (None, [C.c_int] * 3 + [i32p, f32p, f64p]),
+            "orc_area_volume_f32": (None, [C.c_int] * 3 + [i32p, f32p, f32p]),
+            "orc_rbc_forces": (None, [C.c_int] * 5 + [i32p, i32p, f32p, f64p, RbcParams, f32p]),
+            "orc_rbc_forces_f64": (None, [C.c_int] * 4 + [i32p, i32p, f32p, f64p, RbcParams, f64p]),
+            "orc_kantor_energy": (C.c_double, [C.c_int, C.c_int, i32p, i32p, f32p, C.c_double, C.c_double]),
+            "orc_move": (None, [C.c_float, C.c_float, C.c_int, f32p, f32p]),
+            "orc_body_force": (None, [C.c_float, f32p, C.c_int, f32p]),
+            "orc_wrap": (None, [C.c_int] * 4 + [f32p]),
+            "orc_rbc_wrap": (None, [C.c_int] * 5 + [f32p]),
+            "orc_diag": (None, [C.c_int, f32p, C.c_double, f64p]),
+            "orc_read_floats": (C.c_int, [C.c_char_p, f32p, C.c_int]),
+            "orc_num_threads": (C.c_int, []),
+            "orc_dpd_step": (C.c_int, [C.c_int] * 4 + [f32p, f32p, Dpd, f32p, C.c_float, C.c_void_p, C.c_float]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _pp(pp):
+    return np.ascontiguousarray(pp, dtype=np.float32).reshape(-1, 6)
+
+
+# ---- RNG -------------------------------------------------------------------
+class Kiss:
+    """KISS trunk generator (src/math/rnd/imp.cpp:12-34)."""
+
+    def __init__(self, x, y, z, c):
+        self.st = np.zeros(4, np.uint32)
+        lib().orc_kiss_ini(self.st, x, y, z, c)
+
+    @classmethod
+    def halo(cls, fid):
+        k = cls(0, 0, 0, 0)
+        lib().orc_halo_trunk_ini(fid, k.st)
+        return k
+
+    def get(self):
+        return float(np.float32(lib().orc_kiss_get(self.st)))
+
+
+def mean0var1ii(seed, u, v):
+    return np.float32(lib().orc_mean0var1ii(seed, int(u), int(v)))
+
+
+def mean0var1uu(seed, u, v):
+    return np.float32(lib().orc_mean0var1uu(seed, int(u), int(v)))
+
+
+def halo_masks():
+    m = np.zeros(26, np.int32)
+    lib().orc_halo_masks(m)
+    return m
+
+
+def frag_anti(i):
+    return lib().orc_frag_anti(i)
+
+
+def frag_dir(i):
+    return tuple(lib().orc_frag_i2d(i, c) for c in range(3))
+
+
+# ---- cell lists ------------------------------------------------------------
+def clist_build(L, pp, project=False):
+    """Returns (counts, starts[ncells+1], order, ppout) -- stable cell order."""
+    pp = _pp(pp)
+    LX, LY, LZ = L
+    nc = LX * LY * LZ
+    counts = np.zeros(nc, np.int32)
+    starts = np.zeros(nc + 1, np.int32)
+    order = np.zeros(max(len(pp), 1), np.int32)
+    out = np.zeros((max(len(pp), 1), 6), np.float32)
+    nout = lib().orc_clist_build(LX, LY, LZ, len(pp), pp, int(project), counts, starts, order, out)
+    starts[nc] = nout
+    return counts, starts, order[:nout], out[:nout]
+
+
+# ---- solvent forces ----------------------------------------------------------
+def dpd_bulk(L, pp, starts, dpd, seed, f64=False):
+    pp = _pp(pp)
+    if f64:
+        ff = np.zeros((len(pp), 3), np.float64)
+        lib().orc_dpd_bulk_f64(*L, len(pp), pp, starts, Dpd(*dpd), seed, ff)
+    else:
+        ff = np.zeros((len(pp), 3), np.float32)
+        lib().orc_dpd_bulk(*L, len(pp), pp, starts, Dpd(*dpd), seed, ff)
+    return ff
+
+
+def dpd_halo(L, pp, starts, counts, dpd, seeds, f64=False):
+    pp = _pp(pp)
+    seeds = np.ascontiguousarray(seeds, np.float32)
+    if f64:
+        ff = np.zeros((len(pp), 3), np.float64)
+        lib().orc_dpd_halo_f64(*L, len(pp), pp, starts, counts, Dpd(*dpd), seeds, ff)
+    else:
+        ff = np.zeros((len(pp), 3), np.float32)
+        lib().orc_dpd_halo(*L, len(pp), pp, starts, counts, Dpd(*dpd), seeds, ff)
+    return ff
+
+
+def pair_force(dpd, pa, pb, rnd):
+    f = np.zeros(3, np.float32)
+    lib().orc_pair_force(*[float(x) for x in dpd], np.asarray(pa, np.float32),
+                         np.asarray(pb, np.float32), float(rnd), f)
+    return f
+
+
+# ---- FSI -------------------------------------------------------------------
+def fsi_forces(L, pv, ps, starts, dpd, seed_bulk, seed_halo):
+    pv, ps = _pp(pv), _pp(ps)
+    fv = np.zeros((len(pv), 3), np.float32)
+    fs = np.zeros((len(ps), 3), np.float32)
+    lib().orc_fsi_bulk(*L, len(pv), pv, len(ps), ps, starts, Dpd(*dpd), seed_bulk, fv, fs)
+    lib().orc_fsi_halo(*L, len(pv), pv, len(ps), ps, starts, Dpd(*dpd), seed_halo, fv, fs)
+    return fv, fs
+
+
+def fsi_halo_images(L, pv):
+    pv = _pp(pv)
+    n = lib().orc_fsi_halo_images(*L, len(pv), pv, None, None)
+    frag = np.zeros(max(n, 1), np.int32)
+    vert = np.zeros(max(n, 1), np.int32)
+    lib().orc_fsi_halo_images(*L, len(pv), pv, frag.ctypes.data, vert.ctypes.data)
+    return frag[:n], vert[:n]
+
+
+# ---- membrane ----------------------------------------------------------------
+def mesh_md(tri, nv):
+    tri4 = _tri4(tri)
+    return lib().orc_mesh_md(nv, len(tri4), tri4)
+
+
+def _tri4(tri):
+    tri = np.asarray(tri, np.int32)
+    if tri.shape[1] == 3:
+        tri = np.concatenate([tri, np.zeros((len(tri), 1), np.int32)], 1)
+    return np.ascontiguousarray(tri)
+
+
+def adj_build(tri, nv, md=None):
+    tri4 = _tri4(tri)
+    if md is None:
+        md = lib().orc_mesh_md(nv, len(tri4), tri4)
+    a0 = np.zeros(nv * md, np.int32)
+    a1 = np.zeros(nv * md, np.int32)
+    if lib().orc_adj_build(md, len(tri4), nv, tri4, a0, a1) != 0:
+        raise ValueError("mesh is not a closed manifold of valence <= md")
+    return md, a0, a1
+
+
+def area_volume(tri, nv, pp, f32=False):
+    tri4 = _tri4(tri)
+    pp = _pp(pp)
+    nc = len(pp) // nv
+    if f32:
+        av = np.zeros(2 * nc, np.float32)
+        lib().orc_area_volume_f32(nc, nv, len(tri4), tri4, pp, av)
+    else:
+        av = np.zeros(2 * nc, np.float64)
+        lib().orc_area_volume(nc, nv, len(tri4), tri4, pp, av)
+    return av.reshape(nc, 2)
+
+
+def rbc_forces(tri, nv, pp, params, av=None, mode=0, f64=False):
+    """Internal membrane forces; params is a dict of RbcParams fields."""
+    tri4 = _tri4(tri)
+    pp = _pp(pp)
+    md, a0, a1 = adj_build(tri4, nv)
+    nc = len(pp) // nv
+    if av is None:
+        av = area_volume(tri4, nv, pp)
+    av = np.ascontiguousarray(av, np.float64).reshape(-1)
+    par = RbcParams(**params)
+    if f64:
+        ff = np.zeros((len(pp), 3), np.float64)
+        lib().orc_rbc_forces_f64(nc, nv, md, len(tri4), a0, a1, pp, av, par, ff)
+    else:
+        ff = np.zeros((len(pp), 3), np.float32)
+        lib().orc_rbc_forces(mode, nc, nv, md, len(tri4), a0, a1, pp, av, par, ff)
+    return ff
+
+
+def kantor_energy(tri, nv, pp, kb, phi_deg=0.0):
+    md, a0, a1 = adj_build(tri, nv)
+    return lib().orc_kantor_energy(nv, md, a0, a1, _pp(pp), kb, phi_deg)
+
+
+# ---- update --------------------------------------------------------------------
+def move(pp, ff, dt, mass):
+    pp = _pp(pp).copy()
+    lib().orc_move(dt, mass, len(pp), np.ascontiguousarray(ff, np.float32), pp)
+    return pp
+
+
+def body_force(ff, mass, a):
+    ff = np.ascontiguousarray(ff, np.float32).copy()
+    lib().orc_body_force(mass, np.asarray(a, np.float32), len(ff), ff)
+    return ff
+
+
+def wrap(L, pp):
+    pp = _pp(pp).copy()
+    lib().orc_wrap(*L, len(pp), pp)
+    return pp
+
+
+def rbc_wrap(L, pp, nv):
+    pp = _pp(pp).copy()
+    lib().orc_rbc_wrap(*L, len(pp) // nv, nv, pp)
+    return pp
+
+
+def diag(pp, mass):
+    out = np.zeros(5, np.float64)
+    pp = _pp(pp)
+    lib().orc_diag(len(pp), pp, mass, out)
+    return out
+
+
+def read_floats(path, cap=1 << 24):
+    buf = np.zeros(cap, np.float32)
+    n = lib().orc_read_floats(path.encode(), buf, cap)
+    if n < 0:
+        raise FileNotFoundError(path)
+    return buf[:n].copy()
+
+
+def num_threads():
+    return lib().orc_num_threads()
+
+
+def dpd_step(L, pp, dpd, seeds, mass, bodyf, dt):
+    """One plain DPD step in the reference's order (OpenMP)."""
+    pp = _pp(pp).copy()
+    work = np.zeros_like(pp)
+    seeds = np.ascontiguousarray(seeds, np.float32)
+    bf = None if bodyf is None else np.ascontiguousarray(bodyf, np.float32)
+    n = lib().orc_dpd_step(*L, len(pp), pp, work, Dpd(*dpd), seeds, mass,
+                           None if bf is None else bf.ctypes.data, dt)
+    return pp[:n]
