@@ -1,0 +1,333 @@
+"""Benchmark of the per-step particle hot path (plain DPD solvent).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1]
+
+One "step" = wrap + cell-list rebuild, bulk + periodic-halo DPD forces with the
+reference's pair RNG keys, constant body force, update -- the reference's step
+order.  Default workload: the large plain-DPD Poiseuille box 192 x 96 x 96 at
+number density 10 (17,694,720 particles), a = 2.5, gamma = 8, kBT = 0.0444,
+spow = 0.25, dt = 5e-4, body force 0.01 along x; seeded synthetic input.
+The metric is particle-steps/s.  Multi-GPU runs are independent replicas (one
+box per rank, no data-path collective): value = all ranks' particle-steps /
+the max over ranks of the timed region.
+
+--impl reference times the reference's own CPU path of the step (the C
+restatement in oracle/, in the reference's operation order; the reference
+kernels have no CPU build) on this host's cores, on a bounded sample of the
+same workload, and prints the same JSON line with "impl": "reference".
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "c2": dict(L=(192, 96, 96), bodyf=(0.01, 0.0, 0.0), steps=200,
+               name="C2 plain DPD Poiseuille 192x96x96 rho=10 (17,694,720 particles), body force 0.01 x"),
+    "c1": dict(L=(16, 16, 16), bodyf=(0.0, 0.0, 0.0), steps=100,
+               name="C1 plain DPD 16x16x16 rho=10 (40,960 particles)"),
+    # profiling case: the C2 kernels on a box whose state still exceeds L2
+    "p64": dict(L=(64, 64, 64), bodyf=(0.01, 0.0, 0.0), steps=10,
+                name="plain DPD 64x64x64 rho=10 (2,621,440 particles), body force 0.01 x"),
+}
+METRIC = "particle-steps/s @1 B200 (plain DPD step)"
+PAIR_BYTES = 48          # algorithmic bytes per particle of the pair kernel: pos+vel read, force write
+PAIR_FLOP = 100 * 20.94  # ~100 flop per accepted half-pair, 20.94 half-pairs per particle at rho=10
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(world, x):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+    return x
+
+
+def allsum(world, x):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+    return x
+
+
+# ---------------------------------------------------------------------------
+# CPU leg: the oracle's step on the host cores
+# ---------------------------------------------------------------------------
+def cpu_sample_box(L, target_s=3.0):
+    """A periodic sub-box of the workload (same x, y extent and density) sized
+    so that one CPU step takes about target_s seconds."""
+    import oracle
+    from ctc_b200 import systems
+    probe = (32, 32, 16)
+    pp = systems.solvent(probe, seed=99)
+    dpd = systems.dpd_params()
+    seeds = np.random.default_rng(0).random(27).astype(np.float32)
+    t0 = time.perf_counter()
+    oracle.dpd_step(probe, pp, dpd, seeds, 1.0, (0.01, 0, 0), 5e-4)
+    rate = len(pp) / (time.perf_counter() - t0)
+    per_z = 10 * L[0] * L[1]
+    z = int(max(4, min(L[2], target_s * rate / per_z)))
+    return (L[0], L[1], z), rate
+
+
+def cpu_steps(L, nsteps, bodyf):
+    import oracle
+    from ctc_b200 import systems
+    pp = systems.solvent(L, seed=2)
+    dpd = systems.dpd_params()
+    k0 = oracle.Kiss(0, 0, 0, 0)
+    kh = [oracle.Kiss.halo(f) for f in range(26)]
+    times = []
+    for _ in range(nsteps):
+        seeds = np.array([k0.get()] + [k.get() for k in kh], np.float32)
+        t0 = time.perf_counter()
+        pp = oracle.dpd_step(L, pp, dpd, seeds, 1.0, bodyf, 5e-4)
+        times.append(time.perf_counter() - t0)
+    return len(pp), times
+
+
+def run_reference(args, cfg, world, rank):
+    if rank != 0:
+        return
+    import oracle
+    oracle.lib()
+    box, _ = cpu_sample_box(cfg["L"])
+    n, times = cpu_steps(box, args.warmup + args.steps, cfg["bodyf"])
+    t = float(np.sum(times[args.warmup:]))
+    value = n * args.steps / t
+    cores = oracle.num_threads()
+    sample = "periodic sub-box %dx%dx%d (%d particles) of the workload, %d timed steps" % (box + (n, args.steps))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform solvent)",
+        "config": {"workload": cfg["name"], "sample": sample, "parallelism": "host cores (OpenMP)"},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU leg
+# ---------------------------------------------------------------------------
+def run_ours(args, cfg, world, rank, local):
+    import ctypes as C
+
+    import torch
+
+    import ctc_b200 as ctc
+    from ctc_b200 import _lib, systems
+    torch.cuda.set_device(local)
+    L = cfg["L"]
+    pp = systems.solvent(L, seed=2 + rank)
+    n = len(pp)
+    dpd = ctc.DpdParams(*systems.dpd_params())
+    stream = torch.cuda.current_stream()
+    sim = ctc.Sim(L, n, dpd, mass=1.0, dt=systems.DT, bodyf=cfg["bodyf"])
+    sim.set_solvent(pp)
+    sim.step(args.warmup)
+    torch.cuda.synchronize()
+    _lib.check(_lib.lib().ctc_sim_profile(sim.h, 1))
+
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    ms4 = (C.c_double * 4)()
+    nst = C.c_int(0)
+    _lib.check(_lib.lib().ctc_sim_profile_read(sim.h, ms4, C.byref(nst)))
+    _lib.check(_lib.lib().ctc_sim_profile(sim.h, 0))
+    assert ctc.device_error() == 0, "device error during the timed steps"
+    ms_max = allmax(world, ms)
+    total = allsum(world, n * args.steps)
+    value = total / (ms_max * 1e-3)
+
+    # end to end through the public API with host buffers: upload the state
+    # from pinned memory, K steps each with its FP64 diagnostics read back,
+    # download the final state
+    host_in = torch.from_numpy(pp).pin_memory()
+    host_out = torch.empty((n, 6), dtype=torch.float32).pin_memory()
+    diag = (C.c_double * 5)()
+    nout = C.c_int(0)
+    st = C.c_void_p(stream.cuda_stream)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _lib.check(_lib.lib().ctc_sim_set_solvent(sim.h, n, C.c_void_p(host_in.data_ptr()), st))
+    for _ in range(args.steps):
+        _lib.check(_lib.lib().ctc_sim_step(sim.h, 1, st))
+        _lib.check(_lib.lib().ctc_sim_diag(sim.h, diag, st))
+    _lib.check(_lib.lib().ctc_sim_get_solvent(sim.h, C.c_void_p(host_out.data_ptr()), C.byref(nout), st))
+    torch.cuda.synchronize()
+    e2e_s = allmax(world, time.perf_counter() - t0)
+    e2e_value = total / e2e_s
+    state_bytes = 24 * n
+    sim.close()
+
+    if rank != 0:
+        return
+    hbm, peak_kind = peaks()
+    pair_ms = ms4[2] / max(nst.value, 1)
+    achieved = PAIR_BYTES * n / (pair_ms * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "dpd_tiles_traffic.json")
+    if os.path.exists(tp):
+        d = json.load(open(tp))
+        traffic = d["bytes_per_particle"] * n
+    phases = {k: v / max(nst.value, 1) for k, v in zip(("clist", "frag_starts", "pair", "update"), ms4)}
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform solvent, Maxwellian velocities)",
+        "config": {"workload": cfg["name"], "particles_per_gpu": n, "box": list(L), "rho": 10,
+                   "rng": "reference keys", "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (state %.2f GB per buffer)" % (32e-9 * n)},
+        "gpu_launches": 10 * args.steps,   # seeds, 6 cell-list kernels, fragment starts, pair, update
+        "phase_ms": phases,
+        "roofline": {"bound": "hbm", "kernel": "k_dpd_tiles", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "peak_kind": peak_kind,
+                     "note": "pair kernel is FP32-issue bound: %.1f TFLOP/s of ~%d flop/particle" %
+                             (PAIR_FLOP * n / (pair_ms * 1e-3) / 1e12, PAIR_FLOP)},
+        "e2e": {"value": e2e_value, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": state_bytes / args.steps,
+                "d2h_bytes_per_step": 40 + state_bytes / args.steps},
+    }
+    if clk:
+        line["clocks"] = clk
+    if world == 1 and not args.no_cpu:
+        box, _ = cpu_sample_box(L, target_s=3.0)
+        nb, times = cpu_steps(box, 2, cfg["bodyf"])
+        import oracle
+        line["cpu_baseline"] = {"value": nb / float(np.mean(times)), "unit": "particle-steps/s",
+                                "cores": oracle.num_threads(), "kind": "port",
+                                "sample": "periodic sub-box %dx%dx%d (%d particles), 2 steps" % (box + (nb,))}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, cfg, world, rank)
+    else:
+        run_ours(args, cfg, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

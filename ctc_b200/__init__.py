@@ -1,0 +1,270 @@
+"""ctc_b200 -- B200-native per-step particle hot path of uDeviceX (rossinelli/CTC).
+
+The compute path is libctc_b200.so (hand-written sm_100a CUDA behind the C ABI
+of include/ctc_b200.h).  This module is the host-side mirror of the
+reference's module interface for Python callers and the tests: the same
+module and function names (clist_build, fluforces_bulk_apply, ...), the same
+argument meaning and the same accumulate-into-forces convention.  Device
+arrays are torch CUDA tensors (PyTorch is only the device-memory plumbing);
+particle arrays use the reference's AoS layout, shape (n, 6) float32.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import CTC_RNG_REFERENCE, CTC_RNG_STABLE, CtcError, check, device_error, lib
+
+__all__ = ["Clist", "FluForces", "Sim", "DpdParams", "RbcParams", "RbcForce", "Fsi", "dpd_sigma", "scheme_move_apply",
+           "scheme_move_clear_vel", "bforce_apply_cste", "rnd_mean0var1", "CTC_RNG_REFERENCE",
+           "CTC_RNG_STABLE", "CtcError", "device_error"]
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise CtcError("expected a contiguous CUDA tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def DpdParams(a, g, s, spow):
+    """PairDPD {a, g, s, spow} (src/pair/type.h:7-9)."""
+    return _lib.DpdParams(a, g, s, spow)
+
+
+def dpd_sigma(kBT, g, dt):
+    """sigma = sqrt(2 kBT g / dt) (src/pair/imp/main.h:54-62)."""
+    return float(lib().ctc_dpd_sigma(kBT, g, dt))
+
+
+class Clist:
+    """Cell lists of one box (src/clist/imp.h): ``Clist(L, maxp).build(pp)``."""
+
+    def __init__(self, L, maxp):
+        self.L = tuple(int(x) for x in L)
+        self.h = C.c_void_p()
+        check(lib().ctc_clist_ini(*self.L, int(maxp), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
+            lib().ctc_clist_fin(self.h)
+            self.h = None
+
+    def build(self, pp, stream=None):
+        """clist_build: returns (ppout[nout,6], starts[ncells+1], counts[ncells], ids[nout])."""
+        torch = _torch()
+        n = int(pp.shape[0])
+        out = torch.empty_like(pp)
+        nout = C.c_int(0)
+        check(lib().ctc_clist_build(self.h, n, _ptr(pp), _ptr(out), C.byref(nout), _stream(stream)))
+        s, c, i = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        check(lib().ctc_clist_get(self.h, C.byref(s), C.byref(c), C.byref(i)))
+        nc = self.L[0] * self.L[1] * self.L[2]
+        starts = _wrap_dev(s.value, nc + 1, torch.int32, pp.device).clone()
+        counts = _wrap_dev(c.value, nc, torch.int32, pp.device).clone()
+        ids = _wrap_dev(i.value, nout.value, torch.int32, pp.device).clone()
+        return out[:nout.value], starts, counts, ids
+
+
+class _DevArray:
+    """A raw device address seen through __cuda_array_interface__."""
+
+    def __init__(self, addr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (addr, False),
+                                         "version": 2}
+
+
+def _wrap_dev(addr, n, dtype, device):
+    """Copy n elements at a device address into a new tensor."""
+    torch = _torch()
+    if n <= 0:
+        return torch.empty(0, dtype=dtype, device=device)
+    typestr = {torch.int32: "<i4", torch.float32: "<f4"}[dtype]
+    return torch.as_tensor(_DevArray(addr, n, typestr), device=device)
+
+
+class FluForces:
+    """Solvent DPD forces of one periodic box (src/fluforces/imp.h).
+
+    Holds the trunk generators like fluforces_bulk_ini / fluforces_halo_ini:
+    ``bulk_apply`` and ``halo_apply`` draw their seeds as the reference does;
+    ``apply_seeded`` takes explicit seeds (27 floats: bulk, then fragments)."""
+
+    def __init__(self, L, maxp):
+        self.L = tuple(int(x) for x in L)
+        self.h = C.c_void_p()
+        check(lib().ctc_fluforces_ini(*self.L, int(maxp), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
+            lib().ctc_fluforces_fin(self.h)
+            self.h = None
+
+    def bulk_apply(self, params, pp, starts, counts, ff, stream=None):
+        check(lib().ctc_fluforces_bulk_apply(self.h, C.byref(params), int(pp.shape[0]), _ptr(pp), _ptr(starts),
+                                             _ptr(counts), _ptr(ff), _stream(stream)))
+
+    def halo_apply(self, params, pp, starts, counts, ff, stream=None):
+        check(lib().ctc_fluforces_halo_apply(self.h, C.byref(params), int(pp.shape[0]), _ptr(pp), _ptr(starts),
+                                             _ptr(counts), _ptr(ff), _stream(stream)))
+
+    def apply_seeded(self, params, pp, starts, counts, seeds, ff, which=3, rng=CTC_RNG_REFERENCE, stream=None):
+        sd = (C.c_float * 27)(*[float(x) for x in np.asarray(seeds, np.float32).reshape(-1)[:27]])
+        check(lib().ctc_fluforces_apply_seeded(self.h, C.byref(params), int(pp.shape[0]), _ptr(pp), _ptr(starts),
+                                               _ptr(counts), sd, int(which), int(rng), _ptr(ff), _stream(stream)))
+
+
+def RbcParams(**kw):
+    """RbcParams_v (src/rbc/params/imp.h:3-9) from keyword fields."""
+    return _lib.RbcParams(**kw)
+
+
+class RbcForce:
+    """Membrane internal forces of cells of one template (src/rbc/force/imp.h)."""
+
+    def __init__(self, tri, nv, max_cells):
+        tri = np.ascontiguousarray(tri, np.int32).reshape(-1, 3)
+        self.nv, self.nt = int(nv), len(tri)
+        self.h = C.c_void_p()
+        check(lib().ctc_rbc_force_ini(self.nv, self.nt, tri.ctypes.data_as(C.c_void_p), int(max_cells),
+                                      C.byref(self.h)))
+        md = C.c_int(0)
+        check(lib().ctc_rbc_force_md(self.h, C.byref(md)))
+        self.md = md.value
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
+            lib().ctc_rbc_force_fin(self.h)
+            self.h = None
+
+    def set_bending(self, kantor=True):
+        check(lib().ctc_rbc_force_set_bending(self.h, int(bool(kantor))))
+
+    def apply(self, params, pp, ff, dt=5e-4, stream=None):
+        """rbc_force_apply: adds the internal forces of pp (nc*nv, 6) to ff (nc*nv, 3)."""
+        nc = int(pp.shape[0]) // self.nv
+        check(lib().ctc_rbc_force_apply(self.h, C.byref(params), float(dt), nc, _ptr(pp), _ptr(ff),
+                                        _stream(stream)))
+
+    def area_volume(self, pp, stream=None):
+        torch = _torch()
+        nc = int(pp.shape[0]) // self.nv
+        av = torch.empty((nc, 2), dtype=torch.float64, device=pp.device)
+        check(lib().ctc_rbc_area_volume(self.h, nc, _ptr(pp), _ptr(av), _stream(stream)))
+        return av
+
+
+class Fsi:
+    """Solvent-membrane DPD forces of one periodic box (src/fsi/imp.h)."""
+
+    def __init__(self, L, maxv, maxs):
+        self.h = C.c_void_p()
+        check(lib().ctc_fsi_ini(*(int(x) for x in L), int(maxv), int(maxs), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
+            lib().ctc_fsi_fin(self.h)
+            self.h = None
+
+    def apply(self, params, pv, ps, starts, counts, fv, fs, stream=None):
+        check(lib().ctc_fsi_apply(self.h, C.byref(params), int(pv.shape[0]), _ptr(pv), int(ps.shape[0]), _ptr(ps),
+                                  _ptr(starts), _ptr(counts), _ptr(fv), _ptr(fs), _stream(stream)))
+
+    def apply_seeded(self, params, pv, ps, starts, counts, seed_bulk, seed_halo, fv, fs, rng=CTC_RNG_REFERENCE,
+                     stream=None):
+        check(lib().ctc_fsi_apply_seeded(self.h, C.byref(params), int(pv.shape[0]), _ptr(pv), int(ps.shape[0]),
+                                         _ptr(ps), _ptr(starts), _ptr(counts), float(seed_bulk), float(seed_halo),
+                                         int(rng), _ptr(fv), _ptr(fs), _stream(stream)))
+
+
+def scheme_move_apply(dt, mass, ff, pp, stream=None):
+    """src/scheme/move/imp.h:5 -- v += f/m dt; r += v dt (in place on pp)."""
+    check(lib().ctc_scheme_move_apply(dt, mass, int(pp.shape[0]), _ptr(ff), _ptr(pp), _stream(stream)))
+
+
+def scheme_move_clear_vel(pp, stream=None):
+    check(lib().ctc_scheme_move_clear_vel(int(pp.shape[0]), _ptr(pp), _stream(stream)))
+
+
+def bforce_apply_cste(mass, a, ff, stream=None):
+    av = (C.c_float * 3)(*[float(x) for x in a])
+    check(lib().ctc_bforce_apply_cste(mass, av, int(ff.shape[0]), _ptr(ff), _stream(stream)))
+
+
+def pair_force(params, pa, pb, rnd, stream=None):
+    """pair_force<PairDPD> (src/pair/dev.h:111-139) on n pairs of AoS particles."""
+    torch = _torch()
+    f = torch.empty((pa.shape[0], 3), dtype=torch.float32, device=pa.device)
+    check(lib().ctc_pair_force(int(pa.shape[0]), C.byref(params), _ptr(pa), _ptr(pb), _ptr(rnd), _ptr(f),
+                               _stream(stream)))
+    return f
+
+
+def rnd_mean0var1(seed, u, v, unsigned=False, stream=None):
+    """Pair random numbers rnd::mean0var1ii / mean0var1uu (src/math/rnd/dev.h:57-72)."""
+    torch = _torch()
+    out = torch.empty(u.shape[0], dtype=torch.float32, device=u.device)
+    check(lib().ctc_rnd_mean0var1(int(u.shape[0]), float(seed), _ptr(u), _ptr(v), int(bool(unsigned)),
+                                  _ptr(out), _stream(stream)))
+    return out
+
+
+class Sim:
+    """Plain DPD solvent in one periodic box on the fast path (cell-sorted
+    float4 SoA state on the device, one step = wrap + cell lists, bulk + halo
+    DPD, body force, update)."""
+
+    def __init__(self, L, maxp, dpd, mass=1.0, dt=5e-4, bodyf=(0.0, 0.0, 0.0), rng=CTC_RNG_REFERENCE):
+        cfg = _lib.SimConfig()
+        cfg.LX, cfg.LY, cfg.LZ = (int(x) for x in L)
+        cfg.maxp = int(maxp)
+        cfg.dpd = dpd
+        cfg.mass = mass
+        cfg.dt = dt
+        cfg.bodyf = (C.c_float * 3)(*bodyf)
+        cfg.rng = rng
+        self.maxp = int(maxp)
+        self.h = C.c_void_p()
+        check(lib().ctc_sim_create(C.byref(cfg), C.byref(self.h)))
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
+            lib().ctc_sim_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_solvent(self, pp, stream=None):
+        pp = np.ascontiguousarray(pp, np.float32).reshape(-1, 6)
+        check(lib().ctc_sim_set_solvent(self.h, len(pp), pp.ctypes.data_as(C.c_void_p), _stream(stream)))
+
+    def step(self, n=1, stream=None):
+        check(lib().ctc_sim_step(self.h, int(n), _stream(stream)))
+
+    def get_solvent(self, stream=None):
+        out = np.zeros((self.maxp, 6), np.float32)
+        n = C.c_int(0)
+        check(lib().ctc_sim_get_solvent(self.h, out.ctypes.data_as(C.c_void_p), C.byref(n), _stream(stream)))
+        return out[:n.value]
+
+    def diag(self, stream=None):
+        out = (C.c_double * 5)()
+        check(lib().ctc_sim_diag(self.h, out, _stream(stream)))
+        return np.array(out[:])
+
+    def next_seeds(self):
+        s = (C.c_float * 27)()
+        check(lib().ctc_sim_next_seeds(self.h, s))
+        return np.array(s[:], np.float32)

@@ -1,0 +1,114 @@
+"""ctypes binding of libctc_b200.so (the C ABI of include/ctc_b200.h).
+
+The library is the product: if it is missing or fails to load this module
+raises -- there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libctc_b200.so")
+
+CTC_OK, CTC_ERR_ARG, CTC_ERR_CUDA, CTC_ERR_CAPACITY, CTC_ERR_DEVICE = 0, 1, 2, 3, 4
+CTC_RNG_REFERENCE, CTC_RNG_STABLE = 0, 1
+
+vp = C.c_void_p
+ip = C.POINTER(C.c_int)
+fp = C.POINTER(C.c_float)
+
+
+class DpdParams(C.Structure):
+    _fields_ = [("a", C.c_float), ("g", C.c_float), ("s", C.c_float), ("spow", C.c_float)]
+
+
+class RbcParams(C.Structure):
+    _fields_ = [(k, C.c_float) for k in
+                ("gammaC", "gammaT", "kBT", "kb", "phi", "ks", "x0", "mpow", "ka", "kd", "kv",
+                 "totArea", "totVolume")]
+
+
+class SimConfig(C.Structure):
+    _fields_ = [("LX", C.c_int), ("LY", C.c_int), ("LZ", C.c_int), ("maxp", C.c_int),
+                ("dpd", DpdParams), ("mass", C.c_float), ("dt", C.c_float),
+                ("bodyf", C.c_float * 3), ("rng", C.c_int)]
+
+
+# name -> (restype, argtypes); every symbol include/ctc_b200.h declares
+SIGNATURES = {
+    "ctc_status_string": (C.c_char_p, [C.c_int]),
+    "ctc_last_error": (C.c_char_p, []),
+    "ctc_device_error": (C.c_int, [ip]),
+    "ctc_version": (C.c_char_p, []),
+    "ctc_dpd_sigma": (C.c_float, [C.c_float, C.c_float, C.c_float]),
+    "ctc_rnd_mean0var1": (C.c_int, [C.c_int, C.c_float, vp, vp, C.c_int, vp, vp]),
+    "ctc_pair_force": (C.c_int, [C.c_int, C.POINTER(DpdParams), vp, vp, vp, vp, vp]),
+    "ctc_clist_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
+    "ctc_clist_fin": (C.c_int, [vp]),
+    "ctc_clist_build": (C.c_int, [vp, C.c_int, vp, vp, ip, vp]),
+    "ctc_clist_get": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+    "ctc_fluforces_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
+    "ctc_fluforces_fin": (C.c_int, [vp]),
+    "ctc_fluforces_bulk_apply": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, vp, vp, vp, vp]),
+    "ctc_fluforces_halo_apply": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, vp, vp, vp, vp]),
+    "ctc_fluforces_apply_seeded": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, vp, vp, fp, C.c_int,
+                                             C.c_int, vp, vp]),
+    "ctc_rbc_force_ini": (C.c_int, [C.c_int, C.c_int, vp, C.c_int, C.POINTER(vp)]),
+    "ctc_rbc_force_fin": (C.c_int, [vp]),
+    "ctc_rbc_force_md": (C.c_int, [vp, ip]),
+    "ctc_rbc_force_set_bending": (C.c_int, [vp, C.c_int]),
+    "ctc_rbc_force_apply": (C.c_int, [vp, C.POINTER(RbcParams), C.c_float, C.c_int, vp, vp, vp]),
+    "ctc_rbc_area_volume": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+    "ctc_fsi_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
+    "ctc_fsi_fin": (C.c_int, [vp]),
+    "ctc_fsi_apply": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp]),
+    "ctc_fsi_apply_seeded": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, C.c_int, vp, vp, vp, C.c_float,
+                                       C.c_float, C.c_int, vp, vp, vp]),
+    "ctc_scheme_move_apply": (C.c_int, [C.c_float, C.c_float, C.c_int, vp, vp, vp]),
+    "ctc_scheme_move_clear_vel": (C.c_int, [C.c_int, vp, vp]),
+    "ctc_bforce_apply_cste": (C.c_int, [C.c_float, fp, C.c_int, vp, vp]),
+    "ctc_sim_create": (C.c_int, [C.POINTER(SimConfig), C.POINTER(vp)]),
+    "ctc_sim_destroy": (C.c_int, [vp]),
+    "ctc_sim_set_solvent": (C.c_int, [vp, C.c_int, vp, vp]),
+    "ctc_sim_set_solvent_dev": (C.c_int, [vp, C.c_int, vp, vp]),
+    "ctc_sim_step": (C.c_int, [vp, C.c_int, vp]),
+    "ctc_sim_count": (C.c_int, [vp, ip, vp]),
+    "ctc_sim_get_solvent": (C.c_int, [vp, vp, ip, vp]),
+    "ctc_sim_diag": (C.c_int, [vp, C.POINTER(C.c_double), vp]),
+    "ctc_sim_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+    "ctc_sim_next_seeds": (C.c_int, [vp, fp]),
+    "ctc_sim_profile": (C.c_int, [vp, C.c_int]),
+    "ctc_sim_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), ip]),
+}
+
+_lib = None
+
+
+class CtcError(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise CtcError("libctc_b200.so is not built (run __graft_entry__.build() or "
+                           "python -m ctc_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != CTC_OK:
+        L = lib()
+        raise CtcError("%s: %s" % (L.ctc_status_string(status).decode(), L.ctc_last_error().decode()))
+
+
+def device_error():
+    code = C.c_int(0)
+    check(lib().ctc_device_error(C.byref(code)))
+    return code.value

@@ -1,0 +1,517 @@
+// C ABI of ctc_b200 (include/ctc_b200.h): module entry points that replace
+// the reference's clist / fluforces / scheme modules, and the fast-path
+// plain-DPD system.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "clist.h"
+#include "common.cuh"
+#include "dpd.h"
+#include "integrate.h"
+#include "api_util.h"
+
+using namespace ctc;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+static __device__ int g_dev_err;   // the device failure word (one per device)
+
+namespace ctc {
+int fail(int status, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return status;
+}
+
+int *dev_err_ptr() {
+    int *p = nullptr;
+    if (cudaGetSymbolAddress((void**)&p, g_dev_err) != cudaSuccess) return nullptr;
+    return p;
+}
+}  // namespace ctc
+
+extern "C" const char *ctc_status_string(int s) {
+    switch (s) {
+        case CTC_OK: return "ok";
+        case CTC_ERR_ARG: return "invalid argument";
+        case CTC_ERR_CUDA: return "CUDA error";
+        case CTC_ERR_CAPACITY: return "capacity exceeded";
+        case CTC_ERR_DEVICE: return "device kernel failure";
+        default: return "unknown status";
+    }
+}
+
+extern "C" const char *ctc_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *ctc_version(void) { return "0.1.0"; }
+
+extern "C" int ctc_device_error(int *code) {
+    int v = 0, zero = 0;
+    CUDA_TRY(cudaMemcpyFromSymbol(&v, g_dev_err, sizeof(int)));
+    CUDA_TRY(cudaMemcpyToSymbol(g_dev_err, &zero, sizeof(int)));
+    if (code) *code = v;
+    return CTC_OK;
+}
+
+extern "C" float ctc_dpd_sigma(float kBT, float g, float dt) {
+    return (float)std::sqrt(2 * (double)kBT * (double)g / (double)dt);   // src/pair/imp/main.h:54-62
+}
+
+// ---------------------------------------------------------------------------
+// host KISS trunks (src/math/rnd/imp.cpp:12-34)
+// ---------------------------------------------------------------------------
+struct Kiss {
+    unsigned s[4];
+};
+static void kiss_ini(Kiss *k, int x, int y, int z, int c) {
+    k->s[0] = (unsigned)x; k->s[1] = (unsigned)y; k->s[2] = (unsigned)z; k->s[3] = (unsigned)c;
+}
+static float kiss_get(Kiss *k) {
+    unsigned long long t, a = 698769069ULL;
+    unsigned *s = k->s;
+    s[0] = 69069u * s[0] + 12345u;
+    s[1] ^= (s[1] << 13);
+    s[1] ^= (s[1] >> 17);
+    s[1] ^= (s[1] << 5);
+    t = a * s[2] + s[3];
+    s[3] = (unsigned)(t >> 32);
+    s[2] = (unsigned)t;
+    return (float)(s[0] + s[1] + s[2]) / (float)4294967295u;
+}
+// fragment trunks of a 1-rank periodic cart: src/fluforces/imp/ini.h:11-59
+static void halo_trunk_ini(int fid, Kiss *k) {
+    int d[3] = {frag_i2dx(fid), frag_i2dy(fid), frag_i2dz(fid)};
+    int plus = (d[0] + d[1] + d[2] > 0) || ((d[0] + d[1] + d[2] == 0) && (d[0] > 0)) ||
+               ((d[0] == 0) && (d[1] > 0)) || (d[1] == 0 && d[2] > 0);
+    int sg = 2 * plus - 1;
+    int seed = (1 + sg * d[0]) + 3 * ((1 + sg * d[1]) + 3 * (1 + sg * d[2]));
+    kiss_ini(k, 390 + seed, seed + 615, 12309, 23094);
+}
+
+static bool box_ok(int LX, int LY, int LZ) { return LX >= 3 && LY >= 3 && LZ >= 3; }
+
+static void dpd_args_common(DpdArgs *A, int3 L, const ctc_dpd_params *p) {
+    memset(A, 0, sizeof(*A));
+    A->L = L;
+    A->par.a = p->a; A->par.g = p->g; A->par.s = p->s; A->par.spow = p->spow;
+    A->masks = halo_masks();
+    Off27 off;
+    frag_offsets(L, &off);
+    memcpy(A->fss_off, off.d, sizeof(off.d));
+}
+
+extern "C" int ctc_rnd_mean0var1(int n, float seed, const int *u, const int *v, int uu, float *out, void *stream) {
+    if (n < 0 || (n > 0 && (!u || !v || !out))) return fail(CTC_ERR_ARG, "ctc_rnd_mean0var1: bad arguments");
+    CUDA_TRY(rnd_launch(n, seed, u, v, uu, out, (cudaStream_t)stream));
+    return CTC_OK;
+}
+
+extern "C" int ctc_pair_force(int n, const ctc_dpd_params *p, const float *pa, const float *pb, const float *rnd,
+                              float *f, void *stream) {
+    if (n < 0 || !p || (n > 0 && (!pa || !pb || !rnd || !f))) return fail(CTC_ERR_ARG, "ctc_pair_force: bad arguments");
+    DpdPar P;
+    P.a = p->a; P.g = p->g; P.s = p->s; P.spow = p->spow;
+    CUDA_TRY(pair_launch(n, P, pa, pb, rnd, f, (cudaStream_t)stream));
+    return CTC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// cell lists
+// ---------------------------------------------------------------------------
+struct ctc_clist {
+    int3 L;
+    int maxp, nc;
+    float4 *pos_in, *vel_in, *pos_out, *vel_out;
+    int *counts, *starts, *ids;
+    void *scratch;
+    ClistScratch w;
+};
+
+extern "C" int ctc_clist_ini(int LX, int LY, int LZ, int maxp, ctc_clist **pc) {
+    if (!pc || LX <= 0 || LY <= 0 || LZ <= 0 || maxp < 0) return fail(CTC_ERR_ARG, "ctc_clist_ini: bad sizes");
+    ctc_clist *c = new ctc_clist();
+    c->L = make_int3(LX, LY, LZ);
+    c->maxp = maxp;
+    c->nc = LX * LY * LZ;
+    size_t np = (size_t)(maxp > 0 ? maxp : 1);
+    CUDA_TRY(cudaMalloc(&c->pos_in, sizeof(float4) * np));
+    CUDA_TRY(cudaMalloc(&c->vel_in, sizeof(float4) * np));
+    CUDA_TRY(cudaMalloc(&c->pos_out, sizeof(float4) * np));
+    CUDA_TRY(cudaMalloc(&c->vel_out, sizeof(float4) * np));
+    CUDA_TRY(cudaMalloc(&c->ids, sizeof(int) * np));
+    CUDA_TRY(cudaMalloc(&c->counts, sizeof(int) * (size_t)c->nc));
+    CUDA_TRY(cudaMalloc(&c->starts, sizeof(int) * ((size_t)c->nc + 1)));
+    CUDA_TRY(cudaMalloc(&c->scratch, clist_scratch_bytes(c->nc, (int)np)));
+    clist_carve(&c->w, c->scratch, c->nc, (int)np);
+    *pc = c;
+    return CTC_OK;
+}
+
+extern "C" int ctc_clist_fin(ctc_clist *c) {
+    if (!c) return CTC_OK;
+    cudaFree(c->pos_in); cudaFree(c->vel_in); cudaFree(c->pos_out); cudaFree(c->vel_out);
+    cudaFree(c->ids); cudaFree(c->counts); cudaFree(c->starts); cudaFree(c->scratch);
+    delete c;
+    return CTC_OK;
+}
+
+extern "C" int ctc_clist_build(ctc_clist *c, int n, const float *pp, float *ppout, int *nout, void *stream) {
+    if (!c || n < 0 || (n > 0 && (!pp || !ppout))) return fail(CTC_ERR_ARG, "ctc_clist_build: bad arguments");
+    if (n > c->maxp)   // check_input_size, src/clist/imp/main.h:13-17
+        return fail(CTC_ERR_CAPACITY, "Too many input particles for array 0 (%d / %d)", n, c->maxp);
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(aos_to_soa(n, pp, c->pos_in, c->vel_in, st));
+    CUDA_TRY(clist_launch(c->L, n, nullptr, c->pos_in, c->vel_in, 0, c->counts, c->starts, c->pos_out,
+                          c->vel_out, c->ids, c->w, dev_err_ptr(), st));
+    CUDA_TRY(soa_to_aos(c->starts + c->nc, n, c->pos_out, c->vel_out, ppout, st));
+    if (nout) {
+        CUDA_TRY(cudaMemcpyAsync(nout, c->starts + c->nc, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return CTC_OK;
+}
+
+extern "C" int ctc_clist_get(const ctc_clist *c, const int **starts, const int **counts, const int **ids) {
+    if (!c) return fail(CTC_ERR_ARG, "ctc_clist_get: null");
+    if (starts) *starts = c->starts;
+    if (counts) *counts = c->counts;
+    if (ids) *ids = c->ids;
+    return CTC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// solvent DPD module
+// ---------------------------------------------------------------------------
+struct ctc_fluforces {
+    int3 L;
+    int maxp;
+    float4 *pos, *vel;
+    int *fss;
+    Off27 off;
+    Kiss bulk, halo[26];
+};
+
+extern "C" int ctc_fluforces_ini(int LX, int LY, int LZ, int maxp, ctc_fluforces **pf) {
+    if (!pf || !box_ok(LX, LY, LZ) || maxp < 0) return fail(CTC_ERR_ARG, "ctc_fluforces_ini: box must be >= 3 cells");
+    ctc_fluforces *f = new ctc_fluforces();
+    f->L = make_int3(LX, LY, LZ);
+    f->maxp = maxp;
+    size_t np = (size_t)(maxp > 0 ? maxp : 1);
+    CUDA_TRY(cudaMalloc(&f->pos, sizeof(float4) * np));
+    CUDA_TRY(cudaMalloc(&f->vel, sizeof(float4) * np));
+    frag_offsets(f->L, &f->off);
+    CUDA_TRY(cudaMalloc(&f->fss, sizeof(int) * (size_t)f->off.d[26]));
+    kiss_ini(&f->bulk, 0, 0, 0, 0);                 // src/fluforces/imp/ini.h:6
+    for (int i = 0; i < 26; i++) halo_trunk_ini(i, &f->halo[i]);
+    *pf = f;
+    return CTC_OK;
+}
+
+extern "C" int ctc_fluforces_fin(ctc_fluforces *f) {
+    if (!f) return CTC_OK;
+    cudaFree(f->pos); cudaFree(f->vel); cudaFree(f->fss);
+    delete f;
+    return CTC_OK;
+}
+
+extern "C" int ctc_fluforces_apply_seeded(ctc_fluforces *f, const ctc_dpd_params *p, int n, const float *pp,
+                                          const int *starts, const int *counts, const float *seeds, int which,
+                                          int rng, float *ff, void *stream) {
+    if (!f || !p || !seeds || n < 0 || (n > 0 && (!pp || !starts || !counts || !ff)) || which < 1 || which > 3 ||
+        (rng != CTC_RNG_REFERENCE && rng != CTC_RNG_STABLE))
+        return fail(CTC_ERR_ARG, "ctc_fluforces_apply_seeded: bad arguments");
+    if (n > f->maxp) return fail(CTC_ERR_CAPACITY, "fluforces: %d particles > capacity %d", n, f->maxp);
+    if (n > (1 << 27)) return fail(CTC_ERR_CAPACITY, "fluforces: at most 2^27 particles per box");
+    if (n == 0) return CTC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(aos_to_soa(n, pp, f->pos, f->vel, st));
+    DpdArgs A;
+    dpd_args_common(&A, f->L, p);
+    A.pos = f->pos; A.vel = f->vel; A.starts = starts; A.counts = counts;
+    A.out = ff; A.out_stride = 3;
+    memcpy(A.seeds, seeds, sizeof(A.seeds));
+    A.which = which;
+    A.fss = f->fss;
+    A.err = dev_err_ptr();
+    if ((which & 2) && rng == CTC_RNG_REFERENCE) CUDA_TRY(frag_starts_launch(f->L, counts, f->fss, f->off, st));
+    CUDA_TRY(dpd_launch(A, n, rng, st));
+    return CTC_OK;
+}
+
+extern "C" int ctc_fluforces_bulk_apply(ctc_fluforces *f, const ctc_dpd_params *p, int n, const float *pp,
+                                        const int *starts, const int *counts, float *ff, void *stream) {
+    if (!f) return fail(CTC_ERR_ARG, "null module");
+    if (n <= 0) return CTC_OK;                      // no draw for an empty call (bulk/imp/main.h:29-33)
+    float seeds[27] = {0};
+    seeds[0] = kiss_get(&f->bulk);
+    return ctc_fluforces_apply_seeded(f, p, n, pp, starts, counts, seeds, 1, CTC_RNG_REFERENCE, ff, stream);
+}
+
+extern "C" int ctc_fluforces_halo_apply(ctc_fluforces *f, const ctc_dpd_params *p, int n, const float *pp,
+                                        const int *starts, const int *counts, float *ff, void *stream) {
+    if (!f) return fail(CTC_ERR_ARG, "null module");
+    float seeds[27] = {0};
+    for (int i = 0; i < 26; i++) seeds[1 + i] = kiss_get(&f->halo[i]);  // halo_prepare draws all 26
+    if (n <= 0) return CTC_OK;
+    return ctc_fluforces_apply_seeded(f, p, n, pp, starts, counts, seeds, 2, CTC_RNG_REFERENCE, ff, stream);
+}
+
+// ---------------------------------------------------------------------------
+// scheme
+// ---------------------------------------------------------------------------
+extern "C" int ctc_scheme_move_apply(float dt, float mass, int n, const float *ff, float *pp, void *stream) {
+    if (n < 0 || (n > 0 && (!ff || !pp)) || mass <= 0) return fail(CTC_ERR_ARG, "ctc_scheme_move_apply: bad arguments");
+    CUDA_TRY(move_aos(n, dt, mass, ff, pp, (cudaStream_t)stream));
+    return CTC_OK;
+}
+
+extern "C" int ctc_scheme_move_clear_vel(int n, float *pp, void *stream) {
+    if (n < 0 || (n > 0 && !pp)) return fail(CTC_ERR_ARG, "ctc_scheme_move_clear_vel: bad arguments");
+    CUDA_TRY(clear_vel_aos(n, pp, (cudaStream_t)stream));
+    return CTC_OK;
+}
+
+extern "C" int ctc_bforce_apply_cste(float mass, const float *a, int n, float *ff, void *stream) {
+    if (n < 0 || !a || (n > 0 && !ff)) return fail(CTC_ERR_ARG, "ctc_bforce_apply_cste: bad arguments");
+    CUDA_TRY(bforce_aos(n, mass, make_float3(a[0], a[1], a[2]), ff, (cudaStream_t)stream));
+    return CTC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// plain-DPD system on the fast path
+// ---------------------------------------------------------------------------
+struct ctc_sim {
+    ctc_sim_config cfg;
+    int3 L;
+    int nc, n_host;
+    float4 *pos[2], *vel[2], *force;
+    int *counts, *starts, *fss, *count0;   // count0: particle count before the first build
+    void *scratch;
+    ClistScratch w;
+    unsigned *trunk_dev;                   // 27 KISS states on the device
+    float *seeds_dev;
+    double *diag_scratch, *diag_out;
+    Off27 off;
+    int cur;                               // index of the buffer that holds the state
+    bool built;                            // starts/counts describe pos[cur]
+    Kiss trunk_host[27];                   // host mirror, for ctc_sim_next_seeds
+    int prof;                              // record per-phase events each step
+    std::vector<cudaEvent_t> ev;           // 5 events per profiled step
+    int prof_steps;
+};
+
+static void sim_mark(ctc_sim *s, int k, cudaStream_t st) {
+    if (!s->prof) return;
+    size_t idx = 5 * (size_t)s->prof_steps + k;
+    while (s->ev.size() <= idx) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        s->ev.push_back(e);
+    }
+    cudaEventRecord(s->ev[idx], st);
+}
+
+extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
+    if (!cfg || !ps || !box_ok(cfg->LX, cfg->LY, cfg->LZ) || cfg->maxp <= 0 || cfg->maxp > (1 << 27) || cfg->mass <= 0 ||
+        (cfg->rng != CTC_RNG_REFERENCE && cfg->rng != CTC_RNG_STABLE))
+        return fail(CTC_ERR_ARG, "ctc_sim_create: bad configuration");
+    ctc_sim *s = new ctc_sim();
+    s->cfg = *cfg;
+    s->L = make_int3(cfg->LX, cfg->LY, cfg->LZ);
+    s->nc = cfg->LX * cfg->LY * cfg->LZ;
+    size_t np = (size_t)cfg->maxp;
+    for (int b = 0; b < 2; b++) {
+        CUDA_TRY(cudaMalloc(&s->pos[b], sizeof(float4) * np));
+        CUDA_TRY(cudaMalloc(&s->vel[b], sizeof(float4) * np));
+    }
+    CUDA_TRY(cudaMalloc(&s->force, sizeof(float4) * np));
+    CUDA_TRY(cudaMalloc(&s->counts, sizeof(int) * (size_t)s->nc));
+    CUDA_TRY(cudaMalloc(&s->starts, sizeof(int) * ((size_t)s->nc + 1)));
+    CUDA_TRY(cudaMalloc(&s->count0, sizeof(int)));
+    frag_offsets(s->L, &s->off);
+    CUDA_TRY(cudaMalloc(&s->fss, sizeof(int) * (size_t)s->off.d[26]));
+    CUDA_TRY(cudaMalloc(&s->scratch, clist_scratch_bytes(s->nc, (int)np)));
+    clist_carve(&s->w, s->scratch, s->nc, (int)np);
+    CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 27));
+    CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 27));
+    CUDA_TRY(cudaMalloc(&s->diag_scratch, diag_scratch_bytes()));
+    CUDA_TRY(cudaMalloc(&s->diag_out, sizeof(double) * 5));
+    // trunk 0: bulk (0,0,0,0); 1..26: halo fragments.  Stable keys use trunk 0 only.
+    kiss_ini(&s->trunk_host[0], 0, 0, 0, 0);
+    for (int i = 0; i < 26; i++) halo_trunk_ini(i, &s->trunk_host[1 + i]);
+    CUDA_TRY(cudaMemcpy(s->trunk_dev, s->trunk_host, sizeof(unsigned) * 4 * 27, cudaMemcpyHostToDevice));
+    s->cur = 0;
+    s->n_host = 0;
+    s->built = false;
+    *ps = s;
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_destroy(ctc_sim *s) {
+    if (!s) return CTC_OK;
+    for (int b = 0; b < 2; b++) { cudaFree(s->pos[b]); cudaFree(s->vel[b]); }
+    cudaFree(s->force); cudaFree(s->counts); cudaFree(s->starts); cudaFree(s->count0); cudaFree(s->fss);
+    cudaFree(s->scratch); cudaFree(s->trunk_dev); cudaFree(s->seeds_dev); cudaFree(s->diag_scratch);
+    cudaFree(s->diag_out);
+    for (cudaEvent_t e : s->ev) cudaEventDestroy(e);
+    delete s;
+    return CTC_OK;
+}
+
+static int sim_set(ctc_sim *s, int n, const float *pp, bool host, cudaStream_t st) {
+    if (!s || n < 0 || (n > 0 && !pp)) return fail(CTC_ERR_ARG, "ctc_sim_set_solvent: bad arguments");
+    if (n > s->cfg.maxp) return fail(CTC_ERR_CAPACITY, "ctc_sim_set_solvent: %d > capacity %d", n, s->cfg.maxp);
+    const float *src = pp;
+    float *tmp = nullptr;
+    if (host && n > 0) {
+        CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 6 * (size_t)n, st));
+        CUDA_TRY(cudaMemcpyAsync(tmp, pp, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice, st));
+        src = tmp;
+    }
+    s->cur = 0;
+    CUDA_TRY(aos_to_soa(n, src, s->pos[0], s->vel[0], st));
+    CUDA_TRY(cudaMemcpyAsync(s->count0, &n, sizeof(int), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (tmp) CUDA_TRY(cudaFreeAsync(tmp, st));
+    s->n_host = n;
+    s->built = false;
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_set_solvent(ctc_sim *s, int n, const float *pp, void *stream) {
+    return sim_set(s, n, pp, true, (cudaStream_t)stream);
+}
+
+extern "C" int ctc_sim_set_solvent_dev(ctc_sim *s, int n, const float *pp, void *stream) {
+    return sim_set(s, n, pp, false, (cudaStream_t)stream);
+}
+
+// one step: seeds, wrap + cell lists into the other buffer, forces, update
+static int sim_step1(ctc_sim *s, cudaStream_t st) {
+    int src = s->cur, dst = 1 - s->cur;
+    int ntr = s->cfg.rng == CTC_RNG_REFERENCE ? 27 : 1;
+    sim_mark(s, 0, st);
+    CUDA_TRY(draw_seeds_launch(s->trunk_dev, ntr, s->seeds_dev, st));
+    for (int k = 0; k < ntr; k++) kiss_get(&s->trunk_host[k]);
+    // the count pointer of the input is starts[nc] of the previous build: copy
+    // it aside, the build overwrites starts
+    if (s->built) CUDA_TRY(cudaMemcpyAsync(s->count0, s->starts + s->nc, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(clist_launch(s->L, s->n_host, s->count0, s->pos[src], s->vel[src], 1, s->counts, s->starts,
+                          s->pos[dst], s->vel[dst], nullptr, s->w, dev_err_ptr(), st));
+    sim_mark(s, 1, st);
+    DpdArgs A;
+    dpd_args_common(&A, s->L, &s->cfg.dpd);
+    A.pos = s->pos[dst]; A.vel = s->vel[dst]; A.starts = s->starts; A.counts = s->counts;
+    A.out = (float*)s->force; A.out_stride = 4;
+    A.seeds_dev = s->seeds_dev;
+    A.which = 3;
+    A.fss = s->fss;
+    A.err = dev_err_ptr();
+    if (s->cfg.rng == CTC_RNG_REFERENCE) CUDA_TRY(frag_starts_launch(s->L, s->counts, s->fss, s->off, st));
+    CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n_host, st));
+    sim_mark(s, 2, st);
+    CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st));
+    sim_mark(s, 3, st);
+    CUDA_TRY(integrate_launch(s->starts + s->nc, s->n_host, s->pos[dst], s->vel[dst], s->force, s->cfg.dt,
+                              s->cfg.mass, make_float3(s->cfg.bodyf[0], s->cfg.bodyf[1], s->cfg.bodyf[2]), st));
+    sim_mark(s, 4, st);
+    if (s->prof) s->prof_steps++;
+    s->cur = dst;
+    s->built = true;
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_step(ctc_sim *s, int nsteps, void *stream) {
+    if (!s || nsteps < 0) return fail(CTC_ERR_ARG, "ctc_sim_step: bad arguments");
+    for (int k = 0; k < nsteps; k++) {
+        int rc = sim_step1(s, (cudaStream_t)stream);
+        if (rc) return rc;
+    }
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_count(ctc_sim *s, int *n, void *stream) {
+    if (!s || !n) return fail(CTC_ERR_ARG, "ctc_sim_count: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int *p = s->built ? s->starts + s->nc : s->count0;
+    CUDA_TRY(cudaMemcpyAsync(n, p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_get_solvent(ctc_sim *s, float *pp, int *n, void *stream) {
+    if (!s || !pp) return fail(CTC_ERR_ARG, "ctc_sim_get_solvent: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    int cnt = 0;
+    int rc = ctc_sim_count(s, &cnt, stream);
+    if (rc) return rc;
+    float *tmp = nullptr;
+    if (cnt > 0) {
+        CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 6 * (size_t)cnt, st));
+        CUDA_TRY(soa_to_aos(nullptr, cnt, s->pos[s->cur], s->vel[s->cur], tmp, st));
+        CUDA_TRY(cudaMemcpyAsync(pp, tmp, sizeof(float) * 6 * (size_t)cnt, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaFreeAsync(tmp, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    if (n) *n = cnt;
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_diag(ctc_sim *s, double *out5, void *stream) {
+    if (!s || !out5) return fail(CTC_ERR_ARG, "ctc_sim_diag: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int *p = s->built ? s->starts + s->nc : s->count0;
+    CUDA_TRY(diag_launch(p, s->vel[s->cur], (double)s->cfg.mass, s->diag_scratch, s->diag_out, st));
+    CUDA_TRY(cudaMemcpyAsync(out5, s->diag_out, sizeof(double) * 5, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_state(ctc_sim *s, float **pos, float **vel, float **force, const int **starts) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sim_state: null");
+    if (pos) *pos = (float*)s->pos[s->cur];
+    if (vel) *vel = (float*)s->vel[s->cur];
+    if (force) *force = (float*)s->force;
+    if (starts) *starts = s->starts;
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_next_seeds(const ctc_sim *s, float *seeds27) {
+    if (!s || !seeds27) return fail(CTC_ERR_ARG, "ctc_sim_next_seeds: bad arguments");
+    for (int k = 0; k < 27; k++) {
+        Kiss t = s->trunk_host[k];
+        seeds27[k] = kiss_get(&t);
+    }
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_profile(ctc_sim *s, int enable) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sim_profile: null");
+    s->prof = enable != 0;
+    s->prof_steps = 0;
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_profile_read(ctc_sim *s, double *ms4, int *steps) {
+    if (!s || !ms4) return fail(CTC_ERR_ARG, "ctc_sim_profile_read: bad arguments");
+    for (int k = 0; k < 4; k++) ms4[k] = 0;
+    for (int i = 0; i < s->prof_steps; i++)
+        for (int k = 0; k < 4; k++) {
+            float ms = 0;
+            CUDA_TRY(cudaEventSynchronize(s->ev[5 * i + k + 1]));
+            CUDA_TRY(cudaEventElapsedTime(&ms, s->ev[5 * i + k], s->ev[5 * i + k + 1]));
+            ms4[k] += ms;
+        }
+    if (steps) *steps = s->prof_steps;
+    s->prof_steps = 0;
+    return CTC_OK;
+}

@@ -1,0 +1,27 @@
+// Host-side declarations of the cell-list kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace ctc {
+
+struct ClistScratch {
+    int2 *cidslot;     // per input particle: cell, slot | re-entered bit
+    unsigned *keys;    // per output slot: re-entered bit | input index
+    int *sums;         // scan block sums
+    int nsums;
+};
+
+size_t clist_scratch_bytes(int ncells, int maxp);
+void clist_carve(ClistScratch *w, void *base, int ncells, int maxp);
+
+// counts[ncells], starts[ncells + 1] (starts[ncells] = particles kept).
+// n bounds the grid; nptr (device, may be null) holds the actual count.
+cudaError_t clist_launch(int3 L, int n, const int *nptr, const float4 *pos_in, const float4 *vel_in, int wrap,
+                         int *counts, int *starts, float4 *pos_out, float4 *vel_out, int *order,
+                         const ClistScratch &w, int *err, cudaStream_t st);
+
+cudaError_t aos_to_soa(int n, const float *pp, float4 *pos, float4 *vel, cudaStream_t st);
+cudaError_t soa_to_aos(const int *nptr, int nmax, const float4 *pos, const float4 *vel, float *pp,
+                       cudaStream_t st);
+
+}  // namespace ctc

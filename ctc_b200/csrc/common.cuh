@@ -1,0 +1,122 @@
+// Shared device helpers of the B200 particle-step kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/ctc_b200.h"
+
+namespace ctc {
+
+// ---------------------------------------------------------------------------
+// device error word: kernels never trap; they record the first failure here
+// and skip the offending access.  The host reads it back on demand.
+// ---------------------------------------------------------------------------
+enum DevErr : int {
+    DEV_OK = 0,
+    DEV_TILE_OVERFLOW = 1,     // a tile's staged particles exceed shared capacity
+    DEV_PAIR_QUEUE = 2,        // internal queue misuse (never expected)
+    DEV_BAD_PARTICLE = 3,      // NaN / out-of-range position after the wrap
+    DEV_CELL_OVERFLOW = 4,     // more particles in one cell than the kernel supports
+};
+
+__device__ __forceinline__ void set_error(int *err, int code) {
+    if (err) atomicCAS(err, 0, code);
+}
+
+// ---------------------------------------------------------------------------
+// Pair RNG of src/math/rnd/dev.h:1-74, written with explicitly rounded
+// intrinsics so the compiler can neither contract nor reassociate it.
+// The key sum is fma(v,tin, fma(C,silver, fma(u,bronze, A*gold))): the
+// contraction nvcc applies to the reference expression of dev.h:59,67 (each
+// "x + y*z" with y*z the right operand becomes fma(y, z, x)), checked bit for
+// bit against the reference's own kernel built for sm_100a.
+// The 18 logistic passes are 9 Chebyshev-T4 rounds with round-toward-zero FMA.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float rnd_from_key(float seed, float A, float U, float Cc, float V) {
+    const float gold   = 0.6180339887498948482f;
+    const float silver = 0.4142135623730950488f;
+    const float bronze = 0.00008877875787352212838853023f;
+    const float tin    = 0.00004602357186447026756768986f;
+    const float sqrt2  = 1.41421356237309514547f;
+    float p = __fmaf_rn(V, tin, __fmaf_rn(Cc, silver, __fmaf_rn(U, bronze, __fmul_rn(A, gold))));
+    p = __fsub_rn(p, floorf(p));
+    float x = __fsub_rn(seed, p);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        float x2 = __fmul_rn(x, x);
+        x = __fmaf_rz(__fmaf_rz(8.0f, x2, -8.0f), x2, 1.0f);
+    }
+    return __fmul_rn(x, sqrt2);
+}
+
+// mean0var1ii (signed ids, bulk pairs) -- dev.h:57-62
+__device__ __forceinline__ float mean0var1ii(float seed, int u, int v) {
+    return rnd_from_key(seed, __int2float_rn(u & 0x3FF), __int2float_rn(u),
+                        __int2float_rn(v & 0x3FF), __int2float_rn(v));
+}
+
+// mean0var1uu (unsigned ids, halo and FSI pairs) -- dev.h:64-72
+__device__ __forceinline__ float mean0var1uu(float seed, uint32_t u, uint32_t v) {
+    return rnd_from_key(seed, __uint2float_rn(u & 0x3FFu), __uint2float_rn(u),
+                        __uint2float_rn(v & 0x3FFu), __uint2float_rn(v));
+}
+
+// ---------------------------------------------------------------------------
+// DPD pair force of src/pair/dev.h:12-47,111-139 (PairDPD grey view).
+// Written as the same plain expressions in the same order, so that nvcc with
+// -use_fast_math contracts and approximates them exactly as it does the
+// reference (rsqrtf, powf, and every "x + y*z" into an FMA): the result is
+// bit-identical to the reference's kernel built for sm_100a.
+// Returns false when r^2 >= 1 (NORM_BIG: no force).
+// ---------------------------------------------------------------------------
+struct DpdPar {
+    float a, g, s, spow;
+};
+
+// r^2 of the candidate filter, the same contraction as in dpd_force
+__device__ __forceinline__ float dist2(float x, float y, float z) {
+    return __fmaf_rn(z, z, __fmaf_rn(y, y, __fmul_rn(x, x)));
+}
+
+__device__ __forceinline__ bool dpd_force(const DpdPar &P, float4 pa, float4 va, float4 pb,
+                                          float4 vb, float rnd, float3 &f) {
+    float x = pa.x - pb.x, y = pa.y - pb.y, z = pa.z - pb.z;
+    float r2 = x * x + y * y + z * z;                 // norm()
+    if (r2 >= 1) return false;
+    float r;
+    if (r2 < 1e-6f) {
+        x = y = z = 0;
+        r = 0;
+    } else {
+        float invr = rsqrtf(r2);
+        r = r2 * invr;
+        x *= invr; y *= invr; z *= invr;
+    }
+    float dvx = va.x - vb.x, dvy = va.y - vb.y, dvz = va.z - vb.z;
+    float ev = x * dvx + y * dvy + z * dvz;           // dot(er, dv)
+    float rm = max(1 - r, 0.0f);                      // magn_dpd
+    float wr = powf(rm, P.spow);
+    float f0 = (-P.g * wr * ev + P.s * rnd) * wr;
+    f0 += P.a * rm;
+    f.x = f0 * x;
+    f.y = f0 * y;
+    f.z = f0 * z;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// fragments (src/frag/dev.h:19-81): id 0..25 <-> direction in {-1,0,1}^3
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int frag_i2dx(int i) { return (i + 2) % 3 - 1; }
+__host__ __device__ __forceinline__ int frag_i2dy(int i) { return (i / 3 + 2) % 3 - 1; }
+__host__ __device__ __forceinline__ int frag_i2dz(int i) { return (i / 9 + 2) % 3 - 1; }
+__host__ __device__ __forceinline__ int frag_d2i(int x, int y, int z) {
+    return ((x + 2) % 3) + 3 * ((y + 2) % 3) + 9 * ((z + 2) % 3);
+}
+__host__ __device__ __forceinline__ int frag_anti(int i) {
+    return frag_d2i(-frag_i2dx(i), -frag_i2dy(i), -frag_i2dz(i));
+}
+
+inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace ctc

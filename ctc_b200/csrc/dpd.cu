@@ -1,0 +1,443 @@
+// Solvent DPD pair forces for sm_100a: the bulk and periodic-halo
+// interactions of src/fluforces (bulk/dev/main.h:23-97, halo/dev/main.h:1-83).
+//
+// Pair sets and keys are the reference's: a thread per target particle walks
+// the five half-stencil rows of its (float) cell with ib < ia; a particle of
+// the boundary cells walks, for every fragment that holds its cell, the
+// remote window of the anti-fragment (r2map) with the local particle shifted
+// into the image frame.  What differs is how the SIMT lanes are used:
+//   - accepted pairs are compacted through a per-warp shared-memory queue and
+//     evaluated 32 at a time, so the 18-round RNG and the force run with every
+//     lane busy (the reference evaluates a pair inside the divergent
+//     candidate loop, with ~15% of the lanes active);
+//   - forces are accumulated with fire-and-forget global reductions (no
+//     shared-memory float atomics, no per-step texture objects);
+//   - bulk and halo are two launches over the same cell-sorted SoA arrays
+//     (the reference: one bulk launch + 26 fragment launches after a
+//     host-staged exchange).
+//
+// Random numbers.  Reference keys (rng_mode 0): bulk pairs
+// mean0var1ii(seed, ia, ib) with ia > ib sorted indices; halo pairs
+// mean0var1uu(seed[fid], mask ? aid : bid, ...) with fragment-local indices
+// aid/bid as src/exch/flu packs them and the per-fragment seeds and masks of
+// src/fluforces/imp/ini.h:11-59.  Stable keys (rng_mode 1):
+// mean0var1uu(seed, max(id), min(id)) of the particles' global ids.
+#include "common.cuh"
+#include "dpd.h"
+
+namespace ctc {
+
+constexpr int DPD_THREADS = 256;
+constexpr int DPD_WARPS = DPD_THREADS / 32;
+constexpr int QCAP = 64;        // per-warp queue: < 32 waiting + one round of 32
+
+__device__ __forceinline__ int block_exscan256(int v, int *sh, int &total) {
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int s = lane < DPD_WARPS ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < DPD_WARPS) sh[lane] = s;
+    }
+    __syncthreads();
+    total = sh[DPD_WARPS - 1];
+    int r = x - v + (w > 0 ? sh[w - 1] : 0);
+    __syncthreads();
+    return r;
+}
+
+// index of a particle inside fragment fid's packed list (src/exch/flu/dev/map.h:1-21,
+// src/exch/flu/dev/pack.h:2-40): fragment-cell start + offset inside the cell
+__device__ __forceinline__ int frag_index(const DpdArgs &A, int fid, int gcell, int off) {
+    int gx = gcell % A.L.x, gy = (gcell / A.L.x) % A.L.y, gz = gcell / (A.L.x * A.L.y);
+    int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
+    int ox = dx == 1 ? A.L.x - 1 : 0, oy = dy == 1 ? A.L.y - 1 : 0, oz = dz == 1 ? A.L.z - 1 : 0;
+    int ex = dx == 0 ? A.L.x : 1, ey = dy == 0 ? A.L.y : 1;
+    int hci = (gx - ox) + ex * ((gy - oy) + ey * (gz - oz));
+    return __ldg(A.fss + A.fss_off[fid] + hci) + off;
+}
+
+// ---------------------------------------------------------------------------
+// bulk pairs: the reference's traversal (one target particle per thread, the
+// five half-stencil rows of its cell, ib < ia) with the accepted pairs
+// compacted through a per-warp queue, so that the RNG + force evaluation runs
+// with all 32 lanes busy, and the forces accumulated with fire-and-forget
+// global reductions (+f on ia, -f on ib).
+// ---------------------------------------------------------------------------
+constexpr int BULK_T = 256, BULK_W = BULK_T / 32;
+
+__device__ __forceinline__ void red_force(float *out, int stride, int i, float s, float3 f) {
+    if (stride == 4) {   // one 16-byte vector reduction (sm_90+) instead of three scalar ones
+        atomicAdd((float4*)out + i, make_float4(s * f.x, s * f.y, s * f.z, 0.0f));
+        return;
+    }
+    float *o = out + (size_t)stride * i;
+    atomicAdd(o + 0, s * f.x);
+    atomicAdd(o + 1, s * f.y);
+    atomicAdd(o + 2, s * f.z);
+}
+
+template <int RNG>
+__global__ void __launch_bounds__(BULK_T) k_dpd_bulk(const __grid_constant__ DpdArgs A) {
+    __shared__ uint2 queue[BULK_W][QCAP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n = __ldg(A.starts + A.L.x * A.L.y * A.L.z);
+    const int ia = blockIdx.x * BULK_T + threadIdx.x;
+    const bool act = ia < n;
+    const float *seeds = A.seeds_dev ? A.seeds_dev : A.seeds;
+    const DpdPar P = A.par;
+    uint2 *q = queue[warp];
+    int qn = 0;
+
+    float4 pa = make_float4(0, 0, 0, 0);
+    int cx = 0, cy = 0, cz = 0;
+    if (act) {
+        pa = __ldg(A.pos + ia);
+        // get_cid (src/fluforces/bulk/dev/main.h:11-17): float, truncated
+        cx = (int)(pa.x + (float)(A.L.x / 2));
+        cy = (int)(pa.y + (float)(A.L.y / 2));
+        cz = (int)(pa.z + (float)(A.L.z / 2));
+    }
+
+    auto process = [&](int m) {
+        if (lane < m) {
+            uint2 rec = q[lane];
+            int i = (int)rec.x, j = (int)rec.y;
+            float4 p1 = __ldg(A.pos + i), p2 = __ldg(A.pos + j);
+            float4 v1 = __ldg(A.vel + i), v2 = __ldg(A.vel + j);
+            float rnd;
+            if (RNG == 1) {
+                unsigned g1 = (unsigned)__float_as_int(p1.w), g2 = (unsigned)__float_as_int(p2.w);
+                rnd = mean0var1uu(seeds[0], max(g1, g2), min(g1, g2));
+            } else {
+                rnd = mean0var1ii(seeds[0], i, j);      // i > j: the reference's (ia, ib)
+            }
+            float3 f;
+            if (dpd_force(P, p1, v1, p2, v2, rnd, f)) {
+                red_force(A.out, A.out_stride, i, 1.0f, f);
+                red_force(A.out, A.out_stride, j, -1.0f, f);
+            }
+        }
+        __syncwarp();
+    };
+
+    auto push = [&](bool ok, int cand) {
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) q[qn + __popc(bal & ((1u << lane) - 1u))] = make_uint2((unsigned)ia, (unsigned)cand);
+        qn += __popc(bal);
+        __syncwarp();
+        if (qn >= 32) {
+            process(32);
+            qn -= 32;
+            if (lane < qn) q[lane] = q[32 + lane];
+            __syncwarp();
+        }
+    };
+
+    // rows (dz, dy) of src/fluforces/bulk/dev/main.h:88-92; dx runs -1..1, and
+    // -1..0 for the own row.  Every round a lane tests the next UNROLL
+    // candidates of its row at once (independent loads in flight).
+    constexpr int UNROLL = 4;
+    int r = 0, ib = 0, be = 0;
+    for (;;) {
+        if (act) {
+            while (ib >= be && r < 5) {
+                const int dz = r < 3 ? -1 : 0, dy = r < 3 ? r - 1 : (r == 3 ? -1 : 0);
+                r++;
+                const int bz = cz + dz, by = cy + dy;
+                if (bz < 0 || bz >= A.L.z || by < 0 || by >= A.L.y) continue;
+                const int enddx = (dz == 0 && dy == 0) ? 0 : 1;
+                const int sx = max(0, cx - 1), ex = 1 + min(A.L.x - 1, cx + enddx);
+                const int cid0 = A.L.x * (by + A.L.y * bz);
+                ib = __ldg(A.starts + cid0 + sx);
+                be = min(__ldg(A.starts + cid0 + ex), ia);   // ib < ia
+            }
+        }
+        const bool have = act && ib < be;
+        if (!__any_sync(0xffffffffu, have)) break;
+        float4 pb[UNROLL];
+#pragma unroll
+        for (int u = 0; u < UNROLL; u++)
+            if (have && ib + u < be) pb[u] = __ldg(A.pos + ib + u);
+#pragma unroll
+        for (int u = 0; u < UNROLL; u++) {
+            const bool v = have && ib + u < be;
+            const bool ok = v && dist2(pa.x - pb[u].x, pa.y - pb[u].y, pa.z - pb[u].z) <= 1.0f;   // cutoff_range
+            push(ok, ib + u);
+        }
+        if (have) ib = min(ib + UNROLL, be);
+    }
+    if (qn > 0) process(qn);
+}
+
+// ---------------------------------------------------------------------------
+// halo pairs: a particle in the boundary cells of fragment fid against the
+// cells of the anti-fragment seen through the periodic face, as
+// src/fluforces/halo/dev/{map,main}.h: the local particle is shifted by
+// -d*L, the remote window is r2map's (tangential cell +-1 from the float
+// coordinate, clipped), the key is mean0var1uu(seed[fid], mask ? aid : bid,
+// mask ? bid : aid) with fragment-local indices; only the local particle
+// takes the force.
+// ---------------------------------------------------------------------------
+constexpr int HALO_T = 128, HALO_W = HALO_T / 32;
+
+__device__ __forceinline__ void r2size_dev(float r, int nc, int S, int &l, int &s) {
+    int i = (int)(r + (float)(S / 2));
+    l = max(0, i - 1);
+    s = min(nc, i + 2) - l;
+}
+
+template <int RNG>
+__global__ void __launch_bounds__(HALO_T) k_dpd_halo(const __grid_constant__ DpdArgs A) {
+    __shared__ uint4 queue[HALO_W][QCAP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int3 L = A.L;
+    const int n = __ldg(A.starts + L.x * L.y * L.z);
+    const int ia = blockIdx.x * HALO_T + threadIdx.x;
+    const float *seeds = A.seeds_dev ? A.seeds_dev : A.seeds;
+    const DpdPar P = A.par;
+    uint4 *q = queue[warp];
+    int qn = 0;
+
+    // the particle's cell-list cell (computed in double, src/clist/dev/main.h:21-24)
+    bool act = ia < n;
+    float4 pa = make_float4(0, 0, 0, 0);
+    int gx = 0, gy = 0, gz = 0, gcell = 0;
+    unsigned frags = 0;
+    if (act) {
+        pa = __ldg(A.pos + ia);
+        gx = (int)((double)pa.x + (double)(L.x / 2));
+        gy = (int)((double)pa.y + (double)(L.y / 2));
+        gz = (int)((double)pa.z + (double)(L.z / 2));
+        gx = min(max(gx, 0), L.x - 1); gy = min(max(gy, 0), L.y - 1); gz = min(max(gz, 0), L.z - 1);
+        gcell = gx + L.x * (gy + L.y * gz);
+        // fragments whose cells hold this cell (src/exch/flu/dev/map.h:1-21)
+        for (int fid = 0; fid < 26; fid++) {
+            const int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
+            const bool in = (dx == 0 || (dx == 1 ? gx == L.x - 1 : gx == 0)) &&
+                            (dy == 0 || (dy == 1 ? gy == L.y - 1 : gy == 0)) &&
+                            (dz == 0 || (dz == 1 ? gz == L.z - 1 : gz == 0));
+            if (in) frags |= 1u << fid;
+        }
+    }
+    if (!__any_sync(0xffffffffu, frags != 0)) return;   // interior warp
+
+    auto process = [&](int m) {
+        if (lane < m) {
+            const uint4 rec = q[lane];
+            const int i = (int)(rec.x & 0x7ffffffu), fid = (int)(rec.x >> 27), j = (int)rec.y;
+            float4 p1 = __ldg(A.pos + i);
+            const float4 p2 = __ldg(A.pos + j);
+            // the local particle moves into the frame of the image (halo/dev/main.h:43-45)
+            p1.x -= (float)(frag_i2dx(fid) * L.x);
+            p1.y -= (float)(frag_i2dy(fid) * L.y);
+            p1.z -= (float)(frag_i2dz(fid) * L.z);
+            float rnd;
+            if (RNG == 1) {
+                unsigned g1 = (unsigned)__float_as_int(p1.w), g2 = (unsigned)__float_as_int(p2.w);
+                rnd = mean0var1uu(seeds[0], max(g1, g2), min(g1, g2));
+            } else {
+                const bool mask = (A.masks >> fid) & 1u;
+                rnd = mean0var1uu(seeds[1 + fid], mask ? rec.z : rec.w, mask ? rec.w : rec.z);
+            }
+            float3 f;
+            if (dpd_force(P, p1, __ldg(A.vel + i), p2, __ldg(A.vel + j), rnd, f))
+                red_force(A.out, A.out_stride, i, 1.0f, f);
+        }
+        __syncwarp();
+    };
+    auto push = [&](bool ok, uint4 rec) {
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) q[qn + __popc(bal & ((1u << lane) - 1u))] = rec;
+        qn += __popc(bal);
+        __syncwarp();
+        if (qn >= 32) {
+            process(32);
+            qn -= 32;
+            if (lane < qn) q[lane] = q[32 + lane];
+            __syncwarp();
+        }
+    };
+
+    // per lane: fragments (<= 7), then the remote window cells, then particles
+    unsigned left = frags;
+    int fid = -1, aid = 0, anti = 0;
+    int rows = 0, cols = 0, jump = 0, id = 0, row = 0, col = 0;
+    int ib = 0, be = 0, bid0 = 0;
+    float sx = 0, sy = 0, sz = 0;
+    for (;;) {
+        bool have = false;
+        if (act) {
+            while (ib >= be) {
+                if (col < cols) {                         // next remote fragment cell
+                    const int hci = id + row * jump + col;
+                    col++;
+                    // fragment cell -> bulk cell of the anti-fragment
+                    const int adx = frag_i2dx(anti), ady = frag_i2dy(anti), adz = frag_i2dz(anti);
+                    const int ex = adx == 0 ? L.x : 1, ey = ady == 0 ? L.y : 1;
+                    const int hx = hci % ex, hy = (hci / ex) % ey, hz = hci / (ex * ey);
+                    const int bx = (adx == 1 ? L.x - 1 : 0) + hx, by = (ady == 1 ? L.y - 1 : 0) + hy,
+                              bz = (adz == 1 ? L.z - 1 : 0) + hz;
+                    const int c = bx + L.x * (by + L.y * bz);
+                    ib = __ldg(A.starts + c);
+                    be = ib + __ldg(A.counts + c);
+                    bid0 = __ldg(A.fss + A.fss_off[anti] + hci) - ib;
+                } else if (row + 1 < rows) {
+                    row++;
+                    col = 0;
+                } else if (left) {                        // next fragment
+                    fid = __ffs(left) - 1;
+                    left &= left - 1;
+                    anti = frag_anti(fid);
+                    const int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
+                    aid = frag_index(A, fid, gcell, ia - __ldg(A.starts + gcell));
+                    // r2map (src/fluforces/halo/dev/map.h:102-129) on the unshifted position
+                    const int xc = dx == 0 ? L.x : 1, yc = dy == 0 ? L.y : 1;
+                    int xs = 1, ys = 1, zs = 1, l;
+                    id = 0;
+                    if (dz == 0) { r2size_dev(pa.z, L.z, L.z, l, zs); id += l; }
+                    id *= yc;
+                    if (dy == 0) { r2size_dev(pa.y, yc, L.y, l, ys); id += l; }
+                    id *= xc;
+                    if (dx == 0) { r2size_dev(pa.x, xc, L.x, l, xs); id += l; }
+                    const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+                    if (nz == 1) {
+                        if (dx) { rows = zs; cols = ys; jump = yc; }
+                        else if (dy) { rows = zs; cols = xs; jump = xc; }
+                        else { rows = ys; cols = xs; jump = xc; }
+                    } else if (nz == 2) {
+                        rows = jump = 1;
+                        cols = max(xs, max(ys, zs));
+                    } else {
+                        rows = cols = jump = 1;
+                    }
+                    row = 0;
+                    col = 0;
+                    sx = (float)(dx * L.x); sy = (float)(dy * L.y); sz = (float)(dz * L.z);
+                } else {
+                    act = false;
+                    break;
+                }
+            }
+        }
+        have = act && ib < be;
+        if (!__any_sync(0xffffffffu, have)) break;
+        bool ok = false;
+        uint4 rec = make_uint4(0, 0, 0, 0);
+        if (have) {
+            const float4 pb = __ldg(A.pos + ib);
+            ok = dist2((pa.x - sx) - pb.x, (pa.y - sy) - pb.y, (pa.z - sz) - pb.z) < 1.0f;
+            rec = make_uint4((unsigned)ia | ((unsigned)fid << 27), (unsigned)ib, (unsigned)aid,
+                             (unsigned)(ib + bid0));
+            ib++;
+        }
+        push(ok, rec);
+    }
+    if (qn > 0) process(qn);
+}
+
+// exclusive scans of the counts of every fragment's cells (src/exch/flu/dev/map.h:23-97)
+__global__ void k_frag_starts(int3 L, const int *__restrict__ counts, int *__restrict__ fss, Off27 off) {
+    __shared__ int sh[32];
+    int fid = blockIdx.x;
+    int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
+    int ox = dx == 1 ? L.x - 1 : 0, oy = dy == 1 ? L.y - 1 : 0, oz = dz == 1 ? L.z - 1 : 0;
+    int ex = dx == 0 ? L.x : 1, ey = dy == 0 ? L.y : 1, ez = dz == 0 ? L.z : 1;
+    int nc = ex * ey * ez;
+    int *out = fss + off.d[fid];
+    int carry = 0;
+    for (int b = 0; b < nc; b += DPD_THREADS) {
+        int h = b + threadIdx.x, v = 0;
+        if (h < nc) {
+            int x = h % ex, y = (h / ex) % ey, z = h / (ex * ey);
+            v = counts[(ox + x) + L.x * ((oy + y) + L.y * (oz + z))];
+        }
+        int tot, r = block_exscan256(v, sh, tot);
+        if (h < nc) out[h] = carry + r;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) out[nc] = carry;
+}
+
+__global__ void k_rnd(int n, float seed, const int *__restrict__ u, const int *__restrict__ v, int uu,
+                     float *__restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = uu ? mean0var1uu(seed, (unsigned)u[i], (unsigned)v[i]) : mean0var1ii(seed, u[i], v[i]);
+}
+
+__global__ void k_pair(int n, DpdPar P, const float *__restrict__ pa, const float *__restrict__ pb,
+                       const float *__restrict__ rnd, float *__restrict__ f) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *a = pa + 6 * (size_t)i, *b = pb + 6 * (size_t)i;
+    float3 fo = make_float3(0.0f, 0.0f, 0.0f);
+    dpd_force(P, make_float4(a[0], a[1], a[2], 0.0f), make_float4(a[3], a[4], a[5], 0.0f),
+              make_float4(b[0], b[1], b[2], 0.0f), make_float4(b[3], b[4], b[5], 0.0f), rnd[i], fo);
+    f[3 * i] = fo.x; f[3 * i + 1] = fo.y; f[3 * i + 2] = fo.z;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+cudaError_t pair_launch(int n, const DpdPar &P, const float *pa, const float *pb, const float *rnd, float *f,
+                        cudaStream_t st) {
+    if (n > 0) k_pair<<<ceil_div(n, 256), 256, 0, st>>>(n, P, pa, pb, rnd, f);
+    return cudaGetLastError();
+}
+
+cudaError_t rnd_launch(int n, float seed, const int *u, const int *v, int uu, float *out, cudaStream_t st) {
+    if (n > 0) k_rnd<<<ceil_div(n, 256), 256, 0, st>>>(n, seed, u, v, uu, out);
+    return cudaGetLastError();
+}
+
+void frag_offsets(int3 L, Off27 *off) {
+    int s = 0;
+    for (int fid = 0; fid < 26; fid++) {
+        int ex = frag_i2dx(fid) == 0 ? L.x : 1, ey = frag_i2dy(fid) == 0 ? L.y : 1,
+            ez = frag_i2dz(fid) == 0 ? L.z : 1;
+        off->d[fid] = s;
+        s += ex * ey * ez + 1;
+    }
+    off->d[26] = s;
+}
+
+unsigned halo_masks() {
+    unsigned m = 0;
+    for (int fid = 0; fid < 26; fid++) {
+        int a = frag_anti(fid);
+        if ((fid < a ? fid : a) == fid) m |= 1u << fid;   // src/fluforces/imp/ini.h:53-57
+    }
+    return m;
+}
+
+cudaError_t frag_starts_launch(int3 L, const int *counts, int *fss, const Off27 &off, cudaStream_t st) {
+    k_frag_starts<<<26, DPD_THREADS, 0, st>>>(L, counts, fss, off);
+    return cudaGetLastError();
+}
+
+cudaError_t dpd_launch(const DpdArgs &A, int nmax, int rng_mode, cudaStream_t st) {
+    if (nmax <= 0) return cudaSuccess;
+    if (A.which & 1) {
+        if (rng_mode == 1) k_dpd_bulk<1><<<ceil_div(nmax, BULK_T), BULK_T, 0, st>>>(A);
+        else k_dpd_bulk<0><<<ceil_div(nmax, BULK_T), BULK_T, 0, st>>>(A);
+    }
+    if (A.which & 2) {
+        if (rng_mode == 1) k_dpd_halo<1><<<ceil_div(nmax, HALO_T), HALO_T, 0, st>>>(A);
+        else k_dpd_halo<0><<<ceil_div(nmax, HALO_T), HALO_T, 0, st>>>(A);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace ctc

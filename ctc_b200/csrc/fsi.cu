@@ -1,0 +1,168 @@
+// Solvent-membrane (FSI) DPD forces for sm_100a: src/fsi bulk
+// (dev/bulk.h:1-68, dev/map/bulk.h:1-64) and halo (dev/halo.h:1-59) in one
+// launch over the periodic 27-cell neighbourhood of every vertex.
+//
+// One thread per vertex; the vertex force is summed in registers and added
+// once; the solvent reactions are float atomics into the solvent forces (as
+// the reference does, src/fsi/dev/common.h:20-27).  A neighbour cell reached
+// through a periodic face is the reference's halo: the vertex is shifted into
+// the image frame (r + L * d(anti(fid)), src/exch/common/dev.h:25-47) and the
+// pair noise uses the halo seed and the vertex's index in the concatenated
+// image list (fragments packed in ascending vertex order, received in slot
+// anti(fid)).
+#include "common.cuh"
+#include "fsi.h"
+
+namespace ctc {
+
+// fragment mask of a vertex: src/exch/map/dev.h:1-84 (emap_code on the inner
+// box [lo + 1, lo + L - 1), emap_decode into faces, edges, corner)
+__device__ __forceinline__ unsigned emap_mask(int3 L, float x, float y, float z) {
+    int lx = -(L.x / 2), ly = -(L.y / 2), lz = -(L.z / 2);
+    int d[3];
+    d[0] = -1 + (x >= (float)(lx + 1)) + (x >= (float)(lx + L.x - 1));
+    d[1] = -1 + (y >= (float)(ly + 1)) + (y >= (float)(ly + L.y - 1));
+    d[2] = -1 + (z >= (float)(lz + 1)) + (z >= (float)(lz + L.z - 1));
+    unsigned m = 0;
+    for (int c = 0; c < 3; c++)
+        if (d[c]) {
+            int f[3] = {0, 0, 0};
+            f[c] = d[c];
+            m |= 1u << frag_d2i(f[0], f[1], f[2]);
+        }
+    for (int c = 0; c < 3; c++) {
+        int e[3] = {d[0], d[1], d[2]};
+        e[c] = 0;
+        if (e[(c + 1) % 3] && e[(c + 2) % 3]) m |= 1u << frag_d2i(e[0], e[1], e[2]);
+    }
+    if (d[0] && d[1] && d[2]) m |= 1u << frag_d2i(d[0], d[1], d[2]);
+    return m;
+}
+
+__global__ void k_emap(int nv, int3 L, const float *__restrict__ pv, int stride, unsigned *__restrict__ mask) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const float *q = pv + (size_t)stride * i;
+    mask[i] = emap_mask(L, q[0], q[1], q[2]);
+}
+
+// per fragment: rank of each member vertex (ascending vertex index) and count
+__global__ void k_emap_rank(int nv, const unsigned *__restrict__ mask, int *__restrict__ rank,
+                            int *__restrict__ count) {
+    __shared__ int sh[32];
+    int fid = blockIdx.x, carry = 0;
+    for (int b = 0; b < nv; b += blockDim.x) {
+        int i = b + threadIdx.x;
+        int in = i < nv ? (int)((mask[i] >> fid) & 1u) : 0;
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        int x = in;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sh[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int s = lane < nw ? sh[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            sh[lane] = s;
+        }
+        __syncthreads();
+        int excl = x - in + (w > 0 ? sh[w - 1] : 0) + carry;
+        if (i < nv) rank[(size_t)fid * nv + i] = in ? excl : -1;
+        carry += sh[nw - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) count[fid] = carry;
+}
+
+// img_start[fid] = start of receive slot anti(fid) in the concatenated list
+__global__ void k_emap_starts(const int *__restrict__ count, int *__restrict__ img_start) {
+    if (threadIdx.x == 0) {
+        int s = 0, slot_start[26];
+        for (int slot = 0; slot < 26; slot++) { slot_start[slot] = s; s += count[frag_anti(slot)]; }
+        for (int fid = 0; fid < 26; fid++) img_start[fid] = slot_start[frag_anti(fid)];
+    }
+}
+
+template <int RNG>
+__global__ void k_fsi(const __grid_constant__ FsiArgs A) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nv) return;
+    const float *q = A.pv + (size_t)A.pstride * i;
+    const float *qv = A.vv + (size_t)A.pstride * i;
+    float4 pa = make_float4(q[0], q[1], q[2], 0.0f), va = make_float4(qv[0], qv[1], qv[2], 0.0f);
+    const int lx = A.L.x / 2, ly = A.L.y / 2, lz = A.L.z / 2;
+    // the vertex cell as src/fsi/dev/map/bulk.h:13-21 (floorf, may lie outside the box)
+    const int cx = lx + (int)floorf(pa.x), cy = ly + (int)floorf(pa.y), cz = lz + (int)floorf(pa.z);
+    const DpdPar P = A.par;
+    float fx = 0, fy = 0, fz = 0;
+    for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                int gx = cx + dx, gy = cy + dy, gz = cz + dz;
+                int wx = gx < 0 ? -1 : (gx >= A.L.x ? 1 : 0);
+                int wy = gy < 0 ? -1 : (gy >= A.L.y ? 1 : 0);
+                int wz = gz < 0 ? -1 : (gz >= A.L.z ? 1 : 0);
+                gx -= wx * A.L.x; gy -= wy * A.L.y; gz -= wz * A.L.z;
+                if (gx < 0 || gx >= A.L.x || gy < 0 || gy >= A.L.y || gz < 0 || gz >= A.L.z) continue;
+                int cid = gx + A.L.x * (gy + A.L.y * gz);
+                int s = __ldg(A.starts + cid), e = s + __ldg(A.counts + cid);
+                if (s == e) continue;
+                bool halo = (wx | wy | wz) != 0;
+                float4 a = pa;
+                unsigned aid = (unsigned)i;
+                float seed = A.seed_bulk;
+                if (halo) {
+                    int fid = frag_d2i(wx, wy, wz);
+                    if (RNG == 0) {
+                        int r = __ldg(A.img_rank + (size_t)fid * A.nv + i);
+                        if (r < 0) { set_error(A.err, DEV_BAD_PARTICLE); continue; }
+                        aid = (unsigned)(__ldg(A.img_start + fid) + r);
+                        seed = A.seed_halo;
+                    }
+                    a.x = a.x + (float)(-wx * A.L.x);
+                    a.y = a.y + (float)(-wy * A.L.y);
+                    a.z = a.z + (float)(-wz * A.L.z);
+                }
+                for (int j = s; j < e; j++) {
+                    float4 b = __ldg(A.spos + j);
+                    float x = a.x - b.x, y = a.y - b.y, z = a.z - b.z;
+                    if (dist2(x, y, z) >= 1.0f) continue;
+                    float rnd = RNG == 0 ? mean0var1uu(seed, aid, (unsigned)j)
+                                         : mean0var1uu(A.seed_bulk, (unsigned)i, (unsigned)__float_as_int(b.w));
+                    float3 f;
+                    if (!dpd_force(P, a, va, b, __ldg(A.svel + j), rnd, f)) continue;
+                    fx += f.x; fy += f.y; fz += f.z;
+                    float *o = A.fs + (size_t)A.sstride * j;
+                    atomicAdd(o + 0, -f.x);
+                    atomicAdd(o + 1, -f.y);
+                    atomicAdd(o + 2, -f.z);
+                }
+            }
+    float *o = A.fv + (size_t)A.fstride * i;
+    o[0] += fx;
+    o[1] += fy;
+    o[2] += fz;
+}
+
+cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsigned *mask, int *rank, int *count,
+                              int *img_start, cudaStream_t st) {
+    if (nv <= 0) return cudaSuccess;
+    k_emap<<<ceil_div(nv, 256), 256, 0, st>>>(nv, L, pv, stride, mask);
+    k_emap_rank<<<26, 1024, 0, st>>>(nv, mask, rank, count);
+    k_emap_starts<<<1, 32, 0, st>>>(count, img_start);
+    return cudaGetLastError();
+}
+
+cudaError_t fsi_launch(const FsiArgs &A, int rng, cudaStream_t st) {
+    if (A.nv <= 0) return cudaSuccess;
+    if (rng == 1) k_fsi<1><<<ceil_div(A.nv, 128), 128, 0, st>>>(A);
+    else k_fsi<0><<<ceil_div(A.nv, 128), 128, 0, st>>>(A);
+    return cudaGetLastError();
+}
+
+}  // namespace ctc

@@ -1,0 +1,30 @@
+// Host-side declarations of the FSI kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace ctc {
+
+struct FsiArgs {
+    int3 L;
+    int nv;                        // vertices
+    const float *pv, *vv;          // vertex i at pv + pstride * i (velocities likewise)
+    int pstride;                   // 6: Particle AoS (vv = pv + 3), 4: float4 SoA
+    const float4 *spos, *svel;     // cell-sorted solvent (w of spos: particle id)
+    const int *starts, *counts;
+    float *fv;                     // vertex forces, accumulated (fstride floats apart)
+    int fstride;
+    float *fs;                     // solvent forces, atomically accumulated (sstride floats apart)
+    int sstride;
+    DpdPar par;
+    float seed_bulk, seed_halo;
+    const int *img_rank;           // [26 * nv]: rank in fragment fid's list or -1 (reference keys)
+    const int *img_start;          // [26]: first index of fragment fid's images in the halo list
+    int *err;
+};
+
+cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsigned *mask, int *rank, int *count,
+                              int *img_start, cudaStream_t st);
+cudaError_t fsi_launch(const FsiArgs &A, int rng, cudaStream_t st);
+
+}  // namespace ctc

@@ -1,0 +1,17 @@
+// Host-side declarations of the update / diagnostic kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace ctc {
+
+cudaError_t integrate_launch(const int *nptr, int nmax, float4 *pos, float4 *vel, const float4 *force, float dt,
+                             float mass, float3 a, cudaStream_t st);
+cudaError_t move_aos(int n, float dt, float mass, const float *ff, float *pp, cudaStream_t st);
+cudaError_t clear_vel_aos(int n, float *pp, cudaStream_t st);
+cudaError_t bforce_aos(int n, float mass, float3 a, float *ff, cudaStream_t st);
+size_t diag_scratch_bytes();
+cudaError_t diag_launch(const int *nptr, const float4 *vel, double mass, double *scratch, double *out,
+                        cudaStream_t st);
+cudaError_t draw_seeds_launch(unsigned *state, int ntrunk, float *seeds, cudaStream_t st);
+
+}  // namespace ctc

@@ -1,0 +1,176 @@
+// Red-blood-cell membrane forces for sm_100a, FP64 arithmetic.
+//
+//   area/volume  src/rbc/force/area_volume/dev/main.h:10-46 -- per cell, here a
+//                deterministic FP64 block reduction (the reference sums floats
+//                with atomics);
+//   forces       src/rbc/force/dev/main.h:23-77 + dev/common.h:1-108 (global area,
+//                local area, volume, WLC + POW spring, viscous) and Kantor bending
+//                src/rbc/force/bending/kantor/dev/main.h:23-66 +
+//                src/mesh/force/kantor0/dev.h:28-131.
+// One thread per vertex walks its md ring slots over the fixed-valence
+// adjacency table (src/rbc/adj/dev.h:2-31), sums every contribution in double
+// and adds it to the vertex force once: no atomics.  The float steps of the
+// reference -- sqrtf of the squared spring length, powf of the POW term -- are
+// kept as float operations, as the reference computes them.
+#include "common.cuh"
+#include "membrane.h"
+
+namespace ctc {
+
+struct D3 {
+    double x, y, z;
+};
+__device__ __forceinline__ D3 mk(double x, double y, double z) { return D3{x, y, z}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ D3 operator*(double s, D3 a) { return mk(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ double dot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 cross(D3 a, D3 b) {
+    return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+__device__ __forceinline__ D3 ld_pos(const float *pp, int stride, int i) {
+    const float *q = pp + (size_t)stride * i;
+    return mk(q[0], q[1], q[2]);
+}
+__device__ __forceinline__ D3 ld_vel(const float *vv, int stride, int i) {
+    const float *q = vv + (size_t)stride * i;
+    return mk(q[0], q[1], q[2]);
+}
+
+// ---------------------------------------------------------------------------
+// area and volume of every cell
+// ---------------------------------------------------------------------------
+constexpr int AV_T = 256;
+
+__global__ void __launch_bounds__(AV_T) k_area_volume(int nv, int nt, const int *__restrict__ tri,
+                                                      const float *__restrict__ pp, int stride,
+                                                      double *__restrict__ av) {
+    __shared__ double sh[2][AV_T / 32];
+    int c = blockIdx.x;
+    double A = 0, V = 0;
+    for (int t = threadIdx.x; t < nt; t += AV_T) {
+        int i0 = __ldg(tri + 3 * t) + c * nv, i1 = __ldg(tri + 3 * t + 1) + c * nv, i2 = __ldg(tri + 3 * t + 2) + c * nv;
+        D3 r0 = ld_pos(pp, stride, i0), r1 = ld_pos(pp, stride, i1), r2 = ld_pos(pp, stride, i2);
+        D3 n = cross(r1 - r0, r2 - r0);
+        A += 0.5 * sqrt(dot(n, n));
+        V += ((r0.x * r1.y - r0.y * r1.x) * r2.z + (r0.z * r1.x - r0.x * r1.z) * r2.y +
+              (r0.y * r1.z - r0.z * r1.y) * r2.x) / 6.0;
+    }
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        A += __shfl_down_sync(0xffffffffu, A, o);
+        V += __shfl_down_sync(0xffffffffu, V, o);
+    }
+    if (lane == 0) { sh[0][w] = A; sh[1][w] = V; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, v = 0;
+        for (int k = 0; k < AV_T / 32; k++) { a += sh[0][k]; v += sh[1][k]; }
+        av[2 * c] = a;
+        av[2 * c + 1] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// forces
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double sq(double x) { return x * x; }
+__device__ __forceinline__ double wlc0(double r) { return (4 * sq(r) - 9 * r + 6) / (4 * sq(r - 1)); }
+__device__ __forceinline__ double wlc(double lmax, double ks, double r) { return ks / lmax * wlc0(r / lmax); }
+
+// one triangle (i0, i1, i2) seen from i0: farea + fvolume + fspring (common.h:1-78)
+__device__ __forceinline__ D3 ftri(const RbcPar &P, D3 r1, D3 r2, D3 r3, double l0, double a0, double A, double V) {
+    D3 x21 = r2 - r1, x32 = r3 - r2, x31 = r3 - r1;
+    D3 nn = cross(x21, x31);
+    D3 f = cross(nn, x32);
+    double a = 0.5 * sqrt(dot(nn, nn));
+    double fA = -(double)P.ka * (A - (double)P.totArea) / (4 * (double)P.totArea * a);
+    double fa = -(double)P.kd * (a - a0) / (4 * a0 * a);
+    f = (fA + fa) * f;
+    f = f + ((double)P.kv * (V - (double)P.totVolume) / (6 * (double)P.totVolume)) * cross(r3, r2);
+    // spring: r from a float sqrt of the double squared length, as the reference
+    double r = (double)sqrtf((float)dot(x21, x21));
+    double lmax = l0 / (double)P.x0, m = P.mpow;
+    if (r >= lmax) r = 0.99 * lmax;               // RBC_SPRING_CAP, src/inc/def.h:50
+    double fwlc = wlc(lmax, P.ks, r);
+    double fpow = -wlc(lmax, P.ks, l0) * (double)powf((float)l0, (float)(m + 1)) / (double)powf((float)r, (float)(m + 1));
+    return f + (fwlc + fpow) * x21;
+}
+
+// fvisc (common.h:80-92)
+__device__ __forceinline__ D3 fvisc(const RbcPar &P, D3 r1, D3 r2, D3 u1, D3 u2) {
+    D3 du = u2 - u1, dr = r1 - r2;
+    double fac = dot(du, dr) / dot(dr, dr);
+    return (double)P.gammaT * du + ((double)P.gammaC * fac) * dr;
+}
+
+// one Kantor dihedral (kantor0/dev.h:58-123); update 1: force on a, 2: on b
+template <int update>
+__device__ __forceinline__ D3 dih(double cphi, double sphi, double kb, D3 a, D3 b, D3 c, D3 d, int *err) {
+    D3 ab = a - b, ac = a - c, cd = c - d, bd = b - d, bc = b - c, da = d - a;
+    D3 k = cross(ab, ac), n = cross(bd, bc);
+    double aa = dot(k, k), bb = dot(n, n), kn = dot(k, n);
+    if (aa == 0 || bb == 0) { set_error(err, DEV_BAD_PARTICLE); return mk(0, 0, 0); }
+    double ok = rsqrt(aa), on = rsqrt(bb);
+    double ct = kn * ok * on;
+    double os = rsqrt(fmax(1.0 - ct * ct, 1e-6));
+    os = copysign(os, dot(k - n, da));
+    double beta = cphi * kb - ct * (sphi * kb) * os;
+    double b11 = -beta * ct * ok * ok;
+    double b12 = beta * ok * on;
+    if (update == 1) {
+        D3 r32 = c - b;
+        return b11 * cross(k, r32) + b12 * cross(n, r32);
+    } else {
+        double b22 = -beta * ct * on * on;
+        return b11 * cross(k, ac) + b12 * (cross(k, cd) + cross(n, ac)) + b22 * cross(n, cd);
+    }
+}
+
+__global__ void k_membrane(MembraneArgs A) {
+    int pid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pid >= A.nc * A.nv) return;
+    const int md = A.md, nv = A.nv;
+    const int rbc = pid / nv, k = (pid % nv) * md, off = rbc * nv;
+    const RbcPar P = A.par;
+    const D3 r0 = ld_pos(A.pos, A.stride, pid), v0 = ld_vel(A.vel, A.stride, pid);
+    const double Acell = A.av[2 * rbc], Vcell = A.av[2 * rbc + 1];
+    const double phi = (double)P.phi / 180.0 * M_PI;
+    const double cphi = cos(phi), sphi = sin(phi), kb = P.kb;
+    D3 fb = mk(0, 0, 0), ft = mk(0, 0, 0);
+    for (int j = 0; j < md; j++) {
+        // adj_get_map0, src/rbc/adj/dev.h:2-31
+        int i1 = __ldg(A.adj0 + k + j);
+        if (i1 == -1) continue;
+        int i2 = __ldg(A.adj0 + k + (j + 1) % md), i3;
+        if (i2 == -1) { i2 = __ldg(A.adj0 + k); i3 = __ldg(A.adj0 + k + 1); }
+        else { i3 = __ldg(A.adj0 + k + (j + 2) % md); if (i3 == -1) i3 = __ldg(A.adj0 + k); }
+        int i4 = __ldg(A.adj1 + k + j);
+        i1 += off; i2 += off; i3 += off; i4 += off;
+        D3 r1 = ld_pos(A.pos, A.stride, i1), r2 = ld_pos(A.pos, A.stride, i2);
+        D3 r3 = ld_pos(A.pos, A.stride, i3), r4 = ld_pos(A.pos, A.stride, i4);
+        if (A.bending) fb = fb + dih<1>(cphi, sphi, kb, r0, r2, r1, r4, A.err) + dih<2>(cphi, sphi, kb, r1, r0, r2, r3, A.err);
+        ft = ft + ftri(P, r0, r1, r2, A.l0, A.a0, Acell, Vcell);
+        ft = ft + fvisc(P, r0, r1, v0, ld_vel(A.vel, A.stride, i1));
+    }
+    D3 f = fb + ft;
+    float *o = A.force + (size_t)A.fstride * pid;
+    o[0] += (float)f.x;
+    o[1] += (float)f.y;
+    o[2] += (float)f.z;
+}
+
+cudaError_t area_volume_launch(int nc, int nv, int nt, const int *tri, const float *pos, int stride, double *av,
+                               cudaStream_t st) {
+    if (nc > 0) k_area_volume<<<nc, AV_T, 0, st>>>(nv, nt, tri, pos, stride, av);
+    return cudaGetLastError();
+}
+
+cudaError_t membrane_launch(const MembraneArgs &A, cudaStream_t st) {
+    int n = A.nc * A.nv;
+    if (n > 0) k_membrane<<<ceil_div(n, 128), 128, 0, st>>>(A);
+    return cudaGetLastError();
+}
+
+}  // namespace ctc

@@ -1,0 +1,29 @@
+// Host-side declarations of the membrane kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace ctc {
+
+struct RbcPar {   // RbcParams_v, src/rbc/params/imp.h:3-9
+    float gammaC, gammaT, kBT, kb, phi, ks, x0, mpow, ka, kd, kv, totArea, totVolume;
+};
+
+struct MembraneArgs {
+    int nc, nv, md;
+    const int *adj0, *adj1;       // md * nv ring tables shared by all cells
+    const float *pos, *vel;       // vertex i at pos + stride * i (vel likewise)
+    int stride;                   // 6: reference Particle AoS (vel = pos + 3), 4: float4 SoA
+    float *force;                 // accumulated: force + fstride * i
+    int fstride;
+    const double *av;             // per cell area, volume (2 * nc)
+    RbcPar par;
+    double l0, a0;                // stress-ful equilibrium length / area
+    int bending;                  // Kantor bending on/off
+    int *err;
+};
+
+cudaError_t area_volume_launch(int nc, int nv, int nt, const int *tri, const float *pos, int stride, double *av,
+                               cudaStream_t st);
+cudaError_t membrane_launch(const MembraneArgs &A, cudaStream_t st);
+
+}  // namespace ctc

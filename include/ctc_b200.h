@@ -1,0 +1,205 @@
+/* ctc_b200 -- B200-native (sm_100a) per-step particle hot path of uDeviceX
+ * (rossinelli/CTC): cell lists, solvent DPD forces with the pairwise counter
+ * RNG, solvent-membrane (FSI) forces, red-blood-cell membrane forces and the
+ * time update.
+ *
+ * C ABI: plain pointers and sizes, explicit CUDA stream (`void *stream`,
+ * a cudaStream_t; NULL = legacy default stream), int status returns.
+ * Device pointers are marked [dev], host pointers [host].
+ *
+ * Layouts.  The reference-facing entry points take the reference's AoS
+ * arrays: Particle = 6 floats {r[3], v[3]} (src/inc/type.h:6-8), Force = 3
+ * floats (src/inc/type.h:20-22).  Forces are ACCUMULATED into the caller's
+ * array, as the reference modules do; the caller clears them.  The fast path
+ * (ctc_sim_*) keeps cell-sorted SoA float4 state on the device.
+ *
+ * Errors.  The reference prints and exit(1)s (src/utils/error.h:1-16); here
+ * every call returns a status and ctc_last_error() gives the message.  Device
+ * kernels never trap: they record failures in a device word that
+ * ctc_device_error() reads and clears.
+ */
+#ifndef CTC_B200_H
+#define CTC_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CTC_OK = 0,
+    CTC_ERR_ARG = 1,        /* invalid argument or size */
+    CTC_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+    CTC_ERR_CAPACITY = 3,   /* input larger than the object was created for */
+    CTC_ERR_DEVICE = 4      /* a kernel flagged a failure (see ctc_device_error) */
+};
+
+/* device failure codes returned by ctc_device_error */
+enum {
+    CTC_DEV_OK = 0,
+    CTC_DEV_TILE_OVERFLOW = 1,  /* a pair tile held more particles than its shared memory */
+    CTC_DEV_BAD_PARTICLE = 3,   /* a particle was outside the box after the periodic wrap */
+    CTC_DEV_CELL_OVERFLOW = 4
+};
+
+/* random-number keys of the pair noise */
+enum {
+    CTC_RNG_REFERENCE = 0,  /* the reference's keys: sorted / fragment-local indices */
+    CTC_RNG_STABLE = 1      /* keys of the particles' global ids (carried in pos.w) */
+};
+
+const char *ctc_status_string(int status);
+const char *ctc_last_error(void);
+/* reads and clears the device failure word of the current device */
+int ctc_device_error(int *code);
+/* library version "major.minor.patch" */
+const char *ctc_version(void);
+
+/* PairDPD {a, g, s, spow} -- src/pair/type.h:7-9 */
+typedef struct { float a, g, s, spow; } ctc_dpd_params;
+
+/* RbcParams_v -- src/rbc/params/imp.h:3-9 */
+typedef struct {
+    float gammaC, gammaT, kBT, kb, phi, ks, x0, mpow, ka, kd, kv, totArea, totVolume;
+} ctc_rbc_params;
+
+/* sigma = sqrt(2 kBT g / dt), computed in double and stored as float
+ * (replaces pair_compute_dpd_sigma, src/pair/imp/main.h:54-62) */
+float ctc_dpd_sigma(float kBT, float g, float dt);
+
+/* ---- pair RNG: the device generators rnd::mean0var1ii / mean0var1uu ----
+ * (src/math/rnd/dev.h:57-72) for n key pairs u[i], v[i] [dev] with one seed;
+ * uu = 0 treats the keys as signed (ii), 1 as unsigned (uu); out [dev] */
+int ctc_rnd_mean0var1(int n, float seed, const int *u, const int *v, int uu, float *out, void *stream);
+
+/* ---- pair force: pair_force<PairDPD> (src/pair/dev.h:111-139) for n
+ * pairs; pa, pb [dev] Particle AoS, rnd [dev] one random number per pair,
+ * f [dev] Force AoS (overwritten) -- the computation src/u/pair drives */
+int ctc_pair_force(int n, const ctc_dpd_params *p, const float *pa, const float *pb, const float *rnd,
+                   float *f, void *stream);
+
+/* ---- cell lists: replaces src/clist/imp.h:5-33 ------------------------- */
+typedef struct ctc_clist ctc_clist;
+/* clist_ini + clist_ini_map(maxp, 1, ...) (src/clist/imp/ini.h:1-31) */
+int ctc_clist_ini(int LX, int LY, int LZ, int maxp, ctc_clist **c);
+int ctc_clist_fin(ctc_clist *c);
+/* clist_build (src/clist/imp/main.h:75-84): bins the n particles pp [dev,
+ * AoS] into unit cells of the box [-L/2, L/2), writes them cell-sorted to
+ * ppout [dev, AoS] and *nout [host] = particles kept (outside ones are
+ * dropped, as the reference does without projection). */
+int ctc_clist_build(ctc_clist *c, int n, const float *pp, float *ppout, int *nout, void *stream);
+/* clists_get_ss / clists_get_cc / clist_get_ids: device arrays of the last
+ * build; starts has LX*LY*LZ + 1 entries (the last = particles kept); ids[k]
+ * = input index of the k-th sorted particle. */
+int ctc_clist_get(const ctc_clist *c, const int **starts, const int **counts, const int **ids);
+
+/* ---- solvent DPD: replaces src/fluforces/imp.h:8-25 --------------------- */
+typedef struct ctc_fluforces ctc_fluforces;
+/* fluforces_bulk_ini + fluforces_halo_ini for a 1-rank periodic box; the
+ * object holds the trunk generators: the bulk one seeded (0,0,0,0)
+ * (src/fluforces/imp/ini.h:6) and the 26 fragment ones of ini.h:22-59 */
+int ctc_fluforces_ini(int LX, int LY, int LZ, int maxp, ctc_fluforces **f);
+int ctc_fluforces_fin(ctc_fluforces *f);
+/* fluforces_bulk_apply (src/fluforces/imp/main.h:10-20): draws the bulk
+ * seed from the trunk, adds the in-box pair forces of the n cell-sorted
+ * particles pp [dev, AoS] to ff [dev, AoS]; starts/counts [dev] as from
+ * ctc_clist_get */
+int ctc_fluforces_bulk_apply(ctc_fluforces *f, const ctc_dpd_params *p, int n, const float *pp,
+                             const int *starts, const int *counts, float *ff, void *stream);
+/* fluforces_halo_prepare + fluforces_halo_apply (main.h:23-37): draws the 26
+ * fragment seeds and adds the forces of the pairs across the periodic faces */
+int ctc_fluforces_halo_apply(ctc_fluforces *f, const ctc_dpd_params *p, int n, const float *pp,
+                             const int *starts, const int *counts, float *ff, void *stream);
+/* both in one launch with explicit seeds: seeds[0] bulk, seeds[1 + fid]
+ * fragment fid [host]; which: 1 bulk, 2 halo, 3 both; rng: CTC_RNG_* */
+int ctc_fluforces_apply_seeded(ctc_fluforces *f, const ctc_dpd_params *p, int n, const float *pp,
+                               const int *starts, const int *counts, const float *seeds, int which,
+                               int rng, float *ff, void *stream);
+
+/* ---- membranes: replaces src/rbc/force/imp.h:9-28 ----------------------- */
+typedef struct ctc_rbc_force ctc_rbc_force;
+/* rbc_force_ini (src/rbc/force/imp/main.h:9-26): ring adjacency of the cell
+ * template of nv vertices and nt triangles tri[3 nt] [host] (adj_ini,
+ * src/rbc/adj/imp/ini.h:34-45), for up to max_cells cells */
+int ctc_rbc_force_ini(int nv, int nt, const int *tri, int max_cells, ctc_rbc_force **f);
+int ctc_rbc_force_fin(ctc_rbc_force *f);
+/* maximum valence of the template (mesh_read_get_md) */
+int ctc_rbc_force_md(const ctc_rbc_force *f, int *md);
+/* rbc_force_set_bending: 1 = "kantor" (default), 0 = "none" */
+int ctc_rbc_force_set_bending(ctc_rbc_force *f, int kantor);
+/* rbc_force_apply (src/rbc/force/imp/forces.h:45-68), stress-ful, no random
+ * force: per-cell area and volume (FP64), Kantor bending, area, volume,
+ * WLC + POW spring and viscous forces of the nc cells pp [dev, AoS, cell c
+ * vertex v at c*nv + v] added to ff [dev, AoS] */
+int ctc_rbc_force_apply(ctc_rbc_force *f, const ctc_rbc_params *p, float dt, int nc, const float *pp, float *ff,
+                        void *stream);
+/* area_volume_compute (src/rbc/force/area_volume/imp/main.h:38-51) in FP64:
+ * av [dev, 2 nc doubles] = area, volume of every cell */
+int ctc_rbc_area_volume(ctc_rbc_force *f, int nc, const float *pp, double *av, void *stream);
+
+/* ---- solvent-membrane forces: replaces src/fsi/imp.h:6-13 ----------------- */
+typedef struct ctc_fsi ctc_fsi;
+/* fsi_ini of a 1-rank periodic box (trunk rnd_ini(1908, 1409, 290, 12968),
+ * src/fsi/imp/main.h:1-9), for up to maxv vertices and maxs solvent */
+int ctc_fsi_ini(int LX, int LY, int LZ, int maxv, int maxs, ctc_fsi **f);
+int ctc_fsi_fin(ctc_fsi *f);
+/* fsi_bind_solvent + fsi_bulk + fsi_halo (src/fsi/imp/{main,bulk,halo}.h):
+ * draws the bulk then the halo seed; nv vertices pv [dev, AoS] against ns
+ * cell-sorted solvent ps [dev, AoS] with starts/counts [dev]; vertex forces
+ * fv and solvent forces fs [dev, AoS] are accumulated */
+int ctc_fsi_apply(ctc_fsi *f, const ctc_dpd_params *p, int nv, const float *pv, int ns, const float *ps,
+                  const int *starts, const int *counts, float *fv, float *fs, void *stream);
+/* the same with explicit seeds and RNG keys (CTC_RNG_*) */
+int ctc_fsi_apply_seeded(ctc_fsi *f, const ctc_dpd_params *p, int nv, const float *pv, int ns, const float *ps,
+                         const int *starts, const int *counts, float seed_bulk, float seed_halo, int rng,
+                         float *fv, float *fs, void *stream);
+
+/* ---- time update: replaces src/scheme/move/imp.h:5-6, scheme/force ------- */
+/* scheme_move_apply: v += f/m dt; r += v dt on n AoS particles [dev] */
+int ctc_scheme_move_apply(float dt, float mass, int n, const float *ff, float *pp, void *stream);
+/* scheme_move_clear_vel */
+int ctc_scheme_move_clear_vel(int n, float *pp, void *stream);
+/* bforce_apply with a constant acceleration a[3] [host]: f += m a */
+int ctc_bforce_apply_cste(float mass, const float *a, int n, float *ff, void *stream);
+
+/* ---- whole plain-DPD system on the fast path ----------------------------- */
+typedef struct ctc_sim ctc_sim;
+typedef struct {
+    int LX, LY, LZ;          /* box in unit cells */
+    int maxp;                /* solvent capacity */
+    ctc_dpd_params dpd;      /* solvent-solvent */
+    float mass, dt;
+    float bodyf[3];          /* constant body acceleration (0 = none) */
+    int rng;                 /* CTC_RNG_REFERENCE or CTC_RNG_STABLE */
+} ctc_sim_config;
+
+int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **s);
+int ctc_sim_destroy(ctc_sim *s);
+/* upload n solvent particles [host, AoS] */
+int ctc_sim_set_solvent(ctc_sim *s, int n, const float *pp, void *stream);
+/* same from a device AoS array */
+int ctc_sim_set_solvent_dev(ctc_sim *s, int n, const float *pp, void *stream);
+/* advance nsteps steps: wrap + cell lists, bulk + halo DPD, body force,
+ * update -- the reference's step order (src/sim/imp/run.h:8-68) */
+int ctc_sim_step(ctc_sim *s, int nsteps, void *stream);
+/* number of solvent particles (synchronises the stream) */
+int ctc_sim_count(ctc_sim *s, int *n, void *stream);
+/* download the cell-sorted solvent [host, AoS, capacity maxp] */
+int ctc_sim_get_solvent(ctc_sim *s, float *pp, int *n, void *stream);
+/* total momentum (3), kinetic temperature, count -- FP64 reductions on the
+ * device (replaces diag_part_apply, src/io/diag/part/imp/main.h:37-68) */
+int ctc_sim_diag(ctc_sim *s, double *out5, void *stream);
+/* device pointers of the current state (cell-sorted float4 SoA) */
+int ctc_sim_state(ctc_sim *s, float **pos, float **vel, float **force, const int **starts);
+/* current bulk seed and 26 halo seeds of the next step [host, 27 floats] */
+int ctc_sim_next_seeds(const ctc_sim *s, float *seeds27);
+/* per-phase device timing: when enabled every step records CUDA events on
+ * its stream; profile_read returns the summed milliseconds of [0] seeds +
+ * cell lists, [1] fragment starts, [2] pair forces, [3] update, and the
+ * number of steps, then restarts the count */
+int ctc_sim_profile(ctc_sim *s, int enable);
+int ctc_sim_profile_read(ctc_sim *s, double *ms4, int *steps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -54,6 +54,7 @@ def lib():
             "orc_set_rng_contraction": (None, [C.c_int]),
             "orc_get_rng_contraction": (C.c_int, []),
             "orc_pair_force": (None, [C.c_float] * 4 + [f32p, f32p, C.c_float, f32p]),
+            "orc_mean0var1_batch": (None, [C.c_int, C.c_float, i32p, i32p, C.c_int, f32p]),
             "orc_clist_build": (C.c_int, [C.c_int] * 4 + [f32p, C.c_int, i32p, i32p, i32p, f32p]),
             "orc_dpd_bulk": (None, [C.c_int] * 4 + [f32p, i32p, Dpd, C.c_float, f32p]),
             "orc_dpd_bulk_f64": (None, [C.c_int] * 4 + [f32p, i32p, Dpd, C.c_float, f64p]),
@@ -116,6 +117,14 @@ class Kiss:
 
 def mean0var1ii(seed, u, v):
     return np.float32(lib().orc_mean0var1ii(seed, int(u), int(v)))
+
+
+def mean0var1_batch(seed, u, v, unsigned=False):
+    u = np.ascontiguousarray(u, np.int32)
+    v = np.ascontiguousarray(v, np.int32)
+    out = np.zeros(len(u), np.float32)
+    lib().orc_mean0var1_batch(len(u), seed, u, v, int(unsigned), out)
+    return out
 
 
 def mean0var1uu(seed, u, v):

@@ -78,11 +78,13 @@ void orc_set_rng_contraction(int mode) { g_rng_contraction = mode; }
 int  orc_get_rng_contraction(void) { return g_rng_contraction; }
 
 /* low-discrepancy key of (u, v), dev.h:59,67: the sum of four products; the
- * device code contracts the chain into fma(v,t, fma(C,s, fma(A,g, u*b))) */
+ * device code contracts the chain into fma(v,t, fma(C,s, fma(u,b, A*g)))
+ * (each "x + y*z" becomes fma(y, z, x)), as the reference's own kernel built
+ * for sm_100a computes it bit for bit */
 static float key_p(float A, float U, float C, float V) {
     float p;
     if (g_rng_contraction) {
-        p = fmaf(V, RND_TIN, fmaf(C, RND_SILVER, fmaf(A, RND_GOLD, U * RND_BRONZE)));
+        p = fmaf(V, RND_TIN, fmaf(C, RND_SILVER, fmaf(U, RND_BRONZE, A * RND_GOLD)));
     } else {
         float t0 = A * RND_GOLD, t1 = U * RND_BRONZE, t2 = C * RND_SILVER, t3 = V * RND_TIN;
         p = ((t0 + t1) + t2) + t3;
@@ -105,7 +107,7 @@ float orc_mean0var1uu(float seed, uint32_t u, uint32_t v) { /* dev.h:64-72 */
 /* ========================================================================= */
 
 /* r^2 as the device computes x*x + y*y + z*z (contracted) */
-static float dist2f(float x, float y, float z) { return fmaf(z, z, fmaf(x, x, y * y)); }
+static float dist2f(float x, float y, float z) { return fmaf(z, z, fmaf(y, y, x * x)); }
 
 static void pair_force_ref(float a, float g, float s, float spow, const float *pa,
                            const float *pb, float rnd, float f[3]) {
@@ -122,10 +124,10 @@ static void pair_force_ref(float a, float g, float s, float spow, const float *p
         r = r2 * invr;
         x *= invr; y *= invr; z *= invr;
     }
-    ev = fmaf(z, dvz, fmaf(x, dvx, y * dvy));                      /* dot */
+    ev = fmaf(z, dvz, fmaf(y, dvy, x * dvx));                      /* dot */
     rm = 1.0f - r; if (rm < 0.0f) rm = 0.0f;                       /* magn_dpd */
     wr = powf(rm, spow);
-    f0 = fmaf(fmaf((-g) * wr, ev, s * rnd), wr, a * rm);
+    f0 = fmaf(a, rm, fmaf(s, rnd, ((-g) * wr) * ev) * wr);
     f[0] = f0 * x; f[1] = f0 * y; f[2] = f0 * z;
 }
 
@@ -169,6 +171,15 @@ static int clamp_cell(int i, int L) { return i < 0 ? 0 : i >= L ? L - 1 : i; }
 
 int orc_clist_build(int LX, int LY, int LZ, int n, const float *pp, int project,
                     int *counts, int *starts, int *order, float *ppout) {
+    return orc_clist_build_late(LX, LY, LZ, n, pp, project, NULL, counts, starts, order, ppout);
+}
+
+/* as orc_clist_build; particles with late[i] != 0 (those that re-entered the
+ * box through a periodic face) follow the others inside their cell, as the
+ * reference's remote array is binned after the local one
+ * (src/distr/flu/imp/gather.h:1-11) */
+int orc_clist_build_late(int LX, int LY, int LZ, int n, const float *pp, int project,
+                         const unsigned char *late, int *counts, int *starts, int *order, float *ppout) {
     int nc = LX * LY * LZ, i, k, nout = 0;
     int *cid = (int*)malloc(sizeof(int) * (n > 0 ? n : 1));
     int *fill = (int*)malloc(sizeof(int) * nc);
@@ -179,20 +190,22 @@ int orc_clist_build(int LX, int LY, int LZ, int n, const float *pp, int project,
         int ix = (int)((double)r[0] + LX / 2);
         int iy = (int)((double)r[1] + LY / 2);
         int iz = (int)((double)r[2] + LZ / 2);
-        int inside = (r[0] >= -LX / 2) && (r[0] < LX / 2) && (r[1] >= -LY / 2) &&
-                     (r[1] < LY / 2) && (r[2] >= -LZ / 2) && (r[2] < LZ / 2);   /* main.h:6-12 */
+        /* box [lo, lo + L) with lo = -(L/2): the reference's [-L/2, L/2) for even L */
+        int inside = (r[0] >= -(LX / 2)) && (r[0] < LX - LX / 2) && (r[1] >= -(LY / 2)) &&
+                     (r[1] < LY - LY / 2) && (r[2] >= -(LZ / 2)) && (r[2] < LZ - LZ / 2); /* main.h:6-12 */
         if (project) { ix = clamp_cell(ix, LX); iy = clamp_cell(iy, LY); iz = clamp_cell(iz, LZ); }
         if (project || inside) { cid[i] = ix + LX * (iy + LY * iz); counts[cid[i]]++; }
         else cid[i] = -1;
     }
     for (k = 0, i = 0; i < nc; i++) { starts[i] = k; fill[i] = k; k += counts[i]; }
     nout = k;
-    for (i = 0; i < n; i++) {           /* stable: ascending input index in a cell */
-        if (cid[i] < 0) continue;
-        k = fill[cid[i]]++;
-        if (order) order[k] = i;
-        if (ppout) memcpy(ppout + 6 * k, pp + 6 * i, 6 * sizeof(float));
-    }
+    for (int pass = 0; pass < 2; pass++)   /* stable: ascending input index in a cell */
+        for (i = 0; i < n; i++) {
+            if (cid[i] < 0 || (late ? (late[i] != 0) : 0) != pass) continue;
+            k = fill[cid[i]]++;
+            if (order) order[k] = i;
+            if (ppout) memcpy(ppout + 6 * k, pp + 6 * i, 6 * sizeof(float));
+        }
     free(cid); free(fill);
     return nout;
 }
@@ -450,8 +463,12 @@ void orc_fsi_bulk(int LX, int LY, int LZ, int nv, const float *pv, int ns, const
  * fragment in ascending vertex order, received in slot anti(fid) and shifted
  * by L*d(anti(fid)) (src/exch/common/dev.h:25-47) */
 static int emap_fids(int LX, int LY, int LZ, const float *r, int fids[7]) {
-    int L0[3] = {LX - 2, LY - 2, LZ - 2}, d[3], c, j = 0;
-    for (c = 0; c < 3; c++) d[c] = -1 + (r[c] >= (float)(-L0[c] / 2)) + (r[c] >= (float)(L0[c] / 2));
+    int L[3] = {LX, LY, LZ}, d[3], c, j = 0;
+    /* inner box [lo + 1, lo + L - 1): the reference's [-(L-2)/2, (L-2)/2) for even L */
+    for (c = 0; c < 3; c++) {
+        int lo = -(L[c] / 2);
+        d[c] = -1 + (r[c] >= (float)(lo + 1)) + (r[c] >= (float)(lo + L[c] - 1));
+    }
     for (c = 0; c < 3; c++)
         if (d[c]) { int df[3] = {0, 0, 0}; df[c] = d[c]; fids[j++] = orc_frag_d2i(df[0], df[1], df[2]); }
     for (c = 0; c < 3; c++) {
@@ -788,14 +805,25 @@ void orc_body_force(float mass, const float a[3], int n, float *ff) {
 }
 
 /* src/distr/flu/dev.h:1-13 + src/distr/map/dev.h:17-26 + shift by L*d */
-void orc_wrap(int LX, int LY, int LZ, int n, float *pp) {
+void orc_wrap(int LX, int LY, int LZ, int n, float *pp) { orc_wrap_flag(LX, LY, LZ, n, pp, NULL); }
+
+void orc_wrap_flag(int LX, int LY, int LZ, int n, float *pp, unsigned char *moved) {
     int L[3] = {LX, LY, LZ}, i, c;
-    for (i = 0; i < n; i++)
+    for (i = 0; i < n; i++) {
+        if (moved) moved[i] = 0;
         for (c = 0; c < 3; c++) {
             float x = pp[6 * i + c];
-            int d = -1 + (x >= (float)(-L[c] / 2)) + (x >= (float)(L[c] / 2));
-            if (d) pp[6 * i + c] = x - (float)(d * L[c]);
+            int lo = -(L[c] / 2);
+            int d = -1 + (x >= (float)lo) + (x >= (float)(lo + L[c]));
+            if (d) { pp[6 * i + c] = x + (float)(-d * L[c]); if (moved) moved[i] = 1; }
         }
+    }
+}
+
+void orc_mean0var1_batch(int n, float seed, const int *u, const int *v, int uu, float *out) {
+    int i;
+    for (i = 0; i < n; i++)
+        out[i] = uu ? orc_mean0var1uu(seed, (uint32_t)u[i], (uint32_t)v[i]) : orc_mean0var1ii(seed, u[i], v[i]);
 }
 
 /* src/distr/rbc/dev.h:1-25: the bounding-box centre decides */
@@ -813,11 +841,12 @@ void orc_rbc_wrap(int LX, int LY, int LZ, int nc, int nv, float *pp) {
             }
         for (k = 0; k < 3; k++) {
             r = 0.5f * (lo[k] + hi[k]);
-            d[k] = -1 + (r >= (float)(-L[k] / 2)) + (r >= (float)(L[k] / 2));
+            int lo = -(L[k] / 2);
+            d[k] = -1 + (r >= (float)lo) + (r >= (float)(lo + L[k]));
         }
         for (i = 0; i < nv; i++)
             for (k = 0; k < 3; k++)
-                if (d[k]) pp[6 * (c * nv + i) + k] -= (float)(d[k] * L[k]);
+                if (d[k]) pp[6 * (c * nv + i) + k] += (float)(-d[k] * L[k]);
     }
 }
 

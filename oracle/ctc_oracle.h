@@ -46,6 +46,11 @@ void orc_pair_force(float a, float g, float s, float spow, const float pa[6],
 int orc_clist_build(int LX, int LY, int LZ, int n, const float *pp, int project,
                     int *counts, int *starts, int *order, float *ppout);
 
+int orc_clist_build_late(int LX, int LY, int LZ, int n, const float *pp, int project,
+                         const unsigned char *late, int *counts, int *starts, int *order, float *ppout);
+void orc_wrap_flag(int LX, int LY, int LZ, int n, float *pp, unsigned char *moved);
+void orc_mean0var1_batch(int n, float seed, const int *u, const int *v, int uu, float *out);
+
 /* ---- solvent DPD (src/fluforces) ----------------------------------------- */
 typedef struct { float a, g, s, spow; } orc_dpd;
 /* bulk: src/fluforces/bulk/dev/main.h:23-97, accumulates into ff */

@@ -63,7 +63,7 @@ static void bulk_range(int LX, int LY, int LZ, int i0, int i1, const float *pp, 
             for (ib = bs; ib < be && ib < ia; ib++) {
                 const float *pb = pp + 6 * ib;
                 float x = pa[0] - pb[0], y = pa[1] - pb[1], z = pa[2] - pb[2], f[3];
-                if (!(fmaf(z, z, fmaf(x, x, y * y)) <= 1.0f)) continue;
+                if (!(fmaf(z, z, fmaf(y, y, x * x)) <= 1.0f)) continue;
                 orc_pair_force(p.a, p.g, p.s, p.spow, pa, pb, orc_mean0var1ii(seed, ia, ib), f);
                 fa[0] += f[0]; fa[1] += f[1]; fa[2] += f[2];
                 ff[3 * ib + 0] -= f[0]; ff[3 * ib + 1] -= f[1]; ff[3 * ib + 2] -= f[2];
@@ -96,8 +96,10 @@ int orc_dpd_step(int LX, int LY, int LZ, int n, float *pp, float *work, orc_dpd 
     int nc = LX * LY * LZ, nout;
     int *counts = (int*)malloc(sizeof(int) * nc), *starts = (int*)malloc(sizeof(int) * (nc + 1));
     float *ff = (float*)calloc((size_t)3 * (n > 0 ? n : 1), sizeof(float));
-    orc_wrap(LX, LY, LZ, n, pp);
-    nout = orc_clist_build(LX, LY, LZ, n, pp, 0, counts, starts, NULL, work);
+    unsigned char *moved = (unsigned char*)malloc((size_t)(n > 0 ? n : 1));
+    orc_wrap_flag(LX, LY, LZ, n, pp, moved);
+    nout = orc_clist_build_late(LX, LY, LZ, n, pp, 0, moved, counts, starts, NULL, work);
+    free(moved);
     starts[nc] = nout;
     orc_dpd_bulk_parallel(LX, LY, LZ, nout, work, starts, p, seeds[0], ff);
     orc_dpd_halo(LX, LY, LZ, nout, work, starts, counts, p, seeds + 1, ff);

@@ -1,0 +1,113 @@
+"""ctypes front end of oracle/_ref/librefkern.so: the reference's own device
+code (src/math/rnd/dev.h, src/pair/dev.h) built from its sources by
+oracle/ref.mk.  TEST INFRASTRUCTURE ONLY.  Arrays are torch CUDA tensors."""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PATH = os.path.join(_HERE, "_ref", "librefkern.so")
+_lib = None
+
+
+def available():
+    return os.path.exists(PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(PATH)
+        vp = C.c_void_p
+        L.refkern_rnd.argtypes = [C.c_int, C.c_float, vp, vp, C.c_int, vp]
+        L.refkern_pair.argtypes = [C.c_int] + [C.c_float] * 4 + [vp, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def rnd(seed, u, v, unsigned=False):
+    import torch
+    out = torch.empty(u.shape[0], dtype=torch.float32, device=u.device)
+    torch.cuda.synchronize()
+    assert lib().refkern_rnd(int(u.shape[0]), float(seed), _p(u), _p(v), int(unsigned), _p(out)) == 0
+    return out
+
+
+def pair(dpd, pa, pb, r):
+    import torch
+    f = torch.empty((pa.shape[0], 3), dtype=torch.float32, device=pa.device)
+    torch.cuda.synchronize()
+    assert lib().refkern_pair(int(pa.shape[0]), *[float(x) for x in dpd], _p(pa), _p(pb), _p(r), _p(f)) == 0
+    return f
+
+
+def _sig(L):
+    vp = C.c_void_p
+    L.refkern_bulk.argtypes = [C.c_float] * 4 + [C.c_int] * 4 + [vp, vp, C.c_float, vp]
+    L.refkern_halo.argtypes = [C.c_float] * 4 + [C.c_int] * 5 + [vp, vp, vp, vp, C.c_float, C.c_int, vp]
+
+
+def bulk(dpd, L, pp, starts, seed, ff):
+    """fluforces bulk: adds the reference kernel's forces to ff (torch, (n,3))."""
+    import torch
+    lib_ = lib()
+    _sig(lib_)
+    torch.cuda.synchronize()
+    assert lib_.refkern_bulk(*[float(x) for x in dpd], *L, int(pp.shape[0]), _p(pp), _p(starts), float(seed),
+                             _p(ff)) == 0
+
+
+def fragments(L, starts, counts):
+    """Packed fragment lists of src/exch/flu/dev/{map,pack}.h: for every
+    fragment the sorted indices of its particles (fragment cells x-fastest)
+    and the fragment-cell starts (ncells + 1)."""
+    import numpy as np
+    from . import frag_dir
+    L = tuple(int(x) for x in L)
+    out = []
+    for fid in range(26):
+        d = frag_dir(fid)
+        org = [L[c] - 1 if d[c] == 1 else 0 for c in range(3)]
+        ext = [L[c] if d[c] == 0 else 1 for c in range(3)]
+        z, y, x = np.meshgrid(np.arange(ext[2]), np.arange(ext[1]), np.arange(ext[0]), indexing="ij")
+        cid = ((org[0] + x) + L[0] * ((org[1] + y) + L[1] * (org[2] + z))).reshape(-1)
+        cnt = counts[cid]
+        fss = np.zeros(len(cid) + 1, np.int32)
+        fss[1:] = np.cumsum(cnt)
+        ii = np.concatenate([np.arange(starts[c], starts[c] + counts[c]) for c in cid]).astype(np.int32) \
+            if fss[-1] > 0 else np.zeros(0, np.int32)
+        out.append((ii, fss))
+    return out
+
+
+def halo(dpd, L, pp, starts, counts, seeds26, ff):
+    """fluforces halo of a 1-rank periodic box with the reference kernel: for
+    fragment fid the local list is fragment fid, the remote one its
+    anti-fragment (what the self-neighbour sends back), ff accumulated."""
+    import numpy as np
+    import torch
+    from . import frag_anti, halo_masks
+    lib_ = lib()
+    _sig(lib_)
+    starts_h = starts.cpu().numpy() if hasattr(starts, "cpu") else np.asarray(starts)
+    counts_h = counts.cpu().numpy() if hasattr(counts, "cpu") else np.asarray(counts)
+    fr = fragments(L, starts_h, counts_h)
+    masks = halo_masks()
+    dev = pp.device
+    packed = []
+    for ii, fss in fr:
+        idx = torch.as_tensor(ii.astype(np.int64), device=dev)
+        packed.append((pp[idx].contiguous(), torch.as_tensor(ii, device=dev), torch.as_tensor(fss, device=dev)))
+    torch.cuda.synchronize()
+    for fid in range(26):
+        lpp, lii, _ = packed[fid]
+        rpp, _, rss = packed[frag_anti(fid)]
+        n = int(lii.shape[0])
+        if n == 0:
+            continue
+        rp = rpp if rpp.shape[0] > 0 else torch.zeros((1, 6), device=dev)
+        assert lib_.refkern_halo(*[float(x) for x in dpd], *L, fid, n, _p(lpp), _p(lii), _p(rp), _p(rss),
+                                 float(seeds26[fid]), int(masks[fid]), _p(ff)) == 0

@@ -1,0 +1,50 @@
+"""CPU checks of the oracle's membrane restatement (no GPU): adjacency of the
+reference's 642-vertex cell, and forces that are the negative gradient of
+the bending energy and of the area/volume/spring energies."""
+import os
+
+import numpy as np
+
+import oracle
+from ctc_b200 import mesh, systems
+
+from .conftest import GOLDEN
+
+
+def test_adjacency_642():
+    V, F = mesh.read_off(os.path.join(GOLDEN, "rbc.642.off"))
+    md, a0, a1 = oracle.adj_build(F, len(V))
+    assert md == 6
+    val = (a0.reshape(-1, 6) >= 0).sum(1)
+    assert sorted(np.bincount(val).tolist())[-2:] == [12, 630]   # valence 5: 12, 6: 630
+
+
+def test_template_topology():
+    X, F = mesh.rbc_template()
+    assert X.shape == (642, 3) and F.shape == (1280, 3)
+    md, a0, a1 = oracle.adj_build(F, 642)
+    assert md == 6
+    A, V = mesh.area_volume(X, F)
+    assert A > 0 and V > 0
+    # Evans-Fung thickness: about 0.8 at the centre, about 2.6 at most
+    assert abs(X[:, 0].max() - X[:, 0].min() - 7.82) < 0.05
+    assert 2.3 < X[:, 2].max() - X[:, 2].min() < 2.7
+
+
+def test_bending_force_is_energy_gradient():
+    V, F = mesh.read_off(os.path.join(GOLDEN, "rbc.642.off"))
+    rng = np.random.default_rng(0)
+    pp = np.zeros((len(V), 6), np.float32)
+    pp[:, :3] = V + rng.normal(0, 0.05, V.shape)
+    par = dict(gammaC=0.0, gammaT=0.0, kBT=0.0, kb=1.0, phi=0.0, ks=0.0, x0=0.457, mpow=2.0, ka=0.0, kd=0.0,
+               kv=0.0, totArea=1.0, totVolume=1.0)
+    f = oracle.rbc_forces(F, len(V), pp, par, f64=True)
+    h = 1e-3
+    for i in rng.choice(len(V), 5, replace=False):
+        for c in range(3):
+            p1, p2 = pp.copy(), pp.copy()
+            p1[i, c] += h
+            p2[i, c] -= h
+            g = (oracle.kantor_energy(F, len(V), p1, 1.0) - oracle.kantor_energy(F, len(V), p2, 1.0)) / \
+                (float(p1[i, c]) - float(p2[i, c]))
+            assert abs(-g - f[i, c]) < 2e-3 * max(1.0, abs(f[i, c])), (i, c, -g, f[i, c])
