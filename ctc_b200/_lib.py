@@ -46,6 +46,7 @@ SIGNATURES = {
     "ctc_clist_fin": (C.c_int, [vp]),
     "ctc_clist_build": (C.c_int, [vp, C.c_int, vp, vp, ip, vp]),
     "ctc_clist_get": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+    "ctc_clist_build_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]),
     "ctc_fluforces_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
     "ctc_fluforces_fin": (C.c_int, [vp]),
     "ctc_fluforces_bulk_apply": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, vp, vp, vp, vp]),

@@ -92,6 +92,25 @@ int ctc_clist_build(ctc_clist *c, int n, const float *pp, float *ppout, int *nou
  * = input index of the k-th sorted particle. */
 int ctc_clist_get(const ctc_clist *c, const int **starts, const int **counts, const int **ids);
 
+/* ---- cell lists without device allocation ------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * where they need cell lists -- code running inside a host callback or an
+ * allocator hook, where CUDA allocation is not allowed, or a service whose
+ * steady-state path must not allocate so that it cannot fail or fragment
+ * memory mid-run.  Same result as ctc_clist_build: pp [dev, AoS, n] in,
+ * ppout [dev, AoS], starts [dev, LX*LY*LZ + 1], counts [dev, LX*LY*LZ] and
+ * ids [dev, may be NULL] out.  Its scratch is one fixed 3 MiB device array
+ * of the library (held on every GPU that loads it until exit), so a call
+ * takes at most CTC_CLIST_NOALLOC_MAXP particles and CTC_CLIST_NOALLOC_MAXC
+ * cells (CTC_ERR_CAPACITY otherwise).  All calls share that array: calls
+ * whose work overlaps on the GPU race and must be serialised by the caller.
+ * The first call on a device looks up the array's address with that device
+ * current; make it before any stream capture. */
+#define CTC_CLIST_NOALLOC_MAXP 262144
+#define CTC_CLIST_NOALLOC_MAXC 1048576
+int ctc_clist_build_noalloc(int LX, int LY, int LZ, int n, const float *pp, float *ppout, int *starts,
+                            int *counts, int *ids, void *stream);
+
 /* ---- solvent DPD: replaces src/fluforces/imp.h:8-25 --------------------- */
 typedef struct ctc_fluforces ctc_fluforces;
 /* fluforces_bulk_ini + fluforces_halo_ini for a 1-rank periodic box; the
