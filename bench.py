@@ -37,6 +37,8 @@ CONFIGS = {
     # profiling case: the C2 kernels on a box whose state still exceeds L2
     "p64": dict(L=(64, 64, 64), bodyf=(0.01, 0.0, 0.0), steps=10,
                 name="plain DPD 64x64x64 rho=10 (2,621,440 particles), body force 0.01 x"),
+    "c3": dict(L=(64, 64, 64), bodyf=(0.0, 0.0, 0.0), steps=100, rbc=200,
+               name="C3 RBC suspension 64x64x64 rho=10 (2,621,440 solvent) + 200 cells x 642 vertices"),
 }
 METRIC = "particle-steps/s @1 B200 (plain DPD step)"
 PAIR_BYTES = 48          # algorithmic bytes per particle of the pair kernel: pos+vel read, force write
@@ -220,6 +222,12 @@ def run_ours(args, cfg, world, rank, local):
     stream = torch.cuda.current_stream()
     sim = ctc.Sim(L, n, dpd, mass=1.0, dt=systems.DT, bodyf=cfg["bodyf"])
     sim.set_solvent(pp)
+    nvt = 0
+    if cfg.get("rbc"):
+        pv, tri, par = systems.rbc_system(L, cfg["rbc"], seed=3 + rank)
+        fsi = ctc.DpdParams(0.0, systems.GAMMA, systems.dpd_params()[2], systems.SPOW)   # a = 0, gamma = 8
+        sim.set_membranes(pv, tri, 642, par, fsi, mass=systems.RBC_MASS)
+        nvt = len(pv)
     sim.step(args.warmup)
     torch.cuda.synchronize()
     _lib.check(_lib.lib().ctc_sim_profile(sim.h, 1))
@@ -242,7 +250,7 @@ def run_ours(args, cfg, world, rank, local):
     _lib.check(_lib.lib().ctc_sim_profile(sim.h, 0))
     assert ctc.device_error() == 0, "device error during the timed steps"
     ms_max = allmax(world, ms)
-    total = allsum(world, n * args.steps)
+    total = allsum(world, (n + nvt) * args.steps)
     value = total / (ms_max * 1e-3)
 
     # end to end through the public API with host buffers: upload the state
@@ -257,14 +265,18 @@ def run_ours(args, cfg, world, rank, local):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     _lib.check(_lib.lib().ctc_sim_set_solvent(sim.h, n, C.c_void_p(host_in.data_ptr()), st))
+    if nvt:
+        sim.set_membranes(pv, tri, 642, par, fsi, mass=systems.RBC_MASS)
     for _ in range(args.steps):
         _lib.check(_lib.lib().ctc_sim_step(sim.h, 1, st))
         _lib.check(_lib.lib().ctc_sim_diag(sim.h, diag, st))
     _lib.check(_lib.lib().ctc_sim_get_solvent(sim.h, C.c_void_p(host_out.data_ptr()), C.byref(nout), st))
+    if nvt:
+        sim.get_membranes()
     torch.cuda.synchronize()
     e2e_s = allmax(world, time.perf_counter() - t0)
     e2e_value = total / e2e_s
-    state_bytes = 24 * n
+    state_bytes = 24 * (n + nvt)
     sim.close()
 
     if rank != 0:
@@ -283,7 +295,8 @@ def run_ours(args, cfg, world, rank, local):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded uniform solvent, Maxwellian velocities)",
-        "config": {"workload": cfg["name"], "particles_per_gpu": n, "box": list(L), "rho": 10,
+        "config": {"workload": cfg["name"], "particles_per_gpu": n, "membrane_vertices_per_gpu": nvt,
+                   "box": list(L), "rho": 10,
                    "rng": "reference keys", "parallelism": "replicas" if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (state %.2f GB per buffer)" % (32e-9 * n)},
         "gpu_launches": 10 * args.steps,   # seeds, 6 cell-list kernels, fragment starts, pair, update

@@ -250,6 +250,21 @@ class Sim:
         pp = np.ascontiguousarray(pp, np.float32).reshape(-1, 6)
         check(lib().ctc_sim_set_solvent(self.h, len(pp), pp.ctypes.data_as(C.c_void_p), _stream(stream)))
 
+    def set_membranes(self, pv, tri, nv, params, fsi, mass=0.5, stream=None):
+        """Cells of one template: pv (nc*nv, 6) AoS, tri (nt, 3); params a dict of
+        RbcParams fields, fsi a DpdParams."""
+        pv = np.ascontiguousarray(pv, np.float32).reshape(-1, 6)
+        tri = np.ascontiguousarray(tri, np.int32).reshape(-1, 3)
+        self.mnv, self.mnc = int(nv), len(pv) // int(nv)
+        check(lib().ctc_sim_set_membranes(self.h, self.mnc, self.mnv, len(tri), tri.ctypes.data_as(C.c_void_p),
+                                          pv.ctypes.data_as(C.c_void_p), C.byref(_lib.RbcParams(**params)),
+                                          C.byref(fsi), float(mass), _stream(stream)))
+
+    def get_membranes(self, stream=None):
+        out = np.zeros((self.mnc * self.mnv, 6), np.float32)
+        check(lib().ctc_sim_get_membranes(self.h, out.ctypes.data_as(C.c_void_p), _stream(stream)))
+        return out
+
     def step(self, n=1, stream=None):
         check(lib().ctc_sim_step(self.h, int(n), _stream(stream)))
 

@@ -72,6 +72,9 @@ SIGNATURES = {
     "ctc_sim_set_solvent": (C.c_int, [vp, C.c_int, vp, vp]),
     "ctc_sim_set_solvent_dev": (C.c_int, [vp, C.c_int, vp, vp]),
     "ctc_sim_step": (C.c_int, [vp, C.c_int, vp]),
+    "ctc_sim_set_membranes": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, C.POINTER(RbcParams),
+                                        C.POINTER(DpdParams), C.c_float, vp]),
+    "ctc_sim_get_membranes": (C.c_int, [vp, vp, vp]),
     "ctc_sim_count": (C.c_int, [vp, ip, vp]),
     "ctc_sim_get_solvent": (C.c_int, [vp, vp, ip, vp]),
     "ctc_sim_diag": (C.c_int, [vp, C.POINTER(C.c_double), vp]),

@@ -12,6 +12,7 @@
 #include "common.cuh"
 #include "dpd.h"
 #include "integrate.h"
+#include "membrane.h"
 #include "api_util.h"
 
 using namespace ctc;
@@ -307,6 +308,17 @@ struct ctc_sim {
     int prof;                              // record per-phase events each step
     std::vector<cudaEvent_t> ev;           // 5 events per profiled step
     int prof_steps;
+    // membranes (optional): nc cells of nv vertices, unsorted float4 SoA
+    int mnc, mnv;
+    ctc_rbc_force *rbc;
+    ctc_rbc_params mpar;
+    ctc_dpd_params fsi;
+    float mmass;
+    float4 *mpos, *mvel, *mforce;
+    int *mcount;                           // device copy of mnc * mnv
+    unsigned *fmask;                       // FSI image lists (reference keys)
+    int *frank, *fcount, *fimg_start;
+    Kiss fsi_host;                         // host mirror of the FSI trunk
 };
 
 static void sim_mark(ctc_sim *s, int k, cudaStream_t st) {
@@ -341,14 +353,17 @@ extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
     CUDA_TRY(cudaMalloc(&s->fss, sizeof(int) * (size_t)s->off.d[26]));
     CUDA_TRY(cudaMalloc(&s->scratch, clist_scratch_bytes(s->nc, (int)np)));
     clist_carve(&s->w, s->scratch, s->nc, (int)np);
-    CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 27));
-    CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 27));
+    CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 28));   // + the FSI trunk
+    CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 29));
     CUDA_TRY(cudaMalloc(&s->diag_scratch, diag_scratch_bytes()));
     CUDA_TRY(cudaMalloc(&s->diag_out, sizeof(double) * 5));
     // trunk 0: bulk (0,0,0,0); 1..26: halo fragments.  Stable keys use trunk 0 only.
     kiss_ini(&s->trunk_host[0], 0, 0, 0, 0);
     for (int i = 0; i < 26; i++) halo_trunk_ini(i, &s->trunk_host[1 + i]);
     CUDA_TRY(cudaMemcpy(s->trunk_dev, s->trunk_host, sizeof(unsigned) * 4 * 27, cudaMemcpyHostToDevice));
+    // FSI trunk of rank 0, rnd_ini(1908, 1409, 290, 12968) (src/fsi/imp/main.h:7)
+    kiss_ini(&s->fsi_host, 1908, 1409, 290, 12968);
+    CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 27, s->fsi_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
     s->cur = 0;
     s->n_host = 0;
     s->built = false;
@@ -363,6 +378,9 @@ extern "C" int ctc_sim_destroy(ctc_sim *s) {
     cudaFree(s->scratch); cudaFree(s->trunk_dev); cudaFree(s->seeds_dev); cudaFree(s->diag_scratch);
     cudaFree(s->diag_out);
     for (cudaEvent_t e : s->ev) cudaEventDestroy(e);
+    if (s->rbc) ctc_rbc_force_fin(s->rbc);
+    cudaFree(s->mpos); cudaFree(s->mvel); cudaFree(s->mforce); cudaFree(s->mcount);
+    cudaFree(s->fmask); cudaFree(s->frank); cudaFree(s->fcount); cudaFree(s->fimg_start);
     delete s;
     return CTC_OK;
 }
@@ -395,6 +413,60 @@ extern "C" int ctc_sim_set_solvent_dev(ctc_sim *s, int n, const float *pp, void 
     return sim_set(s, n, pp, false, (cudaStream_t)stream);
 }
 
+extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const int *tri, const float *pp,
+                                     const ctc_rbc_params *p, const ctc_dpd_params *fsi, float mass, void *stream) {
+    if (!s || nc < 0 || nv <= 0 || nt <= 0 || !tri || (nc > 0 && !pp) || !p || !fsi || mass <= 0)
+        return fail(CTC_ERR_ARG, "ctc_sim_set_membranes: bad arguments");
+    if ((long)nc * nv > (1 << 27)) return fail(CTC_ERR_CAPACITY, "ctc_sim_set_membranes: too many vertices");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (s->rbc) { ctc_rbc_force_fin(s->rbc); s->rbc = nullptr; }
+    cudaFree(s->mpos); cudaFree(s->mvel); cudaFree(s->mforce); cudaFree(s->mcount);
+    cudaFree(s->fmask); cudaFree(s->frank); cudaFree(s->fcount); cudaFree(s->fimg_start);
+    s->mpos = s->mvel = s->mforce = nullptr;
+    s->mcount = s->frank = s->fcount = s->fimg_start = nullptr;
+    s->fmask = nullptr;
+    int rc = ctc_rbc_force_ini(nv, nt, tri, nc > 0 ? nc : 1, &s->rbc);
+    if (rc) return rc;
+    size_t nvt = (size_t)nc * nv, cap = nvt > 0 ? nvt : 1;
+    CUDA_TRY(cudaMalloc(&s->mpos, sizeof(float4) * cap));
+    CUDA_TRY(cudaMalloc(&s->mvel, sizeof(float4) * cap));
+    CUDA_TRY(cudaMalloc(&s->mforce, sizeof(float4) * cap));
+    CUDA_TRY(cudaMalloc(&s->mcount, sizeof(int)));
+    CUDA_TRY(cudaMalloc(&s->fmask, sizeof(unsigned) * cap));
+    CUDA_TRY(cudaMalloc(&s->frank, sizeof(int) * 26 * cap));
+    CUDA_TRY(cudaMalloc(&s->fcount, sizeof(int) * 26));
+    CUDA_TRY(cudaMalloc(&s->fimg_start, sizeof(int) * 26));
+    int n = (int)nvt;
+    float *tmp = nullptr;
+    if (n > 0) {
+        CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 6 * nvt, st));
+        CUDA_TRY(cudaMemcpyAsync(tmp, pp, sizeof(float) * 6 * nvt, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(aos_to_soa(n, tmp, s->mpos, s->mvel, st));
+    }
+    CUDA_TRY(cudaMemcpyAsync(s->mcount, &n, sizeof(int), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (tmp) CUDA_TRY(cudaFreeAsync(tmp, st));
+    s->mnc = nc; s->mnv = nv;
+    s->mpar = *p;
+    s->fsi = *fsi;
+    s->mmass = mass;
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream) {
+    if (!s || !pp) return fail(CTC_ERR_ARG, "ctc_sim_get_membranes: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t nvt = (size_t)s->mnc * s->mnv;
+    if (nvt == 0) return CTC_OK;
+    float *tmp = nullptr;
+    CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 6 * nvt, st));
+    CUDA_TRY(soa_to_aos(nullptr, (int)nvt, s->mpos, s->mvel, tmp, st));
+    CUDA_TRY(cudaMemcpyAsync(pp, tmp, sizeof(float) * 6 * nvt, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaFreeAsync(tmp, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return CTC_OK;
+}
+
 // one step: seeds, wrap + cell lists into the other buffer, forces, update
 static int sim_step1(ctc_sim *s, cudaStream_t st) {
     int src = s->cur, dst = 1 - s->cur;
@@ -407,6 +479,15 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
     if (s->built) CUDA_TRY(cudaMemcpyAsync(s->count0, s->starts + s->nc, sizeof(int), cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(clist_launch(s->L, s->n_host, s->count0, s->pos[src], s->vel[src], 1, s->counts, s->starts,
                           s->pos[dst], s->vel[dst], nullptr, s->w, dev_err_ptr(), st));
+    const int nvt = s->mnc * s->mnv;
+    if (nvt > 0) {
+        // objects_distribute: whole cells re-enter through a periodic face
+        CUDA_TRY(rbc_wrap_launch(s->mnc, s->mnv, s->L, s->mpos, st));
+        // the FSI trunk is drawn for fsi_bulk, then for fsi_halo
+        CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 27, 2, s->seeds_dev + 27, st));
+        kiss_get(&s->fsi_host);
+        kiss_get(&s->fsi_host);
+    }
     sim_mark(s, 1, st);
     DpdArgs A;
     dpd_args_common(&A, s->L, &s->cfg.dpd);
@@ -420,9 +501,27 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
     CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n_host, st));
     sim_mark(s, 2, st);
     CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st));
+    const float3 bf = make_float3(s->cfg.bodyf[0], s->cfg.bodyf[1], s->cfg.bodyf[2]);
+    if (nvt > 0) {
+        // solvent-membrane forces into the vertex forces and, as reactions, the solvent ones
+        CUDA_TRY(cudaMemsetAsync(s->mforce, 0, sizeof(float4) * (size_t)nvt, st));
+        DpdPar F;
+        F.a = s->fsi.a; F.g = s->fsi.g; F.s = s->fsi.s; F.spow = s->fsi.spow;
+        int rc = fsi_forces(s->L, F, nvt, (const float*)s->mpos, (const float*)s->mvel, 4, s->pos[dst], s->vel[dst],
+                            s->starts, s->counts, (float*)s->mforce, 4, (float*)s->force, 4, 0.0f, 0.0f,
+                            s->seeds_dev + 27, s->cfg.rng, s->fmask, s->frank, s->fcount, s->fimg_start, st);
+        if (rc) return rc;
+    }
     sim_mark(s, 3, st);
     CUDA_TRY(integrate_launch(s->starts + s->nc, s->n_host, s->pos[dst], s->vel[dst], s->force, s->cfg.dt,
-                              s->cfg.mass, make_float3(s->cfg.bodyf[0], s->cfg.bodyf[1], s->cfg.bodyf[2]), st));
+                              s->cfg.mass, bf, st));
+    if (nvt > 0) {
+        // objects_advance: internal forces on top of the FSI ones, then the update
+        int rc = membrane_forces(s->rbc, &s->mpar, s->mnc, (const float*)s->mpos, (const float*)s->mvel, 4,
+                                 (float*)s->mforce, 4, st);
+        if (rc) return rc;
+        CUDA_TRY(integrate_launch(s->mcount, nvt, s->mpos, s->mvel, s->mforce, s->cfg.dt, s->mmass, bf, st));
+    }
     sim_mark(s, 4, st);
     if (s->prof) s->prof_steps++;
     s->cur = dst;

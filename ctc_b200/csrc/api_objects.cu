@@ -128,6 +128,7 @@ static void stressful(int nt, float totArea, double *l0, double *a0) {
     *l0 = l0f;
 }
 
+namespace ctc {
 int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const float *pos, const float *vel, int stride,
                     float *force, int fstride, cudaStream_t st) {
     if (nc > f->max_cells) return fail(CTC_ERR_CAPACITY, "nc=%d > max_cell=%d", nc, f->max_cells);
@@ -147,6 +148,7 @@ int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const flo
     CUDA_TRY(membrane_launch(A, st));
     return CTC_OK;
 }
+}  // namespace ctc
 
 extern "C" int ctc_rbc_force_apply(ctc_rbc_force *f, const ctc_rbc_params *p, float dt, int nc, const float *pp,
                                    float *ff, void *stream) {
@@ -209,10 +211,11 @@ extern "C" int ctc_fsi_fin(ctc_fsi *f) {
     return CTC_OK;
 }
 
+namespace ctc {
 int fsi_forces(int3 L, const DpdPar &P, int nv, const float *pv, const float *vv, int pstride, const float4 *spos,
                const float4 *svel, const int *starts, const int *counts, float *fv, int fstride, float *fs, int sstride,
-               float seed_bulk, float seed_halo, int rng, unsigned *mask, int *rank, int *count, int *img_start,
-               cudaStream_t st) {
+               float seed_bulk, float seed_halo, const float *seeds_dev, int rng, unsigned *mask, int *rank,
+               int *count, int *img_start, cudaStream_t st) {
     if (nv == 0) return CTC_OK;
     if (rng == CTC_RNG_REFERENCE) CUDA_TRY(fsi_images_launch(nv, L, pv, pstride, mask, rank, count, img_start, st));
     FsiArgs A;
@@ -221,12 +224,13 @@ int fsi_forces(int3 L, const DpdPar &P, int nv, const float *pv, const float *vv
     A.spos = spos; A.svel = svel; A.starts = starts; A.counts = counts;
     A.fv = fv; A.fstride = fstride; A.fs = fs; A.sstride = sstride;
     A.par = P;
-    A.seed_bulk = seed_bulk; A.seed_halo = seed_halo;
+    A.seed_bulk = seed_bulk; A.seed_halo = seed_halo; A.seeds_dev = seeds_dev;
     A.img_rank = rank; A.img_start = img_start;
     A.err = dev_err_ptr();
     CUDA_TRY(fsi_launch(A, rng, st));
     return CTC_OK;
 }
+}  // namespace ctc
 
 extern "C" int ctc_fsi_apply_seeded(ctc_fsi *f, const ctc_dpd_params *p, int nv, const float *pv, int ns,
                                     const float *ps, const int *starts, const int *counts, float seed_bulk,
@@ -241,7 +245,7 @@ extern "C" int ctc_fsi_apply_seeded(ctc_fsi *f, const ctc_dpd_params *p, int nv,
     DpdPar P;
     P.a = p->a; P.g = p->g; P.s = p->s; P.spow = p->spow;
     return fsi_forces(f->L, P, nv, pv, pv + 3, 6, f->spos, f->svel, starts, counts, fv, 3, fs, 3, seed_bulk, seed_halo,
-                      rng, f->mask, f->rank, f->count, f->img_start, st);
+                      nullptr, rng, f->mask, f->rank, f->count, f->img_start, st);
 }
 
 extern "C" int ctc_fsi_apply(ctc_fsi *f, const ctc_dpd_params *p, int nv, const float *pv, int ns, const float *ps,

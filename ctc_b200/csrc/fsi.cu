@@ -99,6 +99,8 @@ __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
     // the vertex cell as src/fsi/dev/map/bulk.h:13-21 (floorf, may lie outside the box)
     const int cx = lx + (int)floorf(pa.x), cy = ly + (int)floorf(pa.y), cz = lz + (int)floorf(pa.z);
     const DpdPar P = A.par;
+    const float seed_bulk = A.seeds_dev ? A.seeds_dev[0] : A.seed_bulk;
+    const float seed_halo = A.seeds_dev ? A.seeds_dev[1] : A.seed_halo;
     float fx = 0, fy = 0, fz = 0;
     for (int dz = -1; dz <= 1; dz++)
         for (int dy = -1; dy <= 1; dy++)
@@ -115,14 +117,14 @@ __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
                 bool halo = (wx | wy | wz) != 0;
                 float4 a = pa;
                 unsigned aid = (unsigned)i;
-                float seed = A.seed_bulk;
+                float seed = seed_bulk;
                 if (halo) {
                     int fid = frag_d2i(wx, wy, wz);
                     if (RNG == 0) {
                         int r = __ldg(A.img_rank + (size_t)fid * A.nv + i);
                         if (r < 0) { set_error(A.err, DEV_BAD_PARTICLE); continue; }
                         aid = (unsigned)(__ldg(A.img_start + fid) + r);
-                        seed = A.seed_halo;
+                        seed = seed_halo;
                     }
                     a.x = a.x + (float)(-wx * A.L.x);
                     a.y = a.y + (float)(-wy * A.L.y);
@@ -133,14 +135,18 @@ __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
                     float x = a.x - b.x, y = a.y - b.y, z = a.z - b.z;
                     if (dist2(x, y, z) >= 1.0f) continue;
                     float rnd = RNG == 0 ? mean0var1uu(seed, aid, (unsigned)j)
-                                         : mean0var1uu(A.seed_bulk, (unsigned)i, (unsigned)__float_as_int(b.w));
+                                         : mean0var1uu(seed_bulk, (unsigned)i, (unsigned)__float_as_int(b.w));
                     float3 f;
                     if (!dpd_force(P, a, va, b, __ldg(A.svel + j), rnd, f)) continue;
                     fx += f.x; fy += f.y; fz += f.z;
-                    float *o = A.fs + (size_t)A.sstride * j;
-                    atomicAdd(o + 0, -f.x);
-                    atomicAdd(o + 1, -f.y);
-                    atomicAdd(o + 2, -f.z);
+                    if (A.sstride == 4) {
+                        atomicAdd((float4*)A.fs + j, make_float4(-f.x, -f.y, -f.z, 0.0f));
+                    } else {
+                        float *o = A.fs + (size_t)A.sstride * j;
+                        atomicAdd(o + 0, -f.x);
+                        atomicAdd(o + 1, -f.y);
+                        atomicAdd(o + 2, -f.z);
+                    }
                 }
             }
     float *o = A.fv + (size_t)A.fstride * i;

@@ -18,6 +18,7 @@ struct FsiArgs {
     int sstride;
     DpdPar par;
     float seed_bulk, seed_halo;
+    const float *seeds_dev;        // bulk, halo seed in device memory (overrides the two above)
     const int *img_rank;           // [26 * nv]: rank in fragment fid's list or -1 (reference keys)
     const int *img_start;          // [26]: first index of fragment fid's images in the halo list
     int *err;

@@ -117,7 +117,18 @@ __global__ void k_draw_seeds(unsigned *__restrict__ state, int ntrunk, float *__
     if (k < ntrunk) seeds[k] = __fdiv_rn(__uint2float_rn(kiss_next(state + 4 * k)), 4294967296.0f);
 }
 
+// `count` successive draws from one trunk (the FSI trunk is drawn twice a step)
+__global__ void k_draw_seq(unsigned *__restrict__ state, int count, float *__restrict__ seeds) {
+    if (threadIdx.x == 0)
+        for (int k = 0; k < count; k++) seeds[k] = __fdiv_rn(__uint2float_rn(kiss_next(state)), 4294967296.0f);
+}
+
 // ---------------------------------------------------------------------------
+cudaError_t draw_seq_launch(unsigned *state, int count, float *seeds, cudaStream_t st) {
+    k_draw_seq<<<1, 32, 0, st>>>(state, count, seeds);
+    return cudaGetLastError();
+}
+
 cudaError_t integrate_launch(const int *nptr, int nmax, float4 *pos, float4 *vel, const float4 *force, float dt,
                              float mass, float3 a, cudaStream_t st) {
     if (nmax > 0) k_integrate<<<ceil_div(nmax, 256), 256, 0, st>>>(nptr, pos, vel, force, dt, mass, a);

@@ -161,6 +161,50 @@ __global__ void k_membrane(MembraneArgs A) {
     o[2] += (float)f.z;
 }
 
+// membrane migration of one periodic rank (src/distr/rbc/dev.h:1-25): a cell
+// whose bounding-box centre left the box [lo, lo + L) moves by -L*d as a whole
+__global__ void k_rbc_wrap(int nv, int3 L, float4 *__restrict__ pos) {
+    __shared__ float lo[3][AV_T / 32], hi[3][AV_T / 32];
+    __shared__ float shift[3];
+    const int c = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+    for (int v = threadIdx.x; v < nv; v += AV_T) {
+        float4 r = pos[(size_t)c * nv + v];
+        mn[0] = fminf(mn[0], r.x); mx[0] = fmaxf(mx[0], r.x);
+        mn[1] = fminf(mn[1], r.y); mx[1] = fmaxf(mx[1], r.y);
+        mn[2] = fminf(mn[2], r.z); mx[2] = fmaxf(mx[2], r.z);
+    }
+    for (int k = 0; k < 3; k++)
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[k] = fminf(mn[k], __shfl_down_sync(0xffffffffu, mn[k], o));
+            mx[k] = fmaxf(mx[k], __shfl_down_sync(0xffffffffu, mx[k], o));
+        }
+    if (lane == 0)
+        for (int k = 0; k < 3; k++) { lo[k][w] = mn[k]; hi[k][w] = mx[k]; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        int k = threadIdx.x, Lk = k == 0 ? L.x : (k == 1 ? L.y : L.z), l0 = -(Lk / 2);
+        float a = 1e30f, b = -1e30f;
+        for (int q = 0; q < AV_T / 32; q++) { a = fminf(a, lo[k][q]); b = fmaxf(b, hi[k][q]); }
+        float r = 0.5f * (a + b);
+        int d = -1 + (r >= (float)l0) + (r >= (float)(l0 + Lk));
+        shift[k] = (float)(-d * Lk);
+    }
+    __syncthreads();
+    if (shift[0] != 0.0f || shift[1] != 0.0f || shift[2] != 0.0f)
+        for (int v = threadIdx.x; v < nv; v += AV_T) {
+            float4 *r = pos + (size_t)c * nv + v;
+            float4 x = *r;
+            x.x += shift[0]; x.y += shift[1]; x.z += shift[2];
+            *r = x;
+        }
+}
+
+cudaError_t rbc_wrap_launch(int nc, int nv, int3 L, float4 *pos, cudaStream_t st) {
+    if (nc > 0) k_rbc_wrap<<<nc, AV_T, 0, st>>>(nv, L, pos);
+    return cudaGetLastError();
+}
+
 cudaError_t area_volume_launch(int nc, int nv, int nt, const int *tri, const float *pos, int stride, double *av,
                                cudaStream_t st) {
     if (nc > 0) k_area_volume<<<nc, AV_T, 0, st>>>(nv, nt, tri, pos, stride, av);

@@ -25,5 +25,6 @@ struct MembraneArgs {
 cudaError_t area_volume_launch(int nc, int nv, int nt, const int *tri, const float *pos, int stride, double *av,
                                cudaStream_t st);
 cudaError_t membrane_launch(const MembraneArgs &A, cudaStream_t st);
+cudaError_t rbc_wrap_launch(int nc, int nv, int3 L, float4 *pos, cudaStream_t st);
 
 }  // namespace ctc

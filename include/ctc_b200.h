@@ -202,6 +202,17 @@ int ctc_sim_set_solvent_dev(ctc_sim *s, int n, const float *pp, void *stream);
 int ctc_sim_step(ctc_sim *s, int nsteps, void *stream);
 /* number of solvent particles (synchronises the stream) */
 int ctc_sim_count(ctc_sim *s, int *n, void *stream);
+/* red-blood-cell membranes of the system: nc cells of one template (nv
+ * vertices, nt triangles tri[3 nt] [host]), vertices pp [host, AoS, cell c
+ * vertex v at c*nv + v], membrane parameters p, solvent-membrane pair
+ * parameters fsi, vertex mass.  Each step then adds, in the reference's order
+ * (src/sim/imp/run.h:8-68): cell migration by bounding-box centre, FSI forces
+ * (bulk + periodic images, reactions onto the solvent), the solvent update,
+ * the internal membrane forces and the membrane update. */
+int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const int *tri, const float *pp,
+                          const ctc_rbc_params *p, const ctc_dpd_params *fsi, float mass, void *stream);
+/* download the membrane vertices [host, AoS, nc * nv] */
+int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream);
 /* download the cell-sorted solvent [host, AoS, capacity maxp] */
 int ctc_sim_get_solvent(ctc_sim *s, float *pp, int *n, void *stream);
 /* total momentum (3), kinetic temperature, count -- FP64 reductions on the

@@ -324,3 +324,51 @@ def dpd_step(L, pp, dpd, seeds, mass, bodyf, dt):
     n = lib().orc_dpd_step(*L, len(pp), pp, work, Dpd(*dpd), seeds, mass,
                            None if bf is None else bf.ctypes.data, dt)
     return pp[:n]
+
+
+def _sig_late():
+    L = lib()
+    if not getattr(L, "_late_sig", False):
+        L.orc_wrap_flag.argtypes = [C.c_int] * 4 + [f32p, np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")]
+        L.orc_wrap_flag.restype = None
+        L.orc_clist_build_late.argtypes = [C.c_int] * 4 + [f32p, C.c_int,
+                                                           np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS"),
+                                                           i32p, i32p, i32p, f32p]
+        L.orc_clist_build_late.restype = C.c_int
+        L._late_sig = True
+    return L
+
+
+def distribute(L, pp):
+    """Periodic wrap + cell-list rebuild of one step (src/sim/imp/distr.h:14-55):
+    particles that re-entered follow the others inside their cell.  Returns
+    (counts, starts[ncells+1], ppout)."""
+    Lb = _sig_late()
+    pp = _pp(pp).copy()
+    moved = np.zeros(len(pp), np.uint8)
+    Lb.orc_wrap_flag(*L, len(pp), pp, moved)
+    nc = L[0] * L[1] * L[2]
+    counts = np.zeros(nc, np.int32)
+    starts = np.zeros(nc + 1, np.int32)
+    order = np.zeros(max(len(pp), 1), np.int32)
+    out = np.zeros((max(len(pp), 1), 6), np.float32)
+    nout = Lb.orc_clist_build_late(*L, len(pp), pp, 0, moved, counts, starts, order, out)
+    starts[nc] = nout
+    return counts, starts, out[:nout]
+
+
+def rbc_step(L, ps, pv, tri, nv, dpd, fsi, rbcpar, seeds27, fsi_seeds, bodyf, dt, ms, mv):
+    """One step of solvent + membranes in the reference's order
+    (src/sim/imp/run.h:8-68); returns (solvent sorted, vertices)."""
+    counts, starts, ps = distribute(L, ps)
+    pv = rbc_wrap(L, pv, nv)
+    fs = dpd_bulk(L, ps, starts, dpd, seeds27[0]) + dpd_halo(L, ps, starts, counts, dpd, seeds27[1:])
+    fv, fs2 = fsi_forces(L, pv, ps, starts, fsi, fsi_seeds[0], fsi_seeds[1])
+    fs = fs + fs2
+    a = np.asarray(bodyf if bodyf is not None else (0, 0, 0), np.float32)
+    fs = body_force(fs, ms, a)
+    fv = body_force(fv, mv, a)
+    ps = move(ps, fs, dt, ms)
+    fv = fv + rbc_forces(tri, nv, pv, rbcpar, mode=0)
+    pv = move(pv, fv, dt, mv)
+    return ps, pv

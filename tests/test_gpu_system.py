@@ -1,0 +1,44 @@
+"""The fused system step with membranes (solvent + red blood cells) against
+the oracle's composition of the reference's modules, one step at a time."""
+import numpy as np
+import pytest
+
+import oracle
+from ctc_b200 import systems
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("bodyf", [None, (0.01, 0.0, 0.0)])
+def test_rbc_system_steps_vs_oracle(bodyf):
+    import ctc_b200 as C
+    L = (16, 16, 16)
+    ps = systems.solvent(L, seed=81)
+    pv, tri, par = systems.rbc_system(L, 2, seed=82)
+    nv = len(pv) // 2
+    pv[:nv, 0] += L[0] / 2 - pv[:nv, 0].max() + 1.0        # one cell across the +x face
+    dpd = systems.dpd_params()
+    fsi = (0.0, 8.0, dpd[2], 0.25)
+    sim = C.Sim(L, len(ps), C.DpdParams(*dpd), mass=1.0, dt=systems.DT, bodyf=bodyf or (0, 0, 0))
+    sim.set_solvent(ps)
+    sim.set_membranes(pv, tri, nv, par, C.DpdParams(*fsi), mass=systems.RBC_MASS)
+    k0 = oracle.Kiss(0, 0, 0, 0)
+    kh = [oracle.Kiss.halo(f) for f in range(26)]
+    kf = oracle.Kiss(1908, 1409, 290, 12968)
+    rs, rv = ps, pv
+    for step in range(2):
+        seeds = np.array([k0.get()] + [k.get() for k in kh], np.float32)
+        assert np.array_equal(sim.next_seeds(), seeds)
+        fseeds = (kf.get(), kf.get())
+        sim.step(1)
+        rs, rv = oracle.rbc_step(L, rs, rv, tri, nv, dpd, fsi, par, seeds, fseeds, bodyf, systems.DT, 1.0,
+                                 systems.RBC_MASS)
+        gs, gv = sim.get_solvent(), sim.get_membranes()
+        assert gs.shape == rs.shape
+        assert np.abs(gs[:, :3] - rs[:, :3]).max() < 2e-6
+        assert np.abs(gs[:, 3:] - rs[:, 3:]).max() < 1e-3
+        assert np.abs(gv[:, :3] - rv[:, :3]).max() < 2e-6
+        assert np.abs(gv[:, 3:] - rv[:, 3:]).max() < 1e-3
+        rs, rv = gs, gv          # continue from the device state (chaotic divergence)
+    assert C.device_error() == 0
