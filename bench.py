@@ -43,6 +43,7 @@ CONFIGS = {
 METRIC = "particle-steps/s @1 B200 (plain DPD step)"
 PAIR_BYTES = 48          # algorithmic bytes per particle of the pair kernel: pos+vel read, force write
 PAIR_FLOP = 100 * 20.94  # ~100 flop per accepted half-pair, 20.94 half-pairs per particle at rho=10
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 148 SMs x 128 FP32 lanes x FMA x 1965 MHz
 
 
 def peaks():
@@ -51,6 +52,18 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def bulk_traffic_per_particle():
+    """DRAM bytes per particle of one k_dpd_bulk launch, from the committed ncu
+    summary (a line "traffic_bytes_per_particle: X"), or None."""
+    p = os.path.join(ROOT, "profiles", "k_dpd_bulk_p64.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("traffic_bytes_per_particle:"):
+            return float(line.split(":")[1])
+    return None
 
 
 class Clocks:
@@ -67,7 +80,7 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -230,7 +243,7 @@ def run_ours(args, cfg, world, rank, local):
         nvt = len(pv)
     sim.step(args.warmup)
     torch.cuda.synchronize()
-    _lib.check(_lib.lib().ctc_sim_profile(sim.h, 1))
+    sim.profile(True)
 
     clocks = Clocks(local)
     barrier(world)
@@ -244,10 +257,8 @@ def run_ours(args, cfg, world, rank, local):
     barrier(world)
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
-    ms4 = (C.c_double * 4)()
-    nst = C.c_int(0)
-    _lib.check(_lib.lib().ctc_sim_profile_read(sim.h, ms4, C.byref(nst)))
-    _lib.check(_lib.lib().ctc_sim_profile(sim.h, 0))
+    phases, nst = sim.profile_read()
+    sim.profile(False)
     assert ctc.device_error() == 0, "device error during the timed steps"
     ms_max = allmax(world, ms)
     total = allsum(world, (n + nvt) * args.steps)
@@ -282,14 +293,12 @@ def run_ours(args, cfg, world, rank, local):
     if rank != 0:
         return
     hbm, peak_kind = peaks()
-    pair_ms = ms4[2] / max(nst.value, 1)
-    achieved = PAIR_BYTES * n / (pair_ms * 1e-3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "dpd_tiles_traffic.json")
-    if os.path.exists(tp):
-        d = json.load(open(tp))
-        traffic = d["bytes_per_particle"] * n
-    phases = {k: v / max(nst.value, 1) for k, v in zip(("clist", "frag_starts", "pair", "update"), ms4)}
+    bulk_ms = phases["bulk"]
+    achieved = PAIR_BYTES * n / (bulk_ms * 1e-3) / 1e9
+    traffic = bulk_traffic_per_particle()
+    # seeds, 6 cell-list kernels, fragment starts, bulk, halo, update; with membranes also cell wrap,
+    # FSI seeds, 3 image-list kernels, FSI, area/volume, membrane forces, vertex update
+    launches = 11 + (9 if nvt else 0)
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -299,13 +308,18 @@ def run_ours(args, cfg, world, rank, local):
                    "box": list(L), "rho": 10,
                    "rng": "reference keys", "parallelism": "replicas" if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (state %.2f GB per buffer)" % (32e-9 * n)},
-        "gpu_launches": 10 * args.steps,   # seeds, 6 cell-list kernels, fragment starts, pair, update
+        "gpu_launches": launches * args.steps,
         "phase_ms": phases,
-        "roofline": {"bound": "hbm", "kernel": "k_dpd_tiles", "achieved": achieved, "peak": hbm,
-                     "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                     "peak_kind": peak_kind,
-                     "note": "pair kernel is FP32-issue bound: %.1f TFLOP/s of ~%d flop/particle" %
-                             (PAIR_FLOP * n / (pair_ms * 1e-3) / 1e12, PAIR_FLOP)},
+        "roofline": {"bound": "hbm", "kernel": "k_dpd_bulk", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": traffic * n if traffic else None,
+                     "peak_kind": peak_kind + " (copy bandwidth)",
+                     "algorithmic_bytes_per_particle": PAIR_BYTES,
+                     "fp32": {"achieved_tflops": PAIR_FLOP * n / (bulk_ms * 1e-3) / 1e12,
+                              "peak_tflops": FP32_NOMINAL_TFLOPS, "peak_kind": "nominal",
+                              "frac": PAIR_FLOP * n / (bulk_ms * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS,
+                              "note": "~%d flop per particle (100 per accepted half-pair, 20.94 half-pairs)"
+                                      % PAIR_FLOP}},
         "e2e": {"value": e2e_value, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": 40 + state_bytes / args.steps},

@@ -283,3 +283,16 @@ class Sim:
         s = (C.c_float * 27)()
         check(lib().ctc_sim_next_seeds(self.h, s))
         return np.array(s[:], np.float32)
+
+    def profile(self, enable=True):
+        """Record per-phase CUDA events on every following step."""
+        check(lib().ctc_sim_profile(self.h, int(bool(enable))))
+
+    def profile_read(self):
+        """Mean device milliseconds per step of each phase since profile(),
+        as {phase name: ms}, and the number of steps; restarts the count."""
+        ms = (C.c_double * _lib.CTC_SIM_PHASES)()
+        n = C.c_int(0)
+        check(lib().ctc_sim_profile_read(self.h, ms, C.byref(n)))
+        k = max(n.value, 1)
+        return {nm: ms[i] / k for i, nm in enumerate(_lib.SIM_PHASE_NAMES)}, n.value

@@ -11,6 +11,8 @@ LIB_PATH = os.path.join(HERE, "libctc_b200.so")
 
 CTC_OK, CTC_ERR_ARG, CTC_ERR_CUDA, CTC_ERR_CAPACITY, CTC_ERR_DEVICE = 0, 1, 2, 3, 4
 CTC_RNG_REFERENCE, CTC_RNG_STABLE = 0, 1
+CTC_SIM_PHASES = 7
+SIM_PHASE_NAMES = ("clist", "frag_starts", "bulk", "halo", "fsi", "update", "membrane")
 
 vp = C.c_void_p
 ip = C.POINTER(C.c_int)

@@ -306,7 +306,7 @@ struct ctc_sim {
     bool built;                            // starts/counts describe pos[cur]
     Kiss trunk_host[27];                   // host mirror, for ctc_sim_next_seeds
     int prof;                              // record per-phase events each step
-    std::vector<cudaEvent_t> ev;           // 5 events per profiled step
+    std::vector<cudaEvent_t> ev;           // CTC_SIM_PHASES + 1 events per profiled step
     int prof_steps;
     // membranes (optional): nc cells of nv vertices, unsorted float4 SoA
     int mnc, mnv;
@@ -323,7 +323,7 @@ struct ctc_sim {
 
 static void sim_mark(ctc_sim *s, int k, cudaStream_t st) {
     if (!s->prof) return;
-    size_t idx = 5 * (size_t)s->prof_steps + k;
+    size_t idx = (CTC_SIM_PHASES + 1) * (size_t)s->prof_steps + k;
     while (s->ev.size() <= idx) {
         cudaEvent_t e;
         cudaEventCreate(&e);
@@ -500,7 +500,12 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
     if (s->cfg.rng == CTC_RNG_REFERENCE) CUDA_TRY(frag_starts_launch(s->L, s->counts, s->fss, s->off, st));
     CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n_host, st));
     sim_mark(s, 2, st);
+    A.which = 1;
     CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st));
+    sim_mark(s, 3, st);
+    A.which = 2;
+    CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st));
+    sim_mark(s, 4, st);
     const float3 bf = make_float3(s->cfg.bodyf[0], s->cfg.bodyf[1], s->cfg.bodyf[2]);
     if (nvt > 0) {
         // solvent-membrane forces into the vertex forces and, as reactions, the solvent ones
@@ -512,9 +517,10 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
                             s->seeds_dev + 27, s->cfg.rng, s->fmask, s->frank, s->fcount, s->fimg_start, st);
         if (rc) return rc;
     }
-    sim_mark(s, 3, st);
+    sim_mark(s, 5, st);
     CUDA_TRY(integrate_launch(s->starts + s->nc, s->n_host, s->pos[dst], s->vel[dst], s->force, s->cfg.dt,
                               s->cfg.mass, bf, st));
+    sim_mark(s, 6, st);
     if (nvt > 0) {
         // objects_advance: internal forces on top of the FSI ones, then the update
         int rc = membrane_forces(s->rbc, &s->mpar, s->mnc, (const float*)s->mpos, (const float*)s->mvel, 4,
@@ -522,7 +528,7 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
         if (rc) return rc;
         CUDA_TRY(integrate_launch(s->mcount, nvt, s->mpos, s->mvel, s->mforce, s->cfg.dt, s->mmass, bf, st));
     }
-    sim_mark(s, 4, st);
+    sim_mark(s, 7, st);
     if (s->prof) s->prof_steps++;
     s->cur = dst;
     s->built = true;
@@ -600,15 +606,16 @@ extern "C" int ctc_sim_profile(ctc_sim *s, int enable) {
     return CTC_OK;
 }
 
-extern "C" int ctc_sim_profile_read(ctc_sim *s, double *ms4, int *steps) {
-    if (!s || !ms4) return fail(CTC_ERR_ARG, "ctc_sim_profile_read: bad arguments");
-    for (int k = 0; k < 4; k++) ms4[k] = 0;
+extern "C" int ctc_sim_profile_read(ctc_sim *s, double *out, int *steps) {
+    if (!s || !out) return fail(CTC_ERR_ARG, "ctc_sim_profile_read: bad arguments");
+    const int E = CTC_SIM_PHASES + 1;
+    for (int k = 0; k < CTC_SIM_PHASES; k++) out[k] = 0;
     for (int i = 0; i < s->prof_steps; i++)
-        for (int k = 0; k < 4; k++) {
+        for (int k = 0; k < CTC_SIM_PHASES; k++) {
             float ms = 0;
-            CUDA_TRY(cudaEventSynchronize(s->ev[5 * i + k + 1]));
-            CUDA_TRY(cudaEventElapsedTime(&ms, s->ev[5 * i + k], s->ev[5 * i + k + 1]));
-            ms4[k] += ms;
+            CUDA_TRY(cudaEventSynchronize(s->ev[E * i + k + 1]));
+            CUDA_TRY(cudaEventElapsedTime(&ms, s->ev[E * i + k], s->ev[E * i + k + 1]));
+            out[k] += ms;
         }
     if (steps) *steps = s->prof_steps;
     s->prof_steps = 0;

@@ -223,11 +223,14 @@ int ctc_sim_state(ctc_sim *s, float **pos, float **vel, float **force, const int
 /* current bulk seed and 26 halo seeds of the next step [host, 27 floats] */
 int ctc_sim_next_seeds(const ctc_sim *s, float *seeds27);
 /* per-phase device timing: when enabled every step records CUDA events on
- * its stream; profile_read returns the summed milliseconds of [0] seeds +
- * cell lists, [1] fragment starts, [2] pair forces, [3] update, and the
+ * its stream; profile_read returns the summed milliseconds of the
+ * CTC_SIM_PHASES phases [0] seeds + wrap + cell lists, [1] fragment starts +
+ * force clear, [2] bulk pair forces, [3] halo pair forces, [4] solvent-
+ * membrane forces, [5] solvent update, [6] membrane forces + update, and the
  * number of steps, then restarts the count */
+#define CTC_SIM_PHASES 7
 int ctc_sim_profile(ctc_sim *s, int enable);
-int ctc_sim_profile_read(ctc_sim *s, double *ms4, int *steps);
+int ctc_sim_profile_read(ctc_sim *s, double *ms, int *steps);
 
 #ifdef __cplusplus
 }
