@@ -15,7 +15,7 @@ import numpy as np
 from . import _lib
 from ._lib import CTC_RNG_REFERENCE, CTC_RNG_STABLE, CtcError, check, device_error, lib
 
-__all__ = ["Clist", "FluForces", "Sim", "DpdParams", "RbcParams", "RbcForce", "Fsi", "dpd_sigma", "scheme_move_apply",
+__all__ = ["Clist", "FluForces", "Sim", "Batch", "DpdParams", "RbcParams", "RbcForce", "Fsi", "dpd_sigma", "scheme_move_apply",
            "scheme_move_clear_vel", "bforce_apply_cste", "rnd_mean0var1", "CTC_RNG_REFERENCE",
            "CTC_RNG_STABLE", "CtcError", "device_error"]
 
@@ -296,3 +296,81 @@ class Sim:
         check(lib().ctc_sim_profile_read(self.h, ms, C.byref(n)))
         k = max(n.value, 1)
         return {nm: ms[i] / k for i, nm in enumerate(_lib.SIM_PHASE_NAMES)}, n.value
+
+
+class Batch:
+    """Many independent periodic boxes advanced together: every kernel stage
+    of a step is one launch over all boxes; each box is the system a Sim of
+    its size would be (its own trunks, box-local RNG keys).  L is a list of
+    box sizes, n the solvent particles per box."""
+
+    def __init__(self, L, n, dpd, mass=1.0, dt=5e-4, bodyf=(0.0, 0.0, 0.0), rng=CTC_RNG_REFERENCE):
+        self.L = np.ascontiguousarray(np.asarray(L, np.int32).reshape(-1, 3))
+        self.n = np.ascontiguousarray(np.asarray(n, np.int32).reshape(-1))
+        if len(self.L) != len(self.n):
+            raise CtcError("one particle count per box")
+        cfg = _lib.BatchConfig()
+        cfg.nbox = len(self.n)
+        cfg.L = self.L.ctypes.data_as(C.POINTER(C.c_int))
+        cfg.n = self.n.ctypes.data_as(C.POINTER(C.c_int))
+        cfg.dpd = dpd
+        cfg.mass = mass
+        cfg.dt = dt
+        cfg.bodyf = (C.c_float * 3)(*bodyf)
+        cfg.rng = rng
+        self.h = C.c_void_p()
+        self.mnv, self.nvt = 0, 0
+        check(lib().ctc_batch_create(C.byref(cfg), C.byref(self.h)))
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
+            lib().ctc_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_solvent(self, pp, stream=None):
+        """pp (sum n, 6) float32 AoS, box after box."""
+        pp = np.ascontiguousarray(pp, np.float32).reshape(-1, 6)
+        if len(pp) != int(self.n.sum()):
+            raise CtcError("expected %d particles" % int(self.n.sum()))
+        check(lib().ctc_batch_set_solvent(self.h, pp.ctypes.data_as(C.c_void_p), _stream(stream)))
+
+    def set_membranes(self, cells, pv, tri, nv, params, fsi, mass=0.5, stream=None):
+        """cells[k] membranes in box k; pv (sum cells * nv, 6) AoS box after box."""
+        cells = np.ascontiguousarray(np.asarray(cells, np.int32).reshape(-1))
+        pv = np.ascontiguousarray(pv, np.float32).reshape(-1, 6)
+        tri = np.ascontiguousarray(tri, np.int32).reshape(-1, 3)
+        check(lib().ctc_batch_set_membranes(self.h, cells.ctypes.data_as(C.c_void_p), int(nv), len(tri),
+                                            tri.ctypes.data_as(C.c_void_p), pv.ctypes.data_as(C.c_void_p),
+                                            C.byref(_lib.RbcParams(**params)), C.byref(fsi), float(mass),
+                                            _stream(stream)))
+        self.mnv, self.nvt = int(nv), len(pv)
+
+    def step(self, n=1, stream=None):
+        check(lib().ctc_batch_step(self.h, int(n), _stream(stream)))
+
+    def set_graph(self, enable=True):
+        check(lib().ctc_batch_set_graph(self.h, int(bool(enable))))
+
+    def tune(self, reps=3, stream=None):
+        """Autotune the pair kernels' launch shapes on the current state;
+        returns (bulk threads, bulk unroll, halo threads)."""
+        ch = (C.c_int * 3)()
+        check(lib().ctc_batch_tune(self.h, int(reps), ch, _stream(stream)))
+        return tuple(ch)
+
+    def set_tune(self, choice):
+        ch = (C.c_int * 3)(*choice)
+        check(lib().ctc_batch_set_tune(self.h, ch))
+
+    def get_solvent(self, stream=None):
+        out = np.zeros((int(self.n.sum()), 6), np.float32)
+        check(lib().ctc_batch_get_solvent(self.h, out.ctypes.data_as(C.c_void_p), _stream(stream)))
+        return out
+
+    def get_membranes(self, stream=None):
+        out = np.zeros((self.nvt, 6), np.float32)
+        if self.nvt:
+            check(lib().ctc_batch_get_membranes(self.h, out.ctypes.data_as(C.c_void_p), _stream(stream)))
+        return out

@@ -35,6 +35,11 @@ class SimConfig(C.Structure):
                 ("bodyf", C.c_float * 3), ("rng", C.c_int)]
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [("nbox", C.c_int), ("L", C.POINTER(C.c_int)), ("n", C.POINTER(C.c_int)), ("dpd", DpdParams),
+                ("mass", C.c_float), ("dt", C.c_float), ("bodyf", C.c_float * 3), ("rng", C.c_int)]
+
+
 # name -> (restype, argtypes); every symbol include/ctc_b200.h declares
 SIGNATURES = {
     "ctc_status_string": (C.c_char_p, [C.c_int]),
@@ -84,6 +89,18 @@ SIGNATURES = {
     "ctc_sim_next_seeds": (C.c_int, [vp, fp]),
     "ctc_sim_profile": (C.c_int, [vp, C.c_int]),
     "ctc_sim_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), ip]),
+    "ctc_batch_create": (C.c_int, [C.POINTER(BatchConfig), C.POINTER(vp)]),
+    "ctc_batch_destroy": (C.c_int, [vp]),
+    "ctc_batch_set_solvent": (C.c_int, [vp, vp, vp]),
+    "ctc_batch_set_membranes": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp, C.POINTER(RbcParams),
+                                          C.POINTER(DpdParams), C.c_float, vp]),
+    "ctc_batch_step": (C.c_int, [vp, C.c_int, vp]),
+    "ctc_batch_set_graph": (C.c_int, [vp, C.c_int]),
+    "ctc_batch_tune": (C.c_int, [vp, C.c_int, ip, vp]),
+    "ctc_batch_set_tune": (C.c_int, [vp, ip]),
+    "ctc_batch_get_solvent": (C.c_int, [vp, vp, vp]),
+    "ctc_batch_get_membranes": (C.c_int, [vp, vp, vp]),
+    "ctc_batch_count": (C.c_int, [vp, ip, ip]),
 }
 
 _lib = None

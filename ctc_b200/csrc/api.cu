@@ -67,49 +67,6 @@ extern "C" float ctc_dpd_sigma(float kBT, float g, float dt) {
     return (float)std::sqrt(2 * (double)kBT * (double)g / (double)dt);   // src/pair/imp/main.h:54-62
 }
 
-// ---------------------------------------------------------------------------
-// host KISS trunks (src/math/rnd/imp.cpp:12-34)
-// ---------------------------------------------------------------------------
-struct Kiss {
-    unsigned s[4];
-};
-static void kiss_ini(Kiss *k, int x, int y, int z, int c) {
-    k->s[0] = (unsigned)x; k->s[1] = (unsigned)y; k->s[2] = (unsigned)z; k->s[3] = (unsigned)c;
-}
-static float kiss_get(Kiss *k) {
-    unsigned long long t, a = 698769069ULL;
-    unsigned *s = k->s;
-    s[0] = 69069u * s[0] + 12345u;
-    s[1] ^= (s[1] << 13);
-    s[1] ^= (s[1] >> 17);
-    s[1] ^= (s[1] << 5);
-    t = a * s[2] + s[3];
-    s[3] = (unsigned)(t >> 32);
-    s[2] = (unsigned)t;
-    return (float)(s[0] + s[1] + s[2]) / (float)4294967295u;
-}
-// fragment trunks of a 1-rank periodic cart: src/fluforces/imp/ini.h:11-59
-static void halo_trunk_ini(int fid, Kiss *k) {
-    int d[3] = {frag_i2dx(fid), frag_i2dy(fid), frag_i2dz(fid)};
-    int plus = (d[0] + d[1] + d[2] > 0) || ((d[0] + d[1] + d[2] == 0) && (d[0] > 0)) ||
-               ((d[0] == 0) && (d[1] > 0)) || (d[1] == 0 && d[2] > 0);
-    int sg = 2 * plus - 1;
-    int seed = (1 + sg * d[0]) + 3 * ((1 + sg * d[1]) + 3 * (1 + sg * d[2]));
-    kiss_ini(k, 390 + seed, seed + 615, 12309, 23094);
-}
-
-static bool box_ok(int LX, int LY, int LZ) { return LX >= 3 && LY >= 3 && LZ >= 3; }
-
-static void dpd_args_common(DpdArgs *A, int3 L, const ctc_dpd_params *p) {
-    memset(A, 0, sizeof(*A));
-    A->L = L;
-    A->par.a = p->a; A->par.g = p->g; A->par.s = p->s; A->par.spow = p->spow;
-    A->masks = halo_masks();
-    Off27 off;
-    frag_offsets(L, &off);
-    memcpy(A->fss_off, off.d, sizeof(off.d));
-}
-
 extern "C" int ctc_rnd_mean0var1(int n, float seed, const int *u, const int *v, int uu, float *out, void *stream) {
     if (n < 0 || (n > 0 && (!u || !v || !out))) return fail(CTC_ERR_ARG, "ctc_rnd_mean0var1: bad arguments");
     CUDA_TRY(rnd_launch(n, seed, u, v, uu, out, (cudaStream_t)stream));

@@ -215,9 +215,10 @@ namespace ctc {
 int fsi_forces(int3 L, const DpdPar &P, int nv, const float *pv, const float *vv, int pstride, const float4 *spos,
                const float4 *svel, const int *starts, const int *counts, float *fv, int fstride, float *fs, int sstride,
                float seed_bulk, float seed_halo, const float *seeds_dev, int rng, unsigned *mask, int *rank,
-               int *count, int *img_start, cudaStream_t st) {
+               int *count, int *img_start, cudaStream_t st, const Boxes &B) {
     if (nv == 0) return CTC_OK;
-    if (rng == CTC_RNG_REFERENCE) CUDA_TRY(fsi_images_launch(nv, L, pv, pstride, mask, rank, count, img_start, st));
+    if (rng == CTC_RNG_REFERENCE)
+        CUDA_TRY(fsi_images_launch(nv, L, pv, pstride, mask, rank, count, img_start, st, B));
     FsiArgs A;
     memset(&A, 0, sizeof(A));
     A.L = L; A.nv = nv; A.pv = pv; A.vv = vv; A.pstride = pstride;
@@ -227,6 +228,7 @@ int fsi_forces(int3 L, const DpdPar &P, int nv, const float *pv, const float *vv
     A.seed_bulk = seed_bulk; A.seed_halo = seed_halo; A.seeds_dev = seeds_dev;
     A.img_rank = rank; A.img_start = img_start;
     A.err = dev_err_ptr();
+    A.B = B;
     CUDA_TRY(fsi_launch(A, rng, st));
     return CTC_OK;
 }

@@ -42,17 +42,26 @@ __device__ __forceinline__ int cell_of(float4 p, int3 L) {
 }
 
 // pass 1: cell + slot by warp-aggregated atomics
+// (with many boxes, B.nbox > 0: the particle's box gives L and the offset of
+// its cells in the concatenated cell arrays)
 __global__ void k_clist_count(int n, const int *__restrict__ nptr, const float4 *__restrict__ pos, int3 L,
-                              int wrap, int2 *__restrict__ cidslot, int *__restrict__ counts, int *err) {
+                              int wrap, int2 *__restrict__ cidslot, int *__restrict__ counts, int *err, Boxes B) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (nptr) n = min(n, *nptr);
     int cid = -1;
     bool wrapped = false;
     if (i < n) {
+        int c0 = 0;
+        if (B.nbox > 0) {
+            const int box = box_find(B.p0, B.nbox, i);
+            L = box_L(B, box);
+            c0 = __ldg(B.c0 + box);
+        }
         float4 p = __ldg(pos + i);
         if (wrap) wrap_pos(p, L, wrapped);
         cid = cell_of(p, L);
         if (cid < 0 && wrap) set_error(err, DEV_BAD_PARTICLE);
+        if (cid >= 0) cid += c0;
     }
     unsigned valid = __ballot_sync(0xffffffffu, cid >= 0);
     if (cid >= 0) {
@@ -152,10 +161,12 @@ __global__ void k_clist_place(int n, const int *__restrict__ nptr, const int2 *_
 __global__ void k_clist_gather(int nc, const unsigned *__restrict__ keys, const int2 *__restrict__ cidslot,
                                const int *__restrict__ starts, const float4 *__restrict__ pos_in,
                                const float4 *__restrict__ vel_in, int3 L, int wrap, float4 *__restrict__ pos_out,
-                               float4 *__restrict__ vel_out, int *__restrict__ order) {
+                               float4 *__restrict__ vel_out, int *__restrict__ order, Boxes B) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     int total = __ldg(starts + nc);
     if (k >= total) return;
+    // a box keeps its particle range: the input index's box is the output's
+    if (B.nbox > 0) L = box_L(B, box_find(B.p0, B.nbox, k));
     unsigned key = keys[k];
     int i = (int)(key & 0x7fffffffu);
     int cid = __ldg(&cidslot[i].x);
@@ -215,18 +226,18 @@ void clist_carve(ClistScratch *w, void *base, int ncells, int maxp) {
 
 cudaError_t clist_launch(int3 L, int n, const int *nptr, const float4 *pos_in, const float4 *vel_in, int wrap,
                          int *counts, int *starts, float4 *pos_out, float4 *vel_out, int *order,
-                         const ClistScratch &w, int *err, cudaStream_t st) {
-    int nc = L.x * L.y * L.z;
+                         const ClistScratch &w, int *err, cudaStream_t st, const Boxes &B, int nc_boxes) {
+    int nc = B.nbox > 0 ? nc_boxes : L.x * L.y * L.z;
     cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nc, st);
     const int T = 256;
-    if (n > 0) k_clist_count<<<ceil_div(n, T), T, 0, st>>>(n, nptr, pos_in, L, wrap, w.cidslot, counts, err);
+    if (n > 0) k_clist_count<<<ceil_div(n, T), T, 0, st>>>(n, nptr, pos_in, L, wrap, w.cidslot, counts, err, B);
     k_scan_tiles<<<w.nsums, SCAN_T, 0, st>>>(nc, counts, starts, w.sums);
     k_scan_sums<<<1, SCAN_T, 0, st>>>(w.nsums, w.sums, starts + nc);
     k_scan_add<<<ceil_div(nc, T), T, 0, st>>>(nc, starts, w.sums);
     if (n > 0) {
         k_clist_place<<<ceil_div(n, T), T, 0, st>>>(n, nptr, w.cidslot, starts, w.keys);
         k_clist_gather<<<ceil_div(n, T), T, 0, st>>>(nc, w.keys, w.cidslot, starts, pos_in, vel_in, L, wrap,
-                                                     pos_out, vel_out, order);
+                                                     pos_out, vel_out, order, B);
     }
     return cudaGetLastError();
 }

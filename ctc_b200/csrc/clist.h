@@ -1,6 +1,7 @@
 // Host-side declarations of the cell-list kernels.
 #pragma once
 #include <cuda_runtime.h>
+#include "common.cuh"
 
 namespace ctc {
 
@@ -16,9 +17,12 @@ void clist_carve(ClistScratch *w, void *base, int ncells, int maxp);
 
 // counts[ncells], starts[ncells + 1] (starts[ncells] = particles kept).
 // n bounds the grid; nptr (device, may be null) holds the actual count.
+// With B.nbox > 0 the particles and cells of all boxes are concatenated
+// (nc_boxes cells in all) and L is ignored.
 cudaError_t clist_launch(int3 L, int n, const int *nptr, const float4 *pos_in, const float4 *vel_in, int wrap,
                          int *counts, int *starts, float4 *pos_out, float4 *vel_out, int *order,
-                         const ClistScratch &w, int *err, cudaStream_t st);
+                         const ClistScratch &w, int *err, cudaStream_t st, const Boxes &B = Boxes(),
+                         int nc_boxes = 0);
 
 cudaError_t aos_to_soa(int n, const float *pp, float4 *pos, float4 *vel, cudaStream_t st);
 cudaError_t soa_to_aos(const int *nptr, int nmax, const float4 *pos, const float4 *vel, float *pp,

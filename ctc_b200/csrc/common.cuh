@@ -119,4 +119,35 @@ __host__ __device__ __forceinline__ int frag_anti(int i) {
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
 
+// ---------------------------------------------------------------------------
+// many independent periodic boxes in one launch.  Box b owns the sorted
+// particles [p0[b], p0[b+1]), the cells [c0[b], c0[b+1]) of the concatenated
+// cell lists, the fragment-cell starts fss_tab[27 b + fid], the membrane
+// vertices [v0[b], v0[b+1]) and the seeds seeds[27 b ..] (+ FSI seeds at
+// fsi_seeds[2 b ..]).  Every box is the same system a single-box run of its
+// size would be: RNG keys use box-local indices.  nbox = 0: one box.
+// ---------------------------------------------------------------------------
+struct Boxes {
+    int nbox;
+    const int *p0, *c0, *v0;    // nbox + 1 offsets each
+    const int4 *L;              // box sizes in cells (w unused)
+    const int *fss_tab;         // 27 per box: fragment-cell start offsets
+};
+
+// largest b with off[b] <= i (off ascending, off[0] = 0)
+__device__ __forceinline__ int box_find(const int *off, int nbox, int i) {
+    int lo = 0, hi = nbox - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(off + mid) <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int3 box_L(const Boxes &B, int b) {
+    const int4 l = __ldg(B.L + b);
+    return make_int3(l.x, l.y, l.z);
+}
+
 }  // namespace ctc

@@ -58,15 +58,20 @@ __device__ __forceinline__ int block_exscan256(int v, int *sh, int &total) {
 }
 
 // index of a particle inside fragment fid's packed list (src/exch/flu/dev/map.h:1-21,
-// src/exch/flu/dev/pack.h:2-40): fragment-cell start + offset inside the cell
-__device__ __forceinline__ int frag_index(const DpdArgs &A, int fid, int gcell, int off) {
-    int gx = gcell % A.L.x, gy = (gcell / A.L.x) % A.L.y, gz = gcell / (A.L.x * A.L.y);
+// src/exch/flu/dev/pack.h:2-40): fragment-cell start + offset inside the cell;
+// fss_fid = the box's fragment-cell starts of fragment fid
+__device__ __forceinline__ int frag_index(int3 L, const int *fss_fid, int fid, int gcell, int off) {
+    int gx = gcell % L.x, gy = (gcell / L.x) % L.y, gz = gcell / (L.x * L.y);
     int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
-    int ox = dx == 1 ? A.L.x - 1 : 0, oy = dy == 1 ? A.L.y - 1 : 0, oz = dz == 1 ? A.L.z - 1 : 0;
-    int ex = dx == 0 ? A.L.x : 1, ey = dy == 0 ? A.L.y : 1;
+    int ox = dx == 1 ? L.x - 1 : 0, oy = dy == 1 ? L.y - 1 : 0, oz = dz == 1 ? L.z - 1 : 0;
+    int ex = dx == 0 ? L.x : 1, ey = dy == 0 ? L.y : 1;
     int hci = (gx - ox) + ex * ((gy - oy) + ey * (gz - oz));
-    return __ldg(A.fss + A.fss_off[fid] + hci) + off;
+    return __ldg(fss_fid + hci) + off;
 }
+
+// queue records: (ia, ib), and the box in batched launches
+template <bool BATCH> struct BulkRec { uint2 v; };
+template <> struct BulkRec<true> { uint4 v; };
 
 // ---------------------------------------------------------------------------
 // bulk pairs: the reference's traversal (one target particle per thread, the
@@ -75,8 +80,6 @@ __device__ __forceinline__ int frag_index(const DpdArgs &A, int fid, int gcell, 
 // with all 32 lanes busy, and the forces accumulated with fire-and-forget
 // global reductions (+f on ia, -f on ib).
 // ---------------------------------------------------------------------------
-constexpr int BULK_T = 256, BULK_W = BULK_T / 32;
-
 __device__ __forceinline__ void red_force(float *out, int stride, int i, float s, float3 f) {
     if (stride == 4) {   // one 16-byte vector reduction (sm_90+) instead of three scalar ones
         atomicAdd((float4*)out + i, make_float4(s * f.x, s * f.y, s * f.z, 0.0f));
@@ -88,16 +91,30 @@ __device__ __forceinline__ void red_force(float *out, int stride, int i, float s
     atomicAdd(o + 2, s * f.z);
 }
 
-template <int RNG>
-__global__ void __launch_bounds__(BULK_T) k_dpd_bulk(const __grid_constant__ DpdArgs A) {
-    __shared__ uint2 queue[BULK_W][QCAP];
+// T threads per block, UNROLL candidate loads in flight per lane
+template <int RNG, bool BATCH, int T, int UNROLL>
+__global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs A) {
+    constexpr int W = T / 32;
+    __shared__ BulkRec<BATCH> queue[W][QCAP];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int n = __ldg(A.starts + A.L.x * A.L.y * A.L.z);
-    const int ia = blockIdx.x * BULK_T + threadIdx.x;
+    const int ia = blockIdx.x * T + threadIdx.x;
+    int3 L = A.L;
+    const int *starts = A.starts;
+    int n, box = 0;
+    if (BATCH) {
+        n = __ldg(A.B.p0 + A.B.nbox);
+        if (ia < n) {
+            box = box_find(A.B.p0, A.B.nbox, ia);
+            L = box_L(A.B, box);
+            starts = A.starts + __ldg(A.B.c0 + box);
+        }
+    } else {
+        n = __ldg(A.starts + L.x * L.y * L.z);
+    }
     const bool act = ia < n;
     const float *seeds = A.seeds_dev ? A.seeds_dev : A.seeds;
     const DpdPar P = A.par;
-    uint2 *q = queue[warp];
+    BulkRec<BATCH> *q = queue[warp];
     int qn = 0;
 
     float4 pa = make_float4(0, 0, 0, 0);
@@ -105,23 +122,29 @@ __global__ void __launch_bounds__(BULK_T) k_dpd_bulk(const __grid_constant__ Dpd
     if (act) {
         pa = __ldg(A.pos + ia);
         // get_cid (src/fluforces/bulk/dev/main.h:11-17): float, truncated
-        cx = (int)(pa.x + (float)(A.L.x / 2));
-        cy = (int)(pa.y + (float)(A.L.y / 2));
-        cz = (int)(pa.z + (float)(A.L.z / 2));
+        cx = (int)(pa.x + (float)(L.x / 2));
+        cy = (int)(pa.y + (float)(L.y / 2));
+        cz = (int)(pa.z + (float)(L.z / 2));
     }
 
     auto process = [&](int m) {
         if (lane < m) {
-            uint2 rec = q[lane];
-            int i = (int)rec.x, j = (int)rec.y;
+            const BulkRec<BATCH> rec = q[lane];
+            const int i = (int)rec.v.x, j = (int)rec.v.y;
             float4 p1 = __ldg(A.pos + i), p2 = __ldg(A.pos + j);
             float4 v1 = __ldg(A.vel + i), v2 = __ldg(A.vel + j);
+            float seed = seeds[0];
+            int k0 = 0;                                   // key offset: box-local sorted indices
+            if constexpr (BATCH) {
+                seed = seeds[27 * rec.v.z];
+                k0 = __ldg(A.B.p0 + rec.v.z);
+            }
             float rnd;
             if (RNG == 1) {
                 unsigned g1 = (unsigned)__float_as_int(p1.w), g2 = (unsigned)__float_as_int(p2.w);
-                rnd = mean0var1uu(seeds[0], max(g1, g2), min(g1, g2));
+                rnd = mean0var1uu(seed, max(g1, g2), min(g1, g2));
             } else {
-                rnd = mean0var1ii(seeds[0], i, j);      // i > j: the reference's (ia, ib)
+                rnd = mean0var1ii(seed, i - k0, j - k0);  // i > j: the reference's (ia, ib)
             }
             float3 f;
             if (dpd_force(P, p1, v1, p2, v2, rnd, f)) {
@@ -134,7 +157,11 @@ __global__ void __launch_bounds__(BULK_T) k_dpd_bulk(const __grid_constant__ Dpd
 
     auto push = [&](bool ok, int cand) {
         const unsigned bal = __ballot_sync(0xffffffffu, ok);
-        if (ok) q[qn + __popc(bal & ((1u << lane) - 1u))] = make_uint2((unsigned)ia, (unsigned)cand);
+        if (ok) {
+            BulkRec<BATCH> &e = q[qn + __popc(bal & ((1u << lane) - 1u))];
+            if constexpr (BATCH) e.v = make_uint4((unsigned)ia, (unsigned)cand, (unsigned)box, 0u);
+            else e.v = make_uint2((unsigned)ia, (unsigned)cand);
+        }
         qn += __popc(bal);
         __syncwarp();
         if (qn >= 32) {
@@ -148,7 +175,6 @@ __global__ void __launch_bounds__(BULK_T) k_dpd_bulk(const __grid_constant__ Dpd
     // rows (dz, dy) of src/fluforces/bulk/dev/main.h:88-92; dx runs -1..1, and
     // -1..0 for the own row.  Every round a lane tests the next UNROLL
     // candidates of its row at once (independent loads in flight).
-    constexpr int UNROLL = 4;
     int r = 0, ib = 0, be = 0;
     for (;;) {
         if (act) {
@@ -156,12 +182,12 @@ __global__ void __launch_bounds__(BULK_T) k_dpd_bulk(const __grid_constant__ Dpd
                 const int dz = r < 3 ? -1 : 0, dy = r < 3 ? r - 1 : (r == 3 ? -1 : 0);
                 r++;
                 const int bz = cz + dz, by = cy + dy;
-                if (bz < 0 || bz >= A.L.z || by < 0 || by >= A.L.y) continue;
+                if (bz < 0 || bz >= L.z || by < 0 || by >= L.y) continue;
                 const int enddx = (dz == 0 && dy == 0) ? 0 : 1;
-                const int sx = max(0, cx - 1), ex = 1 + min(A.L.x - 1, cx + enddx);
-                const int cid0 = A.L.x * (by + A.L.y * bz);
-                ib = __ldg(A.starts + cid0 + sx);
-                be = min(__ldg(A.starts + cid0 + ex), ia);   // ib < ia
+                const int sx = max(0, cx - 1), ex = 1 + min(L.x - 1, cx + enddx);
+                const int cid0 = L.x * (by + L.y * bz);
+                ib = __ldg(starts + cid0 + sx);
+                be = min(__ldg(starts + cid0 + ex), ia);   // ib < ia
             }
         }
         const bool have = act && ib < be;
@@ -190,21 +216,34 @@ __global__ void __launch_bounds__(BULK_T) k_dpd_bulk(const __grid_constant__ Dpd
 // mask ? bid : aid) with fragment-local indices; only the local particle
 // takes the force.
 // ---------------------------------------------------------------------------
-constexpr int HALO_T = 128, HALO_W = HALO_T / 32;
-
 __device__ __forceinline__ void r2size_dev(float r, int nc, int S, int &l, int &s) {
     int i = (int)(r + (float)(S / 2));
     l = max(0, i - 1);
     s = min(nc, i + 2) - l;
 }
 
-template <int RNG>
-__global__ void __launch_bounds__(HALO_T) k_dpd_halo(const __grid_constant__ DpdArgs A) {
-    __shared__ uint4 queue[HALO_W][QCAP];
+template <int RNG, bool BATCH, int T>
+__global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs A) {
+    __shared__ uint4 queue[T / 32][QCAP];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int3 L = A.L;
-    const int n = __ldg(A.starts + L.x * L.y * L.z);
-    const int ia = blockIdx.x * HALO_T + threadIdx.x;
+    const int ia = blockIdx.x * T + threadIdx.x;
+    int3 L = A.L;
+    const int *starts = A.starts, *counts = A.counts;
+    const int *fss_off = A.fss_off;                 // fragment-cell start offsets of the box
+    int n;
+    if (BATCH) {
+        n = __ldg(A.B.p0 + A.B.nbox);
+        if (ia < n) {
+            const int box = box_find(A.B.p0, A.B.nbox, ia);
+            L = box_L(A.B, box);
+            const int c0 = __ldg(A.B.c0 + box);
+            starts += c0;
+            counts += c0;
+            fss_off = A.B.fss_tab + 27 * box;
+        }
+    } else {
+        n = __ldg(A.starts + L.x * L.y * L.z);
+    }
     const float *seeds = A.seeds_dev ? A.seeds_dev : A.seeds;
     const DpdPar P = A.par;
     uint4 *q = queue[warp];
@@ -239,17 +278,25 @@ __global__ void __launch_bounds__(HALO_T) k_dpd_halo(const __grid_constant__ Dpd
             const int i = (int)(rec.x & 0x7ffffffu), fid = (int)(rec.x >> 27), j = (int)rec.y;
             float4 p1 = __ldg(A.pos + i);
             const float4 p2 = __ldg(A.pos + j);
+            // the record may come from another lane, whose box may differ
+            int3 Li = L;
+            const float *sb = seeds;
+            if (BATCH) {
+                const int b = box_find(A.B.p0, A.B.nbox, i);
+                Li = box_L(A.B, b);
+                sb += 27 * b;
+            }
             // the local particle moves into the frame of the image (halo/dev/main.h:43-45)
-            p1.x -= (float)(frag_i2dx(fid) * L.x);
-            p1.y -= (float)(frag_i2dy(fid) * L.y);
-            p1.z -= (float)(frag_i2dz(fid) * L.z);
+            p1.x -= (float)(frag_i2dx(fid) * Li.x);
+            p1.y -= (float)(frag_i2dy(fid) * Li.y);
+            p1.z -= (float)(frag_i2dz(fid) * Li.z);
             float rnd;
             if (RNG == 1) {
                 unsigned g1 = (unsigned)__float_as_int(p1.w), g2 = (unsigned)__float_as_int(p2.w);
-                rnd = mean0var1uu(seeds[0], max(g1, g2), min(g1, g2));
+                rnd = mean0var1uu(sb[0], max(g1, g2), min(g1, g2));
             } else {
                 const bool mask = (A.masks >> fid) & 1u;
-                rnd = mean0var1uu(seeds[1 + fid], mask ? rec.z : rec.w, mask ? rec.w : rec.z);
+                rnd = mean0var1uu(sb[1 + fid], mask ? rec.z : rec.w, mask ? rec.w : rec.z);
             }
             float3 f;
             if (dpd_force(P, p1, __ldg(A.vel + i), p2, __ldg(A.vel + j), rnd, f))
@@ -290,9 +337,9 @@ __global__ void __launch_bounds__(HALO_T) k_dpd_halo(const __grid_constant__ Dpd
                     const int bx = (adx == 1 ? L.x - 1 : 0) + hx, by = (ady == 1 ? L.y - 1 : 0) + hy,
                               bz = (adz == 1 ? L.z - 1 : 0) + hz;
                     const int c = bx + L.x * (by + L.y * bz);
-                    ib = __ldg(A.starts + c);
-                    be = ib + __ldg(A.counts + c);
-                    bid0 = __ldg(A.fss + A.fss_off[anti] + hci) - ib;
+                    ib = __ldg(starts + c);
+                    be = ib + __ldg(counts + c);
+                    bid0 = __ldg(A.fss + fss_off[anti] + hci) - ib;
                 } else if (row + 1 < rows) {
                     row++;
                     col = 0;
@@ -301,7 +348,7 @@ __global__ void __launch_bounds__(HALO_T) k_dpd_halo(const __grid_constant__ Dpd
                     left &= left - 1;
                     anti = frag_anti(fid);
                     const int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
-                    aid = frag_index(A, fid, gcell, ia - __ldg(A.starts + gcell));
+                    aid = frag_index(L, A.fss + fss_off[fid], fid, gcell, ia - __ldg(starts + gcell));
                     // r2map (src/fluforces/halo/dev/map.h:102-129) on the unshifted position
                     const int xc = dx == 0 ? L.x : 1, yc = dy == 0 ? L.y : 1;
                     int xs = 1, ys = 1, zs = 1, l;
@@ -347,15 +394,22 @@ __global__ void __launch_bounds__(HALO_T) k_dpd_halo(const __grid_constant__ Dpd
     if (qn > 0) process(qn);
 }
 
-// exclusive scans of the counts of every fragment's cells (src/exch/flu/dev/map.h:23-97)
-__global__ void k_frag_starts(int3 L, const int *__restrict__ counts, int *__restrict__ fss, Off27 off) {
+// exclusive scans of the counts of every fragment's cells (src/exch/flu/dev/map.h:23-97);
+// block (fid, box): out = fss + offset of fragment fid of that box
+__global__ void k_frag_starts(int3 L, const int *__restrict__ counts, int *__restrict__ fss, Off27 off, Boxes B) {
     __shared__ int sh[32];
     int fid = blockIdx.x;
+    int *out = fss + off.d[fid];
+    if (B.nbox > 0) {
+        const int box = blockIdx.y;
+        L = box_L(B, box);
+        counts += __ldg(B.c0 + box);
+        out = fss + __ldg(B.fss_tab + 27 * box + fid);
+    }
     int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
     int ox = dx == 1 ? L.x - 1 : 0, oy = dy == 1 ? L.y - 1 : 0, oz = dz == 1 ? L.z - 1 : 0;
     int ex = dx == 0 ? L.x : 1, ey = dy == 0 ? L.y : 1, ez = dz == 0 ? L.z : 1;
     int nc = ex * ey * ez;
-    int *out = fss + off.d[fid];
     int carry = 0;
     for (int b = 0; b < nc; b += DPD_THREADS) {
         int h = b + threadIdx.x, v = 0;
@@ -423,19 +477,58 @@ unsigned halo_masks() {
 }
 
 cudaError_t frag_starts_launch(int3 L, const int *counts, int *fss, const Off27 &off, cudaStream_t st) {
-    k_frag_starts<<<26, DPD_THREADS, 0, st>>>(L, counts, fss, off);
+    Boxes none{};
+    k_frag_starts<<<26, DPD_THREADS, 0, st>>>(L, counts, fss, off, none);
     return cudaGetLastError();
 }
 
-cudaError_t dpd_launch(const DpdArgs &A, int nmax, int rng_mode, cudaStream_t st) {
+cudaError_t frag_starts_boxes_launch(const Boxes &B, const int *counts, int *fss, cudaStream_t st) {
+    if (B.nbox <= 0) return cudaSuccess;
+    Off27 off{};
+    k_frag_starts<<<dim3(26, B.nbox), DPD_THREADS, 0, st>>>(make_int3(1, 1, 1), counts, fss, off, B);
+    return cudaGetLastError();
+}
+
+template <int RNG, bool BATCH>
+static void launch_bulk(const DpdArgs &A, int nmax, const DpdTune &t, cudaStream_t st) {
+    // every (threads, unroll) shape of DPD_TUNE_BULK_* for the reference keys;
+    // the stable-key variant exists in the default shape only
+#define CTC_BULK(TT, UU)                                                             \
+    if (t.bulk_threads == TT && t.bulk_unroll == UU) {                               \
+        k_dpd_bulk<RNG, BATCH, TT, UU><<<ceil_div(nmax, TT), TT, 0, st>>>(A);        \
+        return;                                                                      \
+    }
+    if (RNG == 0) {
+        CTC_BULK(128, 2) CTC_BULK(128, 4) CTC_BULK(128, 8)
+        CTC_BULK(256, 2) CTC_BULK(256, 8)
+    }
+#undef CTC_BULK
+    k_dpd_bulk<RNG, BATCH, 256, 4><<<ceil_div(nmax, 256), 256, 0, st>>>(A);
+}
+
+template <int RNG, bool BATCH>
+static void launch_halo(const DpdArgs &A, int nmax, const DpdTune &t, cudaStream_t st) {
+    if (RNG == 0 && t.halo_threads == 64) {
+        k_dpd_halo<RNG, BATCH, 64><<<ceil_div(nmax, 64), 64, 0, st>>>(A);
+        return;
+    }
+    if (RNG == 0 && t.halo_threads == 256) {
+        k_dpd_halo<RNG, BATCH, 256><<<ceil_div(nmax, 256), 256, 0, st>>>(A);
+        return;
+    }
+    k_dpd_halo<RNG, BATCH, 128><<<ceil_div(nmax, 128), 128, 0, st>>>(A);
+}
+
+cudaError_t dpd_launch(const DpdArgs &A, int nmax, int rng_mode, cudaStream_t st, const DpdTune &t) {
     if (nmax <= 0) return cudaSuccess;
+    const bool batch = A.B.nbox > 0;
     if (A.which & 1) {
-        if (rng_mode == 1) k_dpd_bulk<1><<<ceil_div(nmax, BULK_T), BULK_T, 0, st>>>(A);
-        else k_dpd_bulk<0><<<ceil_div(nmax, BULK_T), BULK_T, 0, st>>>(A);
+        if (rng_mode == 1) batch ? launch_bulk<1, true>(A, nmax, t, st) : launch_bulk<1, false>(A, nmax, t, st);
+        else batch ? launch_bulk<0, true>(A, nmax, t, st) : launch_bulk<0, false>(A, nmax, t, st);
     }
     if (A.which & 2) {
-        if (rng_mode == 1) k_dpd_halo<1><<<ceil_div(nmax, HALO_T), HALO_T, 0, st>>>(A);
-        else k_dpd_halo<0><<<ceil_div(nmax, HALO_T), HALO_T, 0, st>>>(A);
+        if (rng_mode == 1) batch ? launch_halo<1, true>(A, nmax, t, st) : launch_halo<1, false>(A, nmax, t, st);
+        else batch ? launch_halo<0, true>(A, nmax, t, st) : launch_halo<0, false>(A, nmax, t, st);
     }
     return cudaGetLastError();
 }

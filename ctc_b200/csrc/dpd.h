@@ -25,14 +25,28 @@ struct DpdArgs {
     int fss_off[27];
     int which;              // bit 0: bulk pairs, bit 1: pairs across periodic faces
     int *err;
+    Boxes B;                // B.nbox > 0: many boxes (L, starts, seeds, fss per box)
 };
+
+// launch shapes of the pair kernels, chosen by the autotuner of the batched
+// boxes (the single-box path uses the defaults)
+struct DpdTune {
+    int bulk_threads = 256;   // 128 or 256
+    int bulk_unroll = 4;      // candidate loads in flight per lane: 2, 4 or 8
+    int halo_threads = 128;   // 64, 128 or 256
+};
+constexpr int DPD_TUNE_BULK_T[2] = {128, 256};
+constexpr int DPD_TUNE_BULK_U[3] = {2, 4, 8};
+constexpr int DPD_TUNE_HALO_T[3] = {64, 128, 256};
 
 void frag_offsets(int3 L, Off27 *off);
 unsigned halo_masks();
 cudaError_t frag_starts_launch(int3 L, const int *counts, int *fss, const Off27 &off, cudaStream_t st);
+// the same for every box of B (fss offsets from B.fss_tab)
+cudaError_t frag_starts_boxes_launch(const Boxes &B, const int *counts, int *fss, cudaStream_t st);
 // nmax bounds the particle count (the kernels read the count at starts[ncells]);
 // particle sorted indices must stay below 2^27
-cudaError_t dpd_launch(const DpdArgs &A, int nmax, int rng_mode, cudaStream_t st);
+cudaError_t dpd_launch(const DpdArgs &A, int nmax, int rng_mode, cudaStream_t st, const DpdTune &tune = DpdTune());
 cudaError_t pair_launch(int n, const DpdPar &P, const float *pa, const float *pb, const float *rnd, float *f,
                         cudaStream_t st);
 cudaError_t rnd_launch(int n, float seed, const int *u, const int *v, int uu, float *out, cudaStream_t st);

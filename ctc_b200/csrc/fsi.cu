@@ -39,21 +39,32 @@ __device__ __forceinline__ unsigned emap_mask(int3 L, float x, float y, float z)
     return m;
 }
 
-__global__ void k_emap(int nv, int3 L, const float *__restrict__ pv, int stride, unsigned *__restrict__ mask) {
+// (with many boxes, B.nbox > 0, a vertex's box gives L; ranks, counts and
+// list starts are per box: rank[fid * nv + i] counts the box's vertices only,
+// count and img_start hold 26 entries per box)
+__global__ void k_emap(int nv, int3 L, const float *__restrict__ pv, int stride, unsigned *__restrict__ mask,
+                       Boxes B) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nv) return;
+    if (B.nbox > 0) L = box_L(B, box_find(B.v0, B.nbox, i));
     const float *q = pv + (size_t)stride * i;
     mask[i] = emap_mask(L, q[0], q[1], q[2]);
 }
 
 // per fragment: rank of each member vertex (ascending vertex index) and count
 __global__ void k_emap_rank(int nv, const unsigned *__restrict__ mask, int *__restrict__ rank,
-                            int *__restrict__ count) {
+                            int *__restrict__ count, Boxes B) {
     __shared__ int sh[32];
     int fid = blockIdx.x, carry = 0;
-    for (int b = 0; b < nv; b += blockDim.x) {
+    int i0 = 0, i1 = nv;                 // the box's vertices
+    if (B.nbox > 0) {
+        i0 = __ldg(B.v0 + blockIdx.y);
+        i1 = __ldg(B.v0 + blockIdx.y + 1);
+        count += 26 * blockIdx.y;
+    }
+    for (int b = i0; b < i1; b += blockDim.x) {
         int i = b + threadIdx.x;
-        int in = i < nv ? (int)((mask[i] >> fid) & 1u) : 0;
+        int in = i < i1 ? (int)((mask[i] >> fid) & 1u) : 0;
         int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
         int x = in;
         for (int o = 1; o < 32; o <<= 1) {
@@ -72,7 +83,7 @@ __global__ void k_emap_rank(int nv, const unsigned *__restrict__ mask, int *__re
         }
         __syncthreads();
         int excl = x - in + (w > 0 ? sh[w - 1] : 0) + carry;
-        if (i < nv) rank[(size_t)fid * nv + i] = in ? excl : -1;
+        if (i < i1) rank[(size_t)fid * nv + i] = in ? excl : -1;
         carry += sh[nw - 1];
         __syncthreads();
     }
@@ -81,6 +92,8 @@ __global__ void k_emap_rank(int nv, const unsigned *__restrict__ mask, int *__re
 
 // img_start[fid] = start of receive slot anti(fid) in the concatenated list
 __global__ void k_emap_starts(const int *__restrict__ count, int *__restrict__ img_start) {
+    count += 26 * blockIdx.x;            // one block per box
+    img_start += 26 * blockIdx.x;
     if (threadIdx.x == 0) {
         int s = 0, slot_start[26];
         for (int slot = 0; slot < 26; slot++) { slot_start[slot] = s; s += count[frag_anti(slot)]; }
@@ -95,47 +108,62 @@ __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
     const float *q = A.pv + (size_t)A.pstride * i;
     const float *qv = A.vv + (size_t)A.pstride * i;
     float4 pa = make_float4(q[0], q[1], q[2], 0.0f), va = make_float4(qv[0], qv[1], qv[2], 0.0f);
-    const int lx = A.L.x / 2, ly = A.L.y / 2, lz = A.L.z / 2;
+    int3 L = A.L;
+    const int *starts = A.starts, *counts = A.counts, *img_start = A.img_start;
+    const float *seeds = A.seeds_dev;
+    int vk = i, sk = 0;                  // key offsets: box-local vertex and solvent indices
+    if (A.B.nbox > 0) {
+        const int box = box_find(A.B.v0, A.B.nbox, i);
+        L = box_L(A.B, box);
+        const int c0 = __ldg(A.B.c0 + box);
+        starts += c0;
+        counts += c0;
+        img_start += 26 * box;
+        seeds += 2 * box;
+        vk = i - __ldg(A.B.v0 + box);
+        sk = __ldg(A.B.p0 + box);
+    }
+    const int lx = L.x / 2, ly = L.y / 2, lz = L.z / 2;
     // the vertex cell as src/fsi/dev/map/bulk.h:13-21 (floorf, may lie outside the box)
     const int cx = lx + (int)floorf(pa.x), cy = ly + (int)floorf(pa.y), cz = lz + (int)floorf(pa.z);
     const DpdPar P = A.par;
-    const float seed_bulk = A.seeds_dev ? A.seeds_dev[0] : A.seed_bulk;
-    const float seed_halo = A.seeds_dev ? A.seeds_dev[1] : A.seed_halo;
+    const float seed_bulk = seeds ? seeds[0] : A.seed_bulk;
+    const float seed_halo = seeds ? seeds[1] : A.seed_halo;
     float fx = 0, fy = 0, fz = 0;
     for (int dz = -1; dz <= 1; dz++)
         for (int dy = -1; dy <= 1; dy++)
             for (int dx = -1; dx <= 1; dx++) {
                 int gx = cx + dx, gy = cy + dy, gz = cz + dz;
-                int wx = gx < 0 ? -1 : (gx >= A.L.x ? 1 : 0);
-                int wy = gy < 0 ? -1 : (gy >= A.L.y ? 1 : 0);
-                int wz = gz < 0 ? -1 : (gz >= A.L.z ? 1 : 0);
-                gx -= wx * A.L.x; gy -= wy * A.L.y; gz -= wz * A.L.z;
-                if (gx < 0 || gx >= A.L.x || gy < 0 || gy >= A.L.y || gz < 0 || gz >= A.L.z) continue;
-                int cid = gx + A.L.x * (gy + A.L.y * gz);
-                int s = __ldg(A.starts + cid), e = s + __ldg(A.counts + cid);
+                int wx = gx < 0 ? -1 : (gx >= L.x ? 1 : 0);
+                int wy = gy < 0 ? -1 : (gy >= L.y ? 1 : 0);
+                int wz = gz < 0 ? -1 : (gz >= L.z ? 1 : 0);
+                gx -= wx * L.x; gy -= wy * L.y; gz -= wz * L.z;
+                if (gx < 0 || gx >= L.x || gy < 0 || gy >= L.y || gz < 0 || gz >= L.z) continue;
+                int cid = gx + L.x * (gy + L.y * gz);
+                int s = __ldg(starts + cid), e = s + __ldg(counts + cid);
                 if (s == e) continue;
                 bool halo = (wx | wy | wz) != 0;
                 float4 a = pa;
-                unsigned aid = (unsigned)i;
+                unsigned aid = (unsigned)vk;
                 float seed = seed_bulk;
                 if (halo) {
                     int fid = frag_d2i(wx, wy, wz);
                     if (RNG == 0) {
                         int r = __ldg(A.img_rank + (size_t)fid * A.nv + i);
                         if (r < 0) { set_error(A.err, DEV_BAD_PARTICLE); continue; }
-                        aid = (unsigned)(__ldg(A.img_start + fid) + r);
+                        aid = (unsigned)(__ldg(img_start + fid) + r);
                         seed = seed_halo;
                     }
-                    a.x = a.x + (float)(-wx * A.L.x);
-                    a.y = a.y + (float)(-wy * A.L.y);
-                    a.z = a.z + (float)(-wz * A.L.z);
+                    a.x = a.x + (float)(-wx * L.x);
+                    a.y = a.y + (float)(-wy * L.y);
+                    a.z = a.z + (float)(-wz * L.z);
                 }
                 for (int j = s; j < e; j++) {
                     float4 b = __ldg(A.spos + j);
                     float x = a.x - b.x, y = a.y - b.y, z = a.z - b.z;
                     if (dist2(x, y, z) >= 1.0f) continue;
-                    float rnd = RNG == 0 ? mean0var1uu(seed, aid, (unsigned)j)
-                                         : mean0var1uu(seed_bulk, (unsigned)i, (unsigned)__float_as_int(b.w));
+                    float rnd = RNG == 0 ? mean0var1uu(seed, aid, (unsigned)(j - sk))
+                                         : mean0var1uu(seed_bulk, (unsigned)vk, (unsigned)__float_as_int(b.w));
                     float3 f;
                     if (!dpd_force(P, a, va, b, __ldg(A.svel + j), rnd, f)) continue;
                     fx += f.x; fy += f.y; fz += f.z;
@@ -156,11 +184,12 @@ __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
 }
 
 cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsigned *mask, int *rank, int *count,
-                              int *img_start, cudaStream_t st) {
+                              int *img_start, cudaStream_t st, const Boxes &B) {
     if (nv <= 0) return cudaSuccess;
-    k_emap<<<ceil_div(nv, 256), 256, 0, st>>>(nv, L, pv, stride, mask);
-    k_emap_rank<<<26, 1024, 0, st>>>(nv, mask, rank, count);
-    k_emap_starts<<<1, 32, 0, st>>>(count, img_start);
+    const int nb = B.nbox > 0 ? B.nbox : 1;
+    k_emap<<<ceil_div(nv, 256), 256, 0, st>>>(nv, L, pv, stride, mask, B);
+    k_emap_rank<<<dim3(26, nb), 1024, 0, st>>>(nv, mask, rank, count, B);
+    k_emap_starts<<<nb, 32, 0, st>>>(count, img_start);
     return cudaGetLastError();
 }
 

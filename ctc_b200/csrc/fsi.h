@@ -22,10 +22,12 @@ struct FsiArgs {
     const int *img_rank;           // [26 * nv]: rank in fragment fid's list or -1 (reference keys)
     const int *img_start;          // [26]: first index of fragment fid's images in the halo list
     int *err;
+    Boxes B;                       // B.nbox > 0: vertices, solvent, seeds (2 per box) of many boxes
 };
 
+// with B.nbox > 0, count and img_start hold 26 entries per box
 cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsigned *mask, int *rank, int *count,
-                              int *img_start, cudaStream_t st);
+                              int *img_start, cudaStream_t st, const Boxes &B = Boxes());
 cudaError_t fsi_launch(const FsiArgs &A, int rng, cudaStream_t st);
 
 }  // namespace ctc

@@ -113,19 +113,22 @@ __device__ __forceinline__ unsigned kiss_next(unsigned *s) {
 }
 
 __global__ void k_draw_seeds(unsigned *__restrict__ state, int ntrunk, float *__restrict__ seeds) {
-    int k = threadIdx.x;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < ntrunk) seeds[k] = __fdiv_rn(__uint2float_rn(kiss_next(state + 4 * k)), 4294967296.0f);
 }
 
-// `count` successive draws from one trunk (the FSI trunk is drawn twice a step)
-__global__ void k_draw_seq(unsigned *__restrict__ state, int count, float *__restrict__ seeds) {
-    if (threadIdx.x == 0)
-        for (int k = 0; k < count; k++) seeds[k] = __fdiv_rn(__uint2float_rn(kiss_next(state)), 4294967296.0f);
+// `count` successive draws from each of ntrunk trunks (the FSI trunk is drawn
+// twice a step): seeds[count * t + k]
+__global__ void k_draw_seq(unsigned *__restrict__ state, int ntrunk, int count, float *__restrict__ seeds) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < ntrunk)
+        for (int k = 0; k < count; k++)
+            seeds[count * t + k] = __fdiv_rn(__uint2float_rn(kiss_next(state + 4 * t)), 4294967296.0f);
 }
 
 // ---------------------------------------------------------------------------
-cudaError_t draw_seq_launch(unsigned *state, int count, float *seeds, cudaStream_t st) {
-    k_draw_seq<<<1, 32, 0, st>>>(state, count, seeds);
+cudaError_t draw_seq_launch(unsigned *state, int count, float *seeds, cudaStream_t st, int ntrunk) {
+    k_draw_seq<<<ceil_div(ntrunk, 128), 128, 0, st>>>(state, ntrunk, count, seeds);
     return cudaGetLastError();
 }
 
@@ -160,7 +163,7 @@ cudaError_t diag_launch(const int *nptr, const float4 *vel, double mass, double 
 }
 
 cudaError_t draw_seeds_launch(unsigned *state, int ntrunk, float *seeds, cudaStream_t st) {
-    k_draw_seeds<<<1, 32, 0, st>>>(state, ntrunk, seeds);
+    k_draw_seeds<<<ceil_div(ntrunk, 128), 128, 0, st>>>(state, ntrunk, seeds);
     return cudaGetLastError();
 }
 

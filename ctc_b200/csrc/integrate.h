@@ -13,6 +13,7 @@ size_t diag_scratch_bytes();
 cudaError_t diag_launch(const int *nptr, const float4 *vel, double mass, double *scratch, double *out,
                         cudaStream_t st);
 cudaError_t draw_seeds_launch(unsigned *state, int ntrunk, float *seeds, cudaStream_t st);
-cudaError_t draw_seq_launch(unsigned *state, int count, float *seeds, cudaStream_t st);
+// count successive draws from each of ntrunk trunks: seeds[count * t + k]
+cudaError_t draw_seq_launch(unsigned *state, int count, float *seeds, cudaStream_t st, int ntrunk = 1);
 
 }  // namespace ctc

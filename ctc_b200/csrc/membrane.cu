@@ -163,10 +163,12 @@ __global__ void k_membrane(MembraneArgs A) {
 
 // membrane migration of one periodic rank (src/distr/rbc/dev.h:1-25): a cell
 // whose bounding-box centre left the box [lo, lo + L) moves by -L*d as a whole
-__global__ void k_rbc_wrap(int nv, int3 L, float4 *__restrict__ pos) {
+// (with many boxes, B.nbox > 0, the cell's box -- from its first vertex -- gives L)
+__global__ void k_rbc_wrap(int nv, int3 L, float4 *__restrict__ pos, Boxes B) {
     __shared__ float lo[3][AV_T / 32], hi[3][AV_T / 32];
     __shared__ float shift[3];
     const int c = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (B.nbox > 0) L = box_L(B, box_find(B.v0, B.nbox, c * nv));
     float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
     for (int v = threadIdx.x; v < nv; v += AV_T) {
         float4 r = pos[(size_t)c * nv + v];
@@ -200,8 +202,8 @@ __global__ void k_rbc_wrap(int nv, int3 L, float4 *__restrict__ pos) {
         }
 }
 
-cudaError_t rbc_wrap_launch(int nc, int nv, int3 L, float4 *pos, cudaStream_t st) {
-    if (nc > 0) k_rbc_wrap<<<nc, AV_T, 0, st>>>(nv, L, pos);
+cudaError_t rbc_wrap_launch(int nc, int nv, int3 L, float4 *pos, cudaStream_t st, const Boxes &B) {
+    if (nc > 0) k_rbc_wrap<<<nc, AV_T, 0, st>>>(nv, L, pos, B);
     return cudaGetLastError();
 }
 

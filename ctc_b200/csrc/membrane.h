@@ -1,6 +1,7 @@
 // Host-side declarations of the membrane kernels.
 #pragma once
 #include <cuda_runtime.h>
+#include "common.cuh"
 
 namespace ctc {
 
@@ -25,6 +26,7 @@ struct MembraneArgs {
 cudaError_t area_volume_launch(int nc, int nv, int nt, const int *tri, const float *pos, int stride, double *av,
                                cudaStream_t st);
 cudaError_t membrane_launch(const MembraneArgs &A, cudaStream_t st);
-cudaError_t rbc_wrap_launch(int nc, int nv, int3 L, float4 *pos, cudaStream_t st);
+// with B.nbox > 0, each cell's box gives L
+cudaError_t rbc_wrap_launch(int nc, int nv, int3 L, float4 *pos, cudaStream_t st, const Boxes &B = Boxes());
 
 }  // namespace ctc

@@ -98,3 +98,34 @@ def rbc_system(L, nc, seed=3, kBT=KBT, D=7.82):
     pv[:, 3:] = rng.normal(0.0, np.sqrt(kBT / RBC_MASS), (len(r), 3))
     A, V = mesh.area_volume(X, F)
     return pv, F, rbc_params(A, V, kBT)
+
+
+def batch_system(nbox=512, emin=8, emax=24, rbc_every=4, seed=5, rho=10):
+    """The batched-boxes workload: nbox cubic periodic boxes with edges drawn
+    uniformly from emin..emax, solvent at density rho, one RBC in every
+    rbc_every-th box (index 0, rbc_every, ...).  Boxes with an edge below the
+    cell diameter + 2 rc let an RBC interact with its own periodic image
+    through FSI; its internal forces use unwrapped coordinates, so this is
+    allowed.  Returns (L[nbox, 3], n[nbox], solvent AoS box after box,
+    cells[nbox], membrane vertices AoS box after box, triangles, params)."""
+    rng = np.random.default_rng(seed)
+    edges = rng.integers(emin, emax + 1, size=nbox)
+    L = np.stack([edges] * 3, axis=1).astype(np.int32)
+    parts, n = [], []
+    for k in range(nbox):
+        pp = solvent(tuple(L[k]), rho=rho, seed=int(rng.integers(1 << 31)))
+        parts.append(pp)
+        n.append(len(pp))
+    cells = np.array([1 if (rbc_every and k % rbc_every == 0) else 0 for k in range(nbox)], np.int32)
+    pv, tri, par = [], None, None
+    for k in range(nbox):
+        if cells[k]:
+            v, tri, par = rbc_system(tuple(L[k]), 1, seed=int(rng.integers(1 << 31)))
+            pv.append(v)
+    pv = np.concatenate(pv) if pv else np.zeros((0, 6), np.float32)
+    if tri is None:
+        from . import mesh
+        X, tri = mesh.rbc_template(7.82)
+        A, V = mesh.area_volume(X, tri)
+        par = rbc_params(A, V)
+    return L, np.array(n, np.int32), np.concatenate(parts), cells, pv, tri, par

@@ -232,6 +232,50 @@ int ctc_sim_next_seeds(const ctc_sim *s, float *seeds27);
 int ctc_sim_profile(ctc_sim *s, int enable);
 int ctc_sim_profile_read(ctc_sim *s, double *ms, int *steps);
 
+/* ---- many independent boxes per launch ----------------------------------
+ * No single counterpart in the reference (it runs one domain per MPI rank);
+ * each box is the periodic system a ctc_sim of its size would be -- its own
+ * trunk generators with the reference's seeds, RNG keys of box-local indices,
+ * its own wrap, cell lists and FSI images -- and all boxes advance together:
+ * every kernel stage of a step is ONE launch over all boxes, the step can be
+ * replayed as a CUDA graph, and the pair kernels' launch shapes can be chosen
+ * by timing them on the actual boxes (ctc_batch_tune). */
+typedef struct ctc_batch ctc_batch;
+typedef struct {
+    int nbox;
+    const int *L;            /* [host, 3 nbox] box sizes in unit cells */
+    const int *n;            /* [host, nbox] solvent particles per box (fixed) */
+    ctc_dpd_params dpd;
+    float mass, dt;
+    float bodyf[3];
+    int rng;                 /* CTC_RNG_* */
+} ctc_batch_config;
+int ctc_batch_create(const ctc_batch_config *cfg, ctc_batch **b);
+int ctc_batch_destroy(ctc_batch *b);
+/* solvent of every box [host, AoS, box after box, sum of n] */
+int ctc_batch_set_solvent(ctc_batch *b, const float *pp, void *stream);
+/* cells[k] membranes of one template in box k (nv vertices, nt triangles
+ * tri[3 nt] [host]); pp [host, AoS] box after box, cell after cell */
+int ctc_batch_set_membranes(ctc_batch *b, const int *cells, int nv, int nt, const int *tri, const float *pp,
+                            const ctc_rbc_params *p, const ctc_dpd_params *fsi, float mass, void *stream);
+/* advance every box nsteps steps (the step of ctc_sim_step) */
+int ctc_batch_step(ctc_batch *b, int nsteps, void *stream);
+/* 1: steps replay CUDA graphs captured on first use (one per ping-pong
+ * buffer) on the object's own stream, ordered after the caller's stream work
+ * and before its later work; 0: direct launches */
+int ctc_batch_set_graph(ctc_batch *b, int enable);
+/* autotuner: times every launch shape of the bulk (threads x candidate loads
+ * in flight) and halo (threads) pair kernels reps times on the current state
+ * without advancing it, keeps the fastest; choice [host, 3] = bulk threads,
+ * bulk unroll, halo threads (may be NULL) */
+int ctc_batch_tune(ctc_batch *b, int reps, int *choice, void *stream);
+int ctc_batch_set_tune(ctc_batch *b, const int *choice);
+/* state [host, AoS]: solvent box after box (cell-sorted within a box),
+ * membrane vertices in ctc_batch_set_membranes order */
+int ctc_batch_get_solvent(ctc_batch *b, float *pp, void *stream);
+int ctc_batch_get_membranes(ctc_batch *b, float *pp, void *stream);
+int ctc_batch_count(const ctc_batch *b, int *nsolvent, int *nvertices);
+
 #ifdef __cplusplus
 }
 #endif

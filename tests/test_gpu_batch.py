@@ -1,0 +1,124 @@
+"""Batched boxes: every box of a ctc_batch must be the system a single-box
+ctc_sim of its size is -- same seeds, same box-local RNG keys, same wrap --
+so a batch of boxes of uneven sizes (odd and even edges, some with a red
+blood cell) is compared box by box with separate single-box runs."""
+import numpy as np
+import pytest
+
+from ctc_b200 import systems
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+POS_TOL, VEL_TOL = 2e-6, 1e-3    # the system tests' per-step tolerances (force sums differ in order only)
+
+
+def _boxes(seed=11):
+    L = np.array([[8, 8, 8], [9, 9, 9], [12, 12, 12], [10, 10, 10], [7, 7, 7]], np.int32)
+    rng = np.random.default_rng(seed)
+    solv = [systems.solvent(tuple(l), seed=int(rng.integers(1 << 30))) for l in L]
+    cells = np.array([1, 0, 1, 0, 0], np.int32)
+    mem = {}
+    for k in np.flatnonzero(cells):
+        pv, tri, par = systems.rbc_system(tuple(L[k]), 1, seed=int(rng.integers(1 << 30)))
+        mem[k] = pv
+    return L, solv, cells, mem, tri, par
+
+
+def _new_batch(L, solv, cells, mem, tri, par, dpd, fsi, bodyf):
+    import ctc_b200 as C
+    b = C.Batch(L, [len(p) for p in solv], C.DpdParams(*dpd), mass=1.0, dt=systems.DT, bodyf=bodyf)
+    b.set_solvent(np.concatenate(solv))
+    pv = np.concatenate([mem[k] for k in sorted(mem)])
+    b.set_membranes(cells, pv, tri, 642, par, C.DpdParams(*fsi), mass=systems.RBC_MASS)
+    return b
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_batch_matches_single_boxes(graph):
+    """Step by step: the batch against one single-box system per box, each
+    single box restarted from the batch's state of the previous step (a
+    particle within rounding of a cell face may change cell in one run and
+    not in the other, which re-keys its pairs; restarting keeps the
+    comparison to one step's arithmetic)."""
+    import ctc_b200 as C
+    L, solv, cells, mem, tri, par = _boxes()
+    dpd = systems.dpd_params()
+    fsi = (0.0, 8.0, dpd[2], 0.25)
+    bodyf = (0.01, 0.0, 0.0)
+    b = _new_batch(L, solv, cells, mem, tri, par, dpd, fsi, bodyf)
+    b.set_graph(graph)
+    sims = []
+    for k in range(len(L)):
+        s = C.Sim(tuple(L[k]), len(solv[k]), C.DpdParams(*dpd), mass=1.0, dt=systems.DT, bodyf=bodyf)
+        sims.append(s)
+    prev_s, prev_v = list(solv), dict(mem)
+    for step in range(3):
+        b.step(1)
+        gs, gv = b.get_solvent(), b.get_membranes()
+        o, ov = 0, 0
+        for k, s in enumerate(sims):
+            s.set_solvent(prev_s[k])
+            if k in prev_v:
+                s.set_membranes(prev_v[k], tri, 642, par, C.DpdParams(*fsi), mass=systems.RBC_MASS)
+            s.step(1)
+            rs = s.get_solvent()
+            bs = gs[o:o + len(rs)]
+            o += len(rs)
+            assert np.abs(bs[:, :3] - rs[:, :3]).max() < POS_TOL, (step, k)
+            assert np.abs(bs[:, 3:] - rs[:, 3:]).max() < VEL_TOL, (step, k)
+            prev_s[k] = bs
+            if k in prev_v:
+                rv = s.get_membranes()
+                bv = gv[ov:ov + len(rv)]
+                ov += len(rv)
+                assert np.abs(bv[:, :3] - rv[:, :3]).max() < POS_TOL, (step, k)
+                assert np.abs(bv[:, 3:] - rv[:, 3:]).max() < VEL_TOL, (step, k)
+                prev_v[k] = bv
+        assert o == len(gs) and ov == len(gv)
+    for s in sims:
+        s.close()
+    b.close()
+    assert C.device_error() == 0
+
+
+def test_batch_tune_leaves_state():
+    """The autotuner times the pair kernels on the current state without
+    advancing it or its generators."""
+    import ctc_b200 as C
+    L, solv, cells, mem, tri, par = _boxes(seed=12)
+    dpd = systems.dpd_params()
+    fsi = (0.0, 8.0, dpd[2], 0.25)
+    out = []
+    for tune in (False, True):
+        b = _new_batch(L, solv, cells, mem, tri, par, dpd, fsi, (0, 0, 0))
+        if tune:
+            assert len(b.tune(reps=1)) == 3
+        b.step(1)
+        out.append((b.get_solvent(), b.get_membranes()))
+        b.close()
+    for x, y in zip(*out):
+        assert np.abs(x[:, :3] - y[:, :3]).max() < POS_TOL
+        assert np.abs(x[:, 3:] - y[:, 3:]).max() < VEL_TOL
+    assert C.device_error() == 0
+
+
+def test_batch_launch_shapes_agree():
+    """Every launch shape the autotuner may pick computes the same forces."""
+    import ctc_b200 as C
+    L, solv, cells, mem, tri, par = _boxes(seed=13)
+    dpd = systems.dpd_params()
+    ref = None
+    for shape in [(256, 4, 128), (128, 2, 64), (128, 8, 256), (256, 8, 64)]:
+        b = C.Batch(L, [len(p) for p in solv], C.DpdParams(*dpd), dt=systems.DT)
+        b.set_solvent(np.concatenate(solv))
+        b.set_tune(shape)
+        b.step(1)
+        out = b.get_solvent()
+        b.close()
+        if ref is None:
+            ref = out
+        else:
+            assert np.abs(out[:, :3] - ref[:, :3]).max() < POS_TOL
+            assert np.abs(out[:, 3:] - ref[:, 3:]).max() < VEL_TOL
+    assert C.device_error() == 0
