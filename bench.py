@@ -39,11 +39,15 @@ CONFIGS = {
                 name="plain DPD 64x64x64 rho=10 (2,621,440 particles), body force 0.01 x"),
     "c3": dict(L=(64, 64, 64), bodyf=(0.0, 0.0, 0.0), steps=100, rbc=200,
                name="C3 RBC suspension 64x64x64 rho=10 (2,621,440 solvent) + 200 cells x 642 vertices"),
+    "c4": dict(adjoint=True, L=(32, 32, 32), rbc=20, K=20, kck=5, bodyf=(0.0, 0.0, 0.0),
+               name="C4 adjoint 32x32x32 rho=10 (327,680 solvent) + 20 RBC, loss = mean vertex x-velocity "
+                    "after 20 steps, checkpoints every 5"),
     "c5": dict(batch=True, nbox=512, bodyf=(0.0, 0.0, 0.0), steps=100,
                name="C5 512 periodic boxes, edges uniform in 8..24, rho=10, one RBC in every 4th box"),
 }
 METRIC = "particle-steps/s @1 B200 (plain DPD step)"
 METRIC_BATCH = "particle-steps/s @1 B200 (batched boxes)"
+METRIC_ADJ = "adjoint/forward time @1 B200 (differentiable rollout)"
 PAIR_BYTES = 48          # algorithmic bytes per particle of the pair kernel: pos+vel read, force write
 PAIR_FLOP = 100 * 20.94  # ~100 flop per accepted half-pair, 20.94 half-pairs per particle at rho=10
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # 148 SMs x 128 FP32 lanes x FMA x 1965 MHz
@@ -453,6 +457,96 @@ def run_batch(args, cfg, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# differentiable rollout: reverse pass against forward pass
+# ---------------------------------------------------------------------------
+def run_adjoint(args, cfg, world, rank, local):
+    import torch
+
+    from ctc_b200 import systems
+    from ctc_b200.adjoint import Rollout
+    torch.cuda.set_device(local)
+    L, K, kck = cfg["L"], cfg["K"], cfg["kck"]
+    pp = systems.solvent(L, seed=4 + rank)
+    pv, tri, par = systems.rbc_system(L, cfg["rbc"], seed=4 + rank)
+    dpd = systems.dpd_params()
+    fsi = (0.0, systems.GAMMA, dpd[2], systems.SPOW)
+    r = Rollout(L, pp, dpd, systems.KBT, systems.DT, pv=pv, tri=tri, rbc=par, fsi=fsi, mmass=systems.RBC_MASS)
+    theta = np.array([systems.A_DPD, systems.GAMMA, par["ks"], par["kb"]])
+    r.set_params(theta)
+    stream = torch.cuda.current_stream()
+    for _ in range(max(1, args.warmup)):
+        r.forward(K, kck)
+        r.backward()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd, bwd = [], []
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    for _ in range(args.steps):
+        e[0].record(stream)
+        loss = r.forward(K, kck)
+        e[1].record(stream)
+        g = r.backward()
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        fwd.append(e[0].elapsed_time(e[1]))
+        bwd.append(e[1].elapsed_time(e[2]))
+    clk = clocks.stop()
+    f_ms, b_ms = allmax(world, float(np.median(fwd))), allmax(world, float(np.median(bwd)))
+    # run-to-run noise of the loss (force sums in a different order)
+    noise = abs(r.forward(K, kck) - r.forward(K, kck))
+    # central differences of the loss itself for the parameters, relative steps 1e-2 and 1e-3
+    fd = {}
+    for rel in (1e-2, 1e-3):
+        fd[rel] = []
+        for k in range(4):
+            h = rel * max(1.0, abs(theta[k]))
+            vals = []
+            for sgn in (1, -1):
+                t = theta.copy()
+                t[k] += sgn * h
+                r.set_params(t)
+                vals.append(r.forward(K, kck))
+            fd[rel].append((vals[0] - vals[1]) / (2 * h))
+    r.set_params(theta)
+    r.close()
+    if rank != 0:
+        return
+    n, nvt = len(pp), len(pv)
+    line = {
+        "metric": METRIC_ADJ, "value": b_ms / f_ms, "unit": "reverse pass time / forward pass time",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": (f_ms + b_ms) / K,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (membrane forces f64)",
+        "data": "synthetic (seeded uniform solvent, Maxwellian velocities, seeded RBC placement)",
+        "config": {"workload": cfg["name"], "solvent_particles": n, "membrane_vertices": nvt, "K": K,
+                   "checkpoint_every": kck, "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "rng": "stable keys (random force fixed by its counter)"},
+        "forward_ms": f_ms, "reverse_ms": b_ms,
+        "forward_particle_steps_per_s": (n + nvt) * K / (f_ms * 1e-3),
+        "loss": loss,
+        "grad": {k: float(v) for k, v in zip(("a", "gamma", "ks", "kb"), g["theta"])},
+        "grad_fd": {"step_%g" % rel: {k: float(v) for k, v in zip(("a", "gamma", "ks", "kb"), fd[rel])}
+                    for rel in fd},
+        "grad_abs_err_vs_fd": {"step_%g" % rel: {k: float(abs(a - b)) for k, a, b in
+                                                 zip(("a", "gamma", "ks", "kb"), g["theta"], fd[rel])} for rel in fd},
+        "fd": {"loss_noise": noise,
+               "note": "the loss moves by ~1e-8..1e-7 under these steps and the pair weight (1-r)^0.25 has an "
+                       "unbounded slope at the cutoff: the FP32 differences are not converged (compare the two "
+                       "steps); the tests check the adjoint on well-conditioned losses and against FP64"},
+        # forward step: 6 cell-list kernels, cell wrap, bulk, halo, FSI, update, area/volume, membrane forces,
+        # vertex update (14); reverse step: 2 update adjoints, bulk + halo, FSI, area/volume + membrane, unsort
+        # (8); the reverse pass recomputes all segments but the last
+        "gpu_launches": (14 * K + 8 * K + 14 * (K - kck)) * args.steps,
+        "e2e": {"value": b_ms / f_ms, "unit": "reverse pass time / forward pass time",
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 16 * nvt / K},
+    }
+    if clk:
+        line["clocks"] = clk
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -468,6 +562,8 @@ def main():
         run_reference(args, cfg, world, rank)
     elif cfg.get("batch"):
         run_batch(args, cfg, world, rank, local)
+    elif cfg.get("adjoint"):
+        run_adjoint(args, cfg, world, rank, local)
     else:
         run_ours(args, cfg, world, rank, local)
     if world > 1:

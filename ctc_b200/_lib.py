@@ -40,6 +40,11 @@ class BatchConfig(C.Structure):
                 ("mass", C.c_float), ("dt", C.c_float), ("bodyf", C.c_float * 3), ("rng", C.c_int)]
 
 
+class AdjConfig(C.Structure):
+    _fields_ = [("LX", C.c_int), ("LY", C.c_int), ("LZ", C.c_int), ("dpd", DpdParams), ("kBT", C.c_float),
+                ("mass", C.c_float), ("dt", C.c_float), ("bodyf", C.c_float * 3)]
+
+
 # name -> (restype, argtypes); every symbol include/ctc_b200.h declares
 SIGNATURES = {
     "ctc_status_string": (C.c_char_p, [C.c_int]),
@@ -101,6 +106,15 @@ SIGNATURES = {
     "ctc_batch_get_solvent": (C.c_int, [vp, vp, vp]),
     "ctc_batch_get_membranes": (C.c_int, [vp, vp, vp]),
     "ctc_batch_count": (C.c_int, [vp, ip, ip]),
+    "ctc_adj_create": (C.c_int, [C.POINTER(AdjConfig), C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, vp,
+                                 C.POINTER(RbcParams), C.POINTER(DpdParams), C.c_float, C.POINTER(vp)]),
+    "ctc_adj_destroy": (C.c_int, [vp]),
+    "ctc_adj_set_params": (C.c_int, [vp, C.POINTER(C.c_double)]),
+    "ctc_adj_set_state": (C.c_int, [vp, vp, vp]),
+    "ctc_adj_forward": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_double), vp]),
+    "ctc_adj_backward": (C.c_int, [vp, C.POINTER(C.c_double), vp, vp, vp, vp, vp]),
+    "ctc_adj_backward_cot": (C.c_int, [vp, vp, vp, vp, vp, C.POINTER(C.c_double), vp, vp, vp, vp, vp]),
+    "ctc_adj_get_final": (C.c_int, [vp, vp, vp, vp]),
 }
 
 _lib = None

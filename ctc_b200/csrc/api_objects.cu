@@ -129,6 +129,26 @@ static void stressful(int nt, float totArea, double *l0, double *a0) {
 }
 
 namespace ctc {
+// the MembraneArgs of a membrane module (adjacency, bending) without state
+int membrane_args(const ctc_rbc_force *f, MembraneArgs *A) {
+    if (!f || !A) return fail(CTC_ERR_ARG, "membrane_args: null");
+    memset(A, 0, sizeof(*A));
+    A->nv = f->nv; A->md = f->md;
+    A->adj0 = f->adj0; A->adj1 = f->adj1;
+    A->bending = f->bending;
+    A->err = dev_err_ptr();
+    return CTC_OK;
+}
+
+// the parameters and stress-ful equilibrium lengths of p into A
+void membrane_args_par(MembraneArgs *A, const ctc_rbc_params *p, int nt) {
+    fill_par(&A->par, p);
+    stressful(nt, p->totArea, &A->l0, &A->a0);
+}
+
+const int *membrane_tri(const ctc_rbc_force *f) { return f->tri; }
+int membrane_nt(const ctc_rbc_force *f) { return f->nt; }
+
 int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const float *pos, const float *vel, int stride,
                     float *force, int fstride, cudaStream_t st) {
     if (nc > f->max_cells) return fail(CTC_ERR_CAPACITY, "nc=%d > max_cell=%d", nc, f->max_cells);

@@ -15,6 +15,12 @@ int *dev_err_ptr();                           // device failure word of the curr
 // membrane forces of nc cells (area/volume + forces), accumulated into force
 int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const float *pos, const float *vel, int stride,
                     float *force, int fstride, cudaStream_t st);
+// pieces of a membrane module for the adjoint (membrane.h's MembraneArgs)
+struct MembraneArgs;
+int membrane_args(const ctc_rbc_force *f, MembraneArgs *A);
+void membrane_args_par(MembraneArgs *A, const ctc_rbc_params *p, int nt);
+const int *membrane_tri(const ctc_rbc_force *f);
+int membrane_nt(const ctc_rbc_force *f);
 // FSI of nv vertices against the cell-sorted solvent; seeds_dev (2 floats) may replace the seeds
 int fsi_forces(int3 L, const DpdPar &P, int nv, const float *pv, const float *vv, int pstride, const float4 *spos,
                const float4 *svel, const int *starts, const int *counts, float *fv, int fstride, float *fs, int sstride,

@@ -104,6 +104,41 @@ __device__ __forceinline__ bool dpd_force(const DpdPar &P, float4 pa, float4 va,
     return true;
 }
 
+// Vector-Jacobian product of one pair force f = phi(r, ev) e (e = dr / r,
+// ev = e . dv, dr = pa - pb, dv = va - vb, phi = (-g wr ev + s rnd) wr + a w,
+// w = 1 - r, wr = w^spow) for the cotangent gf of f, with rnd held fixed:
+//   jx = d(f.gf)/d(dr), jv = d(f.gf)/d(dv), da = d(f.gf)/da,
+//   dg = d(f.gf)/dg with sigma = sigma(g) (dsdg = d sigma / d g).
+// Returns false where the force is identically zero (r^2 >= 1, r^2 < 1e-6,
+// or r = 1 exactly, where the slope of wr is unbounded).
+__device__ __forceinline__ bool dpd_vjp(const DpdPar &P, float dsdg, float4 pa, float4 va, float4 pb, float4 vb,
+                                        float rnd, float3 gf, float3 &jx, float3 &jv, float &da, float &dg) {
+    const float x = pa.x - pb.x, y = pa.y - pb.y, z = pa.z - pb.z;
+    const float r2 = x * x + y * y + z * z;
+    if (r2 >= 1.0f || r2 < 1e-6f) return false;
+    const float invr = rsqrtf(r2), r = r2 * invr;
+    const float ex = x * invr, ey = y * invr, ez = z * invr;
+    const float dvx = va.x - vb.x, dvy = va.y - vb.y, dvz = va.z - vb.z;
+    const float ev = ex * dvx + ey * dvy + ez * dvz;
+    const float w = 1.0f - r;
+    if (w <= 0.0f) return false;
+    const float wr = powf(w, P.spow), wr2 = wr * wr;
+    const float phi = (-P.g * wr * ev + P.s * rnd) * wr + P.a * w;
+    // d wr / dr = -spow wr / w;  d wr^2 / dr = -2 spow wr^2 / w
+    const float dphi_dr = -P.a + 2.0f * P.spow * P.g * wr2 * ev / w - P.spow * P.s * rnd * wr / w;
+    const float dphi_dev = -P.g * wr2;
+    const float eg = ex * gf.x + ey * gf.y + ez * gf.z;
+    const float c1 = dphi_dr * eg, c2 = dphi_dev * eg * invr, c3 = phi * invr;
+    jx.x = c1 * ex + c2 * (dvx - ev * ex) + c3 * (gf.x - eg * ex);
+    jx.y = c1 * ey + c2 * (dvy - ev * ey) + c3 * (gf.y - eg * ey);
+    jx.z = c1 * ez + c2 * (dvz - ev * ez) + c3 * (gf.z - eg * ez);
+    const float c4 = dphi_dev * eg;
+    jv = make_float3(c4 * ex, c4 * ey, c4 * ez);
+    da = eg * w;
+    dg = eg * (-wr2 * ev + dsdg * rnd * wr);
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // fragments (src/frag/dev.h:19-81): id 0..25 <-> direction in {-1,0,1}^3
 // ---------------------------------------------------------------------------

@@ -91,8 +91,29 @@ __device__ __forceinline__ void red_force(float *out, int stride, int i, float s
     atomicAdd(o + 2, s * f.z);
 }
 
-// T threads per block, UNROLL candidate loads in flight per lane
-template <int RNG, bool BATCH, int T, int UNROLL>
+// pulls the cotangent of a pair force back (MODE 1): +/- onto both particles
+__device__ __forceinline__ void vjp_red(const DpdArgs &A, int i, int j, float3 jx, float3 jv) {
+    atomicAdd(A.adj_x + i, make_float4(jx.x, jx.y, jx.z, 0.0f));
+    atomicAdd(A.adj_x + j, make_float4(-jx.x, -jx.y, -jx.z, 0.0f));
+    atomicAdd(A.adj_v + i, make_float4(jv.x, jv.y, jv.z, 0.0f));
+    atomicAdd(A.adj_v + j, make_float4(-jv.x, -jv.y, -jv.z, 0.0f));
+}
+
+// per-warp sums of the parameter cotangents into adj_par (FP64)
+__device__ __forceinline__ void vjp_par(const DpdArgs &A, float da, float dg) {
+    for (int o = 16; o > 0; o >>= 1) {
+        da += __shfl_down_sync(0xffffffffu, da, o);
+        dg += __shfl_down_sync(0xffffffffu, dg, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (da != 0.0f || dg != 0.0f)) {
+        atomicAdd(A.adj_par, (double)da);
+        atomicAdd(A.adj_par + 1, (double)dg);
+    }
+}
+
+// T threads per block, UNROLL candidate loads in flight per lane; MODE 0
+// accumulates the forces, MODE 1 their vector-Jacobian product
+template <int RNG, bool BATCH, int T, int UNROLL, int MODE = 0>
 __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs A) {
     constexpr int W = T / 32;
     __shared__ BulkRec<BATCH> queue[W][QCAP];
@@ -116,6 +137,7 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
     const DpdPar P = A.par;
     BulkRec<BATCH> *q = queue[warp];
     int qn = 0;
+    float acc_a = 0.0f, acc_g = 0.0f;               // MODE 1: parameter cotangents
 
     float4 pa = make_float4(0, 0, 0, 0);
     int cx = 0, cy = 0, cz = 0;
@@ -146,10 +168,22 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
             } else {
                 rnd = mean0var1ii(seed, i - k0, j - k0);  // i > j: the reference's (ia, ib)
             }
-            float3 f;
-            if (dpd_force(P, p1, v1, p2, v2, rnd, f)) {
-                red_force(A.out, A.out_stride, i, 1.0f, f);
-                red_force(A.out, A.out_stride, j, -1.0f, f);
+            if constexpr (MODE == 0) {
+                float3 f;
+                if (dpd_force(P, p1, v1, p2, v2, rnd, f)) {
+                    red_force(A.out, A.out_stride, i, 1.0f, f);
+                    red_force(A.out, A.out_stride, j, -1.0f, f);
+                }
+            } else {
+                const float4 gi = __ldg(A.adj_f + i), gj = __ldg(A.adj_f + j);
+                float3 jx, jv;
+                float da, dg;
+                if (dpd_vjp(P, A.dsdg, p1, v1, p2, v2, rnd, make_float3(gi.x - gj.x, gi.y - gj.y, gi.z - gj.z), jx,
+                            jv, da, dg)) {
+                    vjp_red(A, i, j, jx, jv);
+                    acc_a += da;
+                    acc_g += dg;
+                }
             }
         }
         __syncwarp();
@@ -205,6 +239,7 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
         if (have) ib = min(ib + UNROLL, be);
     }
     if (qn > 0) process(qn);
+    if constexpr (MODE == 1) vjp_par(A, acc_a, acc_g);
 }
 
 // ---------------------------------------------------------------------------
@@ -222,7 +257,7 @@ __device__ __forceinline__ void r2size_dev(float r, int nc, int S, int &l, int &
     s = min(nc, i + 2) - l;
 }
 
-template <int RNG, bool BATCH, int T>
+template <int RNG, bool BATCH, int T, int MODE = 0>
 __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs A) {
     __shared__ uint4 queue[T / 32][QCAP];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -247,6 +282,7 @@ __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs 
     const float *seeds = A.seeds_dev ? A.seeds_dev : A.seeds;
     const DpdPar P = A.par;
     uint4 *q = queue[warp];
+    float acc_a = 0.0f, acc_g = 0.0f;               // MODE 1: parameter cotangents
     int qn = 0;
 
     // the particle's cell-list cell (computed in double, src/clist/dev/main.h:21-24)
@@ -298,9 +334,22 @@ __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs 
                 const bool mask = (A.masks >> fid) & 1u;
                 rnd = mean0var1uu(sb[1 + fid], mask ? rec.z : rec.w, mask ? rec.w : rec.z);
             }
-            float3 f;
-            if (dpd_force(P, p1, __ldg(A.vel + i), p2, __ldg(A.vel + j), rnd, f))
-                red_force(A.out, A.out_stride, i, 1.0f, f);
+            if constexpr (MODE == 0) {
+                float3 f;
+                if (dpd_force(P, p1, __ldg(A.vel + i), p2, __ldg(A.vel + j), rnd, f))
+                    red_force(A.out, A.out_stride, i, 1.0f, f);
+            } else {
+                // only the local particle takes the force; both positions enter it
+                const float4 gi = __ldg(A.adj_f + i);
+                float3 jx, jv;
+                float da, dg;
+                if (dpd_vjp(P, A.dsdg, p1, __ldg(A.vel + i), p2, __ldg(A.vel + j), rnd,
+                            make_float3(gi.x, gi.y, gi.z), jx, jv, da, dg)) {
+                    vjp_red(A, i, j, jx, jv);
+                    acc_a += da;
+                    acc_g += dg;
+                }
+            }
         }
         __syncwarp();
     };
@@ -392,6 +441,7 @@ __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs 
         push(ok, rec);
     }
     if (qn > 0) process(qn);
+    if constexpr (MODE == 1) vjp_par(A, acc_a, acc_g);
 }
 
 // exclusive scans of the counts of every fragment's cells (src/exch/flu/dev/map.h:23-97);
@@ -517,6 +567,13 @@ static void launch_halo(const DpdArgs &A, int nmax, const DpdTune &t, cudaStream
         return;
     }
     k_dpd_halo<RNG, BATCH, 128><<<ceil_div(nmax, 128), 128, 0, st>>>(A);
+}
+
+cudaError_t dpd_vjp_launch(const DpdArgs &A, int nmax, cudaStream_t st) {
+    if (nmax <= 0) return cudaSuccess;
+    if (A.which & 1) k_dpd_bulk<1, false, 256, 4, 1><<<ceil_div(nmax, 256), 256, 0, st>>>(A);
+    if (A.which & 2) k_dpd_halo<1, false, 128, 1><<<ceil_div(nmax, 128), 128, 0, st>>>(A);
+    return cudaGetLastError();
 }
 
 cudaError_t dpd_launch(const DpdArgs &A, int nmax, int rng_mode, cudaStream_t st, const DpdTune &t) {

@@ -26,6 +26,14 @@ struct DpdArgs {
     int which;              // bit 0: bulk pairs, bit 1: pairs across periodic faces
     int *err;
     Boxes B;                // B.nbox > 0: many boxes (L, starts, seeds, fss per box)
+    // vector-Jacobian product mode (stable keys, one box): the cotangent of
+    // the forces adj_f is pulled back onto the positions and velocities
+    // (accumulated into adj_x, adj_v) and onto (a, gamma) (adj_par[0..1],
+    // FP64 sums); dsdg = d sigma / d gamma
+    const float4 *adj_f;
+    float4 *adj_x, *adj_v;
+    double *adj_par;
+    float dsdg;
 };
 
 // launch shapes of the pair kernels, chosen by the autotuner of the batched
@@ -47,6 +55,9 @@ cudaError_t frag_starts_boxes_launch(const Boxes &B, const int *counts, int *fss
 // nmax bounds the particle count (the kernels read the count at starts[ncells]);
 // particle sorted indices must stay below 2^27
 cudaError_t dpd_launch(const DpdArgs &A, int nmax, int rng_mode, cudaStream_t st, const DpdTune &tune = DpdTune());
+// vector-Jacobian product of the bulk (which & 1) and halo (which & 2) pair
+// forces, stable keys, one box
+cudaError_t dpd_vjp_launch(const DpdArgs &A, int nmax, cudaStream_t st);
 cudaError_t pair_launch(int n, const DpdPar &P, const float *pa, const float *pb, const float *rnd, float *f,
                         cudaStream_t st);
 cudaError_t rnd_launch(int n, float seed, const int *u, const int *v, int uu, float *out, cudaStream_t st);

@@ -101,7 +101,8 @@ __global__ void k_emap_starts(const int *__restrict__ count, int *__restrict__ i
     }
 }
 
-template <int RNG>
+// MODE 0: forces; MODE 1: their vector-Jacobian product
+template <int RNG, int MODE = 0>
 __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.nv) return;
@@ -130,6 +131,9 @@ __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
     const float seed_bulk = seeds ? seeds[0] : A.seed_bulk;
     const float seed_halo = seeds ? seeds[1] : A.seed_halo;
     float fx = 0, fy = 0, fz = 0;
+    float3 gx_v = make_float3(0.0f, 0.0f, 0.0f), gv_v = make_float3(0.0f, 0.0f, 0.0f);   // MODE 1
+    float4 gfv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (MODE == 1) gfv = __ldg(A.adj_fv + i);
     for (int dz = -1; dz <= 1; dz++)
         for (int dy = -1; dy <= 1; dy++)
             for (int dx = -1; dx <= 1; dx++) {
@@ -164,6 +168,19 @@ __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
                     if (dist2(x, y, z) >= 1.0f) continue;
                     float rnd = RNG == 0 ? mean0var1uu(seed, aid, (unsigned)(j - sk))
                                          : mean0var1uu(seed_bulk, (unsigned)vk, (unsigned)__float_as_int(b.w));
+                    if constexpr (MODE == 1) {
+                        const float4 gs = __ldg(A.adj_fs + j);
+                        float3 jx, jv;
+                        float da, dg;
+                        if (!dpd_vjp(P, 0.0f, a, va, b, __ldg(A.svel + j), rnd,
+                                     make_float3(gfv.x - gs.x, gfv.y - gs.y, gfv.z - gs.z), jx, jv, da, dg))
+                            continue;
+                        gx_v.x += jx.x; gx_v.y += jx.y; gx_v.z += jx.z;
+                        gv_v.x += jv.x; gv_v.y += jv.y; gv_v.z += jv.z;
+                        atomicAdd(A.adj_xs + j, make_float4(-jx.x, -jx.y, -jx.z, 0.0f));
+                        atomicAdd(A.adj_vs + j, make_float4(-jv.x, -jv.y, -jv.z, 0.0f));
+                        continue;
+                    }
                     float3 f;
                     if (!dpd_force(P, a, va, b, __ldg(A.svel + j), rnd, f)) continue;
                     fx += f.x; fy += f.y; fz += f.z;
@@ -177,6 +194,12 @@ __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
                     }
                 }
             }
+    if constexpr (MODE == 1) {
+        float4 *ox = A.adj_xv + i, *ov = A.adj_vv + i;
+        ox->x += gx_v.x; ox->y += gx_v.y; ox->z += gx_v.z;
+        ov->x += gv_v.x; ov->y += gv_v.y; ov->z += gv_v.z;
+        return;
+    }
     float *o = A.fv + (size_t)A.fstride * i;
     o[0] += fx;
     o[1] += fy;
@@ -190,6 +213,11 @@ cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsig
     k_emap<<<ceil_div(nv, 256), 256, 0, st>>>(nv, L, pv, stride, mask, B);
     k_emap_rank<<<dim3(26, nb), 1024, 0, st>>>(nv, mask, rank, count, B);
     k_emap_starts<<<nb, 32, 0, st>>>(count, img_start);
+    return cudaGetLastError();
+}
+
+cudaError_t fsi_vjp_launch(const FsiArgs &A, cudaStream_t st) {
+    if (A.nv > 0) k_fsi<1, 1><<<ceil_div(A.nv, 128), 128, 0, st>>>(A);
     return cudaGetLastError();
 }
 

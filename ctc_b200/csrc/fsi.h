@@ -23,11 +23,17 @@ struct FsiArgs {
     const int *img_start;          // [26]: first index of fragment fid's images in the halo list
     int *err;
     Boxes B;                       // B.nbox > 0: vertices, solvent, seeds (2 per box) of many boxes
+    // vector-Jacobian product (stable keys, one box): cotangents of the vertex
+    // and solvent forces pulled back onto vertex and solvent positions and
+    // velocities (accumulated, float4 arrays)
+    const float4 *adj_fv, *adj_fs;
+    float4 *adj_xv, *adj_vv, *adj_xs, *adj_vs;
 };
 
 // with B.nbox > 0, count and img_start hold 26 entries per box
 cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsigned *mask, int *rank, int *count,
                               int *img_start, cudaStream_t st, const Boxes &B = Boxes());
 cudaError_t fsi_launch(const FsiArgs &A, int rng, cudaStream_t st);
+cudaError_t fsi_vjp_launch(const FsiArgs &A, cudaStream_t st);
 
 }  // namespace ctc

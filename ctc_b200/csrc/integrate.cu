@@ -126,7 +126,47 @@ __global__ void k_draw_seq(unsigned *__restrict__ state, int ntrunk, int count, 
             seeds[count * t + k] = __fdiv_rn(__uint2float_rn(kiss_next(state + 4 * t)), 4294967296.0f);
 }
 
+// adjoint of k_integrate (v' = v + (f + m a) / m dt; x' = x + v' dt): from the
+// cotangents lx, lv of x', v' to those of the pre-update x, v (in place) and
+// of the force lf
+__global__ void k_integrate_adj(int n, const float4 *__restrict__ lx, float4 *__restrict__ lv,
+                                float4 *__restrict__ lf, float dt, float mass) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 x = lx[i];
+    float4 v = lv[i];
+    v.x = __fmaf_rn(dt, x.x, v.x);
+    v.y = __fmaf_rn(dt, x.y, v.y);
+    v.z = __fmaf_rn(dt, x.z, v.z);
+    lv[i] = v;
+    const float c = dt / mass;
+    lf[i] = make_float4(c * v.x, c * v.y, c * v.z, 0.0f);
+}
+
+// adjoint of the cell-list gather (out k <- in order[k]): cotangents back to
+// the input order
+__global__ void k_unsort_adj(int n, const int *__restrict__ order, const float4 *__restrict__ lx_s,
+                             const float4 *__restrict__ lv_s, float4 *__restrict__ lx, float4 *__restrict__ lv) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = order[k];
+    lx[i] = lx_s[k];
+    lv[i] = lv_s[k];
+}
+
 // ---------------------------------------------------------------------------
+cudaError_t integrate_adj_launch(int n, const float4 *lx, float4 *lv, float4 *lf, float dt, float mass,
+                                 cudaStream_t st) {
+    if (n > 0) k_integrate_adj<<<ceil_div(n, 256), 256, 0, st>>>(n, lx, lv, lf, dt, mass);
+    return cudaGetLastError();
+}
+
+cudaError_t unsort_adj_launch(int n, const int *order, const float4 *lx_s, const float4 *lv_s, float4 *lx,
+                              float4 *lv, cudaStream_t st) {
+    if (n > 0) k_unsort_adj<<<ceil_div(n, 256), 256, 0, st>>>(n, order, lx_s, lv_s, lx, lv);
+    return cudaGetLastError();
+}
+
 cudaError_t draw_seq_launch(unsigned *state, int count, float *seeds, cudaStream_t st, int ntrunk) {
     k_draw_seq<<<ceil_div(ntrunk, 128), 128, 0, st>>>(state, ntrunk, count, seeds);
     return cudaGetLastError();

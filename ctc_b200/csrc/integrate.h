@@ -16,4 +16,10 @@ cudaError_t draw_seeds_launch(unsigned *state, int ntrunk, float *seeds, cudaStr
 // count successive draws from each of ntrunk trunks: seeds[count * t + k]
 cudaError_t draw_seq_launch(unsigned *state, int count, float *seeds, cudaStream_t st, int ntrunk = 1);
 
+// adjoints of the update and of the cell-list gather
+cudaError_t integrate_adj_launch(int n, const float4 *lx, float4 *lv, float4 *lf, float dt, float mass,
+                                 cudaStream_t st);
+cudaError_t unsort_adj_launch(int n, const int *order, const float4 *lx_s, const float4 *lv_s, float4 *lx,
+                              float4 *lv, cudaStream_t st);
+
 }  // namespace ctc

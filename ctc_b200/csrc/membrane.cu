@@ -220,3 +220,4 @@ cudaError_t membrane_launch(const MembraneArgs &A, cudaStream_t st) {
 }
 
 }  // namespace ctc
+

@@ -26,6 +26,11 @@ struct MembraneArgs {
 cudaError_t area_volume_launch(int nc, int nv, int nt, const int *tri, const float *pos, int stride, double *av,
                                cudaStream_t st);
 cudaError_t membrane_launch(const MembraneArgs &A, cudaStream_t st);
+// vector-Jacobian product of the forces of membrane_launch (A.pos/A.vel float4
+// SoA) for the cotangent lam: accumulated into adj_x, adj_v; pg[0..1] +=
+// d/dks, d/dkb; avd: scratch of 4 doubles per cell
+cudaError_t membrane_vjp_launch(const MembraneArgs &A, int nt, const int *tri, const float4 *lam, double *avd,
+                                float4 *adj_x, float4 *adj_v, double *pg, cudaStream_t st);
 // with B.nbox > 0, each cell's box gives L
 cudaError_t rbc_wrap_launch(int nc, int nv, int3 L, float4 *pos, cudaStream_t st, const Boxes &B = Boxes());
 

@@ -276,6 +276,45 @@ int ctc_batch_get_solvent(ctc_batch *b, float *pp, void *stream);
 int ctc_batch_get_membranes(ctc_batch *b, float *pp, void *stream);
 int ctc_batch_count(const ctc_batch *b, int *nsolvent, int *nvertices);
 
+/* ---- differentiable rollout ---------------------------------------------
+ * No counterpart in the reference.  K steps of the solvent + membrane system
+ * (the step of ctc_sim_step with CTC_RNG_STABLE keys, so the random force is
+ * held fixed by its counter) and the reverse pass giving the gradient of
+ *     loss = mean x-velocity of the membrane vertices after K steps
+ * with respect to the initial positions / velocities and to theta = {a,
+ * gamma} of the solvent pair force and {ks, kb} of the membranes; sigma
+ * follows gamma as sqrt(2 kBT gamma / dt).  The reverse pass recomputes from
+ * checkpoints taken every kck steps. */
+typedef struct ctc_adj ctc_adj;
+typedef struct {
+    int LX, LY, LZ;
+    ctc_dpd_params dpd;      /* solvent pair force (a, g taken from theta, s from g) */
+    float kBT;
+    float mass, dt;
+    float bodyf[3];
+} ctc_adj_config;
+/* n solvent particles pp and nc cells pv of one template [host, AoS] */
+int ctc_adj_create(const ctc_adj_config *cfg, int n, const float *pp, int nc, int nv, int nt, const int *tri,
+                   const float *pv, const ctc_rbc_params *rbc, const ctc_dpd_params *fsi, float mmass, ctc_adj **a);
+int ctc_adj_destroy(ctc_adj *a);
+/* theta [host, 4 doubles] = a, gamma, ks, kb */
+int ctc_adj_set_params(ctc_adj *a, const double *theta);
+/* replace the initial solvent (pp) and/or membrane (pv) state [host, AoS] */
+int ctc_adj_set_state(ctc_adj *a, const float *pp, const float *pv);
+int ctc_adj_forward(ctc_adj *a, int K, int kck, double *loss, void *stream);
+/* after ctc_adj_forward: gtheta [host, 4], gradients of the initial solvent
+ * positions gx / velocities gv [host, 3 n] and vertex positions gxv /
+ * velocities gvv [host, 3 nc nv]; any may be NULL */
+int ctc_adj_backward(ctc_adj *a, double *gtheta, float *gx, float *gv, float *gxv, float *gvv, void *stream);
+/* the same for the linear loss sum(cx . x + cv . v) of the final state:
+ * cx, cv [host, 3 n] by particle id (its index in the initial pp), cxv, cvv
+ * [host, 3 nc nv] by vertex; NULL = zero */
+int ctc_adj_backward_cot(ctc_adj *a, const float *cx, const float *cv, const float *cxv, const float *cvv,
+                         double *gtheta, float *gx, float *gv, float *gxv, float *gvv, void *stream);
+/* the final state of the last forward rollout [host, AoS]: solvent by
+ * particle id (n), vertices in order (nc nv); either may be NULL */
+int ctc_adj_get_final(ctc_adj *a, float *pp, float *pv, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
