@@ -1,15 +1,20 @@
-"""Benchmark of the per-step particle hot path (plain DPD solvent).
+"""Benchmark of the per-step particle hot path.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5|p64]
 
-One "step" = wrap + cell-list rebuild, bulk + periodic-halo DPD forces with the
-reference's pair RNG keys, constant body force, update -- the reference's step
-order.  Default workload: the large plain-DPD Poiseuille box 192 x 96 x 96 at
-number density 10 (17,694,720 particles), a = 2.5, gamma = 8, kBT = 0.0444,
-spow = 0.25, dt = 5e-4, body force 0.01 along x; seeded synthetic input.
-The metric is particle-steps/s.  Multi-GPU runs are independent replicas (one
-box per rank, no data-path collective): value = all ranks' particle-steps /
-the max over ranks of the timed region.
+Default (c2): one "step" = wrap + cell-list rebuild, bulk + periodic-halo DPD
+forces with the reference's pair RNG keys, constant body force, update -- the
+reference's step order -- on the large plain-DPD Poiseuille box 192 x 96 x 96
+at number density 10 (17,694,720 particles), a = 2.5, gamma = 8,
+kBT = 0.0444, spow = 0.25, dt = 5e-4, body force 0.01 along x; seeded
+synthetic input.  The metric is particle-steps/s.  Multi-GPU runs are
+independent replicas (one box per rank, no data-path collective): value =
+all ranks' particle-steps / the max over ranks of the timed region.
+
+c3 adds 200 red blood cells (FSI + membrane forces) to a 64^3 box; c5 runs
+512 boxes of edges 8..24 (every 4th with one RBC) batched per launch as
+graph-replayed steps against one system per box; c4 times the reverse pass of
+a 20-step differentiable rollout (32^3 + 20 RBCs) against its forward pass.
 
 --impl reference times the reference's own CPU path of the step (the C
 restatement in oracle/, in the reference's operation order; the reference
