@@ -1,6 +1,7 @@
 // C ABI of ctc_b200 (include/ctc_b200.h): module entry points that replace
 // the reference's clist / fluforces / scheme modules, and the fast-path
 // plain-DPD system.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -265,6 +266,7 @@ struct ctc_sim {
     int prof;                              // record per-phase events each step
     std::vector<cudaEvent_t> ev;           // CTC_SIM_PHASES + 1 events per profiled step
     int prof_steps;
+    int *pack, *pack_off, pack_cap;        // boundary particles packed per fragment (halo pairs)
     // membranes (optional): nc cells of nv vertices, unsorted float4 SoA
     int mnc, mnv;
     ctc_rbc_force *rbc;
@@ -313,6 +315,16 @@ extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
     CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 28));   // + the FSI trunk
     CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 29));
     CUDA_TRY(cudaMalloc(&s->diag_scratch, diag_scratch_bytes()));
+    {
+        // a boundary particle appears once per fragment holding its cell: room
+        // for 1.5 x the uniform-density count of those entries
+        Off27 coff;
+        frag_cell_offsets(s->L, &coff);
+        s->pack_cap = (int)std::min<double>((double)(1 << 30),
+                                            1.5 * (double)np * coff.d[26] / (double)s->nc + 4096.0);
+        CUDA_TRY(cudaMalloc(&s->pack, sizeof(int) * (size_t)s->pack_cap));
+        CUDA_TRY(cudaMalloc(&s->pack_off, sizeof(int) * 27));
+    }
     CUDA_TRY(cudaMalloc(&s->diag_out, sizeof(double) * 5));
     // trunk 0: bulk (0,0,0,0); 1..26: halo fragments.  Stable keys use trunk 0 only.
     kiss_ini(&s->trunk_host[0], 0, 0, 0, 0);
@@ -334,6 +346,7 @@ extern "C" int ctc_sim_destroy(ctc_sim *s) {
     cudaFree(s->force); cudaFree(s->counts); cudaFree(s->starts); cudaFree(s->count0); cudaFree(s->fss);
     cudaFree(s->scratch); cudaFree(s->trunk_dev); cudaFree(s->seeds_dev); cudaFree(s->diag_scratch);
     cudaFree(s->diag_out);
+    cudaFree(s->pack); cudaFree(s->pack_off);
     for (cudaEvent_t e : s->ev) cudaEventDestroy(e);
     if (s->rbc) ctc_rbc_force_fin(s->rbc);
     cudaFree(s->mpos); cudaFree(s->mvel); cudaFree(s->mforce); cudaFree(s->mcount);
@@ -454,14 +467,14 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
     A.which = 3;
     A.fss = s->fss;
     A.err = dev_err_ptr();
-    if (s->cfg.rng == CTC_RNG_REFERENCE) CUDA_TRY(frag_starts_launch(s->L, s->counts, s->fss, s->off, st));
+    CUDA_TRY(frag_starts_launch(s->L, s->counts, s->fss, s->off, st));
+    CUDA_TRY(halo_pack_launch(A, s->off, s->pack, s->pack_off, s->pack_cap, st));
     CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n_host, st));
     sim_mark(s, 2, st);
     A.which = 1;
     CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st));
     sim_mark(s, 3, st);
-    A.which = 2;
-    CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st));
+    CUDA_TRY(halo_packed_launch(A, s->pack, s->pack_off, s->pack_cap, s->cfg.rng, st));
     sim_mark(s, 4, st);
     const float3 bf = make_float3(s->cfg.bodyf[0], s->cfg.bodyf[1], s->cfg.bodyf[2]);
     if (nvt > 0) {

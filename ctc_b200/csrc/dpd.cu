@@ -27,35 +27,7 @@
 
 namespace ctc {
 
-constexpr int DPD_THREADS = 256;
-constexpr int DPD_WARPS = DPD_THREADS / 32;
 constexpr int QCAP = 64;        // per-warp queue: < 32 waiting + one round of 32
-
-__device__ __forceinline__ int block_exscan256(int v, int *sh, int &total) {
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) sh[w] = x;
-    __syncthreads();
-    if (w == 0) {
-        int s = lane < DPD_WARPS ? sh[lane] : 0;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, s, o);
-            if (lane >= o) s += y;
-        }
-        if (lane < DPD_WARPS) sh[lane] = s;
-    }
-    __syncthreads();
-    total = sh[DPD_WARPS - 1];
-    int r = x - v + (w > 0 ? sh[w - 1] : 0);
-    __syncthreads();
-    return r;
-}
 
 // index of a particle inside fragment fid's packed list (src/exch/flu/dev/map.h:1-21,
 // src/exch/flu/dev/pack.h:2-40): fragment-cell start + offset inside the cell;
@@ -257,11 +229,12 @@ __device__ __forceinline__ void r2size_dev(float r, int nc, int S, int &l, int &
     s = min(nc, i + 2) - l;
 }
 
-template <int RNG, bool BATCH, int T, int MODE = 0>
-__global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs A) {
-    __shared__ uint4 queue[T / 32][QCAP];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ia = blockIdx.x * T + threadIdx.x;
+// the halo pairs of local particle ia (none if ia >= the particle count) for
+// the fragments of its cell that are also in `only`, through the warp's queue q
+template <int RNG, bool BATCH, int MODE>
+__device__ __forceinline__ void halo_run(const DpdArgs &A, const int ia, const unsigned only, uint4 *q, float &acc_a,
+                                         float &acc_g) {
+    const int lane = threadIdx.x & 31;
     int3 L = A.L;
     const int *starts = A.starts, *counts = A.counts;
     const int *fss_off = A.fss_off;                 // fragment-cell start offsets of the box
@@ -281,8 +254,6 @@ __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs 
     }
     const float *seeds = A.seeds_dev ? A.seeds_dev : A.seeds;
     const DpdPar P = A.par;
-    uint4 *q = queue[warp];
-    float acc_a = 0.0f, acc_g = 0.0f;               // MODE 1: parameter cotangents
     int qn = 0;
 
     // the particle's cell-list cell (computed in double, src/clist/dev/main.h:21-24)
@@ -305,6 +276,7 @@ __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs 
                             (dz == 0 || (dz == 1 ? gz == L.z - 1 : gz == 0));
             if (in) frags |= 1u << fid;
         }
+        frags &= only;
     }
     if (!__any_sync(0xffffffffu, frags != 0)) return;   // interior warp
 
@@ -441,14 +413,87 @@ __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs 
         push(ok, rec);
     }
     if (qn > 0) process(qn);
+}
+
+// one local particle per thread, every fragment of its cell
+template <int RNG, bool BATCH, int T, int MODE = 0>
+__global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs A) {
+    __shared__ uint4 queue[T / 32][QCAP];
+    float acc_a = 0.0f, acc_g = 0.0f;               // MODE 1: parameter cotangents
+    halo_run<RNG, BATCH, MODE>(A, blockIdx.x * T + threadIdx.x, 0xffffffffu, queue[threadIdx.x >> 5], acc_a, acc_g);
     if constexpr (MODE == 1) vjp_par(A, acc_a, acc_g);
 }
 
+// the boundary particles packed per fragment, as the reference's exchange
+// packs them (src/exch/flu/dev/pack.h:2-40): fragment fid's particle a is
+// pack[pack_off[fid] + a]; one (fragment, particle) per thread, grid-stride,
+// so no lane idles on an interior particle or walks a fragment loop
+template <int RNG, int T>
+__global__ void __launch_bounds__(T) k_dpd_halo_packed(const __grid_constant__ DpdArgs A, const int *__restrict__ pack,
+                                                       const int *__restrict__ pack_off, int cap) {
+    __shared__ uint4 queue[T / 32][QCAP];
+    float acc_a = 0.0f, acc_g = 0.0f;
+    const int total = min(__ldg(pack_off + 26), cap);
+    for (int base = blockIdx.x * T; base < total; base += gridDim.x * T) {
+        const int t = base + threadIdx.x;
+        int ia = 0x7fffffff;
+        unsigned only = 0;
+        if (t < total) {
+            int f = 0;
+            for (int k = 1; k < 26; k++) f += __ldg(pack_off + k) <= t;
+            ia = __ldg(pack + t);
+            only = 1u << f;
+        }
+        halo_run<RNG, false, 0>(A, ia, only, queue[threadIdx.x >> 5], acc_a, acc_g);
+    }
+}
+
+// pack_off[f] = boundary particles of the fragments before f (fss holds each
+// fragment's exclusive scan, its total at [cells of f]); pack_off[26] = all
+__global__ void k_halo_pack_off(int3 L, const int *__restrict__ fss, Off27 off, int *__restrict__ pack_off) {
+    if (threadIdx.x != 0) return;
+    int s = 0;
+    for (int f = 0; f < 26; f++) {
+        pack_off[f] = s;
+        const int ex = frag_i2dx(f) == 0 ? L.x : 1, ey = frag_i2dy(f) == 0 ? L.y : 1,
+                  ez = frag_i2dz(f) == 0 ? L.z : 1;
+        s += fss[off.d[f] + ex * ey * ez];
+    }
+    pack_off[26] = s;
+}
+
+// one fragment cell per thread (coff: prefix of the fragments' cell counts):
+// its particles' sorted indices into the pack
+__global__ void k_halo_pack(int3 L, const int *__restrict__ starts, const int *__restrict__ counts,
+                            const int *__restrict__ fss, Off27 off, Off27 coff, const int *__restrict__ pack_off,
+                            int cap, int *__restrict__ pack, int *err) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= coff.d[26]) return;
+    int f = 0;
+    while (f < 25 && coff.d[f + 1] <= g) f++;
+    const int hci = g - coff.d[f];
+    const int dx = frag_i2dx(f), dy = frag_i2dy(f), dz = frag_i2dz(f);
+    const int ex = dx == 0 ? L.x : 1, ey = dy == 0 ? L.y : 1;
+    const int cx = (dx == 1 ? L.x - 1 : 0) + hci % ex, cy = (dy == 1 ? L.y - 1 : 0) + (hci / ex) % ey,
+              cz = (dz == 1 ? L.z - 1 : 0) + hci / (ex * ey);
+    const int cell = cx + L.x * (cy + L.y * cz);
+    const int s0 = __ldg(starts + cell), c = __ldg(counts + cell);
+    const int base = __ldg(pack_off + f) + __ldg(fss + off.d[f] + hci);
+    for (int o = 0; o < c; o++) {
+        if (base + o < cap) pack[base + o] = s0 + o;
+        else set_error(err, DEV_CELL_OVERFLOW);
+    }
+}
+
 // exclusive scans of the counts of every fragment's cells (src/exch/flu/dev/map.h:23-97);
-// block (fid, box): out = fss + offset of fragment fid of that box
-__global__ void k_frag_starts(int3 L, const int *__restrict__ counts, int *__restrict__ fss, Off27 off, Boxes B) {
+// block (fid, box): out = fss + offset of fragment fid of that box.  1024
+// threads, FS_ITEMS consecutive fragment cells each per round.
+constexpr int FS_T = 1024, FS_ITEMS = 8;
+
+__global__ void __launch_bounds__(FS_T) k_frag_starts(int3 L, const int *__restrict__ counts, int *__restrict__ fss,
+                                                      Off27 off, Boxes B) {
     __shared__ int sh[32];
-    int fid = blockIdx.x;
+    const int fid = blockIdx.x;
     int *out = fss + off.d[fid];
     if (B.nbox > 0) {
         const int box = blockIdx.y;
@@ -456,20 +501,53 @@ __global__ void k_frag_starts(int3 L, const int *__restrict__ counts, int *__res
         counts += __ldg(B.c0 + box);
         out = fss + __ldg(B.fss_tab + 27 * box + fid);
     }
-    int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
-    int ox = dx == 1 ? L.x - 1 : 0, oy = dy == 1 ? L.y - 1 : 0, oz = dz == 1 ? L.z - 1 : 0;
-    int ex = dx == 0 ? L.x : 1, ey = dy == 0 ? L.y : 1, ez = dz == 0 ? L.z : 1;
-    int nc = ex * ey * ez;
+    const int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
+    const int ox = dx == 1 ? L.x - 1 : 0, oy = dy == 1 ? L.y - 1 : 0, oz = dz == 1 ? L.z - 1 : 0;
+    const int ex = dx == 0 ? L.x : 1, ey = dy == 0 ? L.y : 1, ez = dz == 0 ? L.z : 1;
+    const int nc = ex * ey * ez;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int carry = 0;
-    for (int b = 0; b < nc; b += DPD_THREADS) {
-        int h = b + threadIdx.x, v = 0;
-        if (h < nc) {
-            int x = h % ex, y = (h / ex) % ey, z = h / (ex * ey);
-            v = counts[(ox + x) + L.x * ((oy + y) + L.y * (oz + z))];
+    for (int b = 0; b < nc; b += FS_T * FS_ITEMS) {
+        const int h0 = b + threadIdx.x * FS_ITEMS;
+        int v[FS_ITEMS], s = 0;
+#pragma unroll
+        for (int k = 0; k < FS_ITEMS; k++) {
+            const int h = h0 + k;
+            v[k] = 0;
+            if (h < nc) {
+                const int x = h % ex, y = (h / ex) % ey, z = h / (ex * ey);
+                v[k] = __ldg(counts + (ox + x) + L.x * ((oy + y) + L.y * (oz + z)));
+            }
+            s += v[k];
         }
-        int tot, r = block_exscan256(v, sh, tot);
-        if (h < nc) out[h] = carry + r;
+        // block exclusive scan of the per-thread sums
+        int x = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sh[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int t = sh[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            sh[lane] = t;
+        }
+        __syncthreads();
+        int r = carry + x - s + (w > 0 ? sh[w - 1] : 0);
+        const int tot = sh[31];
+#pragma unroll
+        for (int k = 0; k < FS_ITEMS; k++) {
+            if (h0 + k < nc) out[h0 + k] = r;
+            r += v[k];
+        }
         carry += tot;
+        __syncthreads();
     }
     if (threadIdx.x == 0) out[nc] = carry;
 }
@@ -528,14 +606,14 @@ unsigned halo_masks() {
 
 cudaError_t frag_starts_launch(int3 L, const int *counts, int *fss, const Off27 &off, cudaStream_t st) {
     Boxes none{};
-    k_frag_starts<<<26, DPD_THREADS, 0, st>>>(L, counts, fss, off, none);
+    k_frag_starts<<<26, FS_T, 0, st>>>(L, counts, fss, off, none);
     return cudaGetLastError();
 }
 
 cudaError_t frag_starts_boxes_launch(const Boxes &B, const int *counts, int *fss, cudaStream_t st) {
     if (B.nbox <= 0) return cudaSuccess;
     Off27 off{};
-    k_frag_starts<<<dim3(26, B.nbox), DPD_THREADS, 0, st>>>(make_int3(1, 1, 1), counts, fss, off, B);
+    k_frag_starts<<<dim3(26, B.nbox), FS_T, 0, st>>>(make_int3(1, 1, 1), counts, fss, off, B);
     return cudaGetLastError();
 }
 
@@ -567,6 +645,32 @@ static void launch_halo(const DpdArgs &A, int nmax, const DpdTune &t, cudaStream
         return;
     }
     k_dpd_halo<RNG, BATCH, 128><<<ceil_div(nmax, 128), 128, 0, st>>>(A);
+}
+
+void frag_cell_offsets(int3 L, Off27 *coff) {
+    int s = 0;
+    for (int f = 0; f < 26; f++) {
+        coff->d[f] = s;
+        s += (frag_i2dx(f) == 0 ? L.x : 1) * (frag_i2dy(f) == 0 ? L.y : 1) * (frag_i2dz(f) == 0 ? L.z : 1);
+    }
+    coff->d[26] = s;
+}
+
+cudaError_t halo_pack_launch(const DpdArgs &A, const Off27 &off, int *pack, int *pack_off, int cap, cudaStream_t st) {
+    Off27 coff;
+    frag_cell_offsets(A.L, &coff);
+    k_halo_pack_off<<<1, 32, 0, st>>>(A.L, A.fss, off, pack_off);
+    k_halo_pack<<<ceil_div(coff.d[26], 256), 256, 0, st>>>(A.L, A.starts, A.counts, A.fss, off, coff, pack_off, cap,
+                                                            pack, A.err);
+    return cudaGetLastError();
+}
+
+cudaError_t halo_packed_launch(const DpdArgs &A, const int *pack, const int *pack_off, int cap, int rng_mode,
+                               cudaStream_t st) {
+    constexpr int T = 128, BLOCKS = 148 * 8;
+    if (rng_mode == 1) k_dpd_halo_packed<1, T><<<BLOCKS, T, 0, st>>>(A, pack, pack_off, cap);
+    else k_dpd_halo_packed<0, T><<<BLOCKS, T, 0, st>>>(A, pack, pack_off, cap);
+    return cudaGetLastError();
 }
 
 cudaError_t dpd_vjp_launch(const DpdArgs &A, int nmax, cudaStream_t st) {

@@ -55,6 +55,14 @@ cudaError_t frag_starts_boxes_launch(const Boxes &B, const int *counts, int *fss
 // nmax bounds the particle count (the kernels read the count at starts[ncells]);
 // particle sorted indices must stay below 2^27
 cudaError_t dpd_launch(const DpdArgs &A, int nmax, int rng_mode, cudaStream_t st, const DpdTune &tune = DpdTune());
+// the boundary particles of every fragment, packed (fragment f's particle a at
+// pack[pack_off[f] + a], pack_off[26] = all, at most cap) from the cell lists
+// and fragment starts of A; then the halo pairs with one (fragment, particle)
+// per thread.  Fragment cells per fragment: frag_cell_offsets.
+void frag_cell_offsets(int3 L, Off27 *coff);
+cudaError_t halo_pack_launch(const DpdArgs &A, const Off27 &off, int *pack, int *pack_off, int cap, cudaStream_t st);
+cudaError_t halo_packed_launch(const DpdArgs &A, const int *pack, const int *pack_off, int cap, int rng_mode,
+                               cudaStream_t st);
 // vector-Jacobian product of the bulk (which & 1) and halo (which & 2) pair
 // forces, stable keys, one box
 cudaError_t dpd_vjp_launch(const DpdArgs &A, int nmax, cudaStream_t st);

@@ -257,3 +257,35 @@ def test_sim_diag_and_conservation_stable():
     assert d1[4] == len(pp)
     assert np.abs(d1[:3]).max() < 1e-3          # momentum conserved to float rounding
     assert abs(d1[3] - systems.KBT) < 0.1 * systems.KBT
+
+
+@pytest.mark.parametrize("L", [(8, 8, 8), (16, 12, 10), (6, 6, 6), (12, 12, 12)])
+def test_sim_step_forces_vs_modules(L):
+    """The fast path's bulk + halo forces of one step (the halo pairs with the
+    boundary particles packed per fragment) against the module entry points'
+    (one thread per particle, held to the reference's kernels at 1e-5):
+    same pairs and keys, so only the order of the sums differs.  (Reference
+    keys: the module entry points take AoS particles without ids.)"""
+    import ctypes
+    rng = 0
+    C = ctc()
+    from ctc_b200 import _lib
+    pp = systems.solvent(L, seed=91)
+    n = len(pp)
+    dpd = C.DpdParams(*systems.dpd_params())
+    sim = C.Sim(L, n, dpd, rng=rng)
+    sim.set_solvent(pp)
+    seeds = sim.next_seeds()
+    sim.step(1)
+    torch.cuda.synchronize()
+    fp = ctypes.c_void_p()
+    _lib.check(_lib.lib().ctc_sim_state(sim.h, None, None, ctypes.byref(fp), None))
+    f = C._wrap_dev(fp.value, 4 * n, torch.float32, torch.device("cuda")).reshape(n, 4)[:, :3].cpu().numpy()
+    out, starts, counts, ids = C.Clist(L, n).build(dev(pp))
+    ff = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    C.FluForces(L, n).apply_seeded(dpd, out, starts, counts, seeds, ff, which=3, rng=rng)
+    ref = ff.cpu().numpy()
+    fn = np.abs(ref).max(1)
+    err = np.abs(f - ref).max(1) / np.maximum(fn, 0.1 * fn.mean())
+    assert err.max() < 1e-5, err.max()
+    assert C.device_error() == 0
