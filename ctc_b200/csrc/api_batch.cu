@@ -38,6 +38,8 @@ struct ctc_batch {
     int *counts = nullptr, *starts = nullptr, *ntot_dev = nullptr, *fss = nullptr;
     void *scratch = nullptr;
     ClistScratch w{};
+    int *pack = nullptr, *pack_off = nullptr, *coff = nullptr;   // boundary particles packed per (box, fragment)
+    int pack_cap = 0, ncells_frag = 0;
     unsigned *trunk = nullptr, *ftrunk = nullptr;   // 27 per box; FSI: 1 per box
     float *seeds = nullptr, *fseeds = nullptr;      // 27 per box; FSI: 2 per box
     int cur = 0;
@@ -83,6 +85,7 @@ extern "C" int ctc_batch_destroy(ctc_batch *b) {
     cudaFree(b->force); cudaFree(b->counts); cudaFree(b->starts); cudaFree(b->ntot_dev); cudaFree(b->fss);
     cudaFree(b->scratch); cudaFree(b->trunk); cudaFree(b->ftrunk); cudaFree(b->seeds); cudaFree(b->fseeds);
     cudaFree(b->d_tab); cudaFree(b->d_L);
+    cudaFree(b->pack); cudaFree(b->pack_off); cudaFree(b->coff);
     if (b->ev_in) cudaEventDestroy(b->ev_in);
     if (b->ev_out) cudaEventDestroy(b->ev_out);
     if (b->own) cudaStreamDestroy(b->own);
@@ -152,6 +155,25 @@ extern "C" int ctc_batch_create(const ctc_batch_config *cfg, ctc_batch **pb) {
     cu(cudaMalloc(&b->ftrunk, sizeof(unsigned) * 4 * (size_t)nb), "trunks");
     cu(cudaMalloc(&b->seeds, sizeof(float) * 27 * (size_t)nb), "seeds");
     cu(cudaMalloc(&b->fseeds, sizeof(float) * 2 * (size_t)nb), "seeds");
+    {
+        // fragment cells of every box, and room for 1.5 x the uniform-density
+        // count of its boundary particles (one entry per fragment of the cell)
+        std::vector<int> coff(26 * (size_t)nb + 1, 0);
+        double entries = 0;
+        for (int k = 0; k < nb; k++) {
+            const int3 L = make_int3(cfg->L[3 * k], cfg->L[3 * k + 1], cfg->L[3 * k + 2]);
+            Off27 cf;
+            frag_cell_offsets(L, &cf);
+            for (int f = 0; f < 26; f++) coff[26 * k + f + 1] = coff[26 * k + f] + (cf.d[f + 1] - cf.d[f]);
+            entries += (double)cfg->n[k] * cf.d[26] / ((double)L.x * L.y * L.z);
+        }
+        b->ncells_frag = coff.back();
+        b->pack_cap = (int)std::min<double>((double)(1 << 30), 1.5 * entries + 4096.0);
+        cu(cudaMalloc(&b->coff, sizeof(int) * coff.size()), "pack");
+        cu(cudaMalloc(&b->pack_off, sizeof(int) * coff.size()), "pack");
+        cu(cudaMalloc(&b->pack, sizeof(int) * (size_t)b->pack_cap), "pack");
+        if (rc == CTC_OK) cu(cudaMemcpy(b->coff, coff.data(), sizeof(int) * coff.size(), cudaMemcpyHostToDevice), "pack");
+    }
     cu(cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking), "stream");
     cu(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming), "event");
     cu(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming), "event");
@@ -272,12 +294,12 @@ static int batch_step1(ctc_batch *b, cudaStream_t st) {
     A.fss = b->fss;
     A.err = dev_err_ptr();
     A.B = b->B;
-    if (b->rng == CTC_RNG_REFERENCE) CUDA_TRY(frag_starts_boxes_launch(b->B, b->counts, b->fss, st));
+    CUDA_TRY(frag_starts_boxes_launch(b->B, b->counts, b->fss, st));
+    CUDA_TRY(halo_pack_boxes_launch(A, b->coff, 26 * b->nbox, b->ncells_frag, b->pack, b->pack_off, b->pack_cap, st));
     CUDA_TRY(cudaMemsetAsync(b->force, 0, sizeof(float4) * (size_t)b->ntot, st));
     A.which = 1;
     CUDA_TRY(dpd_launch(A, b->ntot, b->rng, st, b->tune));
-    A.which = 2;
-    CUDA_TRY(dpd_launch(A, b->ntot, b->rng, st, b->tune));
+    CUDA_TRY(halo_packed_launch(A, b->pack, b->pack_off, b->pack_cap, b->rng, st, 26 * b->nbox, b->tune));
     if (nvt > 0) {
         CUDA_TRY(cudaMemsetAsync(b->mforce, 0, sizeof(float4) * (size_t)nvt, st));
         DpdPar F;
@@ -364,7 +386,7 @@ extern "C" int ctc_batch_tune(ctc_batch *b, int reps, int *choice, void *stream)
     CUDA_TRY(draw_seeds_launch(b->trunk, 27 * b->nbox, b->seeds, st));
     CUDA_TRY(clist_launch(make_int3(1, 1, 1), b->ntot, nullptr, b->pos[src], b->vel[src], 1, b->counts, b->starts,
                           b->pos[dst], b->vel[dst], nullptr, b->w, dev_err_ptr(), st, b->B, b->nctot));
-    if (b->rng == CTC_RNG_REFERENCE) CUDA_TRY(frag_starts_boxes_launch(b->B, b->counts, b->fss, st));
+    CUDA_TRY(frag_starts_boxes_launch(b->B, b->counts, b->fss, st));
     DpdArgs A;
     dpd_args_common(&A, make_int3(1, 1, 1), &b->dpd);
     A.pos = b->pos[dst]; A.vel = b->vel[dst]; A.starts = b->starts; A.counts = b->counts;
@@ -376,11 +398,16 @@ extern "C" int ctc_batch_tune(ctc_batch *b, int reps, int *choice, void *stream)
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
-    auto time_it = [&](int which, const DpdTune &t, float &ms) -> int {
+    CUDA_TRY(halo_pack_boxes_launch(A, b->coff, 26 * b->nbox, b->ncells_frag, b->pack, b->pack_off, b->pack_cap, st));
+    auto launch = [&](int which, const DpdTune &t) -> cudaError_t {
+        if (which == 2) return halo_packed_launch(A, b->pack, b->pack_off, b->pack_cap, b->rng, st, 26 * b->nbox, t);
         A.which = which;
-        CUDA_TRY(dpd_launch(A, b->ntot, b->rng, st, t));   // warm
+        return dpd_launch(A, b->ntot, b->rng, st, t);
+    };
+    auto time_it = [&](int which, const DpdTune &t, float &ms) -> int {
+        CUDA_TRY(launch(which, t));   // warm
         CUDA_TRY(cudaEventRecord(e0, st));
-        for (int r = 0; r < reps; r++) CUDA_TRY(dpd_launch(A, b->ntot, b->rng, st, t));
+        for (int r = 0; r < reps; r++) CUDA_TRY(launch(which, t));
         CUDA_TRY(cudaEventRecord(e1, st));
         CUDA_TRY(cudaEventSynchronize(e1));
         CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));

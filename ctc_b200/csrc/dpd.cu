@@ -425,26 +425,86 @@ __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs 
 }
 
 // the boundary particles packed per fragment, as the reference's exchange
-// packs them (src/exch/flu/dev/pack.h:2-40): fragment fid's particle a is
-// pack[pack_off[fid] + a]; one (fragment, particle) per thread, grid-stride,
-// so no lane idles on an interior particle or walks a fragment loop
-template <int RNG, int T>
+// packs them (src/exch/flu/dev/pack.h:2-40): segment s (fragment s % 26 of
+// box s / 26) holds pack[pack_off[s] .. pack_off[s + 1]); one (fragment,
+// particle) per thread, grid-stride, so no lane idles on an interior particle
+// or walks a fragment loop
+template <int RNG, bool BATCH, int T>
 __global__ void __launch_bounds__(T) k_dpd_halo_packed(const __grid_constant__ DpdArgs A, const int *__restrict__ pack,
-                                                       const int *__restrict__ pack_off, int cap) {
+                                                       const int *__restrict__ pack_off, int nseg, int cap) {
     __shared__ uint4 queue[T / 32][QCAP];
     float acc_a = 0.0f, acc_g = 0.0f;
-    const int total = min(__ldg(pack_off + 26), cap);
+    const int total = min(__ldg(pack_off + nseg), cap);
     for (int base = blockIdx.x * T; base < total; base += gridDim.x * T) {
         const int t = base + threadIdx.x;
         int ia = 0x7fffffff;
         unsigned only = 0;
         if (t < total) {
-            int f = 0;
-            for (int k = 1; k < 26; k++) f += __ldg(pack_off + k) <= t;
+            const int seg = box_find(pack_off, nseg, t);
             ia = __ldg(pack + t);
-            only = 1u << f;
+            only = 1u << (seg % 26);
         }
-        halo_run<RNG, false, 0>(A, ia, only, queue[threadIdx.x >> 5], acc_a, acc_g);
+        halo_run<RNG, BATCH, 0>(A, ia, only, queue[threadIdx.x >> 5], acc_a, acc_g);
+    }
+}
+
+// batched boxes: pack_off over the 26 fragments of every box (coff: prefix of
+// the segments' fragment cells), one block
+__global__ void __launch_bounds__(1024) k_halo_pack_off_boxes(Boxes B, const int *__restrict__ fss,
+                                                              const int *__restrict__ coff, int nseg,
+                                                              int *__restrict__ pack_off) {
+    __shared__ int sh[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int carry = 0;
+    for (int s0 = 0; s0 < nseg; s0 += 1024) {
+        const int s = s0 + threadIdx.x;
+        int v = 0;
+        if (s < nseg) {
+            const int b = s / 26, f = s % 26;
+            v = __ldg(fss + __ldg(B.fss_tab + 27 * b + f) + (__ldg(coff + s + 1) - __ldg(coff + s)));
+        }
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sh[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int t = sh[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            sh[lane] = t;
+        }
+        __syncthreads();
+        if (s < nseg) pack_off[s] = carry + x - v + (w > 0 ? sh[w - 1] : 0);
+        carry += sh[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) pack_off[nseg] = carry;
+}
+
+// batched boxes: one fragment cell per thread, its particles into the pack
+__global__ void k_halo_pack_boxes(Boxes B, const int *__restrict__ starts, const int *__restrict__ counts,
+                                  const int *__restrict__ fss, const int *__restrict__ coff, int nseg,
+                                  const int *__restrict__ pack_off, int cap, int *__restrict__ pack, int *err) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= __ldg(coff + nseg)) return;
+    const int seg = box_find(coff, nseg, g);
+    const int b = seg / 26, f = seg % 26, hci = g - __ldg(coff + seg);
+    const int3 L = box_L(B, b);
+    const int dx = frag_i2dx(f), dy = frag_i2dy(f), dz = frag_i2dz(f);
+    const int ex = dx == 0 ? L.x : 1, ey = dy == 0 ? L.y : 1;
+    const int cx = (dx == 1 ? L.x - 1 : 0) + hci % ex, cy = (dy == 1 ? L.y - 1 : 0) + (hci / ex) % ey,
+              cz = (dz == 1 ? L.z - 1 : 0) + hci / (ex * ey);
+    const int cell = __ldg(B.c0 + b) + cx + L.x * (cy + L.y * cz);
+    const int s0 = __ldg(starts + cell), c = __ldg(counts + cell);
+    const int base = __ldg(pack_off + seg) + __ldg(fss + __ldg(B.fss_tab + 27 * b + f) + hci);
+    for (int o = 0; o < c; o++) {
+        if (base + o < cap) pack[base + o] = s0 + o;
+        else set_error(err, DEV_CELL_OVERFLOW);
     }
 }
 
@@ -665,11 +725,40 @@ cudaError_t halo_pack_launch(const DpdArgs &A, const Off27 &off, int *pack, int 
     return cudaGetLastError();
 }
 
+cudaError_t halo_pack_boxes_launch(const DpdArgs &A, const int *coff, int nseg, int ncells_frag, int *pack,
+                                   int *pack_off, int cap, cudaStream_t st) {
+    k_halo_pack_off_boxes<<<1, 1024, 0, st>>>(A.B, A.fss, coff, nseg, pack_off);
+    if (ncells_frag > 0)
+        k_halo_pack_boxes<<<ceil_div(ncells_frag, 256), 256, 0, st>>>(A.B, A.starts, A.counts, A.fss, coff, nseg,
+                                                                      pack_off, cap, pack, A.err);
+    return cudaGetLastError();
+}
+
 cudaError_t halo_packed_launch(const DpdArgs &A, const int *pack, const int *pack_off, int cap, int rng_mode,
-                               cudaStream_t st) {
-    constexpr int T = 128, BLOCKS = 148 * 8;
-    if (rng_mode == 1) k_dpd_halo_packed<1, T><<<BLOCKS, T, 0, st>>>(A, pack, pack_off, cap);
-    else k_dpd_halo_packed<0, T><<<BLOCKS, T, 0, st>>>(A, pack, pack_off, cap);
+                               cudaStream_t st, int nseg, const DpdTune &t) {
+    constexpr int BLOCKS = 148 * 8;
+    const bool batch = A.B.nbox > 0;
+#define CTC_HALO_P(TT)                                                                                       \
+    if (t.halo_threads == TT) {                                                                              \
+        if (rng_mode == 1) {                                                                                 \
+            if (batch) k_dpd_halo_packed<1, true, TT><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);  \
+            else k_dpd_halo_packed<1, false, TT><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);       \
+        } else {                                                                                             \
+            if (batch) k_dpd_halo_packed<0, true, TT><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);  \
+            else k_dpd_halo_packed<0, false, TT><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);       \
+        }                                                                                                    \
+        return cudaGetLastError();                                                                           \
+    }
+    CTC_HALO_P(64)
+    CTC_HALO_P(256)
+#undef CTC_HALO_P
+    if (rng_mode == 1) {
+        if (batch) k_dpd_halo_packed<1, true, 128><<<BLOCKS, 128, 0, st>>>(A, pack, pack_off, nseg, cap);
+        else k_dpd_halo_packed<1, false, 128><<<BLOCKS, 128, 0, st>>>(A, pack, pack_off, nseg, cap);
+    } else {
+        if (batch) k_dpd_halo_packed<0, true, 128><<<BLOCKS, 128, 0, st>>>(A, pack, pack_off, nseg, cap);
+        else k_dpd_halo_packed<0, false, 128><<<BLOCKS, 128, 0, st>>>(A, pack, pack_off, nseg, cap);
+    }
     return cudaGetLastError();
 }
 

@@ -61,8 +61,13 @@ cudaError_t dpd_launch(const DpdArgs &A, int nmax, int rng_mode, cudaStream_t st
 // per thread.  Fragment cells per fragment: frag_cell_offsets.
 void frag_cell_offsets(int3 L, Off27 *coff);
 cudaError_t halo_pack_launch(const DpdArgs &A, const Off27 &off, int *pack, int *pack_off, int cap, cudaStream_t st);
+// batched boxes: coff [dev, 26 nbox + 1] prefix of the segments' fragment
+// cells (segment s = fragment s % 26 of box s / 26), ncells_frag its total
+cudaError_t halo_pack_boxes_launch(const DpdArgs &A, const int *coff, int nseg, int ncells_frag, int *pack,
+                                   int *pack_off, int cap, cudaStream_t st);
+// nseg = 26 (one box) or 26 nbox (A.B)
 cudaError_t halo_packed_launch(const DpdArgs &A, const int *pack, const int *pack_off, int cap, int rng_mode,
-                               cudaStream_t st);
+                               cudaStream_t st, int nseg = 26, const DpdTune &tune = DpdTune());
 // vector-Jacobian product of the bulk (which & 1) and halo (which & 2) pair
 // forces, stable keys, one box
 cudaError_t dpd_vjp_launch(const DpdArgs &A, int nmax, cudaStream_t st);
