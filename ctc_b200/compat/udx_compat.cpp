@@ -1,0 +1,211 @@
+// C++ compatibility layer: the reference's module entry points, implemented
+// on the C ABI of include/ctc_b200.h, for a uDeviceX build that links
+// libctc_b200 in place of these modules so that its callers (src/sim, the
+// u/* drivers) relink unchanged.  It is compiled inside the reference's build,
+// with the reference's headers on the include path (see Makefile here).
+//
+// Covered: the single-array cell lists (src/clist/imp.h: clist_ini / _fin /
+// _ini_map / _fin_map / clists_get_* / clist_get_ids / clist_build), the
+// bulk solvent forces (src/fluforces/imp.h: fluforces_bulk_*), the membrane
+// forces (src/rbc/force/imp.h: rbc_force_ini / _fin / _set_stressful /
+// _set_bending / _set_rnd0 / _apply) and the update (src/scheme/move/imp.h).
+// Not covered: entry points whose arguments come from the multi-rank
+// exchange (clist_subindex* / clist_build_map / clist_gather_* of the
+// redistribution, fluforces_halo_* over exchanged fragments, fsi_* over
+// wrapped object arrays); for one periodic box per GPU the whole step of
+// ctc_sim_* (or ctc_fluforces_halo_apply, ctc_fsi_apply) replaces them.
+#include <sys/types.h>
+#include <vector_types.h>
+#include <vector_functions.h>
+
+#include <mpi.h>
+
+#include "inc/def.h"
+#include "inc/type.h"
+#include "struct/partlist/type.h"
+#include "struct/parray/imp.h"
+#include "struct/farray/imp.h"
+#include "pair/type.h"
+#include "pair/imp.h"
+#include "flu/type.h"
+#include "clist/imp.h"
+#include "fluforces/imp.h"
+#include "io/mesh_read/imp.h"
+#include "rbc/type.h"
+#include "rbc/params/imp.h"
+#include "rbc/force/imp.h"
+#include "scheme/move/imp.h"
+#include "utils/error.h"
+
+#include "ctc_b200.h"
+
+#include <string.h>
+#include <vector>
+
+#define CTC(call) do { if ((call) != CTC_OK) ERR("ctc_b200: %s", ctc_last_error()); } while (0)
+
+// ---- cell lists (src/clist/imp.h) ---------------------------------------------
+struct Clist {
+    int3 L;
+    ctc_clist *h;            // created by clist_ini_map, which knows the capacity
+    int n;                   // particles of the last build
+};
+struct ClistMap {
+    Clist *c;
+};
+
+void clist_ini(int LX, int LY, int LZ, Clist **c) {
+    *c = new Clist;
+    (*c)->L = make_int3(LX, LY, LZ);
+    (*c)->h = NULL;
+    (*c)->n = 0;
+}
+
+void clist_fin(Clist *c) { delete c; }
+
+void clist_ini_map(int maxp, int nA, const Clist *c, ClistMap **m) {
+    if (nA != 1) ERR("ctc_b200 clist: only single-array maps (nA = 1), got %d", nA);
+    Clist *cc = const_cast<Clist*>(c);
+    if (cc->h) CTC(ctc_clist_fin(cc->h));
+    CTC(ctc_clist_ini(c->L.x, c->L.y, c->L.z, maxp, &cc->h));
+    *m = new ClistMap;
+    (*m)->c = cc;
+}
+
+void clist_fin_map(ClistMap *m) {
+    if (m->c->h) CTC(ctc_clist_fin(m->c->h));
+    m->c->h = NULL;
+    delete m;
+}
+
+const int *clists_get_ss(const Clist *c) {
+    const int *s = NULL;
+    CTC(ctc_clist_get(c->h, &s, NULL, NULL));
+    return s;
+}
+
+const int *clists_get_cc(const Clist *c) {
+    const int *k = NULL;
+    CTC(ctc_clist_get(c->h, NULL, &k, NULL));
+    return k;
+}
+
+int3 clists_get_dim(const Clist *c) { return c->L; }
+int clists_get_n(const Clist *c) { return c->L.x * c->L.y * c->L.z; }
+
+const uint *clist_get_ids(const ClistMap *m) {
+    const int *ids = NULL;
+    CTC(ctc_clist_get(m->c->h, NULL, NULL, &ids));
+    return reinterpret_cast<const uint*>(ids);
+}
+
+void clist_build(int nlo, int nout, const Particle *pplo, Particle *ppout, Clist *c, ClistMap *m) {
+    int kept = 0;
+    CTC(ctc_clist_build(c->h, nlo, reinterpret_cast<const float*>(pplo), reinterpret_cast<float*>(ppout), &kept,
+                        NULL));
+    if (kept != nout) ERR("clist_build: %d particles kept, %d expected", kept, nout);
+    c->n = kept;
+    (void)m;
+}
+
+// ---- bulk solvent forces (src/fluforces/imp.h) --------------------------------
+struct FluForcesBulk {
+    ctc_fluforces *h;
+    const float *pp;
+};
+
+void fluforces_bulk_ini(int3 L, int maxp, FluForcesBulk **b) {
+    *b = new FluForcesBulk;
+    CTC(ctc_fluforces_ini(L.x, L.y, L.z, maxp, &(*b)->h));
+    (*b)->pp = NULL;
+}
+
+void fluforces_bulk_fin(FluForcesBulk *b) {
+    CTC(ctc_fluforces_fin(b->h));
+    delete b;
+}
+
+void fluforces_bulk_prepare(int n, const PaArray *a, FluForcesBulk *b) {
+    if (a->colors) ERR("ctc_b200: coloured solvent is not supported");
+    b->pp = a->pp;            // the cell-sorted Particle array
+    (void)n;
+}
+
+void fluforces_bulk_apply(const PairParams *par, int n, const FluForcesBulk *b, const int *start, const int *count,
+                          const FoArray *ff) {
+    if (ff->stress) ERR("ctc_b200: stresses are not supported");
+    PairDPD p;
+    pair_get_view_dpd(par, &p);
+    const ctc_dpd_params q = {p.a, p.g, p.s, p.spow};
+    CTC(ctc_fluforces_bulk_apply(b->h, &q, n, b->pp, start, count, ff->ff, NULL));
+}
+
+// ---- membrane forces (src/rbc/force/imp.h) ------------------------------------
+struct RbcForce {
+    ctc_rbc_force *h;
+    int nv, nt, cap, kantor;
+    std::vector<int> tri;
+    float totArea;           // stress-ful: the area of the template
+};
+
+void rbc_force_ini(const MeshRead *mesh, RbcForce **f) {
+    const int nt = mesh_read_get_nt(mesh), nv = mesh_read_get_nv(mesh);
+    const int4 *tt = mesh_read_get_tri(mesh);
+    std::vector<int> tri(3 * (size_t)nt);
+    for (int t = 0; t < nt; t++) { tri[3 * t] = tt[t].x; tri[3 * t + 1] = tt[t].y; tri[3 * t + 2] = tt[t].z; }
+    *f = new RbcForce;
+    CTC(ctc_rbc_force_ini(nv, nt, tri.data(), 1, &(*f)->h));
+    (*f)->nv = nv;
+    (*f)->nt = nt;
+    (*f)->cap = 1;
+    (*f)->kantor = 1;
+    (*f)->tri = tri;
+    (*f)->totArea = 0;
+}
+
+void rbc_force_fin(RbcForce *f) {
+    CTC(ctc_rbc_force_fin(f->h));
+    delete f;
+}
+
+void rbc_force_set_stressful(int nt, float totArea, RbcForce *f) {
+    f->nt = nt;
+    f->totArea = totArea;
+}
+
+void rbc_force_set_rnd0(RbcForce *f) { (void)f; }
+
+void rbc_force_set_bending(const MeshRead *mesh, const char *name, RbcForce *f) {
+    (void)mesh;
+    if (!strcmp(name, "kantor")) f->kantor = 1;
+    else if (!strcmp(name, "none")) f->kantor = 0;
+    else ERR("ctc_b200: bending \"%s\" is not supported (kantor, none)", name);
+    CTC(ctc_rbc_force_set_bending(f->h, f->kantor));
+}
+
+void rbc_force_apply(RbcForce *f, const RbcParams *par, float dt, const RbcQuants *q, Force *ff) {
+    const RbcParams_v v = rbc_params_get_view(par);
+    const ctc_rbc_params p = {v.gammaC, v.gammaT, v.kBT, v.kb, v.phi, v.ks, v.x0, v.mpow, v.ka, v.kd, v.kv,
+                              v.totArea, v.totVolume};
+    // the reference's stress-ful lengths use set_stressful's area; the C ABI
+    // takes them from the parameters' total area
+    if (f->totArea != 0 && f->totArea != v.totArea)
+        ERR("ctc_b200: set_stressful area %g differs from the parameters' %g", f->totArea, v.totArea);
+    if (q->nc > f->cap) {     // per-cell scratch for more cells: rebuild the module
+        CTC(ctc_rbc_force_fin(f->h));
+        CTC(ctc_rbc_force_ini(f->nv, f->nt, f->tri.data(), q->nc, &f->h));
+        CTC(ctc_rbc_force_set_bending(f->h, f->kantor));
+        f->cap = q->nc;
+    }
+    CTC(ctc_rbc_force_apply(f->h, &p, dt, q->nc, reinterpret_cast<const float*>(q->pp), reinterpret_cast<float*>(ff),
+                            NULL));
+}
+
+// ---- update (src/scheme/move/imp.h) -------------------------------------------
+void scheme_move_apply(float dt, float mass, int n, const Force *ff, Particle *pp) {
+    CTC(ctc_scheme_move_apply(dt, mass, n, reinterpret_cast<const float*>(ff), reinterpret_cast<float*>(pp), NULL));
+}
+
+void scheme_move_clear_vel(int n, Particle *pp) {
+    CTC(ctc_scheme_move_clear_vel(n, reinterpret_cast<float*>(pp), NULL));
+}

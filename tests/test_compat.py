@@ -1,0 +1,49 @@
+"""The C++ compatibility layer (ctc_b200/compat/udx_compat.cpp) defines the
+reference's module entry points with the reference's own signatures: the
+object compiled against the reference's headers (by __graft_entry__.build()
+where the reference tree is present) must export exactly these symbols."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+OBJ = os.path.join(ROOT, "ctc_b200", "compat", "_build", "udx_compat.o")
+
+# the declarations of src/clist/imp.h, src/fluforces/imp.h (bulk),
+# src/rbc/force/imp.h and src/scheme/move/imp.h, as the C++ compiler names them
+EXPECTED = [
+    "clist_ini(int, int, int, Clist**)",
+    "clist_fin(Clist*)",
+    "clist_ini_map(int, int, Clist const*, ClistMap**)",
+    "clist_fin_map(ClistMap*)",
+    "clists_get_ss(Clist const*)",
+    "clists_get_cc(Clist const*)",
+    "clists_get_dim(Clist const*)",
+    "clists_get_n(Clist const*)",
+    "clist_get_ids(ClistMap const*)",
+    "clist_build(int, int, Particle const*, Particle*, Clist*, ClistMap*)",
+    "fluforces_bulk_ini(int3, int, FluForcesBulk**)",
+    "fluforces_bulk_fin(FluForcesBulk*)",
+    "fluforces_bulk_prepare(int, PaArray const*, FluForcesBulk*)",
+    "fluforces_bulk_apply(PairParams const*, int, FluForcesBulk const*, int const*, int const*, FoArray const*)",
+    "rbc_force_ini(MeshRead const*, RbcForce**)",
+    "rbc_force_fin(RbcForce*)",
+    "rbc_force_set_stressful(int, float, RbcForce*)",
+    "rbc_force_set_rnd0(RbcForce*)",
+    "rbc_force_set_bending(MeshRead const*, char const*, RbcForce*)",
+    "rbc_force_apply(RbcForce*, RbcParams const*, float, RbcQuants const*, Force*)",
+    "scheme_move_apply(float, float, int, Force const*, Particle*)",
+    "scheme_move_clear_vel(int, Particle*)",
+]
+
+
+@pytest.mark.skipif(not os.path.exists(OBJ), reason="compatibility layer not built (needs the reference's headers)")
+def test_compat_layer_exports_reference_signatures():
+    nm = shutil.which("nm")
+    assert nm
+    out = subprocess.run([nm, "-C", "--defined-only", OBJ], capture_output=True, text=True, check=True).stdout
+    defined = {line.split(" ", 2)[2] for line in out.splitlines() if " T " in line}
+    missing = [s for s in EXPECTED if s not in defined]
+    assert not missing, missing
