@@ -206,6 +206,156 @@ __global__ void k_fsi(const __grid_constant__ FsiArgs A) {
     o[2] += fz;
 }
 
+// Forces with the accepted pairs compacted through a per-warp queue and
+// evaluated 32 at a time (one thread per vertex walks its 27 cells; the pair
+// evaluation, 18 RNG rounds and the force, runs with every lane busy): the
+// same pairs, keys and force expressions as k_fsi.  Vertex and solvent
+// forces are accumulated with global reductions.
+constexpr int FSIQ_T = 128, FSIQ_CAP = 64;
+
+__device__ __forceinline__ void red3(float *out, int stride, int i, float s, float3 f) {
+    if (stride == 4) {
+        atomicAdd((float4*)out + i, make_float4(s * f.x, s * f.y, s * f.z, 0.0f));
+        return;
+    }
+    float *o = out + (size_t)stride * i;
+    atomicAdd(o + 0, s * f.x);
+    atomicAdd(o + 1, s * f.y);
+    atomicAdd(o + 2, s * f.z);
+}
+
+template <int RNG>
+__global__ void __launch_bounds__(FSIQ_T) k_fsi_q(const __grid_constant__ FsiArgs A) {
+    __shared__ uint4 queue[FSIQ_T / 32][FSIQ_CAP];
+    const int lane = threadIdx.x & 31;
+    uint4 *q = queue[threadIdx.x >> 5];
+    int qn = 0;
+    const int i = blockIdx.x * FSIQ_T + threadIdx.x;
+    const bool act = i < A.nv;
+    const DpdPar P = A.par;
+
+    // per record: vertex i | halo bit << 31, solvent j, halo key index aid, fid
+    auto process = [&](int m) {
+        if (lane < m) {
+            const uint4 rec = q[lane];
+            const int v = (int)(rec.x & 0x7fffffffu), j = (int)rec.y, fid = (int)rec.w;
+            const bool halo = rec.x >> 31;
+            const float *pq = A.pv + (size_t)A.pstride * v, *pqv = A.vv + (size_t)A.pstride * v;
+            float4 a = make_float4(pq[0], pq[1], pq[2], 0.0f);
+            const float4 va = make_float4(pqv[0], pqv[1], pqv[2], 0.0f);
+            int3 L = A.L;
+            const float *seeds = A.seeds_dev;
+            int vk = v, sk = 0;
+            if (A.B.nbox > 0) {
+                const int box = box_find(A.B.v0, A.B.nbox, v);
+                L = box_L(A.B, box);
+                seeds += 2 * box;
+                vk = v - __ldg(A.B.v0 + box);
+                sk = __ldg(A.B.p0 + box);
+            }
+            const float seed_bulk = seeds ? seeds[0] : A.seed_bulk;
+            const float seed_halo = seeds ? seeds[1] : A.seed_halo;
+            if (halo) {   // the vertex seen from the image side of a periodic face
+                a.x = a.x + (float)(-frag_i2dx(fid) * L.x);
+                a.y = a.y + (float)(-frag_i2dy(fid) * L.y);
+                a.z = a.z + (float)(-frag_i2dz(fid) * L.z);
+            }
+            const float4 b = __ldg(A.spos + j);
+            float rnd;
+            if (RNG == 0) rnd = mean0var1uu(halo ? seed_halo : seed_bulk, halo ? rec.z : (unsigned)vk, (unsigned)(j - sk));
+            else rnd = mean0var1uu(seed_bulk, (unsigned)vk, (unsigned)__float_as_int(b.w));
+            float3 f;
+            if (dpd_force(P, a, va, b, __ldg(A.svel + j), rnd, f)) {
+                red3(A.fv, A.fstride, v, 1.0f, f);
+                red3(A.fs, A.sstride, j, -1.0f, f);
+            }
+        }
+        __syncwarp();
+    };
+    auto push = [&](bool ok, uint4 rec) {
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) q[qn + __popc(bal & ((1u << lane) - 1u))] = rec;
+        qn += __popc(bal);
+        __syncwarp();
+        if (qn >= 32) {
+            process(32);
+            qn -= 32;
+            if (lane < qn) q[lane] = q[32 + lane];
+            __syncwarp();
+        }
+    };
+
+    float4 pa = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    int3 L = A.L;
+    const int *starts = A.starts, *counts = A.counts, *img_start = A.img_start;
+    int vk = i;
+    if (act) {
+        const float *pq = A.pv + (size_t)A.pstride * i;
+        pa = make_float4(pq[0], pq[1], pq[2], 0.0f);
+        if (A.B.nbox > 0) {
+            const int box = box_find(A.B.v0, A.B.nbox, i);
+            L = box_L(A.B, box);
+            const int c0 = __ldg(A.B.c0 + box);
+            starts += c0;
+            counts += c0;
+            img_start += 26 * box;
+            vk = i - __ldg(A.B.v0 + box);
+        }
+    }
+    // the vertex cell as src/fsi/dev/map/bulk.h:13-21 (floorf, may lie outside the box)
+    const int cx = L.x / 2 + (int)floorf(pa.x), cy = L.y / 2 + (int)floorf(pa.y), cz = L.z / 2 + (int)floorf(pa.z);
+    int ci = 0, j = 0, e = 0, fid = 0;
+    unsigned aid = 0;
+    bool halo = false;
+    float4 a = pa;
+    constexpr int U = 4;
+    for (;;) {
+        if (act) {
+            while (j >= e && ci < 27) {
+                const int dx = ci % 3 - 1, dy = (ci / 3) % 3 - 1, dz = ci / 9 - 1;
+                ci++;
+                int gx = cx + dx, gy = cy + dy, gz = cz + dz;
+                const int wx = gx < 0 ? -1 : (gx >= L.x ? 1 : 0);
+                const int wy = gy < 0 ? -1 : (gy >= L.y ? 1 : 0);
+                const int wz = gz < 0 ? -1 : (gz >= L.z ? 1 : 0);
+                gx -= wx * L.x; gy -= wy * L.y; gz -= wz * L.z;
+                if (gx < 0 || gx >= L.x || gy < 0 || gy >= L.y || gz < 0 || gz >= L.z) continue;
+                const int cid = gx + L.x * (gy + L.y * gz);
+                j = __ldg(starts + cid);
+                e = j + __ldg(counts + cid);
+                halo = (wx | wy | wz) != 0;
+                a = pa;
+                aid = (unsigned)vk;
+                fid = 0;
+                if (halo) {
+                    fid = frag_d2i(wx, wy, wz);
+                    if (RNG == 0) {
+                        const int r = __ldg(A.img_rank + (size_t)fid * A.nv + i);
+                        if (r < 0) { set_error(A.err, DEV_BAD_PARTICLE); j = e; continue; }
+                        aid = (unsigned)(__ldg(img_start + fid) + r);
+                    }
+                    a.x = a.x + (float)(-wx * L.x);
+                    a.y = a.y + (float)(-wy * L.y);
+                    a.z = a.z + (float)(-wz * L.z);
+                }
+            }
+        }
+        const bool have = act && j < e;
+        if (!__any_sync(0xffffffffu, have)) break;
+        float4 b[U];
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (have && j + u < e) b[u] = __ldg(A.spos + j + u);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool ok = have && j + u < e && dist2(a.x - b[u].x, a.y - b[u].y, a.z - b[u].z) < 1.0f;
+            push(ok, make_uint4((unsigned)i | (halo ? 0x80000000u : 0u), (unsigned)(j + u), aid, (unsigned)fid));
+        }
+        if (have) j = min(j + U, e);
+    }
+    if (qn > 0) process(qn);
+}
+
 cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsigned *mask, int *rank, int *count,
                               int *img_start, cudaStream_t st, const Boxes &B) {
     if (nv <= 0) return cudaSuccess;
@@ -223,8 +373,8 @@ cudaError_t fsi_vjp_launch(const FsiArgs &A, cudaStream_t st) {
 
 cudaError_t fsi_launch(const FsiArgs &A, int rng, cudaStream_t st) {
     if (A.nv <= 0) return cudaSuccess;
-    if (rng == 1) k_fsi<1><<<ceil_div(A.nv, 128), 128, 0, st>>>(A);
-    else k_fsi<0><<<ceil_div(A.nv, 128), 128, 0, st>>>(A);
+    if (rng == 1) k_fsi_q<1><<<ceil_div(A.nv, FSIQ_T), FSIQ_T, 0, st>>>(A);
+    else k_fsi_q<0><<<ceil_div(A.nv, FSIQ_T), FSIQ_T, 0, st>>>(A);
     return cudaGetLastError();
 }
 
