@@ -232,8 +232,9 @@ __device__ __forceinline__ void r2size_dev(float r, int nc, int S, int &l, int &
 // the halo pairs of local particle ia (none if ia >= the particle count) for
 // the fragments of its cell that are also in `only`, through the warp's queue q
 template <int RNG, bool BATCH, int MODE>
-__device__ __forceinline__ void halo_run(const DpdArgs &A, const int ia, const unsigned only, uint4 *q, float &acc_a,
-                                         float &acc_g) {
+// (packed: aid_known >= 0 is ia's index in fragment `only`, which holds its cell)
+__device__ __forceinline__ void halo_run(const DpdArgs &A, const int ia, const unsigned only, const int aid_known,
+                                         uint4 *q, float &acc_a, float &acc_g) {
     const int lane = threadIdx.x & 31;
     int3 L = A.L;
     const int *starts = A.starts, *counts = A.counts;
@@ -261,7 +262,10 @@ __device__ __forceinline__ void halo_run(const DpdArgs &A, const int ia, const u
     float4 pa = make_float4(0, 0, 0, 0);
     int gx = 0, gy = 0, gz = 0, gcell = 0;
     unsigned frags = 0;
-    if (act) {
+    if (act && aid_known >= 0) {
+        pa = __ldg(A.pos + ia);
+        frags = only;
+    } else if (act) {
         pa = __ldg(A.pos + ia);
         gx = (int)((double)pa.x + (double)(L.x / 2));
         gy = (int)((double)pa.y + (double)(L.y / 2));
@@ -369,7 +373,8 @@ __device__ __forceinline__ void halo_run(const DpdArgs &A, const int ia, const u
                     left &= left - 1;
                     anti = frag_anti(fid);
                     const int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
-                    aid = frag_index(L, A.fss + fss_off[fid], fid, gcell, ia - __ldg(starts + gcell));
+                    aid = aid_known >= 0 ? aid_known
+                                         : frag_index(L, A.fss + fss_off[fid], fid, gcell, ia - __ldg(starts + gcell));
                     // r2map (src/fluforces/halo/dev/map.h:102-129) on the unshifted position
                     const int xc = dx == 0 ? L.x : 1, yc = dy == 0 ? L.y : 1;
                     int xs = 1, ys = 1, zs = 1, l;
@@ -420,7 +425,8 @@ template <int RNG, bool BATCH, int T, int MODE = 0>
 __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs A) {
     __shared__ uint4 queue[T / 32][QCAP];
     float acc_a = 0.0f, acc_g = 0.0f;               // MODE 1: parameter cotangents
-    halo_run<RNG, BATCH, MODE>(A, blockIdx.x * T + threadIdx.x, 0xffffffffu, queue[threadIdx.x >> 5], acc_a, acc_g);
+    halo_run<RNG, BATCH, MODE>(A, blockIdx.x * T + threadIdx.x, 0xffffffffu, -1, queue[threadIdx.x >> 5], acc_a,
+                               acc_g);
     if constexpr (MODE == 1) vjp_par(A, acc_a, acc_g);
 }
 
@@ -437,14 +443,15 @@ __global__ void __launch_bounds__(T) k_dpd_halo_packed(const __grid_constant__ D
     const int total = min(__ldg(pack_off + nseg), cap);
     for (int base = blockIdx.x * T; base < total; base += gridDim.x * T) {
         const int t = base + threadIdx.x;
-        int ia = 0x7fffffff;
+        int ia = 0x7fffffff, aid = 0;
         unsigned only = 0;
         if (t < total) {
             const int seg = box_find(pack_off, nseg, t);
             ia = __ldg(pack + t);
             only = 1u << (seg % 26);
+            aid = t - __ldg(pack_off + seg);        // the index inside the fragment
         }
-        halo_run<RNG, BATCH, 0>(A, ia, only, queue[threadIdx.x >> 5], acc_a, acc_g);
+        halo_run<RNG, BATCH, 0>(A, ia, only, aid, queue[threadIdx.x >> 5], acc_a, acc_g);
     }
 }
 
