@@ -86,3 +86,33 @@ def test_dpd_forces_reference_kernels(L, which):
     C.FluForces(L, len(ps)).apply_seeded(C.DpdParams(*dpd), P, S, N, seeds, ours, which=which)
     e = _errs(ours.cpu().numpy(), ref.cpu().numpy())
     assert e.max() < 1e-5, (e.max(), np.quantile(e, 0.999))
+
+
+def test_bulk_kernel_faster_than_reference_kernel():
+    """Speed bar: the bulk pair forces of a 64^3 box (2.6 M particles) on the
+    same sorted particles, against the reference's own bulk kernel built for
+    sm_100a (median of 5 timed launches each, CUDA events)."""
+    import ctc_b200 as C
+    L = (64, 64, 64)
+    ps, starts, counts = _sorted(L, 13)
+    dpd = systems.dpd_params()
+    seeds = np.random.default_rng(14).random(27).astype(np.float32)
+    P, S, N = dev(ps), dev(starts), dev(counts)
+    out = torch.zeros((len(ps), 3), device="cuda")
+    ff = C.FluForces(L, len(ps))
+
+    def timed(fn):
+        ts = []
+        for _ in range(6):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts[1:]))
+
+    t_ref = timed(lambda: refkern.bulk(dpd, L, P, S, seeds[0], out))
+    t_ours = timed(lambda: ff.apply_seeded(C.DpdParams(*dpd), P, S, N, seeds, out, which=1))
+    print("bulk 64^3: reference kernel %.3f ms, this build %.3f ms" % (t_ref, t_ours))
+    assert t_ours < t_ref, (t_ours, t_ref)
