@@ -441,7 +441,8 @@ def run_batch(args, cfg, world, rank, local):
                    "membrane_vertices": nvt, "cells_with_rbc": int(cells.sum()),
                    "edges": [int(L[:, 0].min()), int(L[:, 0].max())],
                    "parallelism": "replicas" if world > 1 else "1 GPU",
-                   "tuned_shape": {"bulk_threads": tune[0], "bulk_unroll": tune[1], "halo_threads": tune[2]},
+                   "tuned_shape": {"bulk_threads": tune[0], "bulk_unroll": tune[1], "halo_threads": tune[2],
+                                   "halo_unroll": tune[3]},
                    "graph": True, "l2": "inputs larger than L2 (%.2f GB of state)" % (32e-9 * ntot)},
         # seeds, 6 cell-list kernels, cell wrap, FSI seeds, fragment starts, 2 halo packing kernels, bulk,
         # halo, 3 image-list kernels, FSI, update, area/volume, membrane forces, vertex update: each once

@@ -355,13 +355,15 @@ class Batch:
 
     def tune(self, reps=3, stream=None):
         """Autotune the pair kernels' launch shapes on the current state;
-        returns (bulk threads, bulk unroll, halo threads)."""
-        ch = (C.c_int * 3)()
+        returns (bulk threads, bulk unroll, halo threads, halo unroll)."""
+        ch = (C.c_int * 4)()
         check(lib().ctc_batch_tune(self.h, int(reps), ch, _stream(stream)))
         return tuple(ch)
 
     def set_tune(self, choice):
-        ch = (C.c_int * 3)(*choice)
+        """(bulk threads, bulk unroll, halo threads[, halo unroll = 2])."""
+        choice = tuple(choice) + (2,) * (4 - len(choice))
+        ch = (C.c_int * 4)(*choice)
         check(lib().ctc_batch_set_tune(self.h, ch))
 
     def get_solvent(self, stream=None):

@@ -426,34 +426,40 @@ extern "C" int ctc_batch_tune(ctc_batch *b, int reps, int *choice, void *stream)
             if (!rc && ms < best_ms) { best_ms = ms; best.bulk_threads = t.bulk_threads; best.bulk_unroll = t.bulk_unroll; }
         }
     best_ms = 1e30f;
-    for (int hi = 0; hi < 3 && !rc; hi++) {
-        DpdTune t = best;
-        t.halo_threads = DPD_TUNE_HALO_T[hi];
-        float ms = 0;
-        rc = time_it(2, t, ms);
-        if (!rc && ms < best_ms) { best_ms = ms; best.halo_threads = t.halo_threads; }
-    }
+    for (int hi = 0; hi < 3 && !rc; hi++)
+        for (int ui = 0; ui < 2 && !rc; ui++) {
+            DpdTune t = best;
+            t.halo_threads = DPD_TUNE_HALO_T[hi];
+            t.halo_unroll = DPD_TUNE_HALO_U[ui];
+            float ms = 0;
+            rc = time_it(2, t, ms);
+            if (!rc && ms < best_ms) { best_ms = ms; best.halo_threads = t.halo_threads; best.halo_unroll = t.halo_unroll; }
+        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
     CUDA_TRY(cudaMemcpy(b->trunk, keep.data(), sizeof(unsigned) * keep.size(), cudaMemcpyHostToDevice));
     if (best.bulk_threads != b->tune.bulk_threads || best.bulk_unroll != b->tune.bulk_unroll ||
-        best.halo_threads != b->tune.halo_threads)
+        best.halo_threads != b->tune.halo_threads || best.halo_unroll != b->tune.halo_unroll)
         drop_graphs(b);
     b->tune = best;
-    if (choice) { choice[0] = best.bulk_threads; choice[1] = best.bulk_unroll; choice[2] = best.halo_threads; }
+    if (choice) {
+        choice[0] = best.bulk_threads; choice[1] = best.bulk_unroll;
+        choice[2] = best.halo_threads; choice[3] = best.halo_unroll;
+    }
     return CTC_OK;
 }
 
 extern "C" int ctc_batch_set_tune(ctc_batch *b, const int *choice) {
     if (!b || !choice) return fail(CTC_ERR_ARG, "ctc_batch_set_tune: bad arguments");
     DpdTune t;
-    t.bulk_threads = choice[0]; t.bulk_unroll = choice[1]; t.halo_threads = choice[2];
-    bool ok_t = false, ok_u = false, ok_h = false;
+    t.bulk_threads = choice[0]; t.bulk_unroll = choice[1]; t.halo_threads = choice[2]; t.halo_unroll = choice[3];
+    bool ok_t = false, ok_u = false, ok_h = false, ok_hu = false;
     for (int v : DPD_TUNE_BULK_T) ok_t |= v == t.bulk_threads;
     for (int v : DPD_TUNE_BULK_U) ok_u |= v == t.bulk_unroll;
     for (int v : DPD_TUNE_HALO_T) ok_h |= v == t.halo_threads;
-    if (!ok_t || !ok_u || !ok_h) return fail(CTC_ERR_ARG, "ctc_batch_set_tune: unknown launch shape");
+    for (int v : DPD_TUNE_HALO_U) ok_hu |= v == t.halo_unroll;
+    if (!ok_t || !ok_u || !ok_h || !ok_hu) return fail(CTC_ERR_ARG, "ctc_batch_set_tune: unknown launch shape");
     drop_graphs(b);
     b->tune = t;
     return CTC_OK;

@@ -231,8 +231,9 @@ __device__ __forceinline__ void r2size_dev(float r, int nc, int S, int &l, int &
 
 // the halo pairs of local particle ia (none if ia >= the particle count) for
 // the fragments of its cell that are also in `only`, through the warp's queue q
-template <int RNG, bool BATCH, int MODE>
-// (packed: aid_known >= 0 is ia's index in fragment `only`, which holds its cell)
+// (packed: aid_known >= 0 is ia's index in fragment `only`, which holds its
+// cell); HU candidate loads in flight per lane
+template <int RNG, bool BATCH, int MODE, int HU = 2>
 __device__ __forceinline__ void halo_run(const DpdArgs &A, const int ia, const unsigned only, const int aid_known,
                                          uint4 *q, float &acc_a, float &acc_g) {
     const int lane = threadIdx.x & 31;
@@ -406,16 +407,19 @@ __device__ __forceinline__ void halo_run(const DpdArgs &A, const int ia, const u
         }
         have = act && ib < be;
         if (!__any_sync(0xffffffffu, have)) break;
-        bool ok = false;
-        uint4 rec = make_uint4(0, 0, 0, 0);
-        if (have) {
-            const float4 pb = __ldg(A.pos + ib);
-            ok = dist2((pa.x - sx) - pb.x, (pa.y - sy) - pb.y, (pa.z - sz) - pb.z) < 1.0f;
-            rec = make_uint4((unsigned)ia | ((unsigned)fid << 27), (unsigned)ib, (unsigned)aid,
-                             (unsigned)(ib + bid0));
-            ib++;
+        // the next HU candidates of the cell at once (independent loads in flight)
+        float4 pb[HU];
+#pragma unroll
+        for (int u = 0; u < HU; u++)
+            if (have && ib + u < be) pb[u] = __ldg(A.pos + ib + u);
+#pragma unroll
+        for (int u = 0; u < HU; u++) {
+            const bool ok = have && ib + u < be &&
+                            dist2((pa.x - sx) - pb[u].x, (pa.y - sy) - pb[u].y, (pa.z - sz) - pb[u].z) < 1.0f;
+            push(ok, make_uint4((unsigned)ia | ((unsigned)fid << 27), (unsigned)(ib + u), (unsigned)aid,
+                                (unsigned)(ib + u + bid0)));
         }
-        push(ok, rec);
+        if (have) ib = min(ib + HU, be);
     }
     if (qn > 0) process(qn);
 }
@@ -435,7 +439,7 @@ __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs 
 // box s / 26) holds pack[pack_off[s] .. pack_off[s + 1]); one (fragment,
 // particle) per thread, grid-stride, so no lane idles on an interior particle
 // or walks a fragment loop
-template <int RNG, bool BATCH, int T>
+template <int RNG, bool BATCH, int T, int HU>
 __global__ void __launch_bounds__(T) k_dpd_halo_packed(const __grid_constant__ DpdArgs A, const int *__restrict__ pack,
                                                        const int *__restrict__ pack_off, int nseg, int cap) {
     __shared__ uint4 queue[T / 32][QCAP];
@@ -451,7 +455,7 @@ __global__ void __launch_bounds__(T) k_dpd_halo_packed(const __grid_constant__ D
             only = 1u << (seg % 26);
             aid = t - __ldg(pack_off + seg);        // the index inside the fragment
         }
-        halo_run<RNG, BATCH, 0>(A, ia, only, aid, queue[threadIdx.x >> 5], acc_a, acc_g);
+        halo_run<RNG, BATCH, 0, HU>(A, ia, only, aid, queue[threadIdx.x >> 5], acc_a, acc_g);
     }
 }
 
@@ -745,28 +749,21 @@ cudaError_t halo_packed_launch(const DpdArgs &A, const int *pack, const int *pac
                                cudaStream_t st, int nseg, const DpdTune &t) {
     constexpr int BLOCKS = 148 * 8;
     const bool batch = A.B.nbox > 0;
-#define CTC_HALO_P(TT)                                                                                       \
-    if (t.halo_threads == TT) {                                                                              \
-        if (rng_mode == 1) {                                                                                 \
-            if (batch) k_dpd_halo_packed<1, true, TT><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);  \
-            else k_dpd_halo_packed<1, false, TT><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);       \
-        } else {                                                                                             \
-            if (batch) k_dpd_halo_packed<0, true, TT><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);  \
-            else k_dpd_halo_packed<0, false, TT><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);       \
-        }                                                                                                    \
-        return cudaGetLastError();                                                                           \
+#define CTC_HALO_P(TT, UU)                                                                                        \
+    if (t.halo_threads == TT && t.halo_unroll == UU) {                                                            \
+        if (rng_mode == 1) {                                                                                      \
+            if (batch) k_dpd_halo_packed<1, true, TT, UU><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);   \
+            else k_dpd_halo_packed<1, false, TT, UU><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);        \
+        } else {                                                                                                  \
+            if (batch) k_dpd_halo_packed<0, true, TT, UU><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);   \
+            else k_dpd_halo_packed<0, false, TT, UU><<<BLOCKS, TT, 0, st>>>(A, pack, pack_off, nseg, cap);        \
+        }                                                                                                         \
+        return cudaGetLastError();                                                                                \
     }
-    CTC_HALO_P(64)
-    CTC_HALO_P(256)
+    CTC_HALO_P(64, 2) CTC_HALO_P(128, 2) CTC_HALO_P(256, 2)
+    CTC_HALO_P(64, 4) CTC_HALO_P(128, 4) CTC_HALO_P(256, 4)
 #undef CTC_HALO_P
-    if (rng_mode == 1) {
-        if (batch) k_dpd_halo_packed<1, true, 128><<<BLOCKS, 128, 0, st>>>(A, pack, pack_off, nseg, cap);
-        else k_dpd_halo_packed<1, false, 128><<<BLOCKS, 128, 0, st>>>(A, pack, pack_off, nseg, cap);
-    } else {
-        if (batch) k_dpd_halo_packed<0, true, 128><<<BLOCKS, 128, 0, st>>>(A, pack, pack_off, nseg, cap);
-        else k_dpd_halo_packed<0, false, 128><<<BLOCKS, 128, 0, st>>>(A, pack, pack_off, nseg, cap);
-    }
-    return cudaGetLastError();
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t dpd_vjp_launch(const DpdArgs &A, int nmax, cudaStream_t st) {

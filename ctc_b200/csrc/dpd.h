@@ -42,10 +42,12 @@ struct DpdTune {
     int bulk_threads = 256;   // 128 or 256
     int bulk_unroll = 4;      // candidate loads in flight per lane: 2, 4 or 8
     int halo_threads = 128;   // 64, 128 or 256
+    int halo_unroll = 2;      // halo candidate loads in flight per lane: 2 or 4
 };
 constexpr int DPD_TUNE_BULK_T[2] = {128, 256};
 constexpr int DPD_TUNE_BULK_U[3] = {2, 4, 8};
 constexpr int DPD_TUNE_HALO_T[3] = {64, 128, 256};
+constexpr int DPD_TUNE_HALO_U[2] = {2, 4};
 
 void frag_offsets(int3 L, Off27 *off);
 unsigned halo_masks();

@@ -264,10 +264,11 @@ int ctc_batch_step(ctc_batch *b, int nsteps, void *stream);
  * buffer) on the object's own stream, ordered after the caller's stream work
  * and before its later work; 0: direct launches */
 int ctc_batch_set_graph(ctc_batch *b, int enable);
-/* autotuner: times every launch shape of the bulk (threads x candidate loads
- * in flight) and halo (threads) pair kernels reps times on the current state
- * without advancing it, keeps the fastest; choice [host, 3] = bulk threads,
- * bulk unroll, halo threads (may be NULL) */
+/* autotuner: times every launch shape of the bulk and halo pair kernels
+ * (threads x candidate loads in flight) reps times on the current state
+ * without advancing it, keeps the fastest; choice [host, 4] = bulk threads
+ * (128, 256), bulk unroll (2, 4, 8), halo threads (64, 128, 256), halo unroll
+ * (2, 4) (may be NULL) */
 int ctc_batch_tune(ctc_batch *b, int reps, int *choice, void *stream);
 int ctc_batch_set_tune(ctc_batch *b, const int *choice);
 /* state [host, AoS]: solvent box after box (cell-sorted within a box),

@@ -93,7 +93,7 @@ def test_batch_tune_leaves_state():
     for tune in (False, True):
         b = _new_batch(L, solv, cells, mem, tri, par, dpd, fsi, (0, 0, 0))
         if tune:
-            assert len(b.tune(reps=1)) == 3
+            assert len(b.tune(reps=1)) == 4
         b.step(1)
         out.append((b.get_solvent(), b.get_membranes()))
         b.close()
@@ -109,7 +109,7 @@ def test_batch_launch_shapes_agree():
     L, solv, cells, mem, tri, par = _boxes(seed=13)
     dpd = systems.dpd_params()
     ref = None
-    for shape in [(256, 4, 128), (128, 2, 64), (128, 8, 256), (256, 8, 64)]:
+    for shape in [(256, 4, 128, 2), (128, 2, 64, 4), (128, 8, 256, 2), (256, 8, 64, 4), (256, 2, 128, 4)]:
         b = C.Batch(L, [len(p) for p in solv], C.DpdParams(*dpd), dt=systems.DT)
         b.set_solvent(np.concatenate(solv))
         b.set_tune(shape)

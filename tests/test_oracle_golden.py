@@ -43,6 +43,23 @@ def _read_pa(line):
     return [float(v) for v in t[:6]], t[6], t[7]
 
 
+def test_halo_trunks_pairwise():
+    """Known answer of the halo trunk seeding (src/fluforces/imp/ini.h:22-59
+    on a 1-rank periodic cart): fragment f and its anti-fragment start from
+    the same KISS state, so both sides of a pair across a face draw the same
+    random number -- except the edges (-1, 0, 1) and (1, 0, -1), whose
+    "plus" rule picks opposite signs (seeds 21 and 5): pairs across that edge
+    get a different random force on each side, so the halo pairs cannot be
+    evaluated once per pair with the reaction given to the other side."""
+    odd = []
+    for f in range(26):
+        a = oracle.frag_anti(f)
+        kf, ka = oracle.Kiss.halo(f), oracle.Kiss.halo(a)
+        if any(kf.get() != ka.get() for _ in range(4)):
+            odd.append(oracle.frag_dir(f))
+    assert sorted(odd) == [(-1, 0, 1), (1, 0, -1)]
+
+
 def test_pair_0():
     """src/test/pair/0: pairs of src/data/pair/2 with a = 2.6666667, g = 8,
     spow = 0.25 and RND unset (0); every pair here uses the DPD view (the LJ
