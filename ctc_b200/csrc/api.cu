@@ -12,6 +12,7 @@
 #include "clist.h"
 #include "common.cuh"
 #include "dpd.h"
+#include "fsi.h"
 #include "integrate.h"
 #include "membrane.h"
 #include "api_util.h"
@@ -277,6 +278,7 @@ struct ctc_sim {
     int *mcount;                           // device copy of mnc * mnv
     unsigned *fmask;                       // FSI image lists (reference keys)
     int *frank, *fcount, *fimg_start;
+    int *vperm;                            // FSI: spatially coherent order of a cell's vertices
     Kiss fsi_host;                         // host mirror of the FSI trunk
 };
 
@@ -350,7 +352,7 @@ extern "C" int ctc_sim_destroy(ctc_sim *s) {
     for (cudaEvent_t e : s->ev) cudaEventDestroy(e);
     if (s->rbc) ctc_rbc_force_fin(s->rbc);
     cudaFree(s->mpos); cudaFree(s->mvel); cudaFree(s->mforce); cudaFree(s->mcount);
-    cudaFree(s->fmask); cudaFree(s->frank); cudaFree(s->fcount); cudaFree(s->fimg_start);
+    cudaFree(s->fmask); cudaFree(s->frank); cudaFree(s->fcount); cudaFree(s->fimg_start); cudaFree(s->vperm);
     delete s;
     return CTC_OK;
 }
@@ -391,9 +393,9 @@ extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const i
     cudaStream_t st = (cudaStream_t)stream;
     if (s->rbc) { ctc_rbc_force_fin(s->rbc); s->rbc = nullptr; }
     cudaFree(s->mpos); cudaFree(s->mvel); cudaFree(s->mforce); cudaFree(s->mcount);
-    cudaFree(s->fmask); cudaFree(s->frank); cudaFree(s->fcount); cudaFree(s->fimg_start);
+    cudaFree(s->fmask); cudaFree(s->frank); cudaFree(s->fcount); cudaFree(s->fimg_start); cudaFree(s->vperm);
     s->mpos = s->mvel = s->mforce = nullptr;
-    s->mcount = s->frank = s->fcount = s->fimg_start = nullptr;
+    s->mcount = s->frank = s->fcount = s->fimg_start = s->vperm = nullptr;
     s->fmask = nullptr;
     int rc = ctc_rbc_force_ini(nv, nt, tri, nc > 0 ? nc : 1, &s->rbc);
     if (rc) return rc;
@@ -404,8 +406,15 @@ extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const i
     CUDA_TRY(cudaMalloc(&s->mcount, sizeof(int)));
     CUDA_TRY(cudaMalloc(&s->fmask, sizeof(unsigned) * cap));
     CUDA_TRY(cudaMalloc(&s->frank, sizeof(int) * 26 * cap));
-    CUDA_TRY(cudaMalloc(&s->fcount, sizeof(int) * 26));
+    CUDA_TRY(cudaMalloc(&s->fcount, sizeof(int) * fsi_count_ints((int)cap, 0)));
     CUDA_TRY(cudaMalloc(&s->fimg_start, sizeof(int) * 26));
+    CUDA_TRY(cudaMalloc(&s->vperm, sizeof(int) * nv));
+    {
+        std::vector<int> perm(nv);
+        if (nc > 0) fsi_vertex_order(nv, pp, 6, perm.data());
+        else for (int k = 0; k < nv; k++) perm[k] = k;
+        CUDA_TRY(cudaMemcpy(s->vperm, perm.data(), sizeof(int) * nv, cudaMemcpyHostToDevice));
+    }
     int n = (int)nvt;
     float *tmp = nullptr;
     if (n > 0) {
@@ -484,7 +493,8 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
         F.a = s->fsi.a; F.g = s->fsi.g; F.s = s->fsi.s; F.spow = s->fsi.spow;
         int rc = fsi_forces(s->L, F, nvt, (const float*)s->mpos, (const float*)s->mvel, 4, s->pos[dst], s->vel[dst],
                             s->starts, s->counts, (float*)s->mforce, 4, (float*)s->force, 4, 0.0f, 0.0f,
-                            s->seeds_dev + 27, s->cfg.rng, s->fmask, s->frank, s->fcount, s->fimg_start, st);
+                            s->seeds_dev + 27, s->cfg.rng, s->fmask, s->frank, s->fcount, s->fimg_start, st,
+                            Boxes(), s->vperm, s->mnv);
         if (rc) return rc;
     }
     sim_mark(s, 5, st);

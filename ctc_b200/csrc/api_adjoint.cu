@@ -174,7 +174,7 @@ extern "C" int ctc_adj_create(const ctc_adj_config *cfg, int n, const float *pp,
     cu(cudaMalloc(&a->scratch, clist_scratch_bytes(a->nc, n)), "scratch");
     cu(cudaMalloc(&a->fmask, sizeof(unsigned) * V), "fsi");
     cu(cudaMalloc(&a->frank, sizeof(int) * 26 * V), "fsi");
-    cu(cudaMalloc(&a->fcount, sizeof(int) * 26), "fsi");
+    cu(cudaMalloc(&a->fcount, sizeof(int) * fsi_count_ints((int)V, 0)), "fsi");
     cu(cudaMalloc(&a->fimg, sizeof(int) * 26), "fsi");
     cu(cudaMalloc(&a->avd, sizeof(double) * 4 * std::max(1, nc)), "scratch");
     cu(cudaMalloc(&a->gpar, sizeof(double) * 4), "gradients");

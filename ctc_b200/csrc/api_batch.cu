@@ -54,6 +54,7 @@ struct ctc_batch {
     int *mcount = nullptr;
     unsigned *fmask = nullptr;
     int *frank = nullptr, *fcount = nullptr, *fimg = nullptr;
+    int *vperm = nullptr;          // FSI: spatially coherent order of a cell's vertices
     // launch shapes and graphs
     DpdTune tune{};
     bool use_graph = false;
@@ -70,9 +71,9 @@ static void drop_graphs(ctc_batch *b) {
 static void free_membranes(ctc_batch *b) {
     if (b->rbc) { ctc_rbc_force_fin(b->rbc); b->rbc = nullptr; }
     cudaFree(b->mpos); cudaFree(b->mvel); cudaFree(b->mforce); cudaFree(b->mcount);
-    cudaFree(b->fmask); cudaFree(b->frank); cudaFree(b->fcount); cudaFree(b->fimg);
+    cudaFree(b->fmask); cudaFree(b->frank); cudaFree(b->fcount); cudaFree(b->fimg); cudaFree(b->vperm);
     b->mpos = b->mvel = b->mforce = nullptr;
-    b->mcount = b->frank = b->fcount = b->fimg = nullptr;
+    b->mcount = b->frank = b->fcount = b->fimg = b->vperm = nullptr;
     b->fmask = nullptr;
     b->mnc = 0;
 }
@@ -257,6 +258,13 @@ extern "C" int ctc_batch_set_membranes(ctc_batch *b, const int *cells, int nv, i
     CUDA_TRY(cudaMalloc(&b->frank, sizeof(int) * 26 * cap));
     CUDA_TRY(cudaMalloc(&b->fcount, sizeof(int) * 26 * (size_t)b->nbox));
     CUDA_TRY(cudaMalloc(&b->fimg, sizeof(int) * 26 * (size_t)b->nbox));
+    CUDA_TRY(cudaMalloc(&b->vperm, sizeof(int) * nv));
+    {
+        std::vector<int> perm(nv);
+        if (nc > 0) fsi_vertex_order(nv, pp, 6, perm.data());
+        else for (int k = 0; k < nv; k++) perm[k] = k;
+        CUDA_TRY(cudaMemcpy(b->vperm, perm.data(), sizeof(int) * nv, cudaMemcpyHostToDevice));
+    }
     const int n = (int)nvt;
     if (n > 0) {
         float *tmp = nullptr;
@@ -306,7 +314,7 @@ static int batch_step1(ctc_batch *b, cudaStream_t st) {
         F.a = b->fsi.a; F.g = b->fsi.g; F.s = b->fsi.s; F.spow = b->fsi.spow;
         int rc = fsi_forces(make_int3(1, 1, 1), F, nvt, (const float*)b->mpos, (const float*)b->mvel, 4, b->pos[dst],
                             b->vel[dst], b->starts, b->counts, (float*)b->mforce, 4, (float*)b->force, 4, 0.0f, 0.0f,
-                            b->fseeds, b->rng, b->fmask, b->frank, b->fcount, b->fimg, st, b->B);
+                            b->fseeds, b->rng, b->fmask, b->frank, b->fcount, b->fimg, st, b->B, b->vperm, b->mnv);
         if (rc) return rc;
     }
     CUDA_TRY(integrate_launch(b->ntot_dev, b->ntot, b->pos[dst], b->vel[dst], b->force, b->dt, b->mass, b->bodyf, st));

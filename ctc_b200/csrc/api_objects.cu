@@ -215,7 +215,7 @@ extern "C" int ctc_fsi_ini(int LX, int LY, int LZ, int maxv, int maxs, ctc_fsi *
     CUDA_TRY(cudaMalloc(&f->svel, sizeof(float4) * ns));
     CUDA_TRY(cudaMalloc(&f->mask, sizeof(unsigned) * nv));
     CUDA_TRY(cudaMalloc(&f->rank, sizeof(int) * 26 * nv));
-    CUDA_TRY(cudaMalloc(&f->count, sizeof(int) * 26));
+    CUDA_TRY(cudaMalloc(&f->count, sizeof(int) * fsi_count_ints(nv, 0)));
     CUDA_TRY(cudaMalloc(&f->img_start, sizeof(int) * 26));
     // fsi_ini of rank 0: rnd_ini(1908 - rank, 1409 + rank, 290, 12968) (src/fsi/imp/main.h:7)
     f->trunk.s[0] = 1908; f->trunk.s[1] = 1409; f->trunk.s[2] = 290; f->trunk.s[3] = 12968;
@@ -235,7 +235,7 @@ namespace ctc {
 int fsi_forces(int3 L, const DpdPar &P, int nv, const float *pv, const float *vv, int pstride, const float4 *spos,
                const float4 *svel, const int *starts, const int *counts, float *fv, int fstride, float *fs, int sstride,
                float seed_bulk, float seed_halo, const float *seeds_dev, int rng, unsigned *mask, int *rank,
-               int *count, int *img_start, cudaStream_t st, const Boxes &B) {
+               int *count, int *img_start, cudaStream_t st, const Boxes &B, const int *vperm, int vperm_n) {
     if (nv == 0) return CTC_OK;
     if (rng == CTC_RNG_REFERENCE)
         CUDA_TRY(fsi_images_launch(nv, L, pv, pstride, mask, rank, count, img_start, st, B));
@@ -249,6 +249,10 @@ int fsi_forces(int3 L, const DpdPar &P, int nv, const float *pv, const float *vv
     A.img_rank = rank; A.img_start = img_start;
     A.err = dev_err_ptr();
     A.B = B;
+    if (vperm && vperm_n > 0 && nv % vperm_n == 0) {
+        A.vperm = vperm;
+        A.vperm_n = vperm_n;
+    }
     CUDA_TRY(fsi_launch(A, rng, st));
     return CTC_OK;
 }

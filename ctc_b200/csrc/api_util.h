@@ -21,11 +21,14 @@ int membrane_args(const ctc_rbc_force *f, MembraneArgs *A);
 void membrane_args_par(MembraneArgs *A, const ctc_rbc_params *p, int nt);
 const int *membrane_tri(const ctc_rbc_force *f);
 int membrane_nt(const ctc_rbc_force *f);
-// FSI of nv vertices against the cell-sorted solvent; seeds_dev (2 floats) may replace the seeds
+// FSI of nv vertices against the cell-sorted solvent; seeds_dev (2 floats) may replace the seeds;
+// count holds fsi_count_ints(nv, B.nbox) ints; vperm (device, vperm_n ints, may be null): the
+// order in which threads take each cell's vertices
 int fsi_forces(int3 L, const DpdPar &P, int nv, const float *pv, const float *vv, int pstride, const float4 *spos,
                const float4 *svel, const int *starts, const int *counts, float *fv, int fstride, float *fs, int sstride,
                float seed_bulk, float seed_halo, const float *seeds_dev, int rng, unsigned *mask, int *rank,
-               int *count, int *img_start, cudaStream_t st, const Boxes &B = Boxes());
+               int *count, int *img_start, cudaStream_t st, const Boxes &B = Boxes(), const int *vperm = nullptr,
+               int vperm_n = 0);
 
 // ---------------------------------------------------------------------------
 // host KISS trunks (src/math/rnd/imp.cpp:12-34)

@@ -10,6 +10,11 @@
 // pair noise uses the halo seed and the vertex's index in the concatenated
 // image list (fragments packed in ascending vertex order, received in slot
 // anti(fid)).
+#include <algorithm>
+#include <cmath>
+#include <utility>
+#include <vector>
+
 #include "common.cuh"
 #include "fsi.h"
 
@@ -88,6 +93,95 @@ __global__ void k_emap_rank(int nv, const unsigned *__restrict__ mask, int *__re
         __syncthreads();
     }
     if (threadIdx.x == 0) count[fid] = carry;
+}
+
+// one box, in parallel: EMAP_T vertices per block.  Pass 1 (k_emap_count):
+// masks and per-block member counts of every fragment (bcnt[fid * nblk + b]);
+// pass 2 (k_emap_scan, one block per fragment): their exclusive scan in place
+// and the totals; pass 3 (k_emap_rank_par): rank = block offset + offset of
+// the warp + members before the lane in the warp.  The same ranks as
+// k_emap_rank (ascending vertex index within each fragment).
+constexpr int EMAP_T = 1024;
+
+__global__ void __launch_bounds__(EMAP_T) k_emap_count(int nv, int3 L, const float *__restrict__ pv, int stride,
+                                                       unsigned *__restrict__ mask, int *__restrict__ bcnt) {
+    __shared__ int wc[26][EMAP_T / 32];
+    const int i = blockIdx.x * EMAP_T + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned m = 0;
+    if (i < nv) {
+        const float *q = pv + (size_t)stride * i;
+        m = emap_mask(L, q[0], q[1], q[2]);
+        mask[i] = m;
+    }
+    for (int fid = 0; fid < 26; fid++) {
+        const unsigned bal = __ballot_sync(0xffffffffu, (m >> fid) & 1u);
+        if (lane == 0) wc[fid][w] = __popc(bal);
+    }
+    __syncthreads();
+    if (w < 26) {                        // warp fid sums its fragment's warp counts
+        int v = lane < EMAP_T / 32 ? wc[w][lane] : 0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) bcnt[(size_t)w * gridDim.x + blockIdx.x] = v;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_emap_scan(int nblk, int *__restrict__ bcnt, int *__restrict__ count) {
+    __shared__ int sh[32];
+    const int fid = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int *c = bcnt + (size_t)fid * nblk, carry = 0;
+    for (int b0 = 0; b0 < nblk; b0 += 1024) {
+        const int b = b0 + threadIdx.x;
+        const int v = b < nblk ? c[b] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sh[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int t = sh[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            sh[lane] = t;
+        }
+        __syncthreads();
+        if (b < nblk) c[b] = carry + x - v + (w > 0 ? sh[w - 1] : 0);
+        carry += sh[31];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) count[fid] = carry;
+}
+
+__global__ void __launch_bounds__(EMAP_T) k_emap_rank_par(int nv, const unsigned *__restrict__ mask,
+                                                          const int *__restrict__ boff, int *__restrict__ rank) {
+    __shared__ int wo[26][EMAP_T / 32];
+    const int i = blockIdx.x * EMAP_T + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned m = i < nv ? mask[i] : 0u;
+    for (int fid = 0; fid < 26; fid++) {
+        const unsigned bal = __ballot_sync(0xffffffffu, (m >> fid) & 1u);
+        if (lane == 0) wo[fid][w] = __popc(bal);
+    }
+    __syncthreads();
+    if (w < 26) {                        // warp fid: exclusive scan of its fragment's warp counts
+        const int v = lane < EMAP_T / 32 ? wo[w][lane] : 0;
+        int x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane < EMAP_T / 32) wo[w][lane] = x - v;
+    }
+    __syncthreads();
+    if (i >= nv) return;
+    const unsigned below = (1u << lane) - 1u;
+    for (int fid = 0; fid < 26; fid++) {
+        const unsigned bal = __ballot_sync(__activemask(), (m >> fid) & 1u);
+        const int r = __ldg(boff + (size_t)fid * gridDim.x + blockIdx.x) + wo[fid][w] + __popc(bal & below);
+        rank[(size_t)fid * nv + i] = ((m >> fid) & 1u) ? r : -1;
+    }
 }
 
 // img_start[fid] = start of receive slot anti(fid) in the concatenated list
@@ -230,8 +324,10 @@ __global__ void __launch_bounds__(FSIQ_T) k_fsi_q(const __grid_constant__ FsiArg
     const int lane = threadIdx.x & 31;
     uint4 *q = queue[threadIdx.x >> 5];
     int qn = 0;
-    const int i = blockIdx.x * FSIQ_T + threadIdx.x;
-    const bool act = i < A.nv;
+    const int t = blockIdx.x * FSIQ_T + threadIdx.x;
+    const bool act = t < A.nv;
+    int i = t;                           // the vertex this thread takes
+    if (A.vperm && act) i = t - t % A.vperm_n + __ldg(A.vperm + t % A.vperm_n);
     const DpdPar P = A.par;
 
     // per record: vertex i | halo bit << 31, solvent j, halo key index aid, fid
@@ -240,9 +336,15 @@ __global__ void __launch_bounds__(FSIQ_T) k_fsi_q(const __grid_constant__ FsiArg
             const uint4 rec = q[lane];
             const int v = (int)(rec.x & 0x7fffffffu), j = (int)rec.y, fid = (int)rec.w;
             const bool halo = rec.x >> 31;
-            const float *pq = A.pv + (size_t)A.pstride * v, *pqv = A.vv + (size_t)A.pstride * v;
-            float4 a = make_float4(pq[0], pq[1], pq[2], 0.0f);
-            const float4 va = make_float4(pqv[0], pqv[1], pqv[2], 0.0f);
+            float4 a, va;
+            if (A.pstride == 4) {
+                a = __ldg((const float4*)A.pv + v);
+                va = __ldg((const float4*)A.vv + v);
+            } else {
+                const float *pq = A.pv + (size_t)A.pstride * v, *pqv = A.vv + (size_t)A.pstride * v;
+                a = make_float4(pq[0], pq[1], pq[2], 0.0f);
+                va = make_float4(pqv[0], pqv[1], pqv[2], 0.0f);
+            }
             int3 L = A.L;
             const float *seeds = A.seeds_dev;
             int vk = v, sk = 0;
@@ -304,25 +406,43 @@ __global__ void __launch_bounds__(FSIQ_T) k_fsi_q(const __grid_constant__ FsiArg
     }
     // the vertex cell as src/fsi/dev/map/bulk.h:13-21 (floorf, may lie outside the box)
     const int cx = L.x / 2 + (int)floorf(pa.x), cy = L.y / 2 + (int)floorf(pa.y), cz = L.z / 2 + (int)floorf(pa.z);
-    int ci = 0, j = 0, e = 0, fid = 0;
+    // the 27 cells as 9 rows (dz, dy) of 3 cells along x: one contiguous span
+    // when the three cells take the same periodic shift in x, else cell by cell
+    int r = 0, part = 3, j = 0, e = 0, fid = 0;
     unsigned aid = 0;
     bool halo = false;
     float4 a = pa;
     constexpr int U = 4;
     for (;;) {
         if (act) {
-            while (j >= e && ci < 27) {
-                const int dx = ci % 3 - 1, dy = (ci / 3) % 3 - 1, dz = ci / 9 - 1;
-                ci++;
-                int gx = cx + dx, gy = cy + dy, gz = cz + dz;
+            while (j >= e && (r < 9 || part < 3)) {
+                int gx, ncell;
+                if (part < 3) {                  // next cell of a split row (r - 1)
+                    gx = cx - 1 + part;
+                    part++;
+                    ncell = 1;
+                } else {
+                    r++;
+                    gx = cx - 1;
+                    ncell = 3;
+                    const int wlo = gx < 0 ? -1 : (gx >= L.x ? 1 : 0);
+                    const int whi = gx + 2 < 0 ? -1 : (gx + 2 >= L.x ? 1 : 0);
+                    const int g0 = gx - wlo * L.x;
+                    if (wlo != whi || g0 < 0 || g0 + 2 >= L.x) {   // crosses a periodic face in x
+                        part = 0;
+                        continue;
+                    }
+                }
+                const int dy = (r - 1) % 3 - 1, dz = (r - 1) / 3 - 1;
+                int gy = cy + dy, gz = cz + dz;
                 const int wx = gx < 0 ? -1 : (gx >= L.x ? 1 : 0);
                 const int wy = gy < 0 ? -1 : (gy >= L.y ? 1 : 0);
                 const int wz = gz < 0 ? -1 : (gz >= L.z ? 1 : 0);
                 gx -= wx * L.x; gy -= wy * L.y; gz -= wz * L.z;
-                if (gx < 0 || gx >= L.x || gy < 0 || gy >= L.y || gz < 0 || gz >= L.z) continue;
+                if (gx < 0 || gx + ncell > L.x || gy < 0 || gy >= L.y || gz < 0 || gz >= L.z) continue;
                 const int cid = gx + L.x * (gy + L.y * gz);
                 j = __ldg(starts + cid);
-                e = j + __ldg(counts + cid);
+                e = ncell == 3 ? __ldg(starts + cid + 3) : j + __ldg(counts + cid);
                 halo = (wx | wy | wz) != 0;
                 a = pa;
                 aid = (unsigned)vk;
@@ -356,14 +476,54 @@ __global__ void __launch_bounds__(FSIQ_T) k_fsi_q(const __grid_constant__ FsiArg
     if (qn > 0) process(qn);
 }
 
+size_t fsi_count_ints(int nv, int nbox) {
+    if (nbox > 0) return 26 * (size_t)nbox;
+    return 26 + 26 * (size_t)ceil_div(std::max(nv, 1), EMAP_T);
+}
+
 cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsigned *mask, int *rank, int *count,
                               int *img_start, cudaStream_t st, const Boxes &B) {
     if (nv <= 0) return cudaSuccess;
-    const int nb = B.nbox > 0 ? B.nbox : 1;
-    k_emap<<<ceil_div(nv, 256), 256, 0, st>>>(nv, L, pv, stride, mask, B);
-    k_emap_rank<<<dim3(26, nb), 1024, 0, st>>>(nv, mask, rank, count, B);
-    k_emap_starts<<<nb, 32, 0, st>>>(count, img_start);
+    if (B.nbox > 0) {   // a few cells per box: one block per (fragment, box)
+        k_emap<<<ceil_div(nv, 256), 256, 0, st>>>(nv, L, pv, stride, mask, B);
+        k_emap_rank<<<dim3(26, B.nbox), 1024, 0, st>>>(nv, mask, rank, count, B);
+        k_emap_starts<<<B.nbox, 32, 0, st>>>(count, img_start);
+        return cudaGetLastError();
+    }
+    const int nblk = ceil_div(nv, EMAP_T);
+    int *bcnt = count + 26;
+    k_emap_count<<<nblk, EMAP_T, 0, st>>>(nv, L, pv, stride, mask, bcnt);
+    k_emap_scan<<<26, 1024, 0, st>>>(nblk, bcnt, count);
+    k_emap_rank_par<<<nblk, EMAP_T, 0, st>>>(nv, mask, bcnt, rank);
+    k_emap_starts<<<1, 32, 0, st>>>(count, img_start);
     return cudaGetLastError();
+}
+
+void fsi_vertex_order(int nv, const float *pv, int stride, int *perm) {
+    // Morton code of the unit cell of each vertex (10 bits per axis, relative
+    // to the cell's lower corner), ties by vertex index
+    float lo[3] = {1e30f, 1e30f, 1e30f};
+    for (int i = 0; i < nv; i++)
+        for (int c = 0; c < 3; c++) lo[c] = std::min(lo[c], pv[(size_t)stride * i + c]);
+    auto spread = [](unsigned v) {
+        v &= 0x3ffu;
+        v = (v | (v << 16)) & 0x030000ffu;
+        v = (v | (v << 8)) & 0x0300f00fu;
+        v = (v | (v << 4)) & 0x030c30c3u;
+        v = (v | (v << 2)) & 0x09249249u;
+        return v;
+    };
+    std::vector<std::pair<unsigned, int>> key((size_t)nv);
+    for (int i = 0; i < nv; i++) {
+        unsigned k = 0;
+        for (int c = 0; c < 3; c++) {
+            const int q = (int)std::floor(pv[(size_t)stride * i + c] - lo[c]);
+            k |= spread((unsigned)std::max(0, q)) << c;
+        }
+        key[(size_t)i] = {k, i};
+    }
+    std::sort(key.begin(), key.end());
+    for (int i = 0; i < nv; i++) perm[i] = key[(size_t)i].second;
 }
 
 cudaError_t fsi_vjp_launch(const FsiArgs &A, cudaStream_t st) {

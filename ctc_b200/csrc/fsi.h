@@ -28,11 +28,22 @@ struct FsiArgs {
     // velocities (accumulated, float4 arrays)
     const float4 *adj_fv, *adj_fs;
     float4 *adj_xv, *adj_vv, *adj_xs, *adj_vs;
+    // order in which threads take the vertices (forces): thread t takes vertex
+    // (t / vperm_n) * vperm_n + vperm[t % vperm_n] (cells of vperm_n vertices,
+    // each walked in a spatially coherent order of the template); null: t
+    const int *vperm;
+    int vperm_n;
 };
 
+// ints of the count buffer of fsi_images_launch: 26 per box with B.nbox > 0;
+// one box: 26 totals + 26 per block of vertices (block counts, then offsets)
+size_t fsi_count_ints(int nv, int nbox);
 // with B.nbox > 0, count and img_start hold 26 entries per box
 cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsigned *mask, int *rank, int *count,
                               int *img_start, cudaStream_t st, const Boxes &B = Boxes());
+// a spatially coherent visiting order of a cell's nv vertices (Morton order of
+// the unit cells of pv, nv points of 6 or 4 floats at stride) [host]
+void fsi_vertex_order(int nv, const float *pv, int stride, int *perm);
 cudaError_t fsi_launch(const FsiArgs &A, int rng, cudaStream_t st);
 cudaError_t fsi_vjp_launch(const FsiArgs &A, cudaStream_t st);
 
