@@ -66,16 +66,37 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def bulk_traffic_per_particle():
-    """DRAM bytes per particle of one k_dpd_bulk launch, from the committed ncu
-    summary (a line "traffic_bytes_per_particle: X"), or None."""
+def bulk_profile_figure(key):
+    """A per-particle figure of one k_dpd_bulk launch from the committed ncu
+    summary (a line "key: X"), or None."""
     p = os.path.join(ROOT, "profiles", "k_dpd_bulk_p64.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.strip().startswith("traffic_bytes_per_particle:"):
+        if line.strip().startswith(key + ":"):
             return float(line.split(":")[1])
     return None
+
+
+def issue_roofline(n, bulk_ms, clk):
+    """Instruction-issue fraction of k_dpd_bulk, the bound it runs into:
+    warp instructions per particle (ncu capture) x particles / the launch's
+    CUDA-event time, against 148 SMs x 4 schedulers x one warp instruction per
+    cycle at the SM clock sampled during the timed region."""
+    ipp = bulk_profile_figure("warp_instructions_per_particle")
+    if not ipp:
+        return None
+    mhz = (clk or {}).get("sm_mhz") or 1965.0
+    achieved = ipp * n / (bulk_ms * 1e-3)
+    peak = 148 * 4 * mhz * 1e6
+    return {"achieved_warp_inst_per_s": achieved, "peak_warp_inst_per_s": peak, "frac": achieved / peak,
+            "warp_inst_per_particle": ipp, "sm_mhz": mhz,
+            "note": "instructions per particle from profiles/k_dpd_bulk_p64.md (ncu, 64^3 box)"}
+
+
+def bulk_traffic_per_particle():
+    """DRAM bytes per particle of one k_dpd_bulk launch (ncu capture)."""
+    return bulk_profile_figure("traffic_bytes_per_particle")
 
 
 class Clocks:
@@ -332,7 +353,8 @@ def run_ours(args, cfg, world, rank, local):
                               "peak_tflops": FP32_NOMINAL_TFLOPS, "peak_kind": "nominal",
                               "frac": PAIR_FLOP * n / (bulk_ms * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS,
                               "note": "~%d flop per particle (100 per accepted half-pair, 20.94 half-pairs)"
-                                      % PAIR_FLOP}},
+                                      % PAIR_FLOP},
+                     "issue": issue_roofline(n, bulk_ms, clk)},
         "e2e": {"value": e2e_value, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": 40 + state_bytes / args.steps},

@@ -557,13 +557,16 @@ __global__ void k_halo_pack(int3 L, const int *__restrict__ starts, const int *_
 }
 
 // exclusive scans of the counts of every fragment's cells (src/exch/flu/dev/map.h:23-97);
-// block (fid, box): out = fss + offset of fragment fid of that box.  1024
-// threads, FS_ITEMS consecutive fragment cells each per round.
-constexpr int FS_T = 1024, FS_ITEMS = 8;
+// block (fid, box): out = fss + offset of fragment fid of that box.  FS_T
+// threads (1024 for one box, 128 for the small faces of batched boxes),
+// FS_ITEMS consecutive fragment cells each per round.
+constexpr int FS_ITEMS = 8;
 
+template <int FS_T>
 __global__ void __launch_bounds__(FS_T) k_frag_starts(int3 L, const int *__restrict__ counts, int *__restrict__ fss,
                                                       Off27 off, Boxes B) {
-    __shared__ int sh[32];
+    constexpr int NW = FS_T / 32;
+    __shared__ int sh[NW];
     const int fid = blockIdx.x;
     int *out = fss + off.d[fid];
     if (B.nbox > 0) {
@@ -601,17 +604,17 @@ __global__ void __launch_bounds__(FS_T) k_frag_starts(int3 L, const int *__restr
         if (lane == 31) sh[w] = x;
         __syncthreads();
         if (w == 0) {
-            int t = sh[lane];
+            int t = lane < NW ? sh[lane] : 0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, t, o);
                 if (lane >= o) t += y;
             }
-            sh[lane] = t;
+            if (lane < NW) sh[lane] = t;
         }
         __syncthreads();
         int r = carry + x - s + (w > 0 ? sh[w - 1] : 0);
-        const int tot = sh[31];
+        const int tot = sh[NW - 1];
 #pragma unroll
         for (int k = 0; k < FS_ITEMS; k++) {
             if (h0 + k < nc) out[h0 + k] = r;
@@ -677,14 +680,14 @@ unsigned halo_masks() {
 
 cudaError_t frag_starts_launch(int3 L, const int *counts, int *fss, const Off27 &off, cudaStream_t st) {
     Boxes none{};
-    k_frag_starts<<<26, FS_T, 0, st>>>(L, counts, fss, off, none);
+    k_frag_starts<1024><<<26, 1024, 0, st>>>(L, counts, fss, off, none);
     return cudaGetLastError();
 }
 
 cudaError_t frag_starts_boxes_launch(const Boxes &B, const int *counts, int *fss, cudaStream_t st) {
     if (B.nbox <= 0) return cudaSuccess;
     Off27 off{};
-    k_frag_starts<<<dim3(26, B.nbox), FS_T, 0, st>>>(make_int3(1, 1, 1), counts, fss, off, B);
+    k_frag_starts<128><<<dim3(26, B.nbox), 128, 0, st>>>(make_int3(1, 1, 1), counts, fss, off, B);
     return cudaGetLastError();
 }
 

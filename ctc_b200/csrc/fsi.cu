@@ -486,7 +486,7 @@ cudaError_t fsi_images_launch(int nv, int3 L, const float *pv, int stride, unsig
     if (nv <= 0) return cudaSuccess;
     if (B.nbox > 0) {   // a few cells per box: one block per (fragment, box)
         k_emap<<<ceil_div(nv, 256), 256, 0, st>>>(nv, L, pv, stride, mask, B);
-        k_emap_rank<<<dim3(26, B.nbox), 1024, 0, st>>>(nv, mask, rank, count, B);
+        k_emap_rank<<<dim3(26, B.nbox), 256, 0, st>>>(nv, mask, rank, count, B);
         k_emap_starts<<<B.nbox, 32, 0, st>>>(count, img_start);
         return cudaGetLastError();
     }
