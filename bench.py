@@ -44,6 +44,11 @@ CONFIGS = {
                 name="plain DPD 64x64x64 rho=10 (2,621,440 particles), body force 0.01 x"),
     "c3": dict(L=(64, 64, 64), bodyf=(0.0, 0.0, 0.0), steps=100, rbc=200,
                name="C3 RBC suspension 64x64x64 rho=10 (2,621,440 solvent) + 200 cells x 642 vertices"),
+    # next to C3: the same system with membrane-membrane contact (src/cnt, the
+    # DPD + LJ parameters of the reference's contact test)
+    "c3c": dict(L=(64, 64, 64), bodyf=(0.0, 0.0, 0.0), steps=100, rbc=200, contact=(2.6666667, 8.0, 0.25, 0.3, 0.44),
+                name="C3 + membrane-membrane contact (DPD a=2.67 g=8 + LJ s=0.3 e=0.44) 64x64x64 rho=10 "
+                     "+ 200 cells x 642 vertices"),
     "c4": dict(adjoint=True, L=(32, 32, 32), rbc=20, K=20, kck=5, bodyf=(0.0, 0.0, 0.0),
                name="C4 adjoint 32x32x32 rho=10 (327,680 solvent) + 20 RBC, loss = mean vertex x-velocity "
                     "after 20 steps, checkpoints every 5"),
@@ -274,6 +279,9 @@ def run_ours(args, cfg, world, rank, local):
         fsi = ctc.DpdParams(0.0, systems.GAMMA, systems.dpd_params()[2], systems.SPOW)   # a = 0, gamma = 8
         sim.set_membranes(pv, tri, 642, par, fsi, mass=systems.RBC_MASS)
         nvt = len(pv)
+        if cfg.get("contact"):
+            a, g, spow, ljs, lje = cfg["contact"]
+            sim.set_contact(ctc.DpdLjParams(a, g, ctc.dpd_sigma(systems.KBT, g, systems.DT), spow, ljs, lje))
     sim.step(args.warmup)
     torch.cuda.synchronize()
     sim.profile(True)
@@ -331,8 +339,8 @@ def run_ours(args, cfg, world, rank, local):
     traffic = bulk_traffic_per_particle()
     # seeds, 6 cell-list kernels, fragment starts, 2 halo packing kernels, bulk, halo, update; with
     # membranes also cell wrap, FSI seeds, 4 image-list kernels, FSI, area/volume, membrane forces,
-    # vertex update
-    launches = 13 + (10 if nvt else 0)
+    # vertex update; contact adds its seeds, 6 vertex cell-list kernels and the pair kernel
+    launches = 13 + (10 if nvt else 0) + (8 if cfg.get("contact") else 0)
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,

@@ -15,7 +15,8 @@ import numpy as np
 from . import _lib
 from ._lib import CTC_RNG_REFERENCE, CTC_RNG_STABLE, CtcError, check, device_error, lib
 
-__all__ = ["Clist", "FluForces", "Sim", "Batch", "DpdParams", "RbcParams", "RbcForce", "Fsi", "dpd_sigma", "scheme_move_apply",
+__all__ = ["Clist", "FluForces", "Sim", "Batch", "DpdParams", "DpdLjParams", "RbcParams", "RbcForce", "Fsi", "Contact",
+           "dpd_sigma", "scheme_move_apply",
            "scheme_move_clear_vel", "bforce_apply_cste", "rnd_mean0var1", "CTC_RNG_REFERENCE",
            "CTC_RNG_STABLE", "CtcError", "device_error"]
 
@@ -42,6 +43,12 @@ def _ptr(t):
 def DpdParams(a, g, s, spow):
     """PairDPD {a, g, s, spow} (src/pair/type.h:7-9)."""
     return _lib.DpdParams(a, g, s, spow)
+
+
+def DpdLjParams(a, g, s, spow, ljs, lje):
+    """PairDPDLJ {a, g, s, spow, ljs, lje} (src/pair/type.h:22-25): DPD plus a
+    capped Lennard-Jones repulsion, the membrane-membrane contact pair."""
+    return _lib.DpdLjParams(a, g, s, spow, ljs, lje)
 
 
 def dpd_sigma(kBT, g, dt):
@@ -189,6 +196,28 @@ class Fsi:
                                          int(rng), _ptr(fv), _ptr(fs), _stream(stream)))
 
 
+class Contact:
+    """Membrane-membrane contact forces of one object type in a periodic box
+    (src/cnt/imp.h: cnt_build_cells + cnt_bulk + cnt_halo)."""
+
+    def __init__(self, L, maxv):
+        self.h = C.c_void_p()
+        check(lib().ctc_cnt_ini(*(int(x) for x in L), int(maxv), C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
+            lib().ctc_cnt_fin(self.h)
+            self.h = None
+
+    def apply(self, params, pv, fv, stream=None):
+        """Draws the bulk and halo seeds of the trunk; pv (n, 6) AoS, fv (n, 3) accumulated."""
+        check(lib().ctc_cnt_apply(self.h, C.byref(params), int(pv.shape[0]), _ptr(pv), _ptr(fv), _stream(stream)))
+
+    def apply_seeded(self, params, pv, seed_bulk, seed_halo, fv, stream=None):
+        check(lib().ctc_cnt_apply_seeded(self.h, C.byref(params), int(pv.shape[0]), _ptr(pv), float(seed_bulk),
+                                         float(seed_halo), _ptr(fv), _stream(stream)))
+
+
 def scheme_move_apply(dt, mass, ff, pp, stream=None):
     """src/scheme/move/imp.h:5 -- v += f/m dt; r += v dt (in place on pp)."""
     check(lib().ctc_scheme_move_apply(dt, mass, int(pp.shape[0]), _ptr(ff), _ptr(pp), _stream(stream)))
@@ -259,6 +288,10 @@ class Sim:
         check(lib().ctc_sim_set_membranes(self.h, self.mnc, self.mnv, len(tri), tri.ctypes.data_as(C.c_void_p),
                                           pv.ctypes.data_as(C.c_void_p), C.byref(_lib.RbcParams(**params)),
                                           C.byref(fsi), float(mass), _stream(stream)))
+
+    def set_contact(self, params):
+        """Membrane-membrane contact (a DpdLjParams) from the next step on; None: off."""
+        check(lib().ctc_sim_set_contact(self.h, None if params is None else C.byref(params)))
 
     def get_membranes(self, stream=None):
         out = np.zeros((self.mnc * self.mnv, 6), np.float32)

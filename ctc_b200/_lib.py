@@ -11,8 +11,8 @@ LIB_PATH = os.path.join(HERE, "libctc_b200.so")
 
 CTC_OK, CTC_ERR_ARG, CTC_ERR_CUDA, CTC_ERR_CAPACITY, CTC_ERR_DEVICE = 0, 1, 2, 3, 4
 CTC_RNG_REFERENCE, CTC_RNG_STABLE = 0, 1
-CTC_SIM_PHASES = 7
-SIM_PHASE_NAMES = ("clist", "frag_starts", "bulk", "halo", "fsi", "update", "membrane")
+CTC_SIM_PHASES = 8
+SIM_PHASE_NAMES = ("clist", "frag_starts", "bulk", "halo", "fsi", "contact", "update", "membrane")
 
 vp = C.c_void_p
 ip = C.POINTER(C.c_int)
@@ -21,6 +21,11 @@ fp = C.POINTER(C.c_float)
 
 class DpdParams(C.Structure):
     _fields_ = [("a", C.c_float), ("g", C.c_float), ("s", C.c_float), ("spow", C.c_float)]
+
+
+class DpdLjParams(C.Structure):
+    _fields_ = [("a", C.c_float), ("g", C.c_float), ("s", C.c_float), ("spow", C.c_float),
+                ("ljs", C.c_float), ("lje", C.c_float)]
 
 
 class RbcParams(C.Structure):
@@ -71,6 +76,11 @@ SIGNATURES = {
     "ctc_rbc_force_set_bending": (C.c_int, [vp, C.c_int]),
     "ctc_rbc_force_apply": (C.c_int, [vp, C.POINTER(RbcParams), C.c_float, C.c_int, vp, vp, vp]),
     "ctc_rbc_area_volume": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+    "ctc_cnt_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
+    "ctc_cnt_fin": (C.c_int, [vp]),
+    "ctc_cnt_apply": (C.c_int, [vp, C.POINTER(DpdLjParams), C.c_int, vp, vp, vp]),
+    "ctc_cnt_apply_seeded": (C.c_int, [vp, C.POINTER(DpdLjParams), C.c_int, vp, C.c_float, C.c_float, vp, vp]),
+    "ctc_sim_set_contact": (C.c_int, [vp, C.POINTER(DpdLjParams)]),
     "ctc_fsi_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
     "ctc_fsi_fin": (C.c_int, [vp]),
     "ctc_fsi_apply": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp]),

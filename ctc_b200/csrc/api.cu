@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "clist.h"
+#include "cnt.h"
 #include "common.cuh"
 #include "dpd.h"
 #include "fsi.h"
@@ -280,7 +281,24 @@ struct ctc_sim {
     int *frank, *fcount, *fimg_start;
     int *vperm;                            // FSI: spatially coherent order of a cell's vertices
     Kiss fsi_host;                         // host mirror of the FSI trunk
+    // membrane-membrane contact (optional)
+    bool cnt_on;
+    ctc_dpdlj_params cnt;
+    void *cnt_scratch;                     // vertex cell list of the contact pairs
+    CntScratch cw;
+    Kiss cnt_host;                         // host mirror of the contact trunk
 };
+
+// the contact's vertex cell list for the current membranes
+static int sim_cnt_alloc(ctc_sim *s) {
+    cudaFree(s->cnt_scratch);
+    s->cnt_scratch = nullptr;
+    const int nvt = s->mnc * s->mnv;
+    if (!s->cnt_on || nvt <= 0) return CTC_OK;
+    CUDA_TRY(cudaMalloc(&s->cnt_scratch, cnt_scratch_bytes(s->nc, nvt)));
+    cnt_carve(&s->cw, s->cnt_scratch, s->nc, nvt);
+    return CTC_OK;
+}
 
 static void sim_mark(ctc_sim *s, int k, cudaStream_t st) {
     if (!s->prof) return;
@@ -314,8 +332,8 @@ extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
     CUDA_TRY(cudaMalloc(&s->fss, sizeof(int) * (size_t)s->off.d[26]));
     CUDA_TRY(cudaMalloc(&s->scratch, clist_scratch_bytes(s->nc, (int)np)));
     clist_carve(&s->w, s->scratch, s->nc, (int)np);
-    CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 28));   // + the FSI trunk
-    CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 29));
+    CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 29));   // + the FSI and contact trunks
+    CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 31));
     CUDA_TRY(cudaMalloc(&s->diag_scratch, diag_scratch_bytes()));
     {
         // a boundary particle appears once per fragment holding its cell: room
@@ -335,6 +353,9 @@ extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
     // FSI trunk of rank 0, rnd_ini(1908, 1409, 290, 12968) (src/fsi/imp/main.h:7)
     kiss_ini(&s->fsi_host, 1908, 1409, 290, 12968);
     CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 27, s->fsi_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
+    // contact trunk of rank 0, rnd_ini(7119, 187, 18278, 15674) (src/cnt/imp/main.h:21)
+    kiss_ini(&s->cnt_host, 7119, 187, 18278, 15674);
+    CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 28, s->cnt_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
     s->cur = 0;
     s->n_host = 0;
     s->built = false;
@@ -347,6 +368,7 @@ extern "C" int ctc_sim_destroy(ctc_sim *s) {
     for (int b = 0; b < 2; b++) { cudaFree(s->pos[b]); cudaFree(s->vel[b]); }
     cudaFree(s->force); cudaFree(s->counts); cudaFree(s->starts); cudaFree(s->count0); cudaFree(s->fss);
     cudaFree(s->scratch); cudaFree(s->trunk_dev); cudaFree(s->seeds_dev); cudaFree(s->diag_scratch);
+    cudaFree(s->cnt_scratch);
     cudaFree(s->diag_out);
     cudaFree(s->pack); cudaFree(s->pack_off);
     for (cudaEvent_t e : s->ev) cudaEventDestroy(e);
@@ -426,10 +448,19 @@ extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const i
     CUDA_TRY(cudaStreamSynchronize(st));
     if (tmp) CUDA_TRY(cudaFreeAsync(tmp, st));
     s->mnc = nc; s->mnv = nv;
+    int rcc = sim_cnt_alloc(s);
+    if (rcc) return rcc;
     s->mpar = *p;
     s->fsi = *fsi;
     s->mmass = mass;
     return CTC_OK;
+}
+
+extern "C" int ctc_sim_set_contact(ctc_sim *s, const ctc_dpdlj_params *p) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sim_set_contact: null");
+    s->cnt_on = p != nullptr;
+    if (p) s->cnt = *p;
+    return sim_cnt_alloc(s);
 }
 
 extern "C" int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream) {
@@ -466,6 +497,11 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
         CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 27, 2, s->seeds_dev + 27, st));
         kiss_get(&s->fsi_host);
         kiss_get(&s->fsi_host);
+        if (s->cnt_on) {   // the contact trunk: cnt_bulk, then cnt_halo
+            CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 28, 2, s->seeds_dev + 29, st));
+            kiss_get(&s->cnt_host);
+            kiss_get(&s->cnt_host);
+        }
     }
     sim_mark(s, 1, st);
     DpdArgs A;
@@ -498,9 +534,20 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
         if (rc) return rc;
     }
     sim_mark(s, 5, st);
+    if (nvt > 0 && s->cnt_on) {
+        // membrane-membrane contact into the vertex forces (the periodic
+        // images are FSI's; with stable FSI keys they are listed here)
+        if (s->cfg.rng != CTC_RNG_REFERENCE)
+            CUDA_TRY(fsi_images_launch(nvt, s->L, (const float*)s->mpos, 4, s->fmask, s->frank, s->fcount,
+                                       s->fimg_start, st));
+        int rc = cnt_forces(s->L, s->cnt, nvt, (const float*)s->mpos, (const float*)s->mvel, 4, (float*)s->mforce, 4,
+                            0.0f, 0.0f, s->seeds_dev + 29, s->cw, s->fmask, s->frank, s->fimg_start, st);
+        if (rc) return rc;
+    }
+    sim_mark(s, 6, st);
     CUDA_TRY(integrate_launch(s->starts + s->nc, s->n_host, s->pos[dst], s->vel[dst], s->force, s->cfg.dt,
                               s->cfg.mass, bf, st));
-    sim_mark(s, 6, st);
+    sim_mark(s, 7, st);
     if (nvt > 0) {
         // objects_advance: internal forces on top of the FSI ones, then the update
         int rc = membrane_forces(s->rbc, &s->mpar, s->mnc, (const float*)s->mpos, (const float*)s->mvel, 4,
@@ -508,7 +555,7 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
         if (rc) return rc;
         CUDA_TRY(integrate_launch(s->mcount, nvt, s->mpos, s->mvel, s->mforce, s->cfg.dt, s->mmass, bf, st));
     }
-    sim_mark(s, 7, st);
+    sim_mark(s, 8, st);
     if (s->prof) s->prof_steps++;
     s->cur = dst;
     s->built = true;

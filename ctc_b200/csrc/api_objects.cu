@@ -7,6 +7,7 @@
 
 #include "api_util.h"
 #include "clist.h"
+#include "cnt.h"
 #include "common.cuh"
 #include "fsi.h"
 #include "membrane.h"
@@ -281,4 +282,82 @@ extern "C" int ctc_fsi_apply(ctc_fsi *f, const ctc_dpd_params *p, int nv, const 
     float sb = kiss_get4(&f->trunk);
     float sh = kiss_get4(&f->trunk);
     return ctc_fsi_apply_seeded(f, p, nv, pv, ns, ps, starts, counts, sb, sh, CTC_RNG_REFERENCE, fv, fs, stream);
+}
+
+// ---------------------------------------------------------------------------
+// membrane-membrane contact (src/cnt/imp.h)
+// ---------------------------------------------------------------------------
+namespace ctc {
+int cnt_forces(int3 L, const ctc_dpdlj_params &p, int nv, const float *pv, const float *vv, int pstride, float *fv,
+               int fstride, float seed_bulk, float seed_halo, const float *seeds_dev, const CntScratch &w,
+               const unsigned *mask, const int *rank, const int *img_start, cudaStream_t st) {
+    if (nv == 0) return CTC_OK;
+    CUDA_TRY(cnt_cells_launch(L, nv, pv, pstride, w, st));
+    CntArgs A;
+    memset(&A, 0, sizeof(A));
+    A.L = L; A.nv = nv; A.pv = pv; A.vv = vv; A.pstride = pstride;
+    A.fv = fv; A.fstride = fstride;
+    A.par.a = p.a; A.par.g = p.g; A.par.s = p.s; A.par.spow = p.spow;
+    A.ljs = p.ljs; A.lje = p.lje;
+    A.seed_bulk = seed_bulk; A.seed_halo = seed_halo; A.seeds_dev = seeds_dev;
+    A.starts = w.starts; A.ids = w.ids;
+    A.img_mask = mask; A.img_rank = rank; A.img_start = img_start;
+    CUDA_TRY(cnt_launch(A, st));
+    return CTC_OK;
+}
+}  // namespace ctc
+
+struct ctc_cnt {
+    int3 L;
+    int maxv;
+    void *scratch;
+    CntScratch w;
+    unsigned *mask;
+    int *rank, *count, *img_start;
+    Kiss4 trunk;
+};
+
+extern "C" int ctc_cnt_ini(int LX, int LY, int LZ, int maxv, ctc_cnt **pc) {
+    if (!pc || LX < 3 || LY < 3 || LZ < 3 || maxv < 0) return fail(CTC_ERR_ARG, "ctc_cnt_ini: bad arguments");
+    ctc_cnt *c = new ctc_cnt();
+    c->L = make_int3(LX, LY, LZ);
+    c->maxv = maxv;
+    const int nv = maxv > 0 ? maxv : 1, nc = LX * LY * LZ;
+    CUDA_TRY(cudaMalloc(&c->scratch, cnt_scratch_bytes(nc, nv)));
+    cnt_carve(&c->w, c->scratch, nc, nv);
+    CUDA_TRY(cudaMalloc(&c->mask, sizeof(unsigned) * nv));
+    CUDA_TRY(cudaMalloc(&c->rank, sizeof(int) * 26 * (size_t)nv));
+    CUDA_TRY(cudaMalloc(&c->count, sizeof(int) * fsi_count_ints(nv, 0)));
+    CUDA_TRY(cudaMalloc(&c->img_start, sizeof(int) * 26));
+    // cnt_ini of rank 0: rnd_ini(7119 - rank, 187 + rank, 18278, 15674) (src/cnt/imp/main.h:21)
+    c->trunk.s[0] = 7119; c->trunk.s[1] = 187; c->trunk.s[2] = 18278; c->trunk.s[3] = 15674;
+    *pc = c;
+    return CTC_OK;
+}
+
+extern "C" int ctc_cnt_fin(ctc_cnt *c) {
+    if (!c) return CTC_OK;
+    cudaFree(c->scratch); cudaFree(c->mask); cudaFree(c->rank); cudaFree(c->count); cudaFree(c->img_start);
+    delete c;
+    return CTC_OK;
+}
+
+extern "C" int ctc_cnt_apply_seeded(ctc_cnt *c, const ctc_dpdlj_params *p, int nv, const float *pv, float seed_bulk,
+                                    float seed_halo, float *fv, void *stream) {
+    if (!c || !p || nv < 0 || (nv > 0 && (!pv || !fv))) return fail(CTC_ERR_ARG, "ctc_cnt_apply_seeded: bad arguments");
+    if (nv > c->maxv) return fail(CTC_ERR_CAPACITY, "cnt: %d vertices over capacity %d", nv, c->maxv);
+    if (nv == 0) return CTC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    // the periodic images: the object halo of src/exch/obj, as for FSI
+    CUDA_TRY(fsi_images_launch(nv, c->L, pv, 6, c->mask, c->rank, c->count, c->img_start, st));
+    return cnt_forces(c->L, *p, nv, pv, pv + 3, 6, fv, 3, seed_bulk, seed_halo, nullptr, c->w, c->mask, c->rank,
+                      c->img_start, st);
+}
+
+extern "C" int ctc_cnt_apply(ctc_cnt *c, const ctc_dpdlj_params *p, int nv, const float *pv, float *fv, void *stream) {
+    if (!c) return fail(CTC_ERR_ARG, "ctc_cnt_apply: null");
+    // cnt_bulk draws one seed per pair of types (src/cnt/imp/bulk.h:34), cnt_halo one per type (halo.h:34)
+    float sb = kiss_get4(&c->trunk);
+    float sh = kiss_get4(&c->trunk);
+    return ctc_cnt_apply_seeded(c, p, nv, pv, sb, sh, fv, stream);
 }

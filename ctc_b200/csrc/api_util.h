@@ -30,6 +30,14 @@ int fsi_forces(int3 L, const DpdPar &P, int nv, const float *pv, const float *vv
                int *count, int *img_start, cudaStream_t st, const Boxes &B = Boxes(), const int *vperm = nullptr,
                int vperm_n = 0);
 
+// contact forces (src/cnt) of nv vertices on fv, the periodic images (mask,
+// rank, img_start of fsi_images_launch) already listed; seeds_dev (2 floats)
+// may replace the seeds
+struct CntScratch;
+int cnt_forces(int3 L, const ctc_dpdlj_params &p, int nv, const float *pv, const float *vv, int pstride, float *fv,
+               int fstride, float seed_bulk, float seed_halo, const float *seeds_dev, const CntScratch &w,
+               const unsigned *mask, const int *rank, const int *img_start, cudaStream_t st);
+
 // ---------------------------------------------------------------------------
 // host KISS trunks (src/math/rnd/imp.cpp:12-34)
 // ---------------------------------------------------------------------------

@@ -242,6 +242,16 @@ cudaError_t clist_launch(int3 L, int n, const int *nptr, const float4 *pos_in, c
     return cudaGetLastError();
 }
 
+size_t scan_sums_ints(int nc) { return (size_t)ceil_div(nc, SCAN_TILE) + 1; }
+
+cudaError_t scan_launch(int nc, const int *counts, int *starts, int *sums, cudaStream_t st) {
+    const int nsums = ceil_div(nc, SCAN_TILE);
+    k_scan_tiles<<<nsums, SCAN_T, 0, st>>>(nc, counts, starts, sums);
+    k_scan_sums<<<1, SCAN_T, 0, st>>>(nsums, sums, starts + nc);
+    k_scan_add<<<ceil_div(nc, 256), 256, 0, st>>>(nc, starts, sums);
+    return cudaGetLastError();
+}
+
 cudaError_t aos_to_soa(int n, const float *pp, float4 *pos, float4 *vel, cudaStream_t st) {
     if (n > 0) k_aos_to_soa<<<ceil_div(n, 256), 256, 0, st>>>(n, pp, pos, vel);
     return cudaGetLastError();

@@ -24,6 +24,11 @@ cudaError_t clist_launch(int3 L, int n, const int *nptr, const float4 *pos_in, c
                          const ClistScratch &w, int *err, cudaStream_t st, const Boxes &B = Boxes(),
                          int nc_boxes = 0);
 
+// exclusive scan: starts[0..nc) of counts, starts[nc] = total; sums holds
+// scan_sums_ints(nc) ints
+size_t scan_sums_ints(int nc);
+cudaError_t scan_launch(int nc, const int *counts, int *starts, int *sums, cudaStream_t st);
+
 cudaError_t aos_to_soa(int n, const float *pp, float4 *pos, float4 *vel, cudaStream_t st);
 cudaError_t soa_to_aos(const int *nptr, int nmax, const float4 *pos, const float4 *vel, float *pp,
                        cudaStream_t st);

@@ -104,6 +104,44 @@ __device__ __forceinline__ bool dpd_force(const DpdPar &P, float4 pa, float4 va,
     return true;
 }
 
+// DPD + Lennard-Jones pair force of src/pair/dev.h:49-75,111-139 (PairDPDLJ,
+// membrane-membrane contact), the same plain expressions as the reference:
+// the LJ magnitude e 24 invr t6 (2 t6 - 1), t2 = s^2 invr^2, capped to
+// [0, 1e4], added to the DPD magnitude.  For r^2 < 1e-6 the reference leaves
+// invr unset (its direction is zero there); here invr = 0, no LJ term.
+__device__ __forceinline__ bool dpdlj_force(const DpdPar &P, float ljs, float lje, float4 pa, float4 va, float4 pb,
+                                            float4 vb, float rnd, float3 &f) {
+    float x = pa.x - pb.x, y = pa.y - pb.y, z = pa.z - pb.z;
+    float r2 = x * x + y * y + z * z;                 // norm()
+    if (r2 >= 1) return false;
+    float r, invr = 0.0f;
+    if (r2 < 1e-6f) {
+        x = y = z = 0;
+        r = 0;
+    } else {
+        invr = rsqrtf(r2);
+        r = r2 * invr;
+        x *= invr; y *= invr; z *= invr;
+    }
+    float dvx = va.x - vb.x, dvy = va.y - vb.y, dvz = va.z - vb.z;
+    float ev = x * dvx + y * dvy + z * dvz;
+    float rm = max(1 - r, 0.0f);                      // magn_dpd
+    float wr = powf(rm, P.spow);
+    float f0 = (-P.g * wr * ev + P.s * rnd) * wr;
+    f0 += P.a * rm;
+    float t2 = ljs * ljs * invr * invr;               // magn_lj
+    float t4 = t2 * t2;
+    float t6 = t4 * t2;
+    float lj = lje * 24 * invr * t6 * (2 * t6 - 1);
+    if (lj > 1e4f) lj = 1e4f;                         // cap(f, 0, 1e4)
+    else if (lj < 0) lj = 0;
+    f0 += lj;
+    f.x = f0 * x;
+    f.y = f0 * y;
+    f.z = f0 * z;
+    return true;
+}
+
 // Vector-Jacobian product of one pair force f = phi(r, ev) e (e = dr / r,
 // ev = e . dv, dr = pa - pb, dv = va - vb, phi = (-g wr ev + s rnd) wr + a w,
 // w = 1 - r, wr = w^spow) for the cotangent gf of f, with rnd held fixed:

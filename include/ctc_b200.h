@@ -172,6 +172,26 @@ int ctc_fsi_apply_seeded(ctc_fsi *f, const ctc_dpd_params *p, int nv, const floa
                          const int *starts, const int *counts, float seed_bulk, float seed_halo, int rng,
                          float *fv, float *fs, void *stream);
 
+/* ---- membrane-membrane contact: replaces src/cnt/imp.h ------------------- */
+/* PairDPDLJ {a, g, s, spow, ljs, lje} (src/pair/type.h:22-25): DPD plus a
+ * Lennard-Jones repulsion capped to [0, 1e4] */
+typedef struct {
+    float a, g, s, spow, ljs, lje;
+} ctc_dpdlj_params;
+typedef struct ctc_cnt ctc_cnt;
+/* cnt_ini of a 1-rank periodic box (trunk rnd_ini(7119, 187, 18278, 15674),
+ * src/cnt/imp/main.h:6-22) for one object type of up to maxv vertices */
+int ctc_cnt_ini(int LX, int LY, int LZ, int maxv, ctc_cnt **c);
+int ctc_cnt_fin(ctc_cnt *c);
+/* cnt_build_cells + cnt_bulk + cnt_halo (src/cnt/imp/{main,bulk,halo}.h):
+ * draws the bulk then the halo seed; contact forces between the nv vertices
+ * pv [dev, AoS] (every pair within the cutoff, the periodic images included)
+ * accumulated into fv [dev, AoS] */
+int ctc_cnt_apply(ctc_cnt *c, const ctc_dpdlj_params *p, int nv, const float *pv, float *fv, void *stream);
+/* the same with explicit seeds */
+int ctc_cnt_apply_seeded(ctc_cnt *c, const ctc_dpdlj_params *p, int nv, const float *pv, float seed_bulk,
+                         float seed_halo, float *fv, void *stream);
+
 /* ---- time update: replaces src/scheme/move/imp.h:5-6, scheme/force ------- */
 /* scheme_move_apply: v += f/m dt; r += v dt on n AoS particles [dev] */
 int ctc_scheme_move_apply(float dt, float mass, int n, const float *ff, float *pp, void *stream);
@@ -211,6 +231,12 @@ int ctc_sim_count(ctc_sim *s, int *n, void *stream);
  * the internal membrane forces and the membrane update. */
 int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const int *tri, const float *pp,
                           const ctc_rbc_params *p, const ctc_dpd_params *fsi, float mass, void *stream);
+/* membrane-membrane contact of the system's membranes (obj_inter_forces,
+ * src/sim/objinter/imp/main.h:42-92, with a "contact" entry rbc-rbc): from the
+ * next step on, with FSI, the contact forces of src/cnt (bulk + periodic
+ * images) join the vertex forces; p = NULL switches it off.  The trunk is
+ * rnd_ini(7119, 187, 18278, 15674), drawn for the bulk then the halo. */
+int ctc_sim_set_contact(ctc_sim *s, const ctc_dpdlj_params *p);
 /* download the membrane vertices [host, AoS, nc * nv] */
 int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream);
 /* download the cell-sorted solvent [host, AoS, capacity maxp] */
@@ -226,9 +252,10 @@ int ctc_sim_next_seeds(const ctc_sim *s, float *seeds27);
  * its stream; profile_read returns the summed milliseconds of the
  * CTC_SIM_PHASES phases [0] seeds + wrap + cell lists, [1] fragment starts +
  * force clear, [2] bulk pair forces, [3] halo pair forces, [4] solvent-
- * membrane forces, [5] solvent update, [6] membrane forces + update, and the
- * number of steps, then restarts the count */
-#define CTC_SIM_PHASES 7
+ * membrane forces, [5] membrane-membrane contact, [6] solvent update,
+ * [7] membrane forces + update, and the number of steps, then restarts the
+ * count */
+#define CTC_SIM_PHASES 8
 int ctc_sim_profile(ctc_sim *s, int enable);
 int ctc_sim_profile_read(ctc_sim *s, double *ms, int *steps);
 

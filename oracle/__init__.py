@@ -28,6 +28,12 @@ class Dpd(C.Structure):
     _fields_ = [("a", C.c_float), ("g", C.c_float), ("s", C.c_float), ("spow", C.c_float)]
 
 
+class DpdLj(C.Structure):
+    """``PairDPDLJ {a, g, s, spow, ljs, lje}`` (src/pair/type.h:22-25)."""
+    _fields_ = [("a", C.c_float), ("g", C.c_float), ("s", C.c_float), ("spow", C.c_float),
+                ("ljs", C.c_float), ("lje", C.c_float)]
+
+
 class RbcParams(C.Structure):
     """``RbcParams_v`` (src/rbc/params/imp.h:3-9)."""
     _fields_ = [(k, C.c_float) for k in
@@ -69,6 +75,8 @@ def lib():
             "orc_fsi_bulk": (None, [C.c_int] * 4 + [f32p, C.c_int, f32p, i32p, Dpd, C.c_float, f32p, f32p]),
             "orc_fsi_halo": (None, [C.c_int] * 4 + [f32p, C.c_int, f32p, i32p, Dpd, C.c_float, f32p, f32p]),
             "orc_fsi_halo_images": (C.c_int, [C.c_int] * 4 + [f32p, C.c_void_p, C.c_void_p]),
+            "orc_pair_force_dpdlj": (None, [DpdLj, f32p, f32p, C.c_float, f32p]),
+            "orc_cnt_forces": (None, [C.c_int] * 4 + [f32p, DpdLj, C.c_float, C.c_float, f32p]),
             "orc_mesh_md": (C.c_int, [C.c_int, C.c_int, i32p]),
             "orc_adj_build": (C.c_int, [C.c_int] * 3 + [i32p, i32p, i32p]),
             "orc_area_volume": (None, [C.c_int] * 3 + [i32p, f32p, f64p]),
@@ -189,6 +197,24 @@ def pair_force(dpd, pa, pb, rnd):
     lib().orc_pair_force(*[float(x) for x in dpd], np.asarray(pa, np.float32),
                          np.asarray(pb, np.float32), float(rnd), f)
     return f
+
+
+# ---- membrane-membrane contact (src/cnt) -------------------------------------
+def pair_force_dpdlj(p, pa, pb, rnd):
+    """DPD + Lennard-Jones pair force (src/pair/dev.h:49-75); p = (a, g, s, spow, ljs, lje)."""
+    f = np.zeros(3, np.float32)
+    lib().orc_pair_force_dpdlj(DpdLj(*p), np.ascontiguousarray(pa, np.float32), np.ascontiguousarray(pb, np.float32),
+                               float(rnd), f)
+    return f
+
+
+def cnt_forces(L, pv, p, seed_bulk, seed_halo):
+    """Contact forces of one object type (src/cnt bulk + halo) on the vertices
+    pv (AoS); p = (a, g, s, spow, ljs, lje)."""
+    pv = _pp(pv)
+    fv = np.zeros((len(pv), 3), np.float32)
+    lib().orc_cnt_forces(*L, len(pv), pv, DpdLj(*p), float(seed_bulk), float(seed_halo), fv)
+    return fv
 
 
 # ---- FSI -------------------------------------------------------------------
@@ -357,13 +383,18 @@ def distribute(L, pp):
     return counts, starts, out[:nout]
 
 
-def rbc_step(L, ps, pv, tri, nv, dpd, fsi, rbcpar, seeds27, fsi_seeds, bodyf, dt, ms, mv):
+def rbc_step(L, ps, pv, tri, nv, dpd, fsi, rbcpar, seeds27, fsi_seeds, bodyf, dt, ms, mv, cnt=None,
+             cnt_seeds=None):
     """One step of solvent + membranes in the reference's order
-    (src/sim/imp/run.h:8-68); returns (solvent sorted, vertices)."""
+    (src/sim/imp/run.h:8-68), with membrane-membrane contact (cnt: a PairDPDLJ
+    tuple, cnt_seeds: its bulk and halo seeds) among the object forces
+    (src/sim/objinter/imp/main.h:42-92); returns (solvent sorted, vertices)."""
     counts, starts, ps = distribute(L, ps)
     pv = rbc_wrap(L, pv, nv)
     fs = dpd_bulk(L, ps, starts, dpd, seeds27[0]) + dpd_halo(L, ps, starts, counts, dpd, seeds27[1:])
     fv, fs2 = fsi_forces(L, pv, ps, starts, fsi, fsi_seeds[0], fsi_seeds[1])
+    if cnt is not None:
+        fv = fv + cnt_forces(L, pv, cnt, cnt_seeds[0], cnt_seeds[1])
     fs = fs + fs2
     a = np.asarray(bodyf if bodyf is not None else (0, 0, 0), np.float32)
     fs = body_force(fs, ms, a)

@@ -521,6 +521,131 @@ void orc_fsi_halo(int LX, int LY, int LZ, int nv, const float *pv, int ns, const
 }
 
 /* ========================================================================= */
+/* membrane-membrane contact, src/cnt (one object type)                       */
+/* ========================================================================= */
+
+/* PairDPDLJ: the DPD magnitude plus the Lennard-Jones one,
+ * 24 e invr t6 (2 t6 - 1) with t2 = s^2 invr^2, t6 = t2^3, capped to [0, 1e4]
+ * (src/pair/dev.h:49-58, 70-75).  For r^2 < 1e-6 the reference leaves invr
+ * unset (src/pair/dev.h:19-21) and the direction zero; here invr = 0 there,
+ * so the force is zero. */
+static void pair_force_dpdlj_ref(orc_dpdlj p, const float *pa, const float *pb, float rnd, float f[3]) {
+    float x, y, z, r2, invr = 0, r, ev, rm, wr, f0, t2, t4, t6, lj;
+    float dvx, dvy, dvz;
+    x = pa[0] - pb[0]; y = pa[1] - pb[1]; z = pa[2] - pb[2];
+    dvx = pa[3] - pb[3]; dvy = pa[4] - pb[4]; dvz = pa[5] - pb[5];
+    r2 = dist2f(x, y, z);
+    if (r2 >= 1.0f) { f[0] = f[1] = f[2] = 0; return; }         /* NORM_BIG */
+    if (r2 < 1e-6f) {                                              /* NORM_SMALL */
+        x = y = z = 0; r = 0;
+    } else {
+        invr = 1.0f / sqrtf(r2);
+        r = r2 * invr;
+        x *= invr; y *= invr; z *= invr;
+    }
+    ev = fmaf(z, dvz, fmaf(y, dvy, x * dvx));
+    rm = 1.0f - r; if (rm < 0.0f) rm = 0.0f;
+    wr = powf(rm, p.spow);
+    f0 = fmaf(p.a, rm, fmaf(p.s, rnd, ((-p.g) * wr) * ev) * wr);
+    t2 = p.ljs * p.ljs * invr * invr;                              /* magn_lj */
+    t4 = t2 * t2;
+    t6 = t4 * t2;
+    lj = p.lje * 24 * invr * t6 * fmaf(2.0f, t6, -1.0f);
+    if (lj > 1e4f) lj = 1e4f;                                      /* cap(f, 0, 1e4) */
+    else if (lj < 0.0f) lj = 0.0f;
+    f0 += lj;
+    f[0] = f0 * x; f[1] = f0 * y; f[2] = f0 * z;
+}
+
+void orc_pair_force_dpdlj(orc_dpdlj p, const float pa[6], const float pb[6], float rnd, float f[3]) {
+    pair_force_dpdlj_ref(p, pa, pb, rnd, f);
+}
+
+/* vertex cell list of cnt_build_cells (src/cnt/imp/main.h:33-45): the cell of
+ * clist_subindex with project = true (src/clist/dev/main.h:13-42: double
+ * precision index, clamped into the box); inside a cell by vertex index (the
+ * reference's order is its atomics'; the keys do not depend on it) */
+static void cnt_cells(int LX, int LY, int LZ, int nv, const float *pv, int *starts, int *ids) {
+    int nc = LX * LY * LZ, i, *cid = (int*)malloc(sizeof(int) * (nv + 1)), *fill = (int*)calloc(nc + 1, sizeof(int));
+    for (i = 0; i <= nc; i++) starts[i] = 0;
+    for (i = 0; i < nv; i++) {
+        const float *r = pv + 6 * i;
+        int ix = clamp_cell((int)((double)r[0] + LX / 2), LX);
+        int iy = clamp_cell((int)((double)r[1] + LY / 2), LY);
+        int iz = clamp_cell((int)((double)r[2] + LZ / 2), LZ);
+        cid[i] = ix + LX * (iy + LY * iz);
+        starts[cid[i] + 1]++;
+    }
+    for (i = 0; i < nc; i++) starts[i + 1] += starts[i];
+    for (i = 0; i < nv; i++) ids[starts[cid[i]] + fill[cid[i]]++] = i;
+    free(cid); free(fill);
+}
+
+/* r2map of src/cnt/dev/map/bulk.h:1-64: as the FSI rows, with the centre cell
+ * clamped into the box */
+static int cnt_rows_bulk(int LX, int LY, int LZ, const int *start, int zplane, int n, float x, float y, float z,
+                         Rows *m) {
+    int xc = LX / 2 + (int)floorf(x), yc = LY / 2 + (int)floorf(y), zc = LZ / 2 + (int)floorf(z);
+    xc = xc < 0 ? 0 : (xc > LX - 1 ? LX - 1 : xc);
+    yc = yc < 0 ? 0 : (yc > LY - 1 ? LY - 1 : yc);
+    zc = zc < 0 ? 0 : (zc > LZ - 1 ? LZ - 1 : zc);
+    /* centres of a cell inside the box: fsi_rows on the cell centre gives the same rows */
+    return fsi_rows(LX, LY, LZ, start, zplane, n, (float)(xc - LX / 2) + 0.5f, (float)(yc - LY / 2) + 0.5f,
+                    (float)(zc - LZ / 2) + 0.5f, m);
+}
+
+void orc_cnt_forces(int LX, int LY, int LZ, int nv, const float *pv, orc_dpdlj p, float seed_bulk,
+                    float seed_halo, float *fv) {
+    int nc = LX * LY * LZ, *starts = (int*)malloc(sizeof(int) * (nc + 1)), *ids = (int*)malloc(sizeof(int) * (nv + 1));
+    int aid, zp, j, k, nimg, *frag, *vert;
+    float f[3];
+    cnt_cells(LX, LY, LZ, nv, pv, starts, ids);
+    for (aid = 0; aid < nv; aid++) {                   /* src/cnt/dev/bulk.h: self pairs, bid < aid */
+        const float *a = pv + 6 * aid;
+        float fa[3] = {0, 0, 0};
+        for (zp = 0; zp < 3; zp++) {
+            Rows m;
+            if (!cnt_rows_bulk(LX, LY, LZ, starts, zp, nv, a[0], a[1], a[2], &m)) continue;
+            for (j = 0; j < 3; j++)
+                for (k = m.o[j]; k < m.o[j] + m.c[j]; k++) {
+                    int bid = ids[k];
+                    if (aid <= bid) continue;
+                    pair_force_dpdlj_ref(p, a, pv + 6 * bid, orc_mean0var1ii(seed_bulk, aid, bid), f);
+                    fa[0] += f[0]; fa[1] += f[1]; fa[2] += f[2];
+                    fv[3 * bid + 0] -= f[0]; fv[3 * bid + 1] -= f[1]; fv[3 * bid + 2] -= f[2];
+                }
+        }
+        fv[3 * aid + 0] += fa[0]; fv[3 * aid + 1] += fa[1]; fv[3 * aid + 2] += fa[2];
+    }
+    /* src/cnt/dev/halo.h: every image against every local vertex in its rows;
+     * the image's force goes back to its vertex (eobj_unpack_ff) */
+    nimg = orc_fsi_halo_images(LX, LY, LZ, nv, pv, NULL, NULL);
+    frag = (int*)malloc(sizeof(int) * (nimg + 1)); vert = (int*)malloc(sizeof(int) * (nimg + 1));
+    orc_fsi_halo_images(LX, LY, LZ, nv, pv, frag, vert);
+    for (aid = 0; aid < nimg; aid++) {
+        float A[6], fa[3] = {0, 0, 0};
+        int fid = frag[aid];
+        memcpy(A, pv + 6 * vert[aid], sizeof(A));
+        A[0] -= (float)(orc_frag_i2d(fid, 0) * LX);
+        A[1] -= (float)(orc_frag_i2d(fid, 1) * LY);
+        A[2] -= (float)(orc_frag_i2d(fid, 2) * LZ);
+        for (zp = 0; zp < 3; zp++) {
+            Rows m;
+            if (!fsi_rows(LX, LY, LZ, starts, zp, nv, A[0], A[1], A[2], &m)) continue;
+            for (j = 0; j < 3; j++)
+                for (k = m.o[j]; k < m.o[j] + m.c[j]; k++) {
+                    int bid = ids[k];
+                    pair_force_dpdlj_ref(p, A, pv + 6 * bid, orc_mean0var1ii(seed_halo, aid, bid), f);
+                    fa[0] += f[0]; fa[1] += f[1]; fa[2] += f[2];
+                    fv[3 * bid + 0] -= f[0]; fv[3 * bid + 1] -= f[1]; fv[3 * bid + 2] -= f[2];
+                }
+        }
+        fv[3 * vert[aid] + 0] += fa[0]; fv[3 * vert[aid] + 1] += fa[1]; fv[3 * vert[aid] + 2] += fa[2];
+    }
+    free(frag); free(vert); free(starts); free(ids);
+}
+
+/* ========================================================================= */
 /* membrane, src/rbc                                                         */
 /* ========================================================================= */
 

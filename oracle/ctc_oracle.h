@@ -86,6 +86,17 @@ void orc_fsi_halo(int LX, int LY, int LZ, int nv, const float *pv, int ns, const
 /* number of halo images and their (fragment, vertex) lists */
 int  orc_fsi_halo_images(int LX, int LY, int LZ, int nv, const float *pv, int *frag, int *vert);
 
+/* ---- membrane-membrane contact (src/cnt), one object type ----------------- */
+typedef struct { float a, g, s, spow, ljs, lje; } orc_dpdlj;   /* PairDPDLJ, src/pair/type.h:22-25 */
+/* DPD + Lennard-Jones pair force (src/pair/dev.h:49-75, 111-139) */
+void orc_pair_force_dpdlj(orc_dpdlj p, const float pa[6], const float pb[6], float rnd, float f[3]);
+/* contact forces of nv vertices (AoS, 6 floats), accumulated into fv (3 per
+ * vertex): cnt_bulk (src/cnt/imp/bulk.h:8-44, dev/bulk.h) with seed_bulk, then
+ * cnt_halo over the periodic images (src/cnt/imp/halo.h, dev/halo.h) with
+ * seed_halo */
+void orc_cnt_forces(int LX, int LY, int LZ, int nv, const float *pv, orc_dpdlj p, float seed_bulk,
+                    float seed_halo, float *fv);
+
 /* ---- membrane (src/rbc) --------------------------------------------------- */
 typedef struct {
     float gammaC, gammaT, kBT, kb, phi, ks, x0, mpow, ka, kd, kv, totArea, totVolume;

@@ -53,3 +53,16 @@ def test_argument_errors_are_reported_not_fatal():
     rc = L.ctc_fluforces_ini(2, 8, 8, 10, ctypes.byref(h))   # box must be >= 3 cells
     assert rc == _lib.CTC_ERR_ARG
     assert b"box" in L.ctc_last_error()
+
+
+def test_binding_constants_match_the_header():
+    """The Python mirror of the header's #defines (array sizes the binding
+    allocates for the library to fill)."""
+    src = open(os.path.join(ROOT, "include", "ctc_b200.h")).read()
+    for name in ("CTC_SIM_PHASES", "CTC_RNG_REFERENCE", "CTC_RNG_STABLE"):
+        m = re.search(r"#define\s+%s\s+(\d+)" % name, src)
+        if m is None:
+            m = re.search(r"\b%s\s*=\s*(\d+)" % name, src)
+        assert m is not None, name
+        assert getattr(_lib, name) == int(m.group(1)), name
+    assert len(_lib.SIM_PHASE_NAMES) == _lib.CTC_SIM_PHASES
