@@ -265,6 +265,7 @@ class Sim:
         cfg.bodyf = (C.c_float * 3)(*bodyf)
         cfg.rng = rng
         self.maxp = int(maxp)
+        self.L = tuple(int(x) for x in L)
         self.h = C.c_void_p()
         check(lib().ctc_sim_create(C.byref(cfg), C.byref(self.h)))
 
