@@ -290,6 +290,10 @@ class Sim:
                                           pv.ctypes.data_as(C.c_void_p), C.byref(_lib.RbcParams(**params)),
                                           C.byref(fsi), float(mass), _stream(stream)))
 
+    def set_graph(self, enable=True):
+        """Replay the step as CUDA graphs (captured on first use)."""
+        check(lib().ctc_sim_set_graph(self.h, int(bool(enable))))
+
     def set_contact(self, params):
         """Membrane-membrane contact (a DpdLjParams) from the next step on; None: off."""
         check(lib().ctc_sim_set_contact(self.h, None if params is None else C.byref(params)))

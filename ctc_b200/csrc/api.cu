@@ -287,6 +287,11 @@ struct ctc_sim {
     void *cnt_scratch;                     // vertex cell list of the contact pairs
     CntScratch cw;
     Kiss cnt_host;                         // host mirror of the contact trunk
+    // the step as CUDA graphs (one from each ping-pong buffer) on an own stream
+    bool use_graph;
+    cudaGraphExec_t gexec[2];
+    cudaStream_t own;
+    cudaEvent_t ev_in, ev_out;
 };
 
 // the contact's vertex cell list for the current membranes
@@ -363,8 +368,14 @@ extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
     return CTC_OK;
 }
 
+static void sim_drop_graphs(ctc_sim *s);
+
 extern "C" int ctc_sim_destroy(ctc_sim *s) {
     if (!s) return CTC_OK;
+    sim_drop_graphs(s);
+    if (s->own) cudaStreamDestroy(s->own);
+    if (s->ev_in) cudaEventDestroy(s->ev_in);
+    if (s->ev_out) cudaEventDestroy(s->ev_out);
     for (int b = 0; b < 2; b++) { cudaFree(s->pos[b]); cudaFree(s->vel[b]); }
     cudaFree(s->force); cudaFree(s->counts); cudaFree(s->starts); cudaFree(s->count0); cudaFree(s->fss);
     cudaFree(s->scratch); cudaFree(s->trunk_dev); cudaFree(s->seeds_dev); cudaFree(s->diag_scratch);
@@ -390,6 +401,7 @@ static int sim_set(ctc_sim *s, int n, const float *pp, bool host, cudaStream_t s
         src = tmp;
     }
     s->cur = 0;
+    sim_drop_graphs(s);                  // the grids follow the particle count
     CUDA_TRY(aos_to_soa(n, src, s->pos[0], s->vel[0], st));
     CUDA_TRY(cudaMemcpyAsync(s->count0, &n, sizeof(int), cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaStreamSynchronize(st));
@@ -413,6 +425,7 @@ extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const i
         return fail(CTC_ERR_ARG, "ctc_sim_set_membranes: bad arguments");
     if ((long)nc * nv > (1 << 27)) return fail(CTC_ERR_CAPACITY, "ctc_sim_set_membranes: too many vertices");
     cudaStream_t st = (cudaStream_t)stream;
+    sim_drop_graphs(s);
     if (s->rbc) { ctc_rbc_force_fin(s->rbc); s->rbc = nullptr; }
     cudaFree(s->mpos); cudaFree(s->mvel); cudaFree(s->mforce); cudaFree(s->mcount);
     cudaFree(s->fmask); cudaFree(s->frank); cudaFree(s->fcount); cudaFree(s->fimg_start); cudaFree(s->vperm);
@@ -458,6 +471,7 @@ extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const i
 
 extern "C" int ctc_sim_set_contact(ctc_sim *s, const ctc_dpdlj_params *p) {
     if (!s) return fail(CTC_ERR_ARG, "ctc_sim_set_contact: null");
+    sim_drop_graphs(s);
     s->cnt_on = p != nullptr;
     if (p) s->cnt = *p;
     return sim_cnt_alloc(s);
@@ -478,15 +492,16 @@ extern "C" int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream) {
 }
 
 // one step: seeds, wrap + cell lists into the other buffer, forces, update
-static int sim_step1(ctc_sim *s, cudaStream_t st) {
+// the device work of one step from buffer s->cur (built: the cell lists
+// describe it, so its count is starts[nc]); enqueued on st, capturable
+static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
     int src = s->cur, dst = 1 - s->cur;
     int ntr = s->cfg.rng == CTC_RNG_REFERENCE ? 27 : 1;
     sim_mark(s, 0, st);
     CUDA_TRY(draw_seeds_launch(s->trunk_dev, ntr, s->seeds_dev, st));
-    for (int k = 0; k < ntr; k++) kiss_get(&s->trunk_host[k]);
     // the count pointer of the input is starts[nc] of the previous build: copy
     // it aside, the build overwrites starts
-    if (s->built) CUDA_TRY(cudaMemcpyAsync(s->count0, s->starts + s->nc, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    if (built) CUDA_TRY(cudaMemcpyAsync(s->count0, s->starts + s->nc, sizeof(int), cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(clist_launch(s->L, s->n_host, s->count0, s->pos[src], s->vel[src], 1, s->counts, s->starts,
                           s->pos[dst], s->vel[dst], nullptr, s->w, dev_err_ptr(), st));
     const int nvt = s->mnc * s->mnv;
@@ -495,13 +510,8 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
         CUDA_TRY(rbc_wrap_launch(s->mnc, s->mnv, s->L, s->mpos, st));
         // the FSI trunk is drawn for fsi_bulk, then for fsi_halo
         CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 27, 2, s->seeds_dev + 27, st));
-        kiss_get(&s->fsi_host);
-        kiss_get(&s->fsi_host);
-        if (s->cnt_on) {   // the contact trunk: cnt_bulk, then cnt_halo
+        if (s->cnt_on)     // the contact trunk: cnt_bulk, then cnt_halo
             CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 28, 2, s->seeds_dev + 29, st));
-            kiss_get(&s->cnt_host);
-            kiss_get(&s->cnt_host);
-        }
     }
     sim_mark(s, 1, st);
     DpdArgs A;
@@ -556,18 +566,93 @@ static int sim_step1(ctc_sim *s, cudaStream_t st) {
         CUDA_TRY(integrate_launch(s->mcount, nvt, s->mpos, s->mvel, s->mforce, s->cfg.dt, s->mmass, bf, st));
     }
     sim_mark(s, 8, st);
+    return CTC_OK;
+}
+
+// the host side of one step: the mirrors of the trunks the device drew from,
+// the buffer flip
+static void sim_advance(ctc_sim *s) {
+    const int ntr = s->cfg.rng == CTC_RNG_REFERENCE ? 27 : 1;
+    for (int k = 0; k < ntr; k++) kiss_get(&s->trunk_host[k]);
+    if (s->mnc * s->mnv > 0) {
+        kiss_get(&s->fsi_host);
+        kiss_get(&s->fsi_host);
+        if (s->cnt_on) {
+            kiss_get(&s->cnt_host);
+            kiss_get(&s->cnt_host);
+        }
+    }
     if (s->prof) s->prof_steps++;
-    s->cur = dst;
+    s->cur = 1 - s->cur;
     s->built = true;
+}
+
+static int sim_step1(ctc_sim *s, cudaStream_t st) {
+    int rc = sim_enqueue(s, st, s->built);
+    if (rc) return rc;
+    sim_advance(s);
+    return CTC_OK;
+}
+
+// graphs of the step from buffer 0 and from buffer 1 (ctc_sim_set_graph)
+static void sim_drop_graphs(ctc_sim *s) {
+    for (int k = 0; k < 2; k++)
+        if (s->gexec[k]) { cudaGraphExecDestroy(s->gexec[k]); s->gexec[k] = nullptr; }
+}
+
+static int sim_capture(ctc_sim *s, int k) {
+    if (!s->own) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&s->ev_in, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&s->ev_out, cudaEventDisableTiming));
+    }
+    if (!dev_err_ptr()) return fail(CTC_ERR_CUDA, "ctc_sim_step: device error word unavailable");
+    const int keep = s->cur;
+    s->cur = k;
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(s->own, cudaStreamCaptureModeThreadLocal));
+    int rc = sim_enqueue(s, s->own, true);
+    cudaError_t e = cudaStreamEndCapture(s->own, &g);
+    s->cur = keep;
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) return fail(CTC_ERR_CUDA, "ctc_sim_step: capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&s->gexec[k], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(CTC_ERR_CUDA, "ctc_sim_step: instantiate: %s", cudaGetErrorString(e));
     return CTC_OK;
 }
 
 extern "C" int ctc_sim_step(ctc_sim *s, int nsteps, void *stream) {
     if (!s || nsteps < 0) return fail(CTC_ERR_ARG, "ctc_sim_step: bad arguments");
-    for (int k = 0; k < nsteps; k++) {
-        int rc = sim_step1(s, (cudaStream_t)stream);
+    cudaStream_t st = (cudaStream_t)stream;
+    int k = 0;
+    // the first step after new state, and profiled steps, run directly
+    for (; k < nsteps && (!s->use_graph || s->prof || !s->built); k++) {
+        int rc = sim_step1(s, st);
         if (rc) return rc;
     }
+    if (k == nsteps) return CTC_OK;
+    for (int b = 0; b < 2; b++)
+        if (!s->gexec[b]) {
+            int rc = sim_capture(s, b);
+            if (rc) return rc;
+        }
+    // graphs run on the object's own stream, ordered after and before the caller's
+    CUDA_TRY(cudaEventRecord(s->ev_in, st));
+    CUDA_TRY(cudaStreamWaitEvent(s->own, s->ev_in, 0));
+    for (; k < nsteps; k++) {
+        CUDA_TRY(cudaGraphLaunch(s->gexec[s->cur], s->own));
+        sim_advance(s);
+    }
+    CUDA_TRY(cudaEventRecord(s->ev_out, s->own));
+    CUDA_TRY(cudaStreamWaitEvent(st, s->ev_out, 0));
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_set_graph(ctc_sim *s, int enable) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sim_set_graph: null");
+    if (!enable) sim_drop_graphs(s);
+    s->use_graph = enable != 0;
     return CTC_OK;
 }
 

@@ -220,6 +220,11 @@ int ctc_sim_set_solvent_dev(ctc_sim *s, int n, const float *pp, void *stream);
 /* advance nsteps steps: wrap + cell lists, bulk + halo DPD, body force,
  * update -- the reference's step order (src/sim/imp/run.h:8-68) */
 int ctc_sim_step(ctc_sim *s, int nsteps, void *stream);
+/* 1: steps replay CUDA graphs captured on first use (one per ping-pong
+ * buffer) on the object's own stream, ordered after the caller's stream work
+ * and before its later work; the first step after new state and profiled
+ * steps run directly; 0: direct launches */
+int ctc_sim_set_graph(ctc_sim *s, int enable);
 /* number of solvent particles (synchronises the stream) */
 int ctc_sim_count(ctc_sim *s, int *n, void *stream);
 /* red-blood-cell membranes of the system: nc cells of one template (nv
