@@ -12,9 +12,7 @@
 //     not clamped), key mean0var1ii(seed_halo, image index, bid); the image's
 //     force goes back to its vertex (eobj_unpack_ff).
 // A pair across a periodic face is therefore taken twice, once from each
-// image, as the reference does.  One thread per vertex (a few dozen
-// candidates each); the vertex's own force is summed in registers, the
-// partners' with global reductions.
+// image, as the reference does.
 #include <algorithm>
 
 #include "cnt.h"
@@ -85,69 +83,129 @@ __device__ __forceinline__ void vred(float *f, int stride, int i, float s, float
     atomicAdd(o + 2, s * v.z);
 }
 
-// the pairs of a (at position pa, velocity va) with the vertices of the rows
-// around cell (xc, yc, zc): 3 z-planes x 3 y-rows of cells xc-1 .. xc+1, each
-// clipped to the box (src/cnt/dev/map/{bulk,halo}.h); below: only bid < below
-__device__ __forceinline__ void cnt_rows(const CntArgs &A, float4 pa, float4 va, int xc, int yc, int zc, int below,
-                                         int key, float seed, float3 &fa) {
+// One thread per vertex walks its rows: first the bulk rows around its
+// clamped cell (partners bid < aid), then, for each of its periodic images,
+// the rows around the image (every partner).  Accepted pairs go through a
+// per-warp queue and are evaluated 32 at a time (the RNG and the force with
+// every lane busy); both sides take their force by a global reduction.
+// Queue record: owner vertex, partner, key, tag (0: bulk, 1 + fid: image).
+constexpr int CNT_T = 128, CNT_QCAP = 64, CNT_U = 4;
+
+__global__ void __launch_bounds__(CNT_T) k_cnt(const __grid_constant__ CntArgs A) {
+    __shared__ uint4 queue[CNT_T / 32][CNT_QCAP];
+    const int lane = threadIdx.x & 31;
+    uint4 *q = queue[threadIdx.x >> 5];
+    int qn = 0;
     const int3 L = A.L;
-    if (xc - 1 >= L.x || xc + 2 <= 0) return;
-    const int xs = max(0, xc - 1), xn = min(L.x, xc + 2) - xs;
-    for (int zp = 0; zp < 3; zp++) {
-        const int zz = zc - 1 + zp;
-        if (zz < 0 || zz >= L.z) continue;
-        for (int dy = -1; dy <= 1; dy++) {
-            const int yy = yc + dy;
-            if (yy < 0 || yy >= L.y) continue;
-            const int cid = xs + L.x * (yy + L.y * zz);
-            const int e = __ldg(A.starts + cid + xn);
-            for (int k = __ldg(A.starts + cid); k < e; k++) {
-                const int b = __ldg(A.ids + k);
-                if (b >= below) continue;
-                const float4 pb = vload(A.pv, A.pstride, b);
-                if (dist2(pa.x - pb.x, pa.y - pb.y, pa.z - pb.z) >= 1.0f) continue;   // zero force
-                const float rnd = mean0var1ii(seed, key, b);
-                float3 f;
-                if (!dpdlj_force(A.par, A.ljs, A.lje, pa, va, pb, vload(A.vv, A.pstride, b), rnd, f)) continue;
-                fa.x += f.x; fa.y += f.y; fa.z += f.z;
+    const int i = blockIdx.x * CNT_T + threadIdx.x;
+    bool act = i < A.nv;
+    const float seed_bulk = A.seeds_dev ? A.seeds_dev[0] : A.seed_bulk;
+    const float seed_halo = A.seeds_dev ? A.seeds_dev[1] : A.seed_halo;
+
+    auto process = [&](int m) {
+        if (lane < m) {
+            const uint4 rec = q[lane];
+            const int v = (int)rec.x, b = (int)rec.y;
+            float4 a = vload(A.pv, A.pstride, v);
+            if (rec.w) {            // the image through fragment rec.w - 1
+                const int fid = (int)rec.w - 1;
+                a.x = a.x + (float)(-frag_i2dx(fid) * L.x);
+                a.y = a.y + (float)(-frag_i2dy(fid) * L.y);
+                a.z = a.z + (float)(-frag_i2dz(fid) * L.z);
+            }
+            const float rnd = mean0var1ii(rec.w ? seed_halo : seed_bulk, (int)rec.z, b);
+            float3 f;
+            if (dpdlj_force(A.par, A.ljs, A.lje, a, vload(A.vv, A.pstride, v), vload(A.pv, A.pstride, b),
+                            vload(A.vv, A.pstride, b), rnd, f)) {
+                vred(A.fv, A.fstride, v, 1.0f, f);
                 vred(A.fv, A.fstride, b, -1.0f, f);
             }
         }
-    }
-}
+        __syncwarp();
+    };
+    auto push = [&](bool ok, uint4 rec) {
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) q[qn + __popc(bal & ((1u << lane) - 1u))] = rec;
+        qn += __popc(bal);
+        __syncwarp();
+        if (qn >= 32) {
+            process(32);
+            qn -= 32;
+            if (lane < qn) q[lane] = q[32 + lane];
+            __syncwarp();
+        }
+    };
 
-__global__ void __launch_bounds__(128) k_cnt(const __grid_constant__ CntArgs A) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.nv) return;
-    const int3 L = A.L;
-    const float seed_bulk = A.seeds_dev ? A.seeds_dev[0] : A.seed_bulk;
-    const float seed_halo = A.seeds_dev ? A.seeds_dev[1] : A.seed_halo;
-    const float4 pa = vload(A.pv, A.pstride, i), va = vload(A.vv, A.pstride, i);
-    float3 fa = make_float3(0.0f, 0.0f, 0.0f);
-    // bulk: the centre cell clamped into the box (projected positions)
-    {
-        const int xc = min(max(L.x / 2 + (int)floorf(pa.x), 0), L.x - 1);
-        const int yc = min(max(L.y / 2 + (int)floorf(pa.y), 0), L.y - 1);
-        const int zc = min(max(L.z / 2 + (int)floorf(pa.z), 0), L.z - 1);
-        cnt_rows(A, pa, va, xc, yc, zc, i, i, seed_bulk, fa);
+    float4 pa = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    unsigned m = 0;
+    if (act) {
+        pa = vload(A.pv, A.pstride, i);
+        m = __ldg(A.img_mask + i);
     }
-    // halo: the vertex's images, each shifted into the frame of the side it
-    // is sent to (r - L d(fid)), against every local vertex
-    unsigned m = __ldg(A.img_mask + i);
-    while (m) {
-        const int fid = __ffs(m) - 1;
-        m &= m - 1;
-        const int r = __ldg(A.img_rank + (size_t)fid * A.nv + i);
-        if (r < 0) continue;
-        const int aid = __ldg(A.img_start + fid) + r;
-        float4 a = pa;
-        a.x = a.x + (float)(-frag_i2dx(fid) * L.x);
-        a.y = a.y + (float)(-frag_i2dy(fid) * L.y);
-        a.z = a.z + (float)(-frag_i2dz(fid) * L.z);
-        cnt_rows(A, a, va, L.x / 2 + (int)floorf(a.x), L.y / 2 + (int)floorf(a.y), L.z / 2 + (int)floorf(a.z),
-                 0x7fffffff, aid, seed_halo, fa);
+    // the current centre: its position a, cell (xc, yc, zc), partner bound,
+    // key and tag; row = next of its 9 rows (3 z-planes x 3 y-rows)
+    float4 a = pa;
+    int xc = 0, yc = 0, zc = 0, below = 0, key = 0, tag = 0, row = 9, k = 0, ke = 0;
+    bool bulk_done = false;
+    for (;;) {
+        if (act) {
+            while (k >= ke) {
+                if (row < 9) {
+                    const int zz = zc - 1 + row / 3, yy = yc + row % 3 - 1;
+                    row++;
+                    if (xc - 1 >= L.x || xc + 2 <= 0 || zz < 0 || zz >= L.z || yy < 0 || yy >= L.y) continue;
+                    const int xs = max(0, xc - 1), xn = min(L.x, xc + 2) - xs;
+                    const int cid = xs + L.x * (yy + L.y * zz);
+                    k = __ldg(A.starts + cid);
+                    ke = __ldg(A.starts + cid + xn);
+                } else if (!bulk_done) {      // bulk: the centre cell clamped into the box
+                    bulk_done = true;
+                    a = pa;
+                    xc = min(max(L.x / 2 + (int)floorf(pa.x), 0), L.x - 1);
+                    yc = min(max(L.y / 2 + (int)floorf(pa.y), 0), L.y - 1);
+                    zc = min(max(L.z / 2 + (int)floorf(pa.z), 0), L.z - 1);
+                    below = i; key = i; tag = 0; row = 0;
+                } else if (m) {               // next image, shifted by -L d(fid)
+                    const int fid = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int r = __ldg(A.img_rank + (size_t)fid * A.nv + i);
+                    if (r < 0) continue;
+                    key = __ldg(A.img_start + fid) + r;
+                    a = pa;
+                    a.x = a.x + (float)(-frag_i2dx(fid) * L.x);
+                    a.y = a.y + (float)(-frag_i2dy(fid) * L.y);
+                    a.z = a.z + (float)(-frag_i2dz(fid) * L.z);
+                    xc = L.x / 2 + (int)floorf(a.x);
+                    yc = L.y / 2 + (int)floorf(a.y);
+                    zc = L.z / 2 + (int)floorf(a.z);
+                    below = 0x7fffffff; tag = 1 + fid; row = 0;
+                } else {
+                    act = false;
+                    break;
+                }
+            }
+        }
+        const bool have = act && k < ke;
+        if (!__any_sync(0xffffffffu, have)) break;
+        int bid[CNT_U];
+        float4 pb[CNT_U];
+#pragma unroll
+        for (int u = 0; u < CNT_U; u++) {
+            bid[u] = 0x7fffffff;
+            if (have && k + u < ke) {
+                bid[u] = __ldg(A.ids + k + u);
+                pb[u] = vload(A.pv, A.pstride, bid[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < CNT_U; u++) {
+            const bool ok = have && k + u < ke && bid[u] < below &&
+                            dist2(a.x - pb[u].x, a.y - pb[u].y, a.z - pb[u].z) < 1.0f;   // else zero force
+            push(ok, make_uint4((unsigned)i, (unsigned)bid[u], (unsigned)key, (unsigned)tag));
+        }
+        if (have) k = min(k + CNT_U, ke);
     }
-    vred(A.fv, A.fstride, i, 1.0f, fa);
+    if (qn > 0) process(qn);
 }
 
 // ---------------------------------------------------------------------------
@@ -183,7 +241,7 @@ cudaError_t cnt_cells_launch(int3 L, int nv, const float *pv, int pstride, const
 }
 
 cudaError_t cnt_launch(const CntArgs &A, cudaStream_t st) {
-    if (A.nv > 0) k_cnt<<<ceil_div(A.nv, 128), 128, 0, st>>>(A);
+    if (A.nv > 0) k_cnt<<<ceil_div(A.nv, CNT_T), CNT_T, 0, st>>>(A);
     return cudaGetLastError();
 }
 
