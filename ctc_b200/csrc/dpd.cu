@@ -88,7 +88,10 @@ __device__ __forceinline__ void vjp_par(const DpdArgs &A, float da, float dg) {
 template <int RNG, bool BATCH, int T, int UNROLL, int MODE = 0>
 __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs A) {
     constexpr int W = T / 32;
-    __shared__ BulkRec<BATCH> queue[W][QCAP];
+    // ring of accepted pairs per warp, drained every DR pushes: at most
+    // 31 + 32 DR records wait (RQ a power of two above that)
+    constexpr int DR = UNROLL < 4 ? UNROLL : 4, RQ = 256;
+    __shared__ BulkRec<BATCH> queue[W][RQ];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ia = blockIdx.x * T + threadIdx.x;
     int3 L = A.L;
@@ -108,7 +111,7 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
     const float *seeds = A.seeds_dev ? A.seeds_dev : A.seeds;
     const DpdPar P = A.par;
     BulkRec<BATCH> *q = queue[warp];
-    int qn = 0;
+    unsigned head = 0, tail = 0;                    // ring positions (wrap at RQ)
     float acc_a = 0.0f, acc_g = 0.0f;               // MODE 1: parameter cotangents
 
     float4 pa = make_float4(0, 0, 0, 0);
@@ -123,7 +126,7 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
 
     auto process = [&](int m) {
         if (lane < m) {
-            const BulkRec<BATCH> rec = q[lane];
+            const BulkRec<BATCH> rec = q[(head + lane) & (RQ - 1)];
             const int i = (int)rec.v.x, j = (int)rec.v.y;
             float4 p1 = __ldg(A.pos + i), p2 = __ldg(A.pos + j);
             float4 v1 = __ldg(A.vel + i), v2 = __ldg(A.vel + j);
@@ -164,17 +167,17 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
     auto push = [&](bool ok, int cand) {
         const unsigned bal = __ballot_sync(0xffffffffu, ok);
         if (ok) {
-            BulkRec<BATCH> &e = q[qn + __popc(bal & ((1u << lane) - 1u))];
+            BulkRec<BATCH> &e = q[(tail + __popc(bal & ((1u << lane) - 1u))) & (RQ - 1)];
             if constexpr (BATCH) e.v = make_uint4((unsigned)ia, (unsigned)cand, (unsigned)box, 0u);
             else e.v = make_uint2((unsigned)ia, (unsigned)cand);
         }
-        qn += __popc(bal);
+        tail += __popc(bal);
+    };
+    auto drain = [&]() {
         __syncwarp();
-        if (qn >= 32) {
+        while (tail - head >= 32) {
             process(32);
-            qn -= 32;
-            if (lane < qn) q[lane] = q[32 + lane];
-            __syncwarp();
+            head += 32;
         }
     };
 
@@ -207,10 +210,12 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
             const bool v = have && ib + u < be;
             const bool ok = v && dist2(pa.x - pb[u].x, pa.y - pb[u].y, pa.z - pb[u].z) <= 1.0f;   // cutoff_range
             push(ok, ib + u);
+            if ((u + 1) % DR == 0) drain();
         }
         if (have) ib = min(ib + UNROLL, be);
     }
-    if (qn > 0) process(qn);
+    __syncwarp();
+    if (tail != head) process((int)(tail - head));
     if constexpr (MODE == 1) vjp_par(A, acc_a, acc_g);
 }
 
