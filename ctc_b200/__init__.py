@@ -294,6 +294,13 @@ class Sim:
         """Replay the step as CUDA graphs (captured on first use)."""
         check(lib().ctc_sim_set_graph(self.h, int(bool(enable))))
 
+    def tune(self, reps=3, stream=None):
+        """Autotune the pair kernels' launch shapes on the current state (after
+        a step); returns (bulk threads, bulk unroll, halo threads, halo unroll)."""
+        ch = (C.c_int * 4)()
+        check(lib().ctc_sim_tune(self.h, int(reps), ch, _stream(stream)))
+        return tuple(ch)
+
     def set_contact(self, params):
         """Membrane-membrane contact (a DpdLjParams) from the next step on; None: off."""
         check(lib().ctc_sim_set_contact(self.h, None if params is None else C.byref(params)))

@@ -287,6 +287,7 @@ struct ctc_sim {
     void *cnt_scratch;                     // vertex cell list of the contact pairs
     CntScratch cw;
     Kiss cnt_host;                         // host mirror of the contact trunk
+    DpdTune tune;                          // launch shapes of the pair kernels (ctc_sim_tune)
     // the step as CUDA graphs (one from each ping-pong buffer) on an own stream
     bool use_graph;
     cudaGraphExec_t gexec[2];
@@ -527,9 +528,9 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
     CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n_host, st));
     sim_mark(s, 2, st);
     A.which = 1;
-    CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st));
+    CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st, s->tune));
     sim_mark(s, 3, st);
-    CUDA_TRY(halo_packed_launch(A, s->pack, s->pack_off, s->pack_cap, s->cfg.rng, st));
+    CUDA_TRY(halo_packed_launch(A, s->pack, s->pack_off, s->pack_cap, s->cfg.rng, st, 26, s->tune));
     sim_mark(s, 4, st);
     const float3 bf = make_float3(s->cfg.bodyf[0], s->cfg.bodyf[1], s->cfg.bodyf[2]);
     if (nvt > 0) {
@@ -646,6 +647,83 @@ extern "C" int ctc_sim_step(ctc_sim *s, int nsteps, void *stream) {
     }
     CUDA_TRY(cudaEventRecord(s->ev_out, s->own));
     CUDA_TRY(cudaStreamWaitEvent(st, s->ev_out, 0));
+    return CTC_OK;
+}
+
+// times the pair kernels (bulk, halo) of every launch shape on the cell
+// lists of the current state, without advancing it, and keeps the fastest
+extern "C" int ctc_sim_tune(ctc_sim *s, int reps, int *choice, void *stream) {
+    if (!s || reps <= 0) return fail(CTC_ERR_ARG, "ctc_sim_tune: bad arguments");
+    if (!s->built) return fail(CTC_ERR_ARG, "ctc_sim_tune: step once first");
+    cudaStream_t st = (cudaStream_t)stream;
+    // the pair kernels run on the cell lists the next step would build (into
+    // the spare buffer) and accumulate into the force scratch
+    DpdArgs A;
+    dpd_args_common(&A, s->L, &s->cfg.dpd);
+    A.pos = s->pos[s->cur]; A.vel = s->vel[s->cur]; A.starts = s->starts; A.counts = s->counts;
+    A.out = (float*)s->force; A.out_stride = 4;
+    A.seeds_dev = s->seeds_dev;
+    A.fss = s->fss;
+    A.err = dev_err_ptr();
+    const int spare = 1 - s->cur;
+    CUDA_TRY(cudaMemcpyAsync(s->count0, s->starts + s->nc, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(clist_launch(s->L, s->n_host, s->count0, s->pos[s->cur], s->vel[s->cur], 1, s->counts, s->starts,
+                          s->pos[spare], s->vel[spare], nullptr, s->w, dev_err_ptr(), st));
+    A.pos = s->pos[spare]; A.vel = s->vel[spare];
+    CUDA_TRY(frag_starts_launch(s->L, s->counts, s->fss, s->off, st));
+    CUDA_TRY(halo_pack_launch(A, s->off, s->pack, s->pack_off, s->pack_cap, st));
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    auto launch = [&](int which, const DpdTune &t) -> cudaError_t {
+        if (which == 2) return halo_packed_launch(A, s->pack, s->pack_off, s->pack_cap, s->cfg.rng, st, 26, t);
+        A.which = which;
+        return dpd_launch(A, s->n_host, s->cfg.rng, st, t);
+    };
+    auto time_it = [&](int which, const DpdTune &t, float &ms) -> int {
+        CUDA_TRY(launch(which, t));   // warm
+        CUDA_TRY(cudaEventRecord(e0, st));
+        for (int r = 0; r < reps; r++) CUDA_TRY(launch(which, t));
+        CUDA_TRY(cudaEventRecord(e1, st));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        return CTC_OK;
+    };
+    DpdTune best = s->tune;
+    float best_ms = 1e30f;
+    int rc = CTC_OK;
+    for (int ti = 0; ti < 2 && !rc; ti++)
+        for (int ui = 0; ui < 3 && !rc; ui++) {
+            DpdTune t = best;
+            t.bulk_threads = DPD_TUNE_BULK_T[ti];
+            t.bulk_unroll = DPD_TUNE_BULK_U[ui];
+            float ms = 0;
+            rc = time_it(1, t, ms);
+            if (!rc && ms < best_ms) { best_ms = ms; best.bulk_threads = t.bulk_threads; best.bulk_unroll = t.bulk_unroll; }
+        }
+    best_ms = 1e30f;
+    for (int hi = 0; hi < 3 && !rc; hi++)
+        for (int ui = 0; ui < 2 && !rc; ui++) {
+            DpdTune t = best;
+            t.halo_threads = DPD_TUNE_HALO_T[hi];
+            t.halo_unroll = DPD_TUNE_HALO_U[ui];
+            float ms = 0;
+            rc = time_it(2, t, ms);
+            if (!rc && ms < best_ms) { best_ms = ms; best.halo_threads = t.halo_threads; best.halo_unroll = t.halo_unroll; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    // the state pos[cur] is untouched; the next step rebuilds the cell lists
+    // and clears the forces as usual
+    if (best.bulk_threads != s->tune.bulk_threads || best.bulk_unroll != s->tune.bulk_unroll ||
+        best.halo_threads != s->tune.halo_threads || best.halo_unroll != s->tune.halo_unroll)
+        sim_drop_graphs(s);
+    s->tune = best;
+    if (choice) {
+        choice[0] = best.bulk_threads; choice[1] = best.bulk_unroll;
+        choice[2] = best.halo_threads; choice[3] = best.halo_unroll;
+    }
     return CTC_OK;
 }
 

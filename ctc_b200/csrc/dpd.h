@@ -36,8 +36,8 @@ struct DpdArgs {
     float dsdg;
 };
 
-// launch shapes of the pair kernels, chosen by the autotuner of the batched
-// boxes (the single-box path uses the defaults)
+// launch shapes of the pair kernels, chosen by the autotuners (ctc_sim_tune,
+// ctc_batch_tune); the module entry points use the defaults
 struct DpdTune {
     int bulk_threads = 256;   // 128 or 256
     int bulk_unroll = 4;      // candidate loads in flight per lane: 2, 4 or 8

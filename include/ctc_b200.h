@@ -225,6 +225,10 @@ int ctc_sim_step(ctc_sim *s, int nsteps, void *stream);
  * and before its later work; the first step after new state and profiled
  * steps run directly; 0: direct launches */
 int ctc_sim_set_graph(ctc_sim *s, int enable);
+/* autotuner: times every launch shape of the bulk and halo pair kernels
+ * (as ctc_batch_tune) reps times on the current state without advancing it
+ * (after at least one step), keeps the fastest; choice [host, 4] or NULL */
+int ctc_sim_tune(ctc_sim *s, int reps, int *choice, void *stream);
 /* number of solvent particles (synchronises the stream) */
 int ctc_sim_count(ctc_sim *s, int *n, void *stream);
 /* red-blood-cell membranes of the system: nc cells of one template (nv

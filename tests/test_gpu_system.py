@@ -70,3 +70,27 @@ def test_sim_graph_replay_matches_direct_launches():
     assert s0.shape == s1.shape
     assert np.abs(s0 - s1).max() < 1e-4 and np.abs(v0 - v1).max() < 1e-4
     assert C.device_error() == 0
+
+
+def test_sim_tune_leaves_state():
+    """The autotuner times the pair kernels on the current state without
+    advancing it: the next steps match an untuned run's."""
+    import ctc_b200 as C
+    L = (12, 12, 12)
+    ps = systems.solvent(L, seed=93)
+    out = []
+    for tune in (False, True):
+        sim = C.Sim(L, len(ps), C.DpdParams(*systems.dpd_params()), mass=1.0, dt=systems.DT)
+        sim.set_solvent(ps)
+        sim.step(1)
+        if tune:
+            shape = sim.tune(reps=1)
+            assert len(shape) == 4 and shape[0] in (128, 256) and shape[1] in (2, 4, 8)
+            assert shape[2] in (64, 128, 256) and shape[3] in (2, 4)
+        seeds = sim.next_seeds()
+        sim.step(2)
+        out.append((sim.get_solvent(), seeds))
+        sim.close()
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.abs(out[0][0] - out[1][0]).max() < 1e-4
+    assert C.device_error() == 0
