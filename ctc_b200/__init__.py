@@ -156,6 +156,10 @@ class RbcForce:
             lib().ctc_rbc_force_fin(self.h)
             self.h = None
 
+    def set_rnd(self, enable=True, seed=0):
+        """rbc_force_set_rnd1: the membrane random force (counter-based normals)."""
+        check(lib().ctc_rbc_force_set_rnd(self.h, int(bool(enable)), int(seed) & 0xffffffff))
+
     def set_bending(self, kantor=True):
         check(lib().ctc_rbc_force_set_bending(self.h, int(bool(kantor))))
 
@@ -300,6 +304,10 @@ class Sim:
         ch = (C.c_int * 4)()
         check(lib().ctc_sim_tune(self.h, int(reps), ch, _stream(stream)))
         return tuple(ch)
+
+    def set_membrane_noise(self, enable=True, seed=0):
+        """The membrane random force (rbc_force_set_rnd1) from the next step on."""
+        check(lib().ctc_sim_set_membrane_noise(self.h, int(bool(enable)), int(seed) & 0xffffffff))
 
     def set_contact(self, params):
         """Membrane-membrane contact (a DpdLjParams) from the next step on; None: off."""

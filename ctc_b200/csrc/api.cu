@@ -287,6 +287,8 @@ struct ctc_sim {
     void *cnt_scratch;                     // vertex cell list of the contact pairs
     CntScratch cw;
     Kiss cnt_host;                         // host mirror of the contact trunk
+    bool noise_on;                         // membrane random force (ctc_sim_set_membrane_noise)
+    Kiss noise_host;                       // host mirror of its trunk
     DpdTune tune;                          // launch shapes of the pair kernels (ctc_sim_tune)
     // the step as CUDA graphs (one from each ping-pong buffer) on an own stream
     bool use_graph;
@@ -338,8 +340,9 @@ extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
     CUDA_TRY(cudaMalloc(&s->fss, sizeof(int) * (size_t)s->off.d[26]));
     CUDA_TRY(cudaMalloc(&s->scratch, clist_scratch_bytes(s->nc, (int)np)));
     clist_carve(&s->w, s->scratch, s->nc, (int)np);
-    CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 29));   // + the FSI and contact trunks
-    CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 31));
+    // + the FSI, contact and membrane-noise trunks
+    CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 30));
+    CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 32));
     CUDA_TRY(cudaMalloc(&s->diag_scratch, diag_scratch_bytes()));
     {
         // a boundary particle appears once per fragment holding its cell: room
@@ -435,6 +438,7 @@ extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const i
     s->fmask = nullptr;
     int rc = ctc_rbc_force_ini(nv, nt, tri, nc > 0 ? nc : 1, &s->rbc);
     if (rc) return rc;
+    s->noise_on = false;                 // the random force is switched on per membrane set
     size_t nvt = (size_t)nc * nv, cap = nvt > 0 ? nvt : 1;
     CUDA_TRY(cudaMalloc(&s->mpos, sizeof(float4) * cap));
     CUDA_TRY(cudaMalloc(&s->mvel, sizeof(float4) * cap));
@@ -478,6 +482,23 @@ extern "C" int ctc_sim_set_contact(ctc_sim *s, const ctc_dpdlj_params *p) {
     return sim_cnt_alloc(s);
 }
 
+extern "C" int ctc_sim_set_membrane_noise(ctc_sim *s, int enable, unsigned seed) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sim_set_membrane_noise: null");
+    if (enable && !s->rbc) return fail(CTC_ERR_ARG, "ctc_sim_set_membrane_noise: no membranes");
+    if (enable && !(s->cfg.dt > 0)) return fail(CTC_ERR_ARG, "ctc_sim_set_membrane_noise: dt must be > 0");
+    sim_drop_graphs(s);
+    s->noise_on = enable != 0;
+    if (s->rbc) {
+        int rc = ctc_rbc_force_set_rnd(s->rbc, enable, seed);
+        if (rc) return rc;
+    }
+    if (enable) {   // its own trunk, seeded from the seed (KISS state of four words)
+        kiss_ini(&s->noise_host, (int)seed, 0x2545f491, 0x6c078965, 0x1b873593);
+        CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 29, s->noise_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
+    }
+    return CTC_OK;
+}
+
 extern "C" int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream) {
     if (!s || !pp) return fail(CTC_ERR_ARG, "ctc_sim_get_membranes: bad arguments");
     cudaStream_t st = (cudaStream_t)stream;
@@ -513,6 +534,8 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
         CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 27, 2, s->seeds_dev + 27, st));
         if (s->cnt_on)     // the contact trunk: cnt_bulk, then cnt_halo
             CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 28, 2, s->seeds_dev + 29, st));
+        if (s->noise_on)   // the membrane noise: one key per step
+            CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 29, 1, s->seeds_dev + 31, st));
     }
     sim_mark(s, 1, st);
     DpdArgs A;
@@ -562,7 +585,7 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
     if (nvt > 0) {
         // objects_advance: internal forces on top of the FSI ones, then the update
         int rc = membrane_forces(s->rbc, &s->mpar, s->mnc, (const float*)s->mpos, (const float*)s->mvel, 4,
-                                 (float*)s->mforce, 4, st);
+                                 (float*)s->mforce, 4, st, s->cfg.dt, s->seeds_dev + 31);
         if (rc) return rc;
         CUDA_TRY(integrate_launch(s->mcount, nvt, s->mpos, s->mvel, s->mforce, s->cfg.dt, s->mmass, bf, st));
     }
@@ -582,6 +605,7 @@ static void sim_advance(ctc_sim *s) {
             kiss_get(&s->cnt_host);
             kiss_get(&s->cnt_host);
         }
+        if (s->noise_on) kiss_get(&s->noise_host);
     }
     if (s->prof) s->prof_steps++;
     s->cur = 1 - s->cur;

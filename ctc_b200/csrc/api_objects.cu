@@ -61,6 +61,8 @@ struct ctc_rbc_force {
     int nv, nt, md, max_cells, bending;
     int *adj0, *adj1, *tri;
     double *av;
+    int noise;                 // random force (ctc_rbc_force_set_rnd)
+    unsigned noise_seed, calls;
 };
 
 extern "C" int ctc_rbc_force_ini(int nv, int nt, const int *tri, int max_cells, ctc_rbc_force **pf) {
@@ -151,7 +153,7 @@ const int *membrane_tri(const ctc_rbc_force *f) { return f->tri; }
 int membrane_nt(const ctc_rbc_force *f) { return f->nt; }
 
 int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const float *pos, const float *vel, int stride,
-                    float *force, int fstride, cudaStream_t st) {
+                    float *force, int fstride, cudaStream_t st, double dt, const float *noise_seed_dev) {
     if (nc > f->max_cells) return fail(CTC_ERR_CAPACITY, "nc=%d > max_cell=%d", nc, f->max_cells);
     if (nc == 0) return CTC_OK;
     CUDA_TRY(area_volume_launch(nc, f->nv, f->nt, f->tri, pos, stride, f->av, st));
@@ -166,16 +168,33 @@ int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const flo
     stressful(f->nt, p->totArea, &A.l0, &A.a0);
     A.bending = f->bending;
     A.err = dev_err_ptr();
+    if (f->noise) {
+        if (!(dt > 0.0)) return fail(CTC_ERR_ARG, "membrane random force: dt must be > 0");
+        A.noise = 1;
+        A.dt = dt;
+        A.noise_seed_dev = noise_seed_dev;
+        if (!noise_seed_dev) {   // a fresh key per call: Philox of (seed, call)
+            A.noise_key = philox4x32_10(make_uint4(f->calls, 0u, 0u, 0u), make_uint2(f->noise_seed, 0x2545f491u)).x;
+            f->calls++;
+        }
+    }
     CUDA_TRY(membrane_launch(A, st));
     return CTC_OK;
 }
 }  // namespace ctc
 
+extern "C" int ctc_rbc_force_set_rnd(ctc_rbc_force *f, int enable, unsigned seed) {
+    if (!f) return fail(CTC_ERR_ARG, "ctc_rbc_force_set_rnd: null");
+    f->noise = enable != 0;
+    f->noise_seed = seed;
+    f->calls = 0;
+    return CTC_OK;
+}
+
 extern "C" int ctc_rbc_force_apply(ctc_rbc_force *f, const ctc_rbc_params *p, float dt, int nc, const float *pp,
                                    float *ff, void *stream) {
-    (void)dt;   // only the membrane random force (not built) uses dt
     if (!f || !p || nc < 0 || (nc > 0 && (!pp || !ff))) return fail(CTC_ERR_ARG, "ctc_rbc_force_apply: bad arguments");
-    return membrane_forces(f, p, nc, pp, pp + 3, 6, ff, 3, (cudaStream_t)stream);
+    return membrane_forces(f, p, nc, pp, pp + 3, 6, ff, 3, (cudaStream_t)stream, (double)dt);
 }
 
 // ---------------------------------------------------------------------------

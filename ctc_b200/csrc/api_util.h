@@ -13,8 +13,11 @@ int fail(int status, const char *fmt, ...);   // records the message, returns st
 int *dev_err_ptr();                           // device failure word of the current device
 
 // membrane forces of nc cells (area/volume + forces), accumulated into force
+// with the module's random force on (ctc_rbc_force_set_rnd): dt, and the
+// step's seed in device memory (noise_seed_dev), else a key drawn per call
 int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const float *pos, const float *vel, int stride,
-                    float *force, int fstride, cudaStream_t st);
+                    float *force, int fstride, cudaStream_t st, double dt = 0.0,
+                    const float *noise_seed_dev = nullptr);
 // pieces of a membrane module for the adjoint (membrane.h's MembraneArgs)
 struct MembraneArgs;
 int membrane_args(const ctc_rbc_force *f, MembraneArgs *A);

@@ -104,6 +104,29 @@ __device__ __forceinline__ bool dpd_force(const DpdPar &P, float4 pa, float4 va,
     return true;
 }
 
+// Philox-4x32-10, the counter-based generator of Salmon, Moraes, Dror and
+// Shaw ("Parallel random numbers: as easy as 1, 2, 3", SC 2011): ten rounds
+// of two 32x32->64 multiplications by M0, M1 mixed with the key, the key
+// bumped by the Weyl increments W0, W1 between rounds.
+__host__ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+    const unsigned M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+    for (int r = 0; r < 10; r++) {
+        const unsigned long long p0 = (unsigned long long)M0 * c.x, p1 = (unsigned long long)M1 * c.z;
+        c = make_uint4((unsigned)(p1 >> 32) ^ c.y ^ k.x, (unsigned)p1, (unsigned)(p0 >> 32) ^ c.w ^ k.y,
+                       (unsigned)p0);
+        k.x += W0;
+        k.y += W1;
+    }
+    return c;
+}
+
+// a standard normal number from two Philox words (Box-Muller)
+__device__ __forceinline__ double normal_from(uint4 w) {
+    const double u1 = ((double)w.x + 0.5) * 2.3283064365386963e-10;   // (0, 1)
+    const double u2 = (double)w.y * 2.3283064365386963e-10;           // [0, 1)
+    return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
 // DPD + Lennard-Jones pair force of src/pair/dev.h:49-75,111-139 (PairDPDLJ,
 // membrane-membrane contact), the same plain expressions as the reference:
 // the LJ magnitude e 24 invr t6 (2 t6 - 1), t2 = s^2 invr^2, capped to

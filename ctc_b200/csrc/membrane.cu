@@ -139,6 +139,14 @@ __global__ void k_membrane(MembraneArgs A) {
     const double phi = (double)P.phi / 180.0 * M_PI;
     const double cphi = cos(phi), sphi = sin(phi), kb = P.kb;
     D3 fb = mk(0, 0, 0), ft = mk(0, 0, 0);
+    // membrane random force (src/rbc/force/dev/common.h:93-108): the
+    // magnitude's float square root as the reference's frnd0
+    unsigned nkey = 0;
+    double f0n = 0.0;
+    if (A.noise) {
+        nkey = A.noise_seed_dev ? __float_as_uint(__ldg(A.noise_seed_dev)) : A.noise_key;
+        f0n = (double)sqrtf((float)(2.0 * (double)P.gammaC * (double)P.kBT / A.dt));
+    }
     for (int j = 0; j < md; j++) {
         // adj_get_map0, src/rbc/adj/dev.h:2-31
         int i1 = __ldg(A.adj0 + k + j);
@@ -153,6 +161,14 @@ __global__ void k_membrane(MembraneArgs A) {
         if (A.bending) fb = fb + dih<1>(cphi, sphi, kb, r0, r2, r1, r4, A.err) + dih<2>(cphi, sphi, kb, r1, r0, r2, r3, A.err);
         ft = ft + ftri(P, r0, r1, r2, A.l0, A.a0, Acell, Vcell);
         ft = ft + fvisc(P, r0, r1, v0, ld_vel(A.vel, A.stride, i1));
+        if (A.noise) {   // the edge (pid, i1): one normal number for both directions
+            const int a = pid - off, b = i1 - off;
+            const uint4 w = philox4x32_10(make_uint4((unsigned)min(a, b), (unsigned)max(a, b), (unsigned)rbc, 0u),
+                                          make_uint2(nkey, 0x7f4a7c15u));
+            const D3 dr = r0 - r1;
+            const double r = (double)sqrtf((float)dot(dr, dr));
+            if (r > 0.0) ft = ft + (f0n * normal_from(w) / r) * dr;
+        }
     }
     D3 f = fb + ft;
     float *o = A.force + (size_t)A.fstride * pid;

@@ -21,6 +21,14 @@ struct MembraneArgs {
     double l0, a0;                // stress-ful equilibrium length / area
     int bending;                  // Kantor bending on/off
     int *err;
+    // random force of every edge (rbc_force_set_rnd1): sqrt(2 gammaC kBT / dt)
+    // xi (r0 - r1) / |r0 - r1|, xi a standard normal number shared by the
+    // edge's two directions, from Philox keyed by the step's seed bits
+    // (noise_seed_dev if set, else noise_key) and the edge (cell, vertices)
+    int noise;
+    double dt;
+    unsigned noise_key;
+    const float *noise_seed_dev;
 };
 
 cudaError_t area_volume_launch(int nc, int nv, int nt, const int *tri, const float *pos, int stride, double *av,

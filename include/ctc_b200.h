@@ -151,6 +151,13 @@ int ctc_rbc_force_set_bending(ctc_rbc_force *f, int kantor);
  * vertex v at c*nv + v] added to ff [dev, AoS] */
 int ctc_rbc_force_apply(ctc_rbc_force *f, const ctc_rbc_params *p, float dt, int nc, const float *pp, float *ff,
                         void *stream);
+/* rbc_force_set_rnd1 (src/rbc/force/imp/main.h:100-118): the membrane random
+ * force of every edge, sqrt(2 gammaC kBT / dt) xi (r0 - r1) / |r0 - r1| with
+ * xi a standard normal number shared by the edge's two directions.  The
+ * reference draws xi with cuRAND; here they come from a counter-based
+ * generator (Philox-4x32-10 keyed by the edge and a per-call key from seed),
+ * so the sequence differs and the statistics agree.  enable = 0: off. */
+int ctc_rbc_force_set_rnd(ctc_rbc_force *f, int enable, unsigned seed);
 /* area_volume_compute (src/rbc/force/area_volume/imp/main.h:38-51) in FP64:
  * av [dev, 2 nc doubles] = area, volume of every cell */
 int ctc_rbc_area_volume(ctc_rbc_force *f, int nc, const float *pp, double *av, void *stream);
@@ -246,6 +253,9 @@ int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const int *tri, co
  * images) join the vertex forces; p = NULL switches it off.  The trunk is
  * rnd_ini(7119, 187, 18278, 15674), drawn for the bulk then the halo. */
 int ctc_sim_set_contact(ctc_sim *s, const ctc_dpdlj_params *p);
+/* the membrane random force (ctc_rbc_force_set_rnd) in the step, one key per
+ * step from a trunk seeded by seed; set after ctc_sim_set_membranes */
+int ctc_sim_set_membrane_noise(ctc_sim *s, int enable, unsigned seed);
 /* download the membrane vertices [host, AoS, nc * nv] */
 int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream);
 /* download the cell-sorted solvent [host, AoS, capacity maxp] */
