@@ -8,7 +8,8 @@
 // _ini_map / _fin_map / clists_get_* / clist_get_ids / clist_build), the
 // bulk solvent forces (src/fluforces/imp.h: fluforces_bulk_*), the membrane
 // forces (src/rbc/force/imp.h: rbc_force_ini / _fin / _set_stressful /
-// _set_bending / _set_rnd0 / _apply) and the update (src/scheme/move/imp.h).
+// _set_bending / _set_rnd0 / _set_rnd1 / _apply) and the update
+// (src/scheme/move/imp.h).
 // Not covered: entry points whose arguments come from the multi-rank
 // exchange (clist_subindex* / clist_build_map / clist_gather_* of the
 // redistribution, fluforces_halo_* over exchanged fragments, fsi_* over
@@ -144,6 +145,8 @@ void fluforces_bulk_apply(const PairParams *par, int n, const FluForcesBulk *b, 
 struct RbcForce {
     ctc_rbc_force *h;
     int nv, nt, cap, kantor;
+    int rnd;                 // random force on (rbc_force_set_rnd1) and its seed
+    unsigned seed;
     std::vector<int> tri;
     float totArea;           // stress-ful: the area of the template
 };
@@ -159,6 +162,8 @@ void rbc_force_ini(const MeshRead *mesh, RbcForce **f) {
     (*f)->nt = nt;
     (*f)->cap = 1;
     (*f)->kantor = 1;
+    (*f)->rnd = 0;
+    (*f)->seed = 0;
     (*f)->tri = tri;
     (*f)->totArea = 0;
 }
@@ -173,7 +178,17 @@ void rbc_force_set_stressful(int nt, float totArea, RbcForce *f) {
     f->totArea = totArea;
 }
 
-void rbc_force_set_rnd0(RbcForce *f) { (void)f; }
+void rbc_force_set_rnd0(RbcForce *f) {
+    f->rnd = 0;
+    CTC(ctc_rbc_force_set_rnd(f->h, 0, 0));
+}
+
+// the membrane random force, with counter-based normal numbers in place of cuRAND's
+void rbc_force_set_rnd1(int seed, RbcForce *f) {
+    f->rnd = 1;
+    f->seed = (unsigned)seed;
+    CTC(ctc_rbc_force_set_rnd(f->h, 1, f->seed));
+}
 
 void rbc_force_set_bending(const MeshRead *mesh, const char *name, RbcForce *f) {
     (void)mesh;
@@ -195,6 +210,7 @@ void rbc_force_apply(RbcForce *f, const RbcParams *par, float dt, const RbcQuant
         CTC(ctc_rbc_force_fin(f->h));
         CTC(ctc_rbc_force_ini(f->nv, f->nt, f->tri.data(), q->nc, &f->h));
         CTC(ctc_rbc_force_set_bending(f->h, f->kantor));
+        CTC(ctc_rbc_force_set_rnd(f->h, f->rnd, f->seed));
         f->cap = q->nc;
     }
     CTC(ctc_rbc_force_apply(f->h, &p, dt, q->nc, reinterpret_cast<const float*>(q->pp), reinterpret_cast<float*>(ff),

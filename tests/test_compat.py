@@ -32,6 +32,7 @@ EXPECTED = [
     "rbc_force_fin(RbcForce*)",
     "rbc_force_set_stressful(int, float, RbcForce*)",
     "rbc_force_set_rnd0(RbcForce*)",
+    "rbc_force_set_rnd1(int, RbcForce*)",
     "rbc_force_set_bending(MeshRead const*, char const*, RbcForce*)",
     "rbc_force_apply(RbcForce*, RbcParams const*, float, RbcQuants const*, Force*)",
     "scheme_move_apply(float, float, int, Force const*, Particle*)",
