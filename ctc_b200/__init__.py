@@ -16,7 +16,7 @@ from . import _lib
 from ._lib import CTC_RNG_REFERENCE, CTC_RNG_STABLE, CtcError, check, device_error, lib
 
 __all__ = ["Clist", "FluForces", "Sim", "Batch", "DpdParams", "DpdLjParams", "RbcParams", "RbcForce", "Fsi", "Contact",
-           "dpd_sigma", "scheme_move_apply",
+           "dpd_sigma", "mesh_write_ply", "scheme_move_apply",
            "scheme_move_clear_vel", "bforce_apply_cste", "rnd_mean0var1", "CTC_RNG_REFERENCE",
            "CTC_RNG_STABLE", "CtcError", "device_error"]
 
@@ -220,6 +220,17 @@ class Contact:
     def apply_seeded(self, params, pv, seed_bulk, seed_halo, fv, stream=None):
         check(lib().ctc_cnt_apply_seeded(self.h, C.byref(params), int(pv.shape[0]), _ptr(pv), float(seed_bulk),
                                          float(seed_halo), _ptr(fv), _stream(stream)))
+
+
+def mesh_write_ply(path, pv, tri, nv, L, shift="edge"):
+    """mesh_write_particles (src/io/mesh/imp/main.h): the membranes pv
+    (nc*nv, 6) AoS [host] with the template's triangles tri (nt, 3) as the
+    reference's binary PLY; shift "edge" (x + L/2) or "center"."""
+    pv = np.ascontiguousarray(pv, np.float32).reshape(-1, 6)
+    tri = np.ascontiguousarray(tri, np.int32).reshape(-1, 3)
+    check(lib().ctc_mesh_write_ply(str(path).encode(), len(pv) // int(nv), int(nv), len(tri),
+                                   tri.ctypes.data_as(C.c_void_p), pv.ctypes.data_as(C.c_void_p),
+                                   0 if shift == "edge" else 1, *(int(x) for x in L)))
 
 
 def scheme_move_apply(dt, mass, ff, pp, stream=None):

@@ -82,6 +82,8 @@ SIGNATURES = {
     "ctc_cnt_apply_seeded": (C.c_int, [vp, C.POINTER(DpdLjParams), C.c_int, vp, C.c_float, C.c_float, vp, vp]),
     "ctc_sim_set_contact": (C.c_int, [vp, C.POINTER(DpdLjParams)]),
     "ctc_sim_set_graph": (C.c_int, [vp, C.c_int]),
+    "ctc_mesh_write_ply": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int,
+                                     C.c_int]),
     "ctc_sim_set_membrane_noise": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_rbc_force_set_rnd": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_sim_tune": (C.c_int, [vp, C.c_int, ip, vp]),

@@ -199,6 +199,15 @@ int ctc_cnt_apply(ctc_cnt *c, const ctc_dpdlj_params *p, int nv, const float *pv
 int ctc_cnt_apply_seeded(ctc_cnt *c, const ctc_dpdlj_params *p, int nv, const float *pv, float seed_bulk,
                          float seed_halo, float *fv, void *stream);
 
+/* ---- membrane mesh dumps: replaces src/io/mesh/imp.h for one rank -------- */
+/* mesh_write_particles: nc cells of nv vertices pp [host, AoS] with the
+ * template's nt triangles tri[3 nt] [host] as the reference's binary
+ * little-endian PLY file (vertices x y z u v w, faces 3 i0 i1 i2); shift 0:
+ * positions from the box's edge (MESH_WRITE_EDGE, x + L/2), 1: from its
+ * centre (MESH_WRITE_CENTER) */
+int ctc_mesh_write_ply(const char *path, int nc, int nv, int nt, const int *tri, const float *pp, int shift, int LX,
+                       int LY, int LZ);
+
 /* ---- time update: replaces src/scheme/move/imp.h:5-6, scheme/force ------- */
 /* scheme_move_apply: v += f/m dt; r += v dt on n AoS particles [dev] */
 int ctc_scheme_move_apply(float dt, float mass, int n, const float *ff, float *pp, void *stream);
