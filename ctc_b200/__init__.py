@@ -160,8 +160,13 @@ class RbcForce:
         """rbc_force_set_rnd1: the membrane random force (counter-based normals)."""
         check(lib().ctc_rbc_force_set_rnd(self.h, int(bool(enable)), int(seed) & 0xffffffff))
 
+    BENDING = {"none": 0, "kantor": 1, "juelicher": 2}
+
     def set_bending(self, kantor=True):
-        check(lib().ctc_rbc_force_set_bending(self.h, int(bool(kantor))))
+        """rbc_force_set_bending: "kantor" (or True), "none" (or False) or
+        "juelicher" (src/rbc/force/bending/juelicher, kb = 1, H0 = -1/2)."""
+        mode = self.BENDING[kantor] if isinstance(kantor, str) else int(bool(kantor))
+        check(lib().ctc_rbc_force_set_bending(self.h, mode))
 
     def apply(self, params, pp, ff, dt=5e-4, stream=None):
         """rbc_force_apply: adds the internal forces of pp (nc*nv, 6) to ff (nc*nv, 3)."""
@@ -319,6 +324,11 @@ class Sim:
     def set_membrane_noise(self, enable=True, seed=0):
         """The membrane random force (rbc_force_set_rnd1) from the next step on."""
         check(lib().ctc_sim_set_membrane_noise(self.h, int(bool(enable)), int(seed) & 0xffffffff))
+
+    def set_bending(self, mode="kantor"):
+        """The membranes' bending in the step: "kantor", "juelicher" or "none"
+        (set after set_membranes, which starts with "kantor")."""
+        check(lib().ctc_sim_set_bending(self.h, RbcForce.BENDING[mode]))
 
     def set_contact(self, params):
         """Membrane-membrane contact (a DpdLjParams) from the next step on; None: off."""

@@ -85,6 +85,7 @@ SIGNATURES = {
     "ctc_mesh_write_ply": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int,
                                      C.c_int]),
     "ctc_sim_set_membrane_noise": (C.c_int, [vp, C.c_int, C.c_uint]),
+    "ctc_sim_set_bending": (C.c_int, [vp, C.c_int]),
     "ctc_rbc_force_set_rnd": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_sim_tune": (C.c_int, [vp, C.c_int, ip, vp]),
     "ctc_fsi_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),

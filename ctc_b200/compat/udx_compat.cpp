@@ -144,7 +144,7 @@ void fluforces_bulk_apply(const PairParams *par, int n, const FluForcesBulk *b, 
 // ---- membrane forces (src/rbc/force/imp.h) ------------------------------------
 struct RbcForce {
     ctc_rbc_force *h;
-    int nv, nt, cap, kantor;
+    int nv, nt, cap, kantor;            // kantor: bending mode, 0 none, 1 kantor, 2 juelicher
     int rnd;                 // random force on (rbc_force_set_rnd1) and its seed
     unsigned seed;
     std::vector<int> tri;
@@ -194,7 +194,8 @@ void rbc_force_set_bending(const MeshRead *mesh, const char *name, RbcForce *f) 
     (void)mesh;
     if (!strcmp(name, "kantor")) f->kantor = 1;
     else if (!strcmp(name, "none")) f->kantor = 0;
-    else ERR("ctc_b200: bending \"%s\" is not supported (kantor, none)", name);
+    else if (!strcmp(name, "juelicher")) f->kantor = 2;
+    else ERR("ctc_b200: bending \"%s\" is not supported (kantor, juelicher, none)", name);
     CTC(ctc_rbc_force_set_bending(f->h, f->kantor));
 }
 

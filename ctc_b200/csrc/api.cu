@@ -438,7 +438,7 @@ extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const i
     s->fmask = nullptr;
     int rc = ctc_rbc_force_ini(nv, nt, tri, nc > 0 ? nc : 1, &s->rbc);
     if (rc) return rc;
-    s->noise_on = false;                 // the random force is switched on per membrane set
+    s->noise_on = false;                 // the random force and the bending mode are set per membrane set
     size_t nvt = (size_t)nc * nv, cap = nvt > 0 ? nvt : 1;
     CUDA_TRY(cudaMalloc(&s->mpos, sizeof(float4) * cap));
     CUDA_TRY(cudaMalloc(&s->mvel, sizeof(float4) * cap));
@@ -480,6 +480,12 @@ extern "C" int ctc_sim_set_contact(ctc_sim *s, const ctc_dpdlj_params *p) {
     s->cnt_on = p != nullptr;
     if (p) s->cnt = *p;
     return sim_cnt_alloc(s);
+}
+
+extern "C" int ctc_sim_set_bending(ctc_sim *s, int mode) {
+    if (!s || !s->rbc) return fail(CTC_ERR_ARG, "ctc_sim_set_bending: no membranes");
+    sim_drop_graphs(s);
+    return ctc_rbc_force_set_bending(s->rbc, mode);
 }
 
 extern "C" int ctc_sim_set_membrane_noise(ctc_sim *s, int enable, unsigned seed) {

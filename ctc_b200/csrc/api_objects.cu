@@ -63,6 +63,7 @@ struct ctc_rbc_force {
     double *av;
     int noise;                 // random force (ctc_rbc_force_set_rnd)
     unsigned noise_seed, calls;
+    double *jl_av, *jl_lt, *jl_curva;   // Juelicher scratch (bending 2)
 };
 
 extern "C" int ctc_rbc_force_ini(int nv, int nt, const int *tri, int max_cells, ctc_rbc_force **pf) {
@@ -94,6 +95,7 @@ extern "C" int ctc_rbc_force_ini(int nv, int nt, const int *tri, int max_cells, 
 extern "C" int ctc_rbc_force_fin(ctc_rbc_force *f) {
     if (!f) return CTC_OK;
     cudaFree(f->adj0); cudaFree(f->adj1); cudaFree(f->tri); cudaFree(f->av);
+    cudaFree(f->jl_av); cudaFree(f->jl_lt); cudaFree(f->jl_curva);
     delete f;
     return CTC_OK;
 }
@@ -104,9 +106,16 @@ extern "C" int ctc_rbc_force_md(const ctc_rbc_force *f, int *md) {
     return CTC_OK;
 }
 
-extern "C" int ctc_rbc_force_set_bending(ctc_rbc_force *f, int kantor) {
-    if (!f) return fail(CTC_ERR_ARG, "ctc_rbc_force_set_bending: null");
-    f->bending = kantor != 0;
+extern "C" int ctc_rbc_force_set_bending(ctc_rbc_force *f, int mode) {
+    if (!f || mode < 0 || mode > 2) return fail(CTC_ERR_ARG, "ctc_rbc_force_set_bending: bad arguments");
+    if (mode == 2 && !f->jl_av) {
+        if (f->md > 12) return fail(CTC_ERR_ARG, "juelicher bending: valence %d above 12", f->md);
+        const size_t n = (size_t)std::max(f->max_cells, 1) * f->nv;
+        CUDA_TRY(cudaMalloc(&f->jl_av, sizeof(double) * n));
+        CUDA_TRY(cudaMalloc(&f->jl_lt, sizeof(double) * n));
+        CUDA_TRY(cudaMalloc(&f->jl_curva, sizeof(double) * std::max(f->max_cells, 1)));
+    }
+    f->bending = mode;
     return CTC_OK;
 }
 
@@ -166,7 +175,7 @@ int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const flo
     A.av = f->av;
     fill_par(&A.par, p);
     stressful(f->nt, p->totArea, &A.l0, &A.a0);
-    A.bending = f->bending;
+    A.bending = f->bending == 1;          // Kantor inside the ring kernel
     A.err = dev_err_ptr();
     if (f->noise) {
         if (!(dt > 0.0)) return fail(CTC_ERR_ARG, "membrane random force: dt must be > 0");
@@ -179,6 +188,7 @@ int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const flo
         }
     }
     CUDA_TRY(membrane_launch(A, st));
+    if (f->bending == 2) CUDA_TRY(juelicher_launch(A, f->jl_av, f->jl_lt, f->jl_curva, st));
     return CTC_OK;
 }
 }  // namespace ctc

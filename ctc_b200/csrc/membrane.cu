@@ -177,6 +177,160 @@ __global__ void k_membrane(MembraneArgs A) {
     o[2] += (float)f.z;
 }
 
+// ---------------------------------------------------------------------------
+// Juelicher bending (src/rbc/force/bending/juelicher, with the reference's
+// kb = 1, H0 = -1/2, kad = 2 kb / pi): per vertex area A_v (a third of each
+// triangle's Kahan area) and LT_v (sum of |edge| theta over its edges), the
+// per-cell totals, then the forces of force_edg + force_lentheta +
+// force_area (f + fad of juelicher_apply).  The reference scatters them per
+// edge and per triangle with float atomics; here each vertex gathers them
+// over its ring in FP64: its own edges (v, r_j) with the dihedral
+// (r_{j+1}, v, r_j, r_{j-1}), the edges (r_j, r_{j+1}) opposite to it with
+// (v, r_j, r_{j+1}, adj1_j), and its triangles (v, r_j, r_{j+1}) -- the
+// dihedral angle is the same from either half-edge of an edge.
+// ---------------------------------------------------------------------------
+namespace jl {
+__device__ __forceinline__ double kahan_area(D3 r0, D3 r1, D3 r2) {   // src/math/tri/dev.h:39-51
+    double a = sqrt(dot(r0 - r1, r0 - r1)), b = sqrt(dot(r1 - r2, r1 - r2)), c = sqrt(dot(r2 - r0, r2 - r0)), t;
+    if (a < b) { t = a; a = b; b = t; }
+    if (b < c) { t = b; b = c; c = t; }
+    if (a < b) { t = a; a = b; b = t; }
+    return sqrt((a + (b + c)) * (c - (a - b)) * (c + (a - b)) * (a + (b - c))) / 4;
+}
+__device__ __forceinline__ double orient2d(D3 a, D3 b, D3 c, int p) {   // p: yz, zx, xy
+    const double ap = p == 0 ? a.y : (p == 1 ? a.z : a.x), aq = p == 0 ? a.z : (p == 1 ? a.x : a.y);
+    const double bp = p == 0 ? b.y : (p == 1 ? b.z : b.x), bq = p == 0 ? b.z : (p == 1 ? b.x : b.y);
+    const double cp = p == 0 ? c.y : (p == 1 ? c.z : c.x), cq = p == 0 ? c.z : (p == 1 ? c.x : c.y);
+    return (ap - cp) * (bq - cq) - (aq - cq) * (bp - cp);
+}
+__device__ __forceinline__ double orient3d(D3 a, D3 b, D3 c, D3 d) {
+    const double ax = a.x - d.x, ay = a.y - d.y, az = a.z - d.z, bx = b.x - d.x, by = b.y - d.y, bz = b.z - d.z;
+    const double cx = c.x - d.x, cy = c.y - d.y, cz = c.z - d.z;
+    return ax * (by * cz - bz * cy) + bx * (cy * az - cz * ay) + cx * (ay * bz - az * by);
+}
+__device__ __forceinline__ double theta(D3 a, D3 b, D3 c, D3 d) {    // -atan2 of dihedral_xy
+    const D3 k = mk(orient2d(b, c, a, 0), orient2d(b, c, a, 1), orient2d(b, c, a, 2));
+    const D3 l = mk(orient2d(c, b, d, 0), orient2d(c, b, d, 1), orient2d(c, b, d, 2));
+    const double y = -orient3d(a, b, c, d) * sqrt(dot(b - c, b - c));
+    return -atan2(y, dot(k, l));
+}
+__device__ __forceinline__ D3 unit(D3 a) {                           // vec_norm
+    const double s = sqrt(dot(a, a));
+    return (s > 1e-12 || s < -1e-12) ? (1.0 / s) * a : a;
+}
+__device__ __forceinline__ D3 normal(D3 a, D3 b, D3 c) { return unit(cross(b - a, c - a)); }
+__device__ __forceinline__ double cot(D3 a, D3 b, D3 c) {            // at b
+    return dot(a - b, c - b) / (2 * kahan_area(a, b, c));
+}
+// d theta(a, b, c, d) / da and / db (ddih_angle, juelicher/dev/main.h:88-118)
+__device__ __forceinline__ void ddih_ab(D3 a, D3 b, D3 c, D3 d, D3 &da, D3 &db) {
+    const D3 n = normal(a, b, c), k = normal(c, b, d);
+    const double e = sqrt(dot(b - c, b - c));
+    da = (e / (2 * kahan_area(a, b, c))) * n;
+    db = (-cot(b, c, a) / e) * n + (-cot(d, c, b) / e) * k;
+}
+}  // namespace jl
+
+// the ring of vertex pid (its valence, ring[0 .. valence)) and the vertices
+// across its ring edges (opp)
+__device__ __forceinline__ int jl_ring(const MembraneArgs &A, int pid, int *ring, int *opp) {
+    const int k = (pid % A.nv) * A.md, off = pid - pid % A.nv;
+    int n = 0;
+    for (int j = 0; j < A.md; j++) {
+        const int r = __ldg(A.adj0 + k + j);
+        if (r == -1) break;
+        ring[n] = r + off;
+        opp[n] = __ldg(A.adj1 + k + j) + off;
+        n++;
+    }
+    return n;
+}
+
+constexpr int JL_MD = 12;     // ring slots a vertex may have (templates are checked at set-up)
+
+__global__ void k_juelicher_vertex(MembraneArgs A, double *__restrict__ av, double *__restrict__ lt) {
+    const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pid >= A.nc * A.nv) return;
+    int ring[JL_MD], opp[JL_MD];
+    const int n = jl_ring(A, pid, ring, opp);
+    const D3 r0 = ld_pos(A.pos, A.stride, pid);
+    double a = 0, l = 0;
+    for (int j = 0; j < n; j++) {
+        const D3 r1 = ld_pos(A.pos, A.stride, ring[j]), r2 = ld_pos(A.pos, A.stride, ring[(j + 1) % n]);
+        const D3 rm = ld_pos(A.pos, A.stride, ring[(j + n - 1) % n]);
+        a += jl::kahan_area(r0, r1, r2) / 3;
+        l += sqrt(dot(r1 - r0, r1 - r0)) * jl::theta(r2, r0, r1, rm);
+    }
+    av[pid] = a;
+    lt[pid] = l;
+}
+
+// per cell: the mean-curvature factor (compute_mean_curv, float pi and kad as the reference)
+__global__ void __launch_bounds__(AV_T) k_juelicher_cell(int nv, const double *__restrict__ av,
+                                                        const double *__restrict__ lt, double *__restrict__ curva) {
+    __shared__ double sh[2][AV_T / 32];
+    const int c = blockIdx.x;
+    double a = 0, l = 0;
+    for (int v = threadIdx.x; v < nv; v += AV_T) { a += av[(size_t)c * nv + v]; l += lt[(size_t)c * nv + v]; }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        l += __shfl_down_sync(0xffffffffu, l, o);
+    }
+    if (lane == 0) { sh[0][w] = a; sh[1][w] = l; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double A = 0, LT = 0;
+        for (int k = 0; k < AV_T / 32; k++) { A += sh[0][k]; LT += sh[1][k]; }
+        const double pi = (float)3.141592653589793, H0 = -0.5, kad = (float)(2 * 1.0 / pi);
+        curva[c] = (LT / 4 - H0 * A) * (4 * kad * pi / A);
+    }
+}
+
+__global__ void k_juelicher_force(MembraneArgs A, const double *__restrict__ av, const double *__restrict__ lt,
+                                  const double *__restrict__ curva) {
+    const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pid >= A.nc * A.nv) return;
+    const double H0 = -0.5, cv = curva[pid / A.nv];
+    int ring[JL_MD], opp[JL_MD];
+    const int n = jl_ring(A, pid, ring, opp);
+    const D3 r0 = ld_pos(A.pos, A.stride, pid);
+    const double h0 = lt[pid] / av[pid] / 4 - H0;
+    const double carea = 1.0 / 3.0 * (lt[pid] * lt[pid] / 8.0 / av[pid] / av[pid] - 2.0 * H0 * H0);
+    D3 f = mk(0, 0, 0);
+    for (int j = 0; j < n; j++) {
+        const int w = ring[j], wn = ring[(j + 1) % n], wp = ring[(j + n - 1) % n];
+        const D3 r1 = ld_pos(A.pos, A.stride, w), r2 = ld_pos(A.pos, A.stride, wn), rm = ld_pos(A.pos, A.stride, wp);
+        const double hw = lt[w] / av[w] / 4 - H0, hn = lt[wn] / av[wn] / 4 - H0;
+        // own edge (v, w): force_edg on v, then force_lentheta with v as b
+        const double len = sqrt(dot(r1 - r0, r1 - r0)), th = jl::theta(r2, r0, r1, rm);
+        f = f + (((h0 + hw) * th + cv / 4 * th)) * jl::unit(r1 - r0);
+        D3 da, db;
+        jl::ddih_ab(r2, r0, r1, rm, da, db);
+        f = f + (-(h0 + hw) * len - cv / 2.0 * len) * db;
+        // the ring edge (w, wn) opposite to v: force_lentheta with v as a
+        const D3 r4 = ld_pos(A.pos, A.stride, opp[j]);
+        const double len2 = sqrt(dot(r2 - r1, r2 - r1));
+        jl::ddih_ab(r0, r1, r2, r4, da, db);
+        f = f + (-(hw + hn) * len2 - cv / 2.0 * len2) * da;
+        // the triangle (v, w, wn): force_area, d area / d v = n/2 x (wn - w)
+        f = f + carea * cross(0.5 * jl::normal(r0, r1, r2), r2 - r1);
+    }
+    float *o = A.force + (size_t)A.fstride * pid;
+    o[0] += (float)f.x;
+    o[1] += (float)f.y;
+    o[2] += (float)f.z;
+}
+
+cudaError_t juelicher_launch(const MembraneArgs &A, double *av, double *lt, double *curva, cudaStream_t st) {
+    const int n = A.nc * A.nv;
+    if (n <= 0) return cudaSuccess;
+    k_juelicher_vertex<<<ceil_div(n, 128), 128, 0, st>>>(A, av, lt);
+    k_juelicher_cell<<<A.nc, AV_T, 0, st>>>(A.nv, av, lt, curva);
+    k_juelicher_force<<<ceil_div(n, 128), 128, 0, st>>>(A, av, lt, curva);
+    return cudaGetLastError();
+}
+
 // membrane migration of one periodic rank (src/distr/rbc/dev.h:1-25): a cell
 // whose bounding-box centre left the box [lo, lo + L) moves by -L*d as a whole
 // (with many boxes, B.nbox > 0, the cell's box -- from its first vertex -- gives L)

@@ -34,6 +34,9 @@ struct MembraneArgs {
 cudaError_t area_volume_launch(int nc, int nv, int nt, const int *tri, const float *pos, int stride, double *av,
                                cudaStream_t st);
 cudaError_t membrane_launch(const MembraneArgs &A, cudaStream_t st);
+// Juelicher bending of the cells of A added to A.force; scratch: av, lt
+// (nc * nv doubles each), curva (nc doubles); ring valence at most 12
+cudaError_t juelicher_launch(const MembraneArgs &A, double *av, double *lt, double *curva, cudaStream_t st);
 // vector-Jacobian product of the forces of membrane_launch (A.pos/A.vel float4
 // SoA) for the cotangent lam: accumulated into adj_x, adj_v; pg[0..1] +=
 // d/dks, d/dkb; avd: scratch of 4 doubles per cell

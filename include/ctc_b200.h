@@ -143,8 +143,10 @@ int ctc_rbc_force_ini(int nv, int nt, const int *tri, int max_cells, ctc_rbc_for
 int ctc_rbc_force_fin(ctc_rbc_force *f);
 /* maximum valence of the template (mesh_read_get_md) */
 int ctc_rbc_force_md(const ctc_rbc_force *f, int *md);
-/* rbc_force_set_bending: 1 = "kantor" (default), 0 = "none" */
-int ctc_rbc_force_set_bending(ctc_rbc_force *f, int kantor);
+/* rbc_force_set_bending: 1 = "kantor" (default), 0 = "none", 2 = "juelicher"
+ * (src/rbc/force/bending/juelicher, with the reference's hard-coded kb = 1
+ * and spontaneous curvature H0 = -1/2; ring valence at most 12) */
+int ctc_rbc_force_set_bending(ctc_rbc_force *f, int mode);
 /* rbc_force_apply (src/rbc/force/imp/forces.h:45-68), stress-ful, no random
  * force: per-cell area and volume (FP64), Kantor bending, area, volume,
  * WLC + POW spring and viscous forces of the nc cells pp [dev, AoS, cell c
@@ -265,6 +267,9 @@ int ctc_sim_set_contact(ctc_sim *s, const ctc_dpdlj_params *p);
 /* the membrane random force (ctc_rbc_force_set_rnd) in the step, one key per
  * step from a trunk seeded by seed; set after ctc_sim_set_membranes */
 int ctc_sim_set_membrane_noise(ctc_sim *s, int enable, unsigned seed);
+/* the membranes' bending in the step (ctc_rbc_force_set_bending's modes:
+ * 0 none, 1 kantor, 2 juelicher); set after ctc_sim_set_membranes */
+int ctc_sim_set_bending(ctc_sim *s, int mode);
 /* download the membrane vertices [host, AoS, nc * nv] */
 int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream);
 /* download the cell-sorted solvent [host, AoS, capacity maxp] */

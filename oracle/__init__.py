@@ -76,6 +76,7 @@ def lib():
             "orc_fsi_halo": (None, [C.c_int] * 4 + [f32p, C.c_int, f32p, i32p, Dpd, C.c_float, f32p, f32p]),
             "orc_fsi_halo_images": (C.c_int, [C.c_int] * 4 + [f32p, C.c_void_p, C.c_void_p]),
             "orc_pair_force_dpdlj": (None, [DpdLj, f32p, f32p, C.c_float, f32p]),
+            "orc_juelicher_forces": (None, [C.c_int, C.c_int, C.c_int, i32p, f32p, f64p]),
             "orc_cnt_forces": (None, [C.c_int] * 4 + [f32p, DpdLj, C.c_float, C.c_float, f32p]),
             "orc_mesh_md": (C.c_int, [C.c_int, C.c_int, i32p]),
             "orc_adj_build": (C.c_int, [C.c_int] * 3 + [i32p, i32p, i32p]),
@@ -197,6 +198,18 @@ def pair_force(dpd, pa, pb, rnd):
     lib().orc_pair_force(*[float(x) for x in dpd], np.asarray(pa, np.float32),
                          np.asarray(pb, np.float32), float(rnd), f)
     return f
+
+
+# ---- Juelicher bending (src/rbc/force/bending/juelicher) -------------------
+def juelicher_forces(tri, nv, pv):
+    """The Juelicher bending forces (kb = 1, H0 = -1/2 as the reference
+    hard-codes them) of the cells pv (nc*nv, 6) AoS, in double."""
+    pv = _pp(pv)
+    tri = np.ascontiguousarray(np.asarray(tri, np.int32)[:, :3])
+    nc = len(pv) // nv
+    ff = np.zeros((len(pv), 3), np.float64)
+    lib().orc_juelicher_forces(nc, nv, len(tri), tri, pv, ff)
+    return ff
 
 
 # ---- membrane-membrane contact (src/cnt) -------------------------------------
@@ -384,11 +397,13 @@ def distribute(L, pp):
 
 
 def rbc_step(L, ps, pv, tri, nv, dpd, fsi, rbcpar, seeds27, fsi_seeds, bodyf, dt, ms, mv, cnt=None,
-             cnt_seeds=None):
+             cnt_seeds=None, bending="kantor"):
     """One step of solvent + membranes in the reference's order
     (src/sim/imp/run.h:8-68), with membrane-membrane contact (cnt: a PairDPDLJ
     tuple, cnt_seeds: its bulk and halo seeds) among the object forces
-    (src/sim/objinter/imp/main.h:42-92); returns (solvent sorted, vertices)."""
+    (src/sim/objinter/imp/main.h:42-92) and the membranes' bending "kantor"
+    or "juelicher" (src/rbc/force/bending/imp.cpp); returns (solvent sorted,
+    vertices)."""
     counts, starts, ps = distribute(L, ps)
     pv = rbc_wrap(L, pv, nv)
     fs = dpd_bulk(L, ps, starts, dpd, seeds27[0]) + dpd_halo(L, ps, starts, counts, dpd, seeds27[1:])
@@ -400,6 +415,10 @@ def rbc_step(L, ps, pv, tri, nv, dpd, fsi, rbcpar, seeds27, fsi_seeds, bodyf, dt
     fs = body_force(fs, ms, a)
     fv = body_force(fv, mv, a)
     ps = move(ps, fs, dt, ms)
-    fv = fv + rbc_forces(tri, nv, pv, rbcpar, mode=0)
+    if bending == "juelicher":
+        fv = fv + rbc_forces(tri, nv, pv, dict(rbcpar, kb=0.0), mode=0)
+        fv = (fv + juelicher_forces(tri, nv, pv)).astype(np.float32)
+    else:
+        fv = fv + rbc_forces(tri, nv, pv, rbcpar, mode=0)
     pv = move(pv, fv, dt, mv)
     return ps, pv

@@ -521,6 +521,169 @@ void orc_fsi_halo(int LX, int LY, int LZ, int nv, const float *pv, int ns, const
 }
 
 /* ========================================================================= */
+/* Juelicher bending, src/rbc/force/bending/juelicher                         */
+/* ========================================================================= */
+/* triangle helpers of src/math/tri/dev.h */
+static void v3sub(const double *a, const double *b, double *c) { c[0] = a[0] - b[0]; c[1] = a[1] - b[1]; c[2] = a[2] - b[2]; }
+static double v3dot(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static double v3abs(const double *a) { return sqrt(v3dot(a, a)); }
+static void v3cross(const double *a, const double *b, double *c) {
+    c[0] = a[1] * b[2] - b[1] * a[2]; c[1] = b[0] * a[2] - a[0] * b[2]; c[2] = a[0] * b[1] - b[0] * a[1];
+}
+static double kahan_area(const double *r0, const double *r1, const double *r2) {   /* tri/dev.h:39-51 */
+    double u[3], a, b, c, t;
+    v3sub(r0, r1, u); a = v3abs(u);
+    v3sub(r1, r2, u); b = v3abs(u);
+    v3sub(r2, r0, u); c = v3abs(u);
+    /* sort3(&c, &b, &a): a >= b >= c */
+    if (a < b) { t = a; a = b; b = t; }
+    if (b < c) { t = b; b = c; c = t; }
+    if (a < b) { t = a; a = b; b = t; }
+    return sqrt((a + (b + c)) * (c - (a - b)) * (c + (a - b)) * (a + (b - c))) / 4;
+}
+static double orient2d(const double *a, const double *b, const double *c, int P, int Q) {
+    return (a[P] - c[P]) * (b[Q] - c[Q]) - (a[Q] - c[Q]) * (b[P] - c[P]);
+}
+static double orient3d(const double *a, const double *b, const double *c, const double *d) {
+    double ax = a[0] - d[0], ay = a[1] - d[1], az = a[2] - d[2], bx = b[0] - d[0], by = b[1] - d[1], bz = b[2] - d[2];
+    double cx = c[0] - d[0], cy = c[1] - d[1], cz = c[2] - d[2];
+    return ax * (by * cz - bz * cy) + bx * (cy * az - cz * ay) + cx * (ay * bz - az * by);
+}
+static double tri_dih(const double *a, const double *b, const double *c, const double *d) {   /* dihedral_xy */
+    double k[3], l[3], bc[3], x, y;
+    k[0] = orient2d(b, c, a, 1, 2); k[1] = orient2d(b, c, a, 2, 0); k[2] = orient2d(b, c, a, 0, 1);
+    l[0] = orient2d(c, b, d, 1, 2); l[1] = orient2d(c, b, d, 2, 0); l[2] = orient2d(c, b, d, 0, 1);
+    v3sub(b, c, bc);
+    y = -orient3d(a, b, c, d) * v3abs(bc);
+    x = v3dot(k, l);
+    return -atan2(y, x);
+}
+static void v3norm(const double *a, double *b) {                   /* vec_norm: unchanged if ~0 */
+    double s = v3abs(a);
+    if (s > 1e-12 || s < -1e-12) { b[0] = a[0] / s; b[1] = a[1] / s; b[2] = a[2] / s; }
+    else { b[0] = a[0]; b[1] = a[1]; b[2] = a[2]; }
+}
+static void tri_normal(const double *a, const double *b, const double *c, double *e) {
+    double u[3], v[3], n[3];
+    v3sub(b, a, u); v3sub(c, a, v); v3cross(u, v, n); v3norm(n, e);
+}
+static double tri_cot(const double *a, const double *b, const double *c) {   /* at b */
+    double u[3], v[3];
+    v3sub(a, b, u); v3sub(c, b, v);
+    return v3dot(u, v) / (2 * kahan_area(a, b, c));
+}
+/* ddih_angle (juelicher/dev/main.h:88-118) */
+static void ddih(const double *a, const double *b, const double *c, const double *d, double *da, double *db,
+                 double *dc, double *dd) {
+    double n[3], k[3], u[3], e, An, Ak, cn, bn, bk, ck;
+    int q;
+    tri_normal(a, b, c, n);
+    tri_normal(c, b, d, k);
+    v3sub(b, c, u); e = v3abs(u);
+    An = kahan_area(a, b, c); Ak = kahan_area(c, b, d);
+    cn = tri_cot(b, c, a); bn = tri_cot(a, b, c); bk = tri_cot(c, b, d); ck = tri_cot(d, c, b);
+    for (q = 0; q < 3; q++) {
+        da[q] = n[q] * (e / (2 * An));
+        dd[q] = k[q] * (e / (2 * Ak));
+        dc[q] = -bn / e * n[q] - bk / e * k[q];
+        db[q] = -cn / e * n[q] - ck / e * k[q];
+    }
+}
+/* dtri_area (juelicher/dev/main.h:127-135) */
+static void dtri_area(const double *a, const double *b, const double *c, double *da, double *db, double *dc) {
+    double n[3], ab[3], bc[3], ca[3];
+    int q;
+    tri_normal(a, b, c, n);
+    for (q = 0; q < 3; q++) n[q] *= 0.5;
+    v3sub(b, a, ab); v3sub(c, b, bc); v3sub(a, c, ca);
+    v3cross(n, bc, da); v3cross(n, ca, db); v3cross(n, ab, dc);
+}
+
+/* the dihedral list (i, j, k, l) of every edge (juelicher/imp/main.h:46-52):
+ * edge j-k, i the third vertex of the triangle of the half-edge j -> k, l
+ * that of the triangle of k -> j; one entry per edge, from its j < k side */
+static int juelicher_dih(int nt, const int *tri, int *dih) {
+    int t, s, u, r, ne = 0;
+    for (t = 0; t < nt; t++)
+        for (s = 0; s < 3; s++) {
+            int j = tri[3 * t + s], k = tri[3 * t + (s + 1) % 3], i = tri[3 * t + (s + 2) % 3], l = -1;
+            if (j > k) continue;
+            for (u = 0; u < nt && l < 0; u++)
+                for (r = 0; r < 3; r++)
+                    if (tri[3 * u + r] == k && tri[3 * u + (r + 1) % 3] == j) { l = tri[3 * u + (r + 2) % 3]; break; }
+            dih[4 * ne] = i; dih[4 * ne + 1] = j; dih[4 * ne + 2] = k; dih[4 * ne + 3] = l;
+            ne++;
+        }
+    return ne;
+}
+
+void orc_juelicher_forces(int nc, int nv, int nt, const int *tri, const float *pp, double *ff) {
+    const double pi = (float)3.141592653589793, H0 = -0.5, kb = 1.0;   /* juelicher/imp/forces.h:54-57 */
+    const double kad = (float)(2 * kb / pi);
+    int *dih = (int*)malloc(sizeof(int) * 4 * 3 * nt), ne = juelicher_dih(nt, tri, dih), c, e, t, v, q;
+    double *r = (double*)malloc(sizeof(double) * 3 * nv), *area = (double*)malloc(sizeof(double) * nv);
+    double *lt = (double*)malloc(sizeof(double) * nv), *theta = (double*)malloc(sizeof(double) * ne);
+    double *f = (double*)malloc(sizeof(double) * 3 * nv);
+    for (c = 0; c < nc; c++) {
+        double A = 0, LT = 0, curva;
+        for (v = 0; v < nv; v++) {
+            for (q = 0; q < 3; q++) r[3 * v + q] = pp[6 * ((size_t)c * nv + v) + q];
+            area[v] = lt[v] = 0;
+            f[3 * v] = f[3 * v + 1] = f[3 * v + 2] = 0;
+        }
+        for (t = 0; t < nt; t++) {                                    /* compute_area */
+            const int *T = tri + 3 * t;
+            double a0 = kahan_area(r + 3 * T[0], r + 3 * T[1], r + 3 * T[2]) / 3;
+            area[T[0]] += a0; area[T[1]] += a0; area[T[2]] += a0;
+        }
+        for (e = 0; e < ne; e++) {                                    /* compute_theta_len */
+            const int *D = dih + 4 * e;
+            double u[3];
+            theta[e] = tri_dih(r + 3 * D[0], r + 3 * D[1], r + 3 * D[2], r + 3 * D[3]);
+            v3sub(r + 3 * D[2], r + 3 * D[1], u);
+            lt[D[1]] += v3abs(u) * theta[e];
+            lt[D[2]] += v3abs(u) * theta[e];
+        }
+        for (v = 0; v < nv; v++) { A += area[v]; LT += lt[v]; }
+        curva = (LT / 4 - H0 * A) * (4 * kad * pi / A);               /* compute_mean_curv */
+        for (e = 0; e < ne; e++) {
+            const int *D = dih + 4 * e;
+            const int i = D[0], j = D[1], k = D[2], l = D[3];
+            double u[3], en[3], len, hj, hk, coef, da[3], db[3], dc[3], dd[3];
+            hj = lt[j] / area[j] / 4 - H0;
+            hk = lt[k] / area[k] / 4 - H0;
+            /* force_edg (dev/main.h:245-263): d|c - b| = (-e, e) */
+            v3sub(r + 3 * k, r + 3 * j, u);
+            v3norm(u, en);
+            coef = -(hj + hk) * theta[e] - curva / 4 * theta[e];
+            for (q = 0; q < 3; q++) { f[3 * j + q] -= coef * en[q]; f[3 * k + q] += coef * en[q]; }
+            /* force_lentheta (dev/main.h:292-321) */
+            len = v3abs(u);
+            ddih(r + 3 * i, r + 3 * j, r + 3 * k, r + 3 * l, da, db, dc, dd);
+            coef = -(hj + hk) * len - curva / 2.0 * len;
+            for (q = 0; q < 3; q++) {
+                f[3 * i + q] += coef * da[q]; f[3 * j + q] += coef * db[q];
+                f[3 * k + q] += coef * dc[q]; f[3 * l + q] += coef * dd[q];
+            }
+        }
+        for (t = 0; t < nt; t++) {                                    /* force_area (dev/main.h:348-376) */
+            const int *T = tri + 3 * t;
+            double d[3][3];
+            int s;
+            dtri_area(r + 3 * T[0], r + 3 * T[1], r + 3 * T[2], d[0], d[1], d[2]);
+            for (s = 0; s < 3; s++) {
+                const int w = T[s];
+                const double coef = 1.0 / 3.0 * (lt[w] * lt[w] / 8.0 / area[w] / area[w] - 2.0 * H0 * H0);
+                for (q = 0; q < 3; q++) f[3 * w + q] += coef * d[s][q];
+            }
+        }
+        for (v = 0; v < nv; v++)                                      /* accumulate: f + fad */
+            for (q = 0; q < 3; q++) ff[3 * ((size_t)c * nv + v) + q] += f[3 * v + q];
+    }
+    free(dih); free(r); free(area); free(lt); free(theta); free(f);
+}
+
+/* ========================================================================= */
 /* membrane-membrane contact, src/cnt (one object type)                       */
 /* ========================================================================= */
 

@@ -121,6 +121,11 @@ void orc_rbc_forces_f64(int nc, int nv, int md, int nt, const int *adj0, const i
 double orc_kantor_energy(int nv, int md, const int *adj0, const int *adj1, const float *pp,
                          double kb, double phi_deg);
 
+/* Juelicher bending (src/rbc/force/bending/juelicher, kb = 1 and H0 = -1/2 as
+ * the reference hard-codes them) of nc cells of one template: the forces
+ * f + fad of juelicher_apply in double, added to ff (3 per vertex) */
+void orc_juelicher_forces(int nc, int nv, int nt, const int *tri, const float *pp, double *ff);
+
 /* ---- update (src/scheme/move, src/scheme/force) --------------------------- */
 void orc_move(float dt, float mass, int n, const float *ff, float *pp);
 void orc_body_force(float mass, const float a[3], int n, float *ff);

@@ -1,5 +1,6 @@
 """ctypes front end of oracle/_ref/librefkern.so: the reference's own device
-code (src/math/rnd/dev.h, src/pair/dev.h) built from its sources by
+code (src/math/rnd/dev.h, src/pair/dev.h, the fluforces and Juelicher
+kernels) built from its sources by
 oracle/ref.mk.  TEST INFRASTRUCTURE ONLY.  Arrays are torch CUDA tensors."""
 import ctypes as C
 import os
@@ -111,3 +112,34 @@ def halo(dpd, L, pp, starts, counts, seeds26, ff):
         rp = rpp if rpp.shape[0] > 0 else torch.zeros((1, 6), device=dev)
         assert lib_.refkern_halo(*[float(x) for x in dpd], *L, fid, n, _p(lpp), _p(lii), _p(rp), _p(rss),
                                  float(seeds26[fid]), int(masks[fid]), _p(ff)) == 0
+
+
+def dihedrals(tri):
+    """One (i, j, k, l) per edge j-k as juelicher_ini lists them
+    (src/rbc/force/bending/juelicher/imp/main.h:46-52): i the third vertex of
+    the triangle of the half-edge j -> k, l that of k -> j (taken from the
+    j < k side; the dihedral angle and its derivatives are the same from
+    either side)."""
+    import numpy as np
+    tri = np.asarray(tri)[:, :3]
+    third = {}
+    for a, b, c in tri:
+        third[(a, b)], third[(b, c)], third[(c, a)] = c, a, b
+    return np.array([(i, j, k, third[(k, j)]) for (j, k), i in third.items() if j < k], np.int32)
+
+
+def juelicher(tri, nv, pp, ff):
+    """juelicher_apply's kernels on the cells pp (torch (nc*nv, 6) AoS); adds
+    their forces to ff (torch, (nc*nv, 3))."""
+    import numpy as np
+    import torch
+    tri = np.asarray(tri)[:, :3]
+    t4 = torch.zeros((len(tri), 4), dtype=torch.int32)
+    t4[:, :3] = torch.as_tensor(tri.astype(np.int32))
+    d4 = torch.as_tensor(dihedrals(tri))
+    t4, d4 = t4.to(pp.device), d4.to(pp.device)
+    vp = C.c_void_p
+    lib_ = lib()
+    lib_.refkern_juelicher.argtypes = [C.c_int] * 4 + [vp, vp, vp, vp]
+    torch.cuda.synchronize()
+    assert lib_.refkern_juelicher(int(pp.shape[0]) // nv, nv, len(t4), len(d4), _p(pp), _p(t4), _p(d4), _p(ff)) == 0

@@ -6,6 +6,7 @@
 //   refkern_pair  -> pair_force<PairDPD, PairFo>       (src/pair/dev.h)
 //   refkern_bulk  -> fbulk_dev::apply                  (src/fluforces/bulk/dev/main.h)
 //   refkern_halo  -> fhalo_dev::apply, one fragment    (src/fluforces/halo/dev/main.h)
+//   refkern_juelicher -> juelicher_apply's kernels    (src/rbc/force/bending/juelicher/dev/main.h)
 #include <stdio.h>
 #include <assert.h>
 #include "inc/def.h"
@@ -130,4 +131,56 @@ extern "C" int refkern_halo(float a, float g, float s, float spow, int LX, int L
     FoArray_v fa = {ff};
     fhalo_dev::apply<<<(nl + 127) / 128, 128>>>(fid, p, make_int3(LX, LY, LZ), lf, rf, rnd, fa);
     return (int)cudaDeviceSynchronize();
+}
+
+// ---------------------------------------------------------------------------
+// the reference's Juelicher bending kernels (src/rbc/force/bending/juelicher/
+// dev/main.h), launched in the order of juelicher_apply (imp/forces.h:40-125)
+// with its hard-coded constants; dih = the (i, j, k, l) of every edge as
+// juelicher_ini (imp/main.h:1-56) lists them
+// ---------------------------------------------------------------------------
+#include "math/tri/dev.h"
+#include "algo/utils/shfl.h"
+#include "algo/utils/dev.h"
+namespace juelicher_dev {
+#include "rbc/force/bending/juelicher/dev/main.h"
+}
+
+static int nblk(int n) { return (n + 127) / 128; }
+
+/* juelicher_apply on nc cells of nv AoS particles; ff (3 floats a vertex) accumulated */
+extern "C" int refkern_juelicher(int nc, int nv, int nt, int ne, const float *pp, const int *tri4, const int *dih4,
+                                 float *ff) {
+    if (nc <= 0) return 0;
+    float pi = 3.141592653589793, H0 = -1.0 / 2.0, kb = 1.0, kad = 2 * kb / pi;
+    float *area, *lentheta, *theta, *lt_tot, *a_tot, *curva, *f, *fad;
+    const size_t nvc = (size_t)nv * nc;
+    if (cudaMalloc(&area, sizeof(float) * nvc) || cudaMalloc(&lentheta, sizeof(float) * nvc) ||
+        cudaMalloc(&theta, sizeof(float) * (size_t)ne * nc) || cudaMalloc(&lt_tot, sizeof(float) * nc) ||
+        cudaMalloc(&a_tot, sizeof(float) * nc) || cudaMalloc(&curva, sizeof(float) * nc) ||
+        cudaMalloc(&f, sizeof(float) * 3 * nvc) || cudaMalloc(&fad, sizeof(float) * 3 * nvc))
+        return 1;
+    const Particle *P = (const Particle *)pp;
+    const int4 *tri = (const int4 *)tri4, *dih = (const int4 *)dih4;
+    dim3 sblk((nv + 127) / 128, nc);
+    cudaMemset(area, 0, sizeof(float) * nvc);
+    juelicher_dev::compute_area<<<nblk(nt * nc), 128>>>(nv, nt, nc, P, tri, area);
+    cudaMemset(a_tot, 0, sizeof(float) * nc);
+    juelicher_dev::sum<<<sblk, 128>>>(nv, area, a_tot);
+    cudaMemset(theta, 0, sizeof(float) * (size_t)ne * nc);
+    cudaMemset(lentheta, 0, sizeof(float) * nvc);
+    juelicher_dev::compute_theta_len<<<nblk(ne * nc), 128>>>(nv, ne, nc, P, dih, theta, lentheta);
+    cudaMemset(lt_tot, 0, sizeof(float) * nc);
+    juelicher_dev::sum<<<sblk, 128>>>(nv, lentheta, lt_tot);
+    juelicher_dev::compute_mean_curv<<<nblk(nc), 128>>>(nc, H0, kad, lt_tot, a_tot, curva);
+    cudaMemset(f, 0, sizeof(float) * 3 * nvc);
+    cudaMemset(fad, 0, sizeof(float) * 3 * nvc);
+    juelicher_dev::force_edg<<<nblk(ne * nc), 128>>>(nv, ne, nc, H0, P, dih, curva, theta, lentheta, area, f, fad);
+    juelicher_dev::force_lentheta<<<nblk(ne * nc), 128>>>(nv, ne, nc, H0, P, dih, curva, lentheta, area, f, fad);
+    juelicher_dev::force_area<<<nblk(nt * nc), 128>>>(nv, nt, nc, H0, P, tri, lentheta, area, f);
+    juelicher_dev::accumulate<<<nblk(nv * nc), 128>>>(nv * nc, f, fad, (Force *)ff);
+    int rc = (int)cudaDeviceSynchronize();
+    cudaFree(area); cudaFree(lentheta); cudaFree(theta); cudaFree(lt_tot);
+    cudaFree(a_tot); cudaFree(curva); cudaFree(f); cudaFree(fad);
+    return rc;
 }

@@ -48,3 +48,31 @@ def test_bending_force_is_energy_gradient():
             g = (oracle.kantor_energy(F, len(V), p1, 1.0) - oracle.kantor_energy(F, len(V), p2, 1.0)) / \
                 (float(p1[i, c]) - float(p2[i, c]))
             assert abs(-g - f[i, c]) < 2e-3 * max(1.0, abs(f[i, c])), (i, c, -g, f[i, c])
+
+
+def test_juelicher_oracle_invariants():
+    """The oracle's Juelicher bending (src/rbc/force/bending/juelicher):
+    translation invariant and rotation covariant; one dihedral per edge; not
+    momentum-free, as the reference's own force_area applies each vertex's
+    coefficient to its own area derivative only (not an exact gradient)."""
+    from oracle import refkern
+    V, F = mesh.read_off(os.path.join(GOLDEN, "rbc.642.off"))
+    assert len(refkern.dihedrals(F)) == 3 * len(F) // 2
+    rng = np.random.default_rng(1)
+    pp = np.zeros((len(V), 6), np.float32)
+    pp[:, :3] = V + rng.normal(0, 0.05, V.shape)
+    f = oracle.juelicher_forces(F, len(V), pp)
+    scale = np.abs(f).max()
+    assert scale > 1
+    sh = pp.copy()
+    sh[:, :3] += np.float32(1.0)
+    assert np.abs(oracle.juelicher_forces(F, len(V), sh) - f).max() < 1e-5 * scale
+    R = mesh.random_rotation(rng)
+    pr = pp.copy()
+    pr[:, :3] = (pp[:, :3].astype(np.float64) @ R.T).astype(np.float32)
+    assert np.abs(oracle.juelicher_forces(F, len(V), pr) - f @ R.T).max() < 1e-5 * scale
+    # two cells: each cell's forces are its own
+    two = np.concatenate([pp, sh])
+    f2 = oracle.juelicher_forces(F, len(V), two)
+    assert np.abs(f2[:len(V)] - f).max() < 1e-12 * scale
+    assert 1e-6 < np.abs(f.sum(0)).max() / np.abs(f).sum() < 1e-2
