@@ -227,6 +227,79 @@ class Contact:
                                          float(seed_halo), _ptr(fv), _stream(stream)))
 
 
+def _vp(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def bop_write(name, data, vars):
+    """A bop file name.bop + name.values: data (n, nvars) float32 or int32
+    [host], vars the space-separated variable names."""
+    data = np.ascontiguousarray(data)
+    t = _lib.CTC_BOP_INT if data.dtype.kind in "iu" else _lib.CTC_BOP_FLOAT
+    data = np.ascontiguousarray(data, np.int32 if t == _lib.CTC_BOP_INT else np.float32)
+    check(lib().ctc_bop_write(str(name).encode(), len(data), t, vars.encode(), _vp(data)))
+
+
+def bop_read(header):
+    """The records of a bop file (header: its .bop path) as an (n, nvars)
+    float32 or int32 array; ascii and iascii values files are read too."""
+    n, t, nv = C.c_long(), C.c_int(), C.c_int()
+    check(lib().ctc_bop_read(str(header).encode(), 0, C.byref(n), C.byref(t), C.byref(nv), None))
+    out = np.zeros((n.value, nv.value), np.float32 if t.value == _lib.CTC_BOP_FLOAT else np.int32)
+    check(lib().ctc_bop_read(str(header).encode(), out.size, C.byref(n), None, None, _vp(out)))
+    return out
+
+
+def _restart_id(id):
+    return {"templ": _lib.CTC_RESTART_TEMPL, "final": _lib.CTC_RESTART_FINAL}.get(id, id)
+
+
+def restart_write_pp(base, code, id, pp):
+    """restart_write_pp (src/io/restart/imp.h): base/code/ID.bop with ID
+    "templ", "final" or %05d; pp (n, 6) x y z vx vy vz [host]."""
+    pp = np.ascontiguousarray(pp, np.float32).reshape(-1, 6)
+    check(lib().ctc_restart_write_pp(str(base).encode(), code.encode(), _restart_id(id), len(pp), _vp(pp)))
+
+
+def restart_write_ii(base, code, id, ii):
+    ii = np.ascontiguousarray(ii, np.int32).reshape(-1)
+    check(lib().ctc_restart_write_ii(str(base).encode(), code.encode(), _restart_id(id), len(ii), _vp(ii)))
+
+
+def _restart_read(fn, base, code, id, shape, dtype):
+    n = C.c_long()
+    check(fn(str(base).encode(), code.encode(), _restart_id(id), 0, C.byref(n), None))
+    out = np.zeros((n.value,) + shape, dtype)
+    check(fn(str(base).encode(), code.encode(), _restart_id(id), n.value, C.byref(n), _vp(out)))
+    return out
+
+
+def restart_read_pp(base, code, id):
+    return _restart_read(lib().ctc_restart_read_pp, base, code, id, (6,), np.float32)
+
+
+def restart_read_ii(base, code, id):
+    return _restart_read(lib().ctc_restart_read_ii, base, code, id, (), np.int32)
+
+
+def io_bop_parts(dump_base, name, id, pp, L, ff=None):
+    """io_bop_parts / io_bop_parts_forces (src/io/bop/imp.h) of one rank:
+    dump_base/bop/name-%05d, positions from the box's edge."""
+    pp = np.ascontiguousarray(pp, np.float32).reshape(-1, 6)
+    fp = None
+    if ff is not None:
+        ff = np.ascontiguousarray(ff, np.float32).reshape(-1, 3)
+        fp = _vp(ff)
+    check(lib().ctc_io_bop_parts(str(dump_base).encode(), name.encode(), int(id), len(pp), _vp(pp), fp,
+                                 *(int(x) for x in L)))
+
+
+def io_bop_ids(dump_base, name, id, ii, colors=False):
+    """io_bop_ids (variable "ids") or, colors=True, io_bop_colors ("color")."""
+    ii = np.ascontiguousarray(ii, np.int32).reshape(-1)
+    check(lib().ctc_io_bop_ints(str(dump_base).encode(), name.encode(), int(id), len(ii), _vp(ii), int(bool(colors))))
+
+
 def mesh_write_ply(path, pv, tri, nv, L, shift="edge"):
     """mesh_write_particles (src/io/mesh/imp/main.h): the membranes pv
     (nc*nv, 6) AoS [host] with the template's triangles tri (nt, 3) as the
@@ -341,6 +414,14 @@ class Sim:
 
     def step(self, n=1, stream=None):
         check(lib().ctc_sim_step(self.h, int(n), _stream(stream)))
+
+    def strt_dump(self, base, id, name="rbc"):
+        """The restart files of the state (flu_strt_dump and rbc_strt_dump,
+        src/flu/imp/start.h, src/rbc/imp/start.h): base/flu.pp/ID and, with
+        membranes, base/<name>.pp/ID."""
+        restart_write_pp(base, "flu.pp", id, self.get_solvent())
+        if getattr(self, "mnv", 0):
+            restart_write_pp(base, name + ".pp", id, self.get_membranes())
 
     def get_solvent(self, stream=None):
         out = np.zeros((self.maxp, 6), np.float32)

@@ -12,6 +12,8 @@ LIB_PATH = os.path.join(HERE, "libctc_b200.so")
 CTC_OK, CTC_ERR_ARG, CTC_ERR_CUDA, CTC_ERR_CAPACITY, CTC_ERR_DEVICE = 0, 1, 2, 3, 4
 CTC_RNG_REFERENCE, CTC_RNG_STABLE = 0, 1
 CTC_SIM_PHASES = 8
+CTC_BOP_FLOAT, CTC_BOP_INT = 0, 1
+CTC_RESTART_TEMPL, CTC_RESTART_FINAL = -1, -2
 SIM_PHASE_NAMES = ("clist", "frag_starts", "bulk", "halo", "fsi", "contact", "update", "membrane")
 
 vp = C.c_void_p
@@ -86,6 +88,14 @@ SIGNATURES = {
                                      C.c_int]),
     "ctc_sim_set_membrane_noise": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_sim_set_bending": (C.c_int, [vp, C.c_int]),
+    "ctc_bop_write": (C.c_int, [C.c_char_p, C.c_long, C.c_int, C.c_char_p, vp]),
+    "ctc_bop_read": (C.c_int, [C.c_char_p, C.c_long, C.POINTER(C.c_long), ip, ip, vp]),
+    "ctc_restart_write_pp": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, vp]),
+    "ctc_restart_write_ii": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, vp]),
+    "ctc_restart_read_pp": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, C.POINTER(C.c_long), vp]),
+    "ctc_restart_read_ii": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, C.POINTER(C.c_long), vp]),
+    "ctc_io_bop_parts": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, vp, vp, C.c_int, C.c_int, C.c_int]),
+    "ctc_io_bop_ints": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, vp, C.c_int]),
     "ctc_rbc_force_set_rnd": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_sim_tune": (C.c_int, [vp, C.c_int, ip, vp]),
     "ctc_fsi_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),

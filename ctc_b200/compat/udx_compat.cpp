@@ -36,6 +36,9 @@
 #include "rbc/params/imp.h"
 #include "rbc/force/imp.h"
 #include "scheme/move/imp.h"
+#include <stdio.h>
+#include <limits.h>
+#include "io/restart/imp.h"
 #include "utils/error.h"
 
 #include "ctc_b200.h"
@@ -225,4 +228,26 @@ void scheme_move_apply(float dt, float mass, int n, const Force *ff, Particle *p
 
 void scheme_move_clear_vel(int n, Particle *pp) {
     CTC(ctc_scheme_move_clear_vel(n, reinterpret_cast<float*>(pp), NULL));
+}
+
+// ---- restart files (src/io/restart/imp.h), one rank: particles and ints -------
+void restart_write_pp(MPI_Comm, const char *base, const char *code, int id, long n, const Particle *pp) {
+    CTC(ctc_restart_write_pp(base, code, id, n, reinterpret_cast<const float*>(pp)));
+}
+
+void restart_write_ii(MPI_Comm, const char *base, const char *code, int id, long n, const int *ii) {
+    CTC(ctc_restart_write_ii(base, code, id, n, ii));
+}
+
+// the reference reads into buffers sized by its callers, with no capacity argument
+void restart_read_pp(MPI_Comm, const char *base, const char *code, int id, int *n, Particle *pp) {
+    long m = 0;
+    CTC(ctc_restart_read_pp(base, code, id, LONG_MAX / 6, &m, reinterpret_cast<float*>(pp)));
+    *n = (int)m;
+}
+
+void restart_read_ii(MPI_Comm, const char *base, const char *code, int id, int *n, int *ii) {
+    long m = 0;
+    CTC(ctc_restart_read_ii(base, code, id, LONG_MAX, &m, ii));
+    *n = (int)m;
 }

@@ -210,6 +210,34 @@ int ctc_cnt_apply_seeded(ctc_cnt *c, const ctc_dpdlj_params *p, int nv, const fl
 int ctc_mesh_write_ply(const char *path, int nc, int nv, int nt, const int *tri, const float *pp, int shift, int LX,
                        int LY, int LZ);
 
+/* ---- bop particle files and restart files: replaces src/io/restart/imp.h
+ * and src/io/bop/imp.h for one rank (host code, host arrays) -------------- */
+/* a bop file NAME: text header NAME.bop (count; DATA_FILE: NAME.values;
+ * DATA_FORMAT: float|int|ascii|iascii; VARIABLES: names) and the values */
+#define CTC_BOP_FLOAT 0
+#define CTC_BOP_INT 1
+/* writes NAME.bop + NAME.values: n records of the variables vars (space
+ * separated) as raw little-endian 4-byte words; creates missing folders */
+int ctc_bop_write(const char *name, long n, int type, const char *vars, const void *data);
+/* reads a header (and, when data != NULL, its values, at most cap 4-byte
+ * words; ascii as float, iascii as int): records n, CTC_BOP_* type, nvars */
+int ctc_bop_read(const char *header, long cap, long *n, int *type, int *nvars, void *data);
+/* restart_write_pp / _ii, restart_read_pp / _ii: file base/code/ID with ID
+ * "templ" (CTC_RESTART_TEMPL), "final" (CTC_RESTART_FINAL) or %05d; pp six
+ * floats a particle (x y z vx vy vz), ii one int; cap = records that fit */
+#define CTC_RESTART_TEMPL (-1)
+#define CTC_RESTART_FINAL (-2)
+int ctc_restart_write_pp(const char *base, const char *code, int id, long n, const float *pp);
+int ctc_restart_write_ii(const char *base, const char *code, int id, long n, const int *ii);
+int ctc_restart_read_pp(const char *base, const char *code, int id, long cap, long *n, float *pp);
+int ctc_restart_read_ii(const char *base, const char *code, int id, long cap, long *n, int *ii);
+/* io_bop_parts (ff == NULL) / io_bop_parts_forces (ff: three floats a
+ * particle): dump_base/bop/name-%05d with positions from the box's edge
+ * (x + L/2); io_bop_ids (colors 0, variable "ids") / io_bop_colors (1, "color") */
+int ctc_io_bop_parts(const char *dump_base, const char *name, int id, long n, const float *pp, const float *ff,
+                     int LX, int LY, int LZ);
+int ctc_io_bop_ints(const char *dump_base, const char *name, int id, long n, const int *ii, int colors);
+
 /* ---- time update: replaces src/scheme/move/imp.h:5-6, scheme/force ------- */
 /* scheme_move_apply: v += f/m dt; r += v dt on n AoS particles [dev] */
 int ctc_scheme_move_apply(float dt, float mass, int n, const float *ff, float *pp, void *stream);

@@ -12,7 +12,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 OBJ = os.path.join(ROOT, "ctc_b200", "compat", "_build", "udx_compat.o")
 
 # the declarations of src/clist/imp.h, src/fluforces/imp.h (bulk),
-# src/rbc/force/imp.h and src/scheme/move/imp.h, as the C++ compiler names them
+# src/rbc/force/imp.h, src/scheme/move/imp.h and src/io/restart/imp.h (the
+# MPI_Comm of the compile check is its stand-in type), as the C++ compiler
+# names them
 EXPECTED = [
     "clist_ini(int, int, int, Clist**)",
     "clist_fin(Clist*)",
@@ -37,6 +39,10 @@ EXPECTED = [
     "rbc_force_apply(RbcForce*, RbcParams const*, float, RbcQuants const*, Force*)",
     "scheme_move_apply(float, float, int, Force const*, Particle*)",
     "scheme_move_clear_vel(int, Particle*)",
+    "restart_write_pp(ctc_compat_check_comm*, char const*, char const*, int, long, Particle const*)",
+    "restart_write_ii(ctc_compat_check_comm*, char const*, char const*, int, long, int const*)",
+    "restart_read_pp(ctc_compat_check_comm*, char const*, char const*, int, int*, Particle*)",
+    "restart_read_ii(ctc_compat_check_comm*, char const*, char const*, int, int*, int*)",
 ]
 
 
