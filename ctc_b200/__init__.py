@@ -300,6 +300,119 @@ def io_bop_ids(dump_base, name, id, ii, colors=False):
     check(lib().ctc_io_bop_ints(str(dump_base).encode(), name.encode(), int(id), len(ii), _vp(ii), int(bool(colors))))
 
 
+def wvel(kind="cste", u=(0.0, 0.0, 0.0), gdot=0.0, vdir=0, gdir=1, half=0, w=0.0, h=1.0):
+    """A wall velocity (wvel_set_cste / _shear / _shear_sin / _hs)."""
+    t = {"cste": _lib.CTC_WVEL_CSTE, "shear": _lib.CTC_WVEL_SHEAR, "shear_sin": _lib.CTC_WVEL_SHEAR_SIN,
+         "hs": _lib.CTC_WVEL_HS}[kind]
+    uu = (float(u), 0.0, 0.0) if np.isscalar(u) else tuple(float(x) for x in u)
+    return _lib.Wvel(t, (C.c_float * 3)(*uu), float(gdot), int(vdir), int(gdir), int(half), float(w), float(h))
+
+
+def sdf_read(path):
+    """A field file (sdf.dat): grid size N, extents ext and the values (N2, N1, N0)."""
+    N = (C.c_int * 3)()
+    ext = (C.c_float * 3)()
+    check(lib().ctc_sdf_read(str(path).encode(), N, ext, None))
+    D = np.zeros((N[2], N[1], N[0]), np.float32)
+    check(lib().ctc_sdf_read(str(path).encode(), N, ext, _vp(D)))
+    return list(N), list(ext), D
+
+
+def sdf_resample(N, ext, D, L):
+    """Host-only texture build: (T, tex (T2, T1, T0), o, s, threshold)."""
+    ext = np.ascontiguousarray(ext, np.float32)
+    D = np.ascontiguousarray(D, np.float32)
+    T = (C.c_int * 3)()
+    check(lib().ctc_sdf_resample(*(int(x) for x in N), _vp(ext), _vp(D), *(int(x) for x in L), T, None, None, None,
+                                 None))
+    tex = np.zeros((T[2], T[1], T[0]), np.float32)
+    o, s, thr = np.zeros(3, np.float32), np.zeros(3, np.float32), np.zeros(1, np.float32)
+    check(lib().ctc_sdf_resample(*(int(x) for x in N), _vp(ext), _vp(D), *(int(x) for x in L), T, _vp(o), _vp(s),
+                                 _vp(thr), _vp(tex)))
+    return list(T), tex, o, s, float(thr[0])
+
+
+class Sdf:
+    """sdf_ini + sdf_gen (src/wall/sdf): a field file path, or (N, ext, D)."""
+
+    def __init__(self, L, path=None, grid=None):
+        self.h = C.c_void_p()
+        self.L = tuple(int(x) for x in L)
+        if path is not None:
+            check(lib().ctc_sdf_ini(str(path).encode(), *self.L, C.byref(self.h)))
+        else:
+            N, ext, D = grid
+            ext = np.ascontiguousarray(ext, np.float32)
+            D = np.ascontiguousarray(D, np.float32)
+            check(lib().ctc_sdf_ini_grid(*(int(x) for x in N), _vp(ext), _vp(D), *self.L, C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
+            lib().ctc_sdf_fin(self.h)
+            self.h = C.c_void_p()
+
+    def texture(self):
+        T = (C.c_int * 3)()
+        check(lib().ctc_sdf_texture(self.h, T, None, None, None, None))
+        tex = np.zeros((T[2], T[1], T[0]), np.float32)
+        o, s, thr = np.zeros(3, np.float32), np.zeros(3, np.float32), np.zeros(1, np.float32)
+        check(lib().ctc_sdf_texture(self.h, T, _vp(o), _vp(s), _vp(thr), _vp(tex)))
+        return list(T), tex, o, s, float(thr[0])
+
+    def eval(self, pp, out, stream=None):
+        check(lib().ctc_sdf_eval(self.h, int(pp.shape[0]), _ptr(pp), _ptr(out), _stream(stream)))
+
+    def label(self, pp, out, stream=None):
+        check(lib().ctc_sdf_label(self.h, int(pp.shape[0]), _ptr(pp), _ptr(out), _stream(stream)))
+
+
+class Wall:
+    """wall_gen_quants + wall_gen_ticket (src/wall): freezes the solvent
+    particles pp (host (n, 6)) inside the wall; self.bulk holds the rest."""
+
+    def __init__(self, sdf, pp):
+        self.sdf = sdf                 # the field outlives the wall
+        self.h = C.c_void_p()
+        pp = np.ascontiguousarray(pp, np.float32).reshape(-1, 6).copy()
+        n = C.c_int(0)
+        check(lib().ctc_wall_ini(sdf.h, len(pp), _vp(pp), C.byref(n), C.byref(self.h)))
+        self.bulk = pp[:n.value]
+
+    def __del__(self):
+        if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
+            lib().ctc_wall_fin(self.h)
+            self.h = C.c_void_p()
+
+    def particles(self):
+        n = C.c_int(0)
+        check(lib().ctc_wall_particles(self.h, C.byref(n), None, None))
+        L = self.sdf.L
+        pos = np.zeros((n.value, 4), np.float32)
+        st = np.zeros((L[0] + 12) * (L[1] + 12) * (L[2] + 12) + 1, np.int32)
+        check(lib().ctc_wall_particles(self.h, C.byref(n), _vp(pos), _vp(st)))
+        return pos, st
+
+    def set_vel(self, v):
+        check(lib().ctc_wall_set_vel(self.h, C.byref(v)))
+
+    def update_vel(self, t):
+        check(lib().ctc_wall_update_vel(self.h, float(t)))
+
+    def force(self, params, pp, ff, seed=None, stream=None):
+        if seed is None:
+            check(lib().ctc_wall_force(self.h, C.byref(params), int(pp.shape[0]), _ptr(pp), _ptr(ff),
+                                       _stream(stream)))
+        else:
+            check(lib().ctc_wall_force_seeded(self.h, C.byref(params), int(pp.shape[0]), _ptr(pp), float(seed),
+                                              _ptr(ff), _stream(stream)))
+
+    def bounce(self, dt, pp, stream=None):
+        check(lib().ctc_wall_bounce(self.h, float(dt), int(pp.shape[0]), _ptr(pp), _stream(stream)))
+
+    def repulse(self, lam, pp, ff, stream=None):
+        check(lib().ctc_wall_repulse(self.h, float(lam), int(pp.shape[0]), _ptr(pp), _ptr(ff), _stream(stream)))
+
+
 def mesh_write_ply(path, pv, tri, nv, L, shift="edge"):
     """mesh_write_particles (src/io/mesh/imp/main.h): the membranes pv
     (nc*nv, 6) AoS [host] with the template's triangles tri (nt, 3) as the
@@ -397,6 +510,19 @@ class Sim:
     def set_membrane_noise(self, enable=True, seed=0):
         """The membrane random force (rbc_force_set_rnd1) from the next step on."""
         check(lib().ctc_sim_set_membrane_noise(self.h, int(bool(enable)), int(seed) & 0xffffffff))
+
+    def set_walls(self, sdf, v=None, lam=0.0, stream=None):
+        """Freezes the current solvent against the field sdf (an Sdf of this
+        box) and puts the walls in the step: wall forces on the solvent and
+        the membranes, the membranes' repulsion lam, bounce-back; v the wall
+        velocity (wvel(...), constant zero by default).  None removes them."""
+        if sdf is None:
+            check(lib().ctc_sim_set_walls(self.h, None, None, 0.0, _stream(stream)))
+            self._sdf = None
+            return
+        v = v if v is not None else wvel("cste")
+        check(lib().ctc_sim_set_walls(self.h, sdf.h, C.byref(v), float(lam), _stream(stream)))
+        self._sdf = sdf                  # the field outlives the walls
 
     def set_bending(self, mode="kantor"):
         """The membranes' bending in the step: "kantor", "juelicher" or "none"

@@ -11,10 +11,11 @@ LIB_PATH = os.path.join(HERE, "libctc_b200.so")
 
 CTC_OK, CTC_ERR_ARG, CTC_ERR_CUDA, CTC_ERR_CAPACITY, CTC_ERR_DEVICE = 0, 1, 2, 3, 4
 CTC_RNG_REFERENCE, CTC_RNG_STABLE = 0, 1
-CTC_SIM_PHASES = 8
+CTC_SIM_PHASES = 9
 CTC_BOP_FLOAT, CTC_BOP_INT = 0, 1
 CTC_RESTART_TEMPL, CTC_RESTART_FINAL = -1, -2
-SIM_PHASE_NAMES = ("clist", "frag_starts", "bulk", "halo", "fsi", "contact", "update", "membrane")
+CTC_WVEL_CSTE, CTC_WVEL_SHEAR, CTC_WVEL_SHEAR_SIN, CTC_WVEL_HS = 0, 1, 2, 3
+SIM_PHASE_NAMES = ("clist", "frag_starts", "bulk", "halo", "wall", "fsi", "contact", "update", "membrane")
 
 vp = C.c_void_p
 ip = C.POINTER(C.c_int)
@@ -28,6 +29,12 @@ class DpdParams(C.Structure):
 class DpdLjParams(C.Structure):
     _fields_ = [("a", C.c_float), ("g", C.c_float), ("s", C.c_float), ("spow", C.c_float),
                 ("ljs", C.c_float), ("lje", C.c_float)]
+
+
+class Wvel(C.Structure):
+    """ctc_wvel: the wall velocity (CTC_WVEL_CSTE / SHEAR / SHEAR_SIN / HS)."""
+    _fields_ = [("type", C.c_int), ("u", C.c_float * 3), ("gdot", C.c_float), ("vdir", C.c_int), ("gdir", C.c_int),
+                ("half", C.c_int), ("w", C.c_float), ("h", C.c_float)]
 
 
 class RbcParams(C.Structure):
@@ -88,6 +95,7 @@ SIGNATURES = {
                                      C.c_int]),
     "ctc_sim_set_membrane_noise": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_sim_set_bending": (C.c_int, [vp, C.c_int]),
+    "ctc_sim_set_walls": (C.c_int, [vp, vp, C.POINTER(Wvel), C.c_float, vp]),
     "ctc_bop_write": (C.c_int, [C.c_char_p, C.c_long, C.c_int, C.c_char_p, vp]),
     "ctc_bop_read": (C.c_int, [C.c_char_p, C.c_long, C.POINTER(C.c_long), ip, ip, vp]),
     "ctc_restart_write_pp": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, vp]),
@@ -96,6 +104,23 @@ SIGNATURES = {
     "ctc_restart_read_ii": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, C.POINTER(C.c_long), vp]),
     "ctc_io_bop_parts": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, vp, vp, C.c_int, C.c_int, C.c_int]),
     "ctc_io_bop_ints": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, vp, C.c_int]),
+    "ctc_sdf_ini": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
+    "ctc_sdf_ini_grid": (C.c_int, [C.c_int] * 3 + [vp, vp] + [C.c_int] * 3 + [C.POINTER(vp)]),
+    "ctc_sdf_fin": (C.c_int, [vp]),
+    "ctc_sdf_read": (C.c_int, [C.c_char_p, ip, vp, vp]),
+    "ctc_sdf_resample": (C.c_int, [C.c_int] * 3 + [vp, vp] + [C.c_int] * 3 + [ip, vp, vp, vp, vp]),
+    "ctc_sdf_texture": (C.c_int, [vp, ip, vp, vp, vp, vp]),
+    "ctc_sdf_eval": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+    "ctc_sdf_label": (C.c_int, [vp, C.c_int, vp, vp, vp]),
+    "ctc_wall_ini": (C.c_int, [vp, C.c_int, vp, ip, C.POINTER(vp)]),
+    "ctc_wall_fin": (C.c_int, [vp]),
+    "ctc_wall_particles": (C.c_int, [vp, ip, vp, vp]),
+    "ctc_wall_set_vel": (C.c_int, [vp, C.POINTER(Wvel)]),
+    "ctc_wall_update_vel": (C.c_int, [vp, C.c_float]),
+    "ctc_wall_force": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, vp, vp]),
+    "ctc_wall_force_seeded": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, C.c_float, vp, vp]),
+    "ctc_wall_bounce": (C.c_int, [vp, C.c_float, C.c_int, vp, vp]),
+    "ctc_wall_repulse": (C.c_int, [vp, C.c_float, C.c_int, vp, vp, vp]),
     "ctc_rbc_force_set_rnd": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_sim_tune": (C.c_int, [vp, C.c_int, ip, vp]),
     "ctc_fsi_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),

@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "dpd.h"
 #include "fsi.h"
+#include "wall.h"
 #include "integrate.h"
 #include "membrane.h"
 #include "api_util.h"
@@ -290,6 +291,11 @@ struct ctc_sim {
     bool noise_on;                         // membrane random force (ctc_sim_set_membrane_noise)
     Kiss noise_host;                       // host mirror of its trunk
     DpdTune tune;                          // launch shapes of the pair kernels (ctc_sim_tune)
+    // walls (optional): the frozen wall of ctc_sim_set_walls on a borrowed field
+    ctc_wall *wall;
+    float wall_lambda;                     // membranes' wall repulsion (0: none)
+    Kiss wall_host;                        // host mirror of the wall ticket's generator
+    long nstep;                            // steps taken (the wall velocity's clock)
     // the step as CUDA graphs (one from each ping-pong buffer) on an own stream
     bool use_graph;
     cudaGraphExec_t gexec[2];
@@ -341,8 +347,8 @@ extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
     CUDA_TRY(cudaMalloc(&s->scratch, clist_scratch_bytes(s->nc, (int)np)));
     clist_carve(&s->w, s->scratch, s->nc, (int)np);
     // + the FSI, contact and membrane-noise trunks
-    CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 30));
-    CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 32));
+    CUDA_TRY(cudaMalloc(&s->trunk_dev, sizeof(unsigned) * 4 * 31));
+    CUDA_TRY(cudaMalloc(&s->seeds_dev, sizeof(float) * 34));
     CUDA_TRY(cudaMalloc(&s->diag_scratch, diag_scratch_bytes()));
     {
         // a boundary particle appears once per fragment holding its cell: room
@@ -382,6 +388,7 @@ extern "C" int ctc_sim_destroy(ctc_sim *s) {
     if (s->ev_out) cudaEventDestroy(s->ev_out);
     for (int b = 0; b < 2; b++) { cudaFree(s->pos[b]); cudaFree(s->vel[b]); }
     cudaFree(s->force); cudaFree(s->counts); cudaFree(s->starts); cudaFree(s->count0); cudaFree(s->fss);
+    if (s->wall) ctc_wall_fin(s->wall);
     cudaFree(s->scratch); cudaFree(s->trunk_dev); cudaFree(s->seeds_dev); cudaFree(s->diag_scratch);
     cudaFree(s->cnt_scratch);
     cudaFree(s->diag_out);
@@ -482,6 +489,29 @@ extern "C" int ctc_sim_set_contact(ctc_sim *s, const ctc_dpdlj_params *p) {
     return sim_cnt_alloc(s);
 }
 
+extern "C" int ctc_sim_set_walls(ctc_sim *s, const ctc_sdf *sdf, const ctc_wvel *v, float lambda, void *stream) {
+    if (!s || (sdf && (!wvel_ok(v) || sdf->L[0] != s->L.x || sdf->L[1] != s->L.y || sdf->L[2] != s->L.z)))
+        return fail(CTC_ERR_ARG, "ctc_sim_set_walls: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    sim_drop_graphs(s);
+    if (s->wall) { ctc_wall_fin(s->wall); s->wall = nullptr; }
+    if (!sdf) return CTC_OK;
+    // freeze the current solvent: wall_gen of src/sim/walls/imp/main.h:9-24
+    std::vector<float> pp(6 * (size_t)std::max(s->cfg.maxp, 1));
+    int n = 0, n_out = 0;
+    int rc = ctc_sim_get_solvent(s, pp.data(), &n, stream);
+    if (rc) return rc;
+    ctc_wall *w = new ctc_wall();
+    rc = wall_build(sdf, n, pp.data(), &n_out, w, st);
+    if (rc) { cudaFree(w->pos); cudaFree(w->starts); delete w; return rc; }
+    w->vel = *v;
+    s->wall = w;
+    s->wall_lambda = lambda;
+    kiss_ini(&s->wall_host, 42, 42, 42, 42);
+    CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 30, s->wall_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
+    return sim_set(s, n_out, pp.data(), true, st);
+}
+
 extern "C" int ctc_sim_set_bending(ctc_sim *s, int mode) {
     if (!s || !s->rbc) return fail(CTC_ERR_ARG, "ctc_sim_set_bending: no membranes");
     sim_drop_graphs(s);
@@ -543,6 +573,8 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
         if (s->noise_on)   // the membrane noise: one key per step
             CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 29, 1, s->seeds_dev + 31, st));
     }
+    if (s->wall)           // the wall ticket: the solvent's call, then the membranes'
+        CUDA_TRY(draw_seq_launch(s->trunk_dev + 4 * 30, nvt > 0 ? 2 : 1, s->seeds_dev + 32, st));
     sim_mark(s, 1, st);
     DpdArgs A;
     dpd_args_common(&A, s->L, &s->cfg.dpd);
@@ -555,16 +587,36 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
     CUDA_TRY(frag_starts_launch(s->L, s->counts, s->fss, s->off, st));
     CUDA_TRY(halo_pack_launch(A, s->off, s->pack, s->pack_off, s->pack_cap, st));
     CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n_host, st));
+    if (nvt > 0) CUDA_TRY(cudaMemsetAsync(s->mforce, 0, sizeof(float4) * (size_t)nvt, st));
     sim_mark(s, 2, st);
     A.which = 1;
     CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st, s->tune));
     sim_mark(s, 3, st);
     CUDA_TRY(halo_packed_launch(A, s->pack, s->pack_off, s->pack_cap, s->cfg.rng, st, 26, s->tune));
     sim_mark(s, 4, st);
+    WvelView wstep;
+    if (s->wall) {
+        // forces_wall: the wall on the solvent, then on the membranes (their
+        // FSI parameters), then the membranes' wall repulsion
+        wstep = wvel_step(s->wall->vel, (float)(s->nstep * (double)s->cfg.dt));
+        s->wall->step = wstep;
+        WallForceArgs W = wall_args(s->wall, &s->cfg.dpd, s->n_host, (const float*)s->pos[dst],
+                                    (const float*)s->vel[dst], 4, (float*)s->force, 4, 0.0f, s->seeds_dev + 32);
+        W.nptr = s->starts + s->nc;
+        CUDA_TRY(wall_force_launch(W, st));
+        if (nvt > 0) {
+            W = wall_args(s->wall, &s->fsi, nvt, (const float*)s->mpos, (const float*)s->mvel, 4, (float*)s->mforce,
+                          4, 0.0f, s->seeds_dev + 33);
+            CUDA_TRY(wall_force_launch(W, st));
+            if (s->wall_lambda != 0.0f)
+                CUDA_TRY(wall_repulse_launch(sdf_view(s->wall->sdf), s->wall_lambda, nvt, (const float*)s->mpos, 4,
+                                             (float*)s->mforce, 4, st));
+        }
+    }
+    sim_mark(s, 5, st);
     const float3 bf = make_float3(s->cfg.bodyf[0], s->cfg.bodyf[1], s->cfg.bodyf[2]);
     if (nvt > 0) {
         // solvent-membrane forces into the vertex forces and, as reactions, the solvent ones
-        CUDA_TRY(cudaMemsetAsync(s->mforce, 0, sizeof(float4) * (size_t)nvt, st));
         DpdPar F;
         F.a = s->fsi.a; F.g = s->fsi.g; F.s = s->fsi.s; F.spow = s->fsi.spow;
         int rc = fsi_forces(s->L, F, nvt, (const float*)s->mpos, (const float*)s->mvel, 4, s->pos[dst], s->vel[dst],
@@ -573,7 +625,7 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
                             Boxes(), s->vperm, s->mnv);
         if (rc) return rc;
     }
-    sim_mark(s, 5, st);
+    sim_mark(s, 6, st);
     if (nvt > 0 && s->cnt_on) {
         // membrane-membrane contact into the vertex forces (the periodic
         // images are FSI's; with stable FSI keys they are listed here)
@@ -584,10 +636,10 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
                             0.0f, 0.0f, s->seeds_dev + 29, s->cw, s->fmask, s->frank, s->fimg_start, st);
         if (rc) return rc;
     }
-    sim_mark(s, 6, st);
+    sim_mark(s, 7, st);
     CUDA_TRY(integrate_launch(s->starts + s->nc, s->n_host, s->pos[dst], s->vel[dst], s->force, s->cfg.dt,
                               s->cfg.mass, bf, st));
-    sim_mark(s, 7, st);
+    sim_mark(s, 8, st);
     if (nvt > 0) {
         // objects_advance: internal forces on top of the FSI ones, then the update
         int rc = membrane_forces(s->rbc, &s->mpar, s->mnc, (const float*)s->mpos, (const float*)s->mvel, 4,
@@ -595,7 +647,14 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
         if (rc) return rc;
         CUDA_TRY(integrate_launch(s->mcount, nvt, s->mpos, s->mvel, s->mforce, s->cfg.dt, s->mmass, bf, st));
     }
-    sim_mark(s, 8, st);
+    if (s->wall) {   // bounce_wall: the solvent, then the membranes' vertices
+        const SdfView S = sdf_view(s->wall->sdf);
+        CUDA_TRY(wall_bounce_launch(S, wstep, s->cfg.dt, s->n_host, (float*)s->pos[dst], (float*)s->vel[dst], 4, st,
+                                    s->starts + s->nc));
+        if (nvt > 0)
+            CUDA_TRY(wall_bounce_launch(S, wstep, s->cfg.dt, nvt, (float*)s->mpos, (float*)s->mvel, 4, st));
+    }
+    sim_mark(s, 9, st);
     return CTC_OK;
 }
 
@@ -613,6 +672,11 @@ static void sim_advance(ctc_sim *s) {
         }
         if (s->noise_on) kiss_get(&s->noise_host);
     }
+    if (s->wall) {
+        kiss_get(&s->wall_host);
+        if (s->mnc * s->mnv > 0) kiss_get(&s->wall_host);
+    }
+    s->nstep++;
     if (s->prof) s->prof_steps++;
     s->cur = 1 - s->cur;
     s->built = true;
@@ -658,7 +722,9 @@ extern "C" int ctc_sim_step(ctc_sim *s, int nsteps, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     int k = 0;
     // the first step after new state, and profiled steps, run directly
-    for (; k < nsteps && (!s->use_graph || s->prof || !s->built); k++) {
+    // (and every step with a time-dependent wall velocity, which a graph would freeze)
+    const bool timed_wall = s->wall && s->wall->vel.type == CTC_WVEL_SHEAR_SIN;
+    for (; k < nsteps && (!s->use_graph || s->prof || !s->built || timed_wall); k++) {
         int rc = sim_step1(s, st);
         if (rc) return rc;
     }

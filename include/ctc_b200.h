@@ -238,6 +238,70 @@ int ctc_io_bop_parts(const char *dump_base, const char *name, int id, long n, co
                      int LX, int LY, int LZ);
 int ctc_io_bop_ints(const char *dump_base, const char *name, int id, long n, const int *ii, int colors);
 
+/* ---- walls: replaces src/wall (sdf, frozen wall particles, wall forces,
+ * bounce-back, repulsion) and src/wall/wvel for one periodic rank ---------- */
+typedef struct ctc_sdf ctc_sdf;
+typedef struct ctc_wall ctc_wall;
+/* sdf_ini + sdf_gen: the field file sdf.dat (a line of three extents, a line
+ * of three grid sizes N, then N0 N1 N2 floats, x fastest) scaled to the box
+ * (LX, LY, LZ) and resampled onto the texture grid of the box plus a 6-cell
+ * margin with the reference's cubic B-spline; the field lives on the device */
+int ctc_sdf_ini(const char *path, int LX, int LY, int LZ, ctc_sdf **s);
+/* the same from a field in memory [host] */
+int ctc_sdf_ini_grid(int NX, int NY, int NZ, const float *ext, const float *D, int LX, int LY, int LZ, ctc_sdf **s);
+int ctc_sdf_fin(ctc_sdf *s);
+/* a field file's grid size N[3], extents ext[3] and, if D != NULL, values */
+int ctc_sdf_read(const char *path, int *N, float *ext, float *D);
+/* host only (no device): the texture grid size T[3] and, if tex != NULL, the
+ * resampled values, the local-to-texture transform (t = s r + o) and the
+ * far threshold, exactly as ctc_sdf_ini_grid builds them */
+int ctc_sdf_resample(int NX, int NY, int NZ, const float *ext, const float *D, int LX, int LY, int LZ, int *T,
+                     float *o, float *s, float *thr, float *tex);
+/* the field's texture grid, transform, threshold and (tex != NULL) values [host] */
+int ctc_sdf_texture(const ctc_sdf *s, int *T, float *o, float *sp, float *thr, float *tex);
+/* sdf_eval at n particles pp [dev, AoS]: out [dev]; labels (wall_label_dev):
+ * 0 bulk (s < 0), 1 wall (0 <= s <= 2), 2 deep (s > 2) */
+int ctc_sdf_eval(const ctc_sdf *s, int n, const float *pp, float *out, void *stream);
+int ctc_sdf_label(const ctc_sdf *s, int n, const float *pp, int *labels, void *stream);
+
+/* wall velocity (wvel_set_cste / _shear / _shear_sin / _hs) */
+#define CTC_WVEL_CSTE 0
+#define CTC_WVEL_SHEAR 1
+#define CTC_WVEL_SHEAR_SIN 2
+#define CTC_WVEL_HS 3
+typedef struct {
+    int type;
+    float u[3];                 /* CSTE: velocity; HS: u[0] = u */
+    float gdot;                 /* SHEAR, SHEAR_SIN: rate (times sin(w t)) */
+    int vdir, gdir, half;       /* velocity and gradient directions, half profile */
+    float w;                    /* SHEAR_SIN: angular frequency */
+    float h;                    /* HS */
+} ctc_wvel;
+
+/* wall_gen_quants + wall_gen_ticket: the n solvent particles pp [host, AoS]
+ * inside the wall freeze (0 <= sdf <= 2; deeper ones are dropped); the bulk
+ * ones stay in pp, in order, n_out of them.  The frozen particles and their
+ * periodic images within the margin form the wall's cell list.  The field s
+ * must outlive the wall.  Wall velocity: constant 0 until ctc_wall_set_vel */
+int ctc_wall_ini(const ctc_sdf *s, int n, float *pp, int *n_out, ctc_wall **w);
+int ctc_wall_fin(ctc_wall *w);
+/* the frozen particles: count n and, if given, positions pos4 (x y z 0,
+ * cell-sorted) and the cell starts (ncells + 1) [host] */
+int ctc_wall_particles(const ctc_wall *w, int *n, float *pos4, int *starts);
+int ctc_wall_set_vel(ctc_wall *w, const ctc_wvel *v);
+/* wall_update_vel: the velocity of the step at time t (SHEAR_SIN) */
+int ctc_wall_update_vel(ctc_wall *w, float t);
+/* wall_force / wall_interact: DPD forces of the wall on n particles pp [dev,
+ * AoS] added to ff [dev, 3 floats each]; the seed is drawn from the wall's
+ * generator rnd_ini(42, 42, 42, 42), one per call, or given */
+int ctc_wall_force(ctc_wall *w, const ctc_dpd_params *p, int n, const float *pp, float *ff, void *stream);
+int ctc_wall_force_seeded(ctc_wall *w, const ctc_dpd_params *p, int n, const float *pp, float seed, float *ff,
+                          void *stream);
+/* sdf_bounce: particles pp [dev, AoS] that ended inside the wall bounce back */
+int ctc_wall_bounce(ctc_wall *w, float dt, int n, float *pp, void *stream);
+/* wall_repulse with the parameter lambda: added to ff [dev, 3 floats each] */
+int ctc_wall_repulse(ctc_wall *w, float lambda, int n, const float *pp, float *ff, void *stream);
+
 /* ---- time update: replaces src/scheme/move/imp.h:5-6, scheme/force ------- */
 /* scheme_move_apply: v += f/m dt; r += v dt on n AoS particles [dev] */
 int ctc_scheme_move_apply(float dt, float mass, int n, const float *ff, float *pp, void *stream);
@@ -298,6 +362,14 @@ int ctc_sim_set_membrane_noise(ctc_sim *s, int enable, unsigned seed);
 /* the membranes' bending in the step (ctc_rbc_force_set_bending's modes:
  * 0 none, 1 kantor, 2 juelicher); set after ctc_sim_set_membranes */
 int ctc_sim_set_bending(ctc_sim *s, int mode);
+/* walls in the step (src/sim/walls, src/sim/imp/{force,update}.h): the
+ * current solvent freezes against the field sdf (borrowed: it must outlive
+ * the walls; same box), the bulk particles stay; from the next step on the
+ * wall forces act on the solvent and, with the FSI parameters, on the
+ * membranes (plus the repulsion lambda if non-zero), and both bounce back
+ * from the walls after the update; v is the wall velocity (its clock starts
+ * at the simulation's first step).  sdf = NULL removes the walls. */
+int ctc_sim_set_walls(ctc_sim *s, const ctc_sdf *sdf, const ctc_wvel *v, float lambda, void *stream);
 /* download the membrane vertices [host, AoS, nc * nv] */
 int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream);
 /* download the cell-sorted solvent [host, AoS, capacity maxp] */
@@ -312,11 +384,11 @@ int ctc_sim_next_seeds(const ctc_sim *s, float *seeds27);
 /* per-phase device timing: when enabled every step records CUDA events on
  * its stream; profile_read returns the summed milliseconds of the
  * CTC_SIM_PHASES phases [0] seeds + wrap + cell lists, [1] fragment starts +
- * force clear, [2] bulk pair forces, [3] halo pair forces, [4] solvent-
- * membrane forces, [5] membrane-membrane contact, [6] solvent update,
- * [7] membrane forces + update, and the number of steps, then restarts the
- * count */
-#define CTC_SIM_PHASES 8
+ * force clear, [2] bulk pair forces, [3] halo pair forces, [4] wall forces,
+ * [5] solvent-membrane forces, [6] membrane-membrane contact, [7] solvent
+ * update, [8] membrane forces + update + wall bounce-back, and the number of
+ * steps, then restarts the count */
+#define CTC_SIM_PHASES 9
 int ctc_sim_profile(ctc_sim *s, int enable);
 int ctc_sim_profile_read(ctc_sim *s, double *ms, int *steps);
 

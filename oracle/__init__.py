@@ -41,6 +41,13 @@ class RbcParams(C.Structure):
                  "totArea", "totVolume")]
 
 
+class Wvel(C.Structure):
+    """The wall velocity of one step: type 0 constant u, 1 shear (gdot, vdir,
+    gdir, half), 2 Hele-Shaw (u[0], h)."""
+    _fields_ = [("type", C.c_int), ("u", C.c_float * 3), ("gdot", C.c_float), ("vdir", C.c_int),
+                ("gdir", C.c_int), ("half", C.c_int), ("h", C.c_float)]
+
+
 def build():
     """Compile the oracle with its Makefile (gcc, OpenMP)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -93,6 +100,15 @@ def lib():
             "orc_read_floats": (C.c_int, [C.c_char_p, f32p, C.c_int]),
             "orc_num_threads": (C.c_int, []),
             "orc_dpd_step": (C.c_int, [C.c_int] * 4 + [f32p, f32p, Dpd, f32p, C.c_float, C.c_void_p, C.c_float]),
+            "orc_sdf_tex_size": (None, [i32p, i32p]),
+            "orc_sdf_resample": (None, [i32p, f32p, f32p, i32p, i32p, f32p, f32p, f32p, f32p]),
+            "orc_sdf_eval": (None, [f32p, i32p, f32p, f32p, C.c_float, C.c_int, f32p, f32p]),
+            "orc_wall_freeze": (C.c_int, [f32p, i32p, f32p, f32p, C.c_float, i32p, C.c_int, f32p, f32p, i32p,
+                                          i32p]),
+            "orc_wall_force": (None, [f32p, i32p, f32p, f32p, C.c_float, i32p, f32p, i32p, C.c_int, Wvel]
+                               + [C.c_float] * 5 + [C.c_int, f32p, f32p]),
+            "orc_wall_bounce": (None, [f32p, i32p, f32p, f32p, C.c_float, Wvel, C.c_float, C.c_int, f32p]),
+            "orc_wall_repulse": (None, [f32p, i32p, f32p, f32p, C.c_float, C.c_float, C.c_int, f32p, f32p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -422,3 +438,66 @@ def rbc_step(L, ps, pv, tri, nv, dpd, fsi, rbcpar, seeds27, fsi_seeds, bodyf, dt
         fv = fv + rbc_forces(tri, nv, pv, rbcpar, mode=0)
     pv = move(pv, fv, dt, mv)
     return ps, pv
+
+
+# ---- walls (src/wall) --------------------------------------------------------
+def sdf_read(path):
+    """The sdf.dat field: (N, ext, D (N2, N1, N0) float32)."""
+    with open(path, "rb") as f:
+        ext = [float(x) for x in f.readline().split()]
+        N = [int(x) for x in f.readline().split()]
+        D = np.frombuffer(f.read(4 * N[0] * N[1] * N[2]), np.float32).reshape(N[2], N[1], N[0])
+    return N, ext, D
+
+
+class Sdf:
+    """The field of one periodic box L on the reference's texture grid
+    (sdf_gen, src/wall/sdf/imp/gen.h) and the wall operations on it."""
+
+    def __init__(self, N, ext, D, L):
+        self.L = np.asarray(L, np.int32)
+        self.T = np.zeros(3, np.int32)
+        lib().orc_sdf_tex_size(self.L, self.T)
+        self.tex = np.zeros(int(np.prod(self.T)), np.float32)
+        self.o, self.s, self.thr = np.zeros(3, np.float32), np.zeros(3, np.float32), np.zeros(1, np.float32)
+        lib().orc_sdf_resample(np.asarray(N, np.int32), np.asarray(ext, np.float32),
+                               np.ascontiguousarray(D, np.float32).reshape(-1), self.L, self.T, self.tex,
+                               self.o, self.s, self.thr)
+
+    def _a(self):
+        return self.tex, self.T, self.o, self.s, float(self.thr[0])
+
+    def eval(self, pp):
+        pp = _pp(pp)
+        out = np.zeros(len(pp), np.float32)
+        lib().orc_sdf_eval(*self._a(), len(pp), pp, out)
+        return out
+
+    def freeze(self, pp):
+        """(bulk particles, wall positions (n, 4) cell-sorted, cell starts)."""
+        pp = _pp(pp).copy()
+        wpos = np.zeros((27 * max(len(pp), 1), 4), np.float32)
+        nc = int(np.prod(self.L + 12))
+        ws = np.zeros(nc + 1, np.int32)
+        nw = np.zeros(1, np.int32)
+        k = lib().orc_wall_freeze(*self._a(), self.L, len(pp), pp, wpos, ws, nw)
+        return pp[:k], wpos[:nw[0]], ws
+
+    def force(self, wpos, wstart, wv, dpd, seed, pp):
+        pp = _pp(pp)
+        ff = np.zeros((len(pp), 3), np.float32)
+        lib().orc_wall_force(*self._a(), self.L, np.ascontiguousarray(wpos, np.float32),
+                             np.ascontiguousarray(wstart, np.int32), len(wpos), wv, *[float(x) for x in dpd],
+                             float(seed), len(pp), pp, ff)
+        return ff
+
+    def bounce(self, wv, dt, pp):
+        pp = _pp(pp).copy()
+        lib().orc_wall_bounce(*self._a(), wv, float(dt), len(pp), pp)
+        return pp
+
+    def repulse(self, lam, pp):
+        pp = _pp(pp)
+        ff = np.zeros((len(pp), 3), np.float32)
+        lib().orc_wall_repulse(*self._a(), float(lam), len(pp), pp, ff)
+        return ff

@@ -140,4 +140,23 @@ void orc_diag(int n, const float *pp, double mass, double out[5]); /* mom xyz, k
 #ifdef __cplusplus
 }
 #endif
+/* ---- walls (ctc_oracle_wall.c; src/wall) ---------------------------------- */
+/* the wall velocity of a step: type 0 constant u, 1 shear (gdot, vdir, gdir,
+ * half), 2 Hele-Shaw (u[0], h) */
+typedef struct { int type; float u[3]; float gdot; int vdir, gdir, half; float h; } orc_wvel;
+void orc_sdf_tex_size(const int L[3], int T[3]);
+void orc_sdf_resample(const int N[3], const float ext[3], const float *D, const int L[3], const int T[3],
+                      float *tex, float o[3], float s[3], float *thr);
+void orc_sdf_eval(const float *tex, const int T[3], const float o[3], const float s[3], float thr, int n,
+                  const float *pp, float *out);
+int  orc_wall_freeze(const float *tex, const int T[3], const float o[3], const float s[3], float thr,
+                     const int L[3], int n, float *pp, float *wpos, int *wstart, int *nw);
+void orc_wall_force(const float *tex, const int T[3], const float o[3], const float s[3], float thr,
+                    const int L[3], const float *wpos, const int *wstart, int nw, orc_wvel wv, float a, float g,
+                    float sg, float spow, float seed, int n, const float *pp, float *ff);
+void orc_wall_bounce(const float *tex, const int T[3], const float o[3], const float s[3], float thr, orc_wvel wv,
+                     float dt, int n, float *pp);
+void orc_wall_repulse(const float *tex, const int T[3], const float o[3], const float s[3], float thr, float lambda,
+                      int n, const float *pp, float *ff);
+
 #endif

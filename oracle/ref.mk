@@ -12,7 +12,7 @@ NVCC    ?= nvcc
 # the reference's own device flags (src/make/main.mk:18-26), for sm_100a
 REF_NVCC := -gencode arch=compute_100a,code=sm_100a -std=c++11 -O3 -g -use_fast_math -restrict -DNDEBUG
 
-all: $(OUT)/gen_random $(OUT)/librefkern.so
+all: $(OUT)/gen_random $(OUT)/librefkern.so $(OUT)/librefsdf.so
 
 # the reference's fixture generator (pre/units/gen_random.cpp, plain C++)
 $(OUT)/gen_random: $(REF)/pre/units/gen_random.cpp $(REF)/pre/units/common/dump.cpp
@@ -21,8 +21,22 @@ $(OUT)/gen_random: $(REF)/pre/units/gen_random.cpp $(REF)/pre/units/common/dump.
 
 # reference device code (src/math/rnd/dev.h, src/pair/dev.h, ...) behind a C
 # shim; oracle/refkern/conf.h stands in for the generated build configuration
-$(OUT)/librefkern.so: oracle/refkern/refkern.cu oracle/refkern/conf.h
+$(OUT)/librefkern.so: oracle/refkern/refkern.cu oracle/refkern/refwall.cu oracle/refkern/conf.h
 	mkdir -p $(OUT)
-	$(NVCC) $(REF_NVCC) -Ioracle/refkern -I$(REF)/src -Xcompiler -fPIC -shared -o $@ oracle/refkern/refkern.cu
+	$(NVCC) $(REF_NVCC) -Ioracle/refkern -Ictc_b200/compat/check -I$(REF)/src -Xcompiler -fPIC -shared -o $@ \
+	    oracle/refkern/refkern.cu \
+	    oracle/refkern/refwall.cu
+
+# the reference's host-side SDF pipeline (field reading, scaling, B-spline
+# resampling, grid transforms) from its sources, with the reference's host
+# flags (src/make/main.mk: -std=c++11 -O3); oracle/refkern/refsdf.cpp holds
+# the one-rank coordinate accessors and stubs for the log and the HDF5 writer;
+# <stdio.h> comes first as the real <mpi.h> brings it
+REF_SDF_SRC := $(REF)/src/utils/error.cpp $(REF)/src/utils/imp.cpp $(REF)/src/utils/os.cpp \
+	$(REF)/src/math/tform/imp.cpp $(REF)/src/wall/sdf/field/imp.cpp $(REF)/src/wall/sdf/tform/imp.cpp
+$(OUT)/librefsdf.so: oracle/refkern/refsdf.cpp oracle/refkern/conf.h $(REF_SDF_SRC)
+	mkdir -p $(OUT)
+	$(CXX) -std=c++11 -O3 -fPIC -shared -include stdio.h -Ioracle/refkern -Ictc_b200/compat/check -I$(REF)/src \
+	    -I/usr/local/cuda/include -o $@ oracle/refkern/refsdf.cpp $(REF_SDF_SRC)
 
 .PHONY: all

@@ -143,3 +143,69 @@ def juelicher(tri, nv, pp, ff):
     lib_.refkern_juelicher.argtypes = [C.c_int] * 4 + [vp, vp, vp, vp]
     torch.cuda.synchronize()
     assert lib_.refkern_juelicher(int(pp.shape[0]) // nv, nv, len(t4), len(d4), _p(pp), _p(t4), _p(d4), _p(ff)) == 0
+
+
+# ---- walls (oracle/refkern/refwall.cu) -------------------------------------
+class RefWvel(C.Structure):
+    _fields_ = [("type", C.c_int), ("u", C.c_float * 3), ("gdot", C.c_float), ("vdir", C.c_int),
+                ("gdir", C.c_int), ("half", C.c_int), ("h", C.c_float)]
+
+
+def _wsig(L):
+    vp = C.c_void_p
+    L.refwall_sdf.restype = vp
+    L.refwall_sdf.argtypes = [C.c_int] * 3 + [vp, vp, vp, C.c_float]
+    L.refwall_sdf_fin.argtypes = [vp]
+    L.refwall_eval.argtypes = [vp, C.c_int, vp, vp]
+    L.refwall_label.argtypes = [vp, C.c_int, vp, vp]
+    L.refwall_force.argtypes = [vp] + [C.c_int] * 3 + [vp, vp, C.c_int, C.c_int, RefWvel] + [C.c_float] * 5 + \
+        [C.c_int, vp, vp]
+    L.refwall_bounce.argtypes = [vp] + [C.c_int] * 3 + [RefWvel, C.c_float, C.c_int, vp]
+    L.refwall_repulse.argtypes = [vp, C.c_float, C.c_int, vp, vp]
+
+
+class RefSdf:
+    """The reference's field on a 3D texture: tex (T2, T1, T0) float32 [host]."""
+
+    def __init__(self, tex, o, s, thr):
+        import numpy as np
+        self.lib = lib()
+        _wsig(self.lib)
+        tex = np.ascontiguousarray(tex, np.float32)
+        o, s = np.ascontiguousarray(o, np.float32), np.ascontiguousarray(s, np.float32)
+        T2, T1, T0 = tex.shape
+        self.h = self.lib.refwall_sdf(T0, T1, T2, tex.ctypes.data_as(C.c_void_p), o.ctypes.data_as(C.c_void_p),
+                                      s.ctypes.data_as(C.c_void_p), float(thr))
+        assert self.h
+
+    def close(self):
+        if self.h:
+            self.lib.refwall_sdf_fin(self.h)
+            self.h = None
+
+    def eval(self, pp, out):
+        import torch
+        torch.cuda.synchronize()
+        assert self.lib.refwall_eval(self.h, int(pp.shape[0]), _p(pp), _p(out)) == 0
+
+    def label(self, pp, out):
+        import torch
+        torch.cuda.synchronize()
+        assert self.lib.refwall_label(self.h, int(pp.shape[0]), _p(pp), _p(out)) == 0
+
+    def force(self, L, wpos, wstart, wv, dpd, seed, pp, ff):
+        import torch
+        torch.cuda.synchronize()
+        assert self.lib.refwall_force(self.h, *L, _p(wpos), _p(wstart), int(wpos.shape[0]), int(wstart.shape[0]) - 1,
+                                      wv, *[float(x) for x in dpd], float(seed), int(pp.shape[0]), _p(pp),
+                                      _p(ff)) == 0
+
+    def bounce(self, L, wv, dt, pp):
+        import torch
+        torch.cuda.synchronize()
+        assert self.lib.refwall_bounce(self.h, *L, wv, float(dt), int(pp.shape[0]), _p(pp)) == 0
+
+    def repulse(self, lam, pp, ff):
+        import torch
+        torch.cuda.synchronize()
+        assert self.lib.refwall_repulse(self.h, float(lam), int(pp.shape[0]), _p(pp), _p(ff)) == 0
