@@ -52,6 +52,10 @@ CONFIGS = {
     # next to C3: the same system with Juelicher bending (src/rbc/force/bending/juelicher)
     "c3j": dict(L=(64, 64, 64), bodyf=(0.0, 0.0, 0.0), steps=100, rbc=200, bending="juelicher",
                 name="C3 with Juelicher bending (kb=1, H0=-1/2) 64x64x64 rho=10 + 200 cells x 642 vertices"),
+    # next to C2: plane Poiseuille flow between walls (src/wall; the field of
+    # the reference's wall tests, data/sdf/wall1, committed as a test fixture)
+    "c2w": dict(L=(64, 64, 64), bodyf=(0.0333333, 0.0, 0.0), steps=100, walls="wall.dat",
+                name="walls: DPD 64x64x64 rho=10 between the plates of the wall1 field, body force 0.0333 x"),
     "c4": dict(adjoint=True, L=(32, 32, 32), rbc=20, K=20, kck=5, bodyf=(0.0, 0.0, 0.0),
                name="C4 adjoint 32x32x32 rho=10 (327,680 solvent) + 20 RBC, loss = mean vertex x-velocity "
                     "after 20 steps, checkpoints every 5"),
@@ -287,6 +291,12 @@ def run_ours(args, cfg, world, rank, local):
             sim.set_contact(ctc.DpdLjParams(a, g, ctc.dpd_sigma(systems.KBT, g, systems.DT), spow, ljs, lje))
         if cfg.get("bending"):
             sim.set_bending(cfg["bending"])
+    if cfg.get("walls"):
+        # the solvent inside the plates freezes into the wall; the rest flows
+        sdf = ctc.Sdf(L, path=os.path.join(ROOT, "tests", "golden", "sdf", cfg["walls"]))
+        sim.set_walls(sdf, ctc.wvel("cste"))
+        pp = sim.get_solvent()
+        n = len(pp)
     # launch shapes tuned on the first step's state; the step replayed as CUDA
     # graphs (captured during the warm-up)
     sim.step(1)
@@ -352,7 +362,9 @@ def run_ours(args, cfg, world, rank, local):
     # seeds, 6 cell-list kernels, fragment starts, 2 halo packing kernels, bulk, halo, update; with
     # membranes also cell wrap, FSI seeds, 4 image-list kernels, FSI, area/volume, membrane forces,
     # vertex update; contact adds its seeds, 6 vertex cell-list kernels and the pair kernel
-    launches = 13 + (10 if nvt else 0) + (8 if cfg.get("contact") else 0) + (3 if cfg.get("bending") == "juelicher" else 0)
+    # juelicher bending 3 kernels; walls their seed, the wall forces and bounce-back
+    launches = 13 + (10 if nvt else 0) + (8 if cfg.get("contact") else 0) + \
+        (3 if cfg.get("bending") == "juelicher" else 0) + (3 if cfg.get("walls") else 0)
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
