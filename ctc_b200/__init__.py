@@ -395,6 +395,18 @@ class Wall:
     def set_vel(self, v):
         check(lib().ctc_wall_set_vel(self.h, C.byref(v)))
 
+    def strt_dump_templ(self, base):
+        """wall_strt_dump_templ: base/wall.pp/templ."""
+        check(lib().ctc_wall_strt_dump_templ(self.h, str(base).encode()))
+
+    @classmethod
+    def strt(cls, sdf, base):
+        """A wall from the restart template base/wall.pp/templ."""
+        w = cls.__new__(cls)
+        w.sdf, w.h, w.bulk = sdf, C.c_void_p(), None
+        check(lib().ctc_wall_strt_ini(sdf.h, str(base).encode(), C.byref(w.h)))
+        return w
+
     def update_vel(self, t):
         check(lib().ctc_wall_update_vel(self.h, float(t)))
 
@@ -523,6 +535,16 @@ class Sim:
         v = v if v is not None else wvel("cste")
         check(lib().ctc_sim_set_walls(self.h, sdf.h, C.byref(v), float(lam), _stream(stream)))
         self._sdf = sdf                  # the field outlives the walls
+
+    def set_walls_strt(self, sdf, base, v=None, lam=0.0):
+        """Walls from the restart template base/wall.pp/templ (the solvent as it is)."""
+        v = v if v is not None else wvel("cste")
+        check(lib().ctc_sim_set_walls_strt(self.h, sdf.h, str(base).encode(), C.byref(v), float(lam)))
+        self._sdf = sdf
+
+    def wall_strt_dump_templ(self, base):
+        """The walls' restart template base/wall.pp/templ."""
+        check(lib().ctc_sim_wall_strt_dump_templ(self.h, str(base).encode()))
 
     def set_bending(self, mode="kantor"):
         """The membranes' bending in the step: "kantor", "juelicher" or "none"

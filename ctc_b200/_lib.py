@@ -96,6 +96,10 @@ SIGNATURES = {
     "ctc_sim_set_membrane_noise": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_sim_set_bending": (C.c_int, [vp, C.c_int]),
     "ctc_sim_set_walls": (C.c_int, [vp, vp, C.POINTER(Wvel), C.c_float, vp]),
+    "ctc_sim_set_walls_strt": (C.c_int, [vp, vp, C.c_char_p, C.POINTER(Wvel), C.c_float]),
+    "ctc_sim_wall_strt_dump_templ": (C.c_int, [vp, C.c_char_p]),
+    "ctc_wall_strt_dump_templ": (C.c_int, [vp, C.c_char_p]),
+    "ctc_wall_strt_ini": (C.c_int, [vp, C.c_char_p, C.POINTER(vp)]),
     "ctc_bop_write": (C.c_int, [C.c_char_p, C.c_long, C.c_int, C.c_char_p, vp]),
     "ctc_bop_read": (C.c_int, [C.c_char_p, C.c_long, C.POINTER(C.c_long), ip, ip, vp]),
     "ctc_restart_write_pp": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, vp]),

@@ -512,6 +512,28 @@ extern "C" int ctc_sim_set_walls(ctc_sim *s, const ctc_sdf *sdf, const ctc_wvel 
     return sim_set(s, n_out, pp.data(), true, st);
 }
 
+extern "C" int ctc_sim_set_walls_strt(ctc_sim *s, const ctc_sdf *sdf, const char *base, const ctc_wvel *v,
+                                      float lambda) {
+    if (!s || !sdf || !base || !wvel_ok(v) || sdf->L[0] != s->L.x || sdf->L[1] != s->L.y || sdf->L[2] != s->L.z)
+        return fail(CTC_ERR_ARG, "ctc_sim_set_walls_strt: bad arguments");
+    sim_drop_graphs(s);
+    if (s->wall) { ctc_wall_fin(s->wall); s->wall = nullptr; }
+    ctc_wall *w = new ctc_wall();
+    int rc = wall_from_templ(sdf, base, w);
+    if (rc) { cudaFree(w->pos); cudaFree(w->starts); delete w; return rc; }
+    w->vel = *v;
+    s->wall = w;
+    s->wall_lambda = lambda;
+    kiss_ini(&s->wall_host, 42, 42, 42, 42);
+    CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 30, s->wall_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_wall_strt_dump_templ(ctc_sim *s, const char *base) {
+    if (!s || !s->wall) return fail(CTC_ERR_ARG, "ctc_sim_wall_strt_dump_templ: no walls");
+    return ctc_wall_strt_dump_templ(s->wall, base);
+}
+
 extern "C" int ctc_sim_set_bending(ctc_sim *s, int mode) {
     if (!s || !s->rbc) return fail(CTC_ERR_ARG, "ctc_sim_set_bending: no membranes");
     sim_drop_graphs(s);

@@ -202,6 +202,14 @@ int wall_build(const ctc_sdf *sdf, int n, float *pp, int *n_out, ctc_wall *w, cu
             if (in) wall.insert(wall.end(), r, r + 3);
         }
     }
+    return wall_cells(sdf, wall, w);
+}
+
+// wall_gen_ticket: the wall particles wall (x y z) binned into the cell list
+// of the extended box, by cell then in their order
+int wall_cells(const ctc_sdf *sdf, const std::vector<float> &wall, ctc_wall *w) {
+    const int L[3] = {sdf->L[0], sdf->L[1], sdf->L[2]};
+    const int LW[3] = {L[0] + 2 * WALL_M, L[1] + 2 * WALL_M, L[2] + 2 * WALL_M};
     const int nw = (int)(wall.size() / 3), nc = LW[0] * LW[1] * LW[2];
     // cell of the reference's cell list (src/clist/dev/main.h:21-24) on the extended box
     std::vector<int> cid(nw), cnt(nc + 1, 0);
@@ -316,5 +324,45 @@ extern "C" int ctc_wall_bounce(ctc_wall *w, float dt, int n, float *pp, void *st
 extern "C" int ctc_wall_repulse(ctc_wall *w, float lambda, int n, const float *pp, float *ff, void *stream) {
     if (!w || n < 0 || (n > 0 && (!pp || !ff))) return fail(CTC_ERR_ARG, "ctc_wall_repulse: bad arguments");
     CUDA_TRY(wall_repulse_launch(sdf_view(w->sdf), lambda, n, pp, 6, ff, 3, (cudaStream_t)stream));
+    return CTC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the wall template of the restart files (src/wall/imp/strt.h): base/wall.pp/templ
+// ---------------------------------------------------------------------------
+extern "C" int ctc_wall_strt_dump_templ(const ctc_wall *w, const char *base) {
+    if (!w || !base) return fail(CTC_ERR_ARG, "ctc_wall_strt_dump_templ: bad arguments");
+    std::vector<float4> p4(w->n > 0 ? w->n : 1);
+    if (w->n > 0) CUDA_TRY(cudaMemcpy(p4.data(), w->pos, sizeof(float4) * w->n, cudaMemcpyDeviceToHost));
+    std::vector<float> pp(6 * (size_t)w->n, 0.0f);            // float42particle: zero velocities
+    for (int i = 0; i < w->n; i++) { pp[6 * i] = p4[i].x; pp[6 * i + 1] = p4[i].y; pp[6 * i + 2] = p4[i].z; }
+    return ctc_restart_write_pp(base, "wall.pp", CTC_RESTART_TEMPL, w->n, pp.data());
+}
+
+namespace ctc {
+int wall_from_templ(const ctc_sdf *sdf, const char *base, ctc_wall *w) {
+    long n = 0;
+    int rc = ctc_restart_read_pp(base, "wall.pp", CTC_RESTART_TEMPL, 0, &n, nullptr);
+    if (rc) return rc;
+    std::vector<float> pp(6 * (size_t)(n > 0 ? n : 1));
+    rc = ctc_restart_read_pp(base, "wall.pp", CTC_RESTART_TEMPL, n, &n, pp.data());
+    if (rc) return rc;
+    std::vector<float> wall(3 * (size_t)n);
+    for (long i = 0; i < n; i++)
+        for (int c = 0; c < 3; c++) wall[3 * i + c] = pp[6 * i + c];
+    return wall_cells(sdf, wall, w);
+}
+}  // namespace ctc
+
+extern "C" int ctc_wall_strt_ini(const ctc_sdf *sdf, const char *base, ctc_wall **pw) {
+    if (!sdf || !base || !pw) return fail(CTC_ERR_ARG, "ctc_wall_strt_ini: bad arguments");
+    ctc_wall *w = new ctc_wall();
+    int rc = wall_from_templ(sdf, base, w);
+    if (rc) {
+        cudaFree(w->pos); cudaFree(w->starts);
+        delete w;
+        return rc;
+    }
+    *pw = w;
     return CTC_OK;
 }

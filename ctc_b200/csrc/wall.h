@@ -103,6 +103,9 @@ WvelView wvel_step(const ctc_wvel &p, float t);
 bool wvel_ok(const ctc_wvel *p);
 // freezes the n host particles pp (AoS) inside the wall into w; the bulk ones stay in pp (n_out)
 int wall_build(const ctc_sdf *sdf, int n, float *pp, int *n_out, ctc_wall *w, cudaStream_t st);
+// the cell list of the wall particles wall (x y z), and the wall of a restart template base/wall.pp/templ
+int wall_cells(const ctc_sdf *sdf, const std::vector<float> &wall, ctc_wall *w);
+int wall_from_templ(const ctc_sdf *sdf, const char *base, ctc_wall *w);
 WallForceArgs wall_args(const ctc_wall *w, const ctc_dpd_params *p, int n, const float *pos, const float *vel,
                         int stride, float *force, int fstride, float seed, const float *seed_dev);
 }  // namespace ctc

@@ -301,6 +301,11 @@ int ctc_wall_force_seeded(ctc_wall *w, const ctc_dpd_params *p, int n, const flo
 int ctc_wall_bounce(ctc_wall *w, float dt, int n, float *pp, void *stream);
 /* wall_repulse with the parameter lambda: added to ff [dev, 3 floats each] */
 int ctc_wall_repulse(ctc_wall *w, float lambda, int n, const float *pp, float *ff, void *stream);
+/* wall_strt_dump_templ / wall_strt_quants + wall_gen_ticket: the frozen
+ * particles as the restart template base/wall.pp/templ (positions, zero
+ * velocities), and a wall built from such a template */
+int ctc_wall_strt_dump_templ(const ctc_wall *w, const char *base);
+int ctc_wall_strt_ini(const ctc_sdf *s, const char *base, ctc_wall **w);
 
 /* ---- time update: replaces src/scheme/move/imp.h:5-6, scheme/force ------- */
 /* scheme_move_apply: v += f/m dt; r += v dt on n AoS particles [dev] */
@@ -370,6 +375,11 @@ int ctc_sim_set_bending(ctc_sim *s, int mode);
  * from the walls after the update; v is the wall velocity (its clock starts
  * at the simulation's first step).  sdf = NULL removes the walls. */
 int ctc_sim_set_walls(ctc_sim *s, const ctc_sdf *sdf, const ctc_wvel *v, float lambda, void *stream);
+/* walls from the restart template base/wall.pp/templ (wall_restart, src/sim/
+ * walls/imp/main.h:26-36): the solvent is left as it is; and the template of
+ * the walls in the step */
+int ctc_sim_set_walls_strt(ctc_sim *s, const ctc_sdf *sdf, const char *base, const ctc_wvel *v, float lambda);
+int ctc_sim_wall_strt_dump_templ(ctc_sim *s, const char *base);
 /* download the membrane vertices [host, AoS, nc * nv] */
 int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream);
 /* download the cell-sorted solvent [host, AoS, capacity maxp] */

@@ -272,3 +272,36 @@ def test_sim_walls_channel_flow_and_graph_replay():
         sim.close()
     assert np.abs(out[0] - out[1]).max() < 1e-3
     assert C.device_error() == 0
+
+
+def test_wall_restart_template(tmp_path):
+    """wall_strt_dump_templ then a wall from the template: the same wall, and
+    a system restarted with it steps as the original."""
+    import ctc_b200 as C
+    L = (16, 16, 16)
+    path = os.path.join(SDF, "wall.dat")
+    q = oracle.Sdf(*oracle.sdf_read(path), L)
+    sdf = C.Sdf(L, path=path)
+    pp = _solvent(L, 19, q=q)
+    w = C.Wall(sdf, pp)
+    w.strt_dump_templ(tmp_path)
+    t = C.restart_read_pp(tmp_path, "wall.pp", "templ")
+    pos, st = w.particles()
+    assert np.array_equal(t[:, :3], pos[:, :3]) and (t[:, 3:] == 0).all()
+    w2 = C.Wall.strt(sdf, tmp_path)
+    pos2, st2 = w2.particles()
+    assert np.array_equal(pos, pos2) and np.array_equal(st, st2)
+    dpd = systems.dpd_params()
+    a = C.Sim(L, len(pp), C.DpdParams(*dpd), mass=1.0, dt=systems.DT, bodyf=(0.1, 0.0, 0.0))
+    a.set_solvent(pp)
+    a.set_walls(sdf, C.wvel("cste"))
+    a.wall_strt_dump_templ(tmp_path / "sim")
+    b = C.Sim(L, len(pp), C.DpdParams(*dpd), mass=1.0, dt=systems.DT, bodyf=(0.1, 0.0, 0.0))
+    b.set_solvent(a.get_solvent())
+    b.set_walls_strt(sdf, tmp_path / "sim", C.wvel("cste"))
+    a.step(2)
+    b.step(2)
+    assert np.abs(a.get_solvent() - b.get_solvent()).max() < 1e-5
+    a.close()
+    b.close()
+    assert C.device_error() == 0
