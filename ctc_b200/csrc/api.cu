@@ -475,6 +475,10 @@ extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const i
     s->mnc = nc; s->mnv = nv;
     int rcc = sim_cnt_alloc(s);
     if (rcc) return rcc;
+    if (s->wall) {   // the wall forces' scratch covers the vertices too
+        rcc = wall_scratch(s->wall, std::max(s->cfg.maxp, nc * nv));
+        if (rcc) return rcc;
+    }
     s->mpar = *p;
     s->fsi = *fsi;
     s->mmass = mass;
@@ -507,6 +511,8 @@ extern "C" int ctc_sim_set_walls(ctc_sim *s, const ctc_sdf *sdf, const ctc_wvel 
     w->vel = *v;
     s->wall = w;
     s->wall_lambda = lambda;
+    rc = wall_scratch(w, std::max(s->cfg.maxp, s->mnc * s->mnv));
+    if (rc) return rc;
     kiss_ini(&s->wall_host, 42, 42, 42, 42);
     CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 30, s->wall_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
     return sim_set(s, n_out, pp.data(), true, st);
@@ -524,6 +530,8 @@ extern "C" int ctc_sim_set_walls_strt(ctc_sim *s, const ctc_sdf *sdf, const char
     w->vel = *v;
     s->wall = w;
     s->wall_lambda = lambda;
+    rc = wall_scratch(w, std::max(s->cfg.maxp, s->mnc * s->mnv));
+    if (rc) return rc;
     kiss_ini(&s->wall_host, 42, 42, 42, 42);
     CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 30, s->wall_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
     return CTC_OK;

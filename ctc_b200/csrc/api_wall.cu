@@ -241,6 +241,18 @@ int wall_cells(const ctc_sdf *sdf, const std::vector<float> &wall, ctc_wall *w) 
     return CTC_OK;
 }
 
+int wall_scratch(ctc_wall *w, int n) {
+    if (!w->count) CUDA_TRY(cudaMalloc(&w->count, sizeof(int)));
+    if (n > w->list_cap) {
+        cudaFree(w->list);
+        w->list = nullptr;
+        w->list_cap = 0;
+        CUDA_TRY(cudaMalloc(&w->list, sizeof(int) * (size_t)n));
+        w->list_cap = n;
+    }
+    return CTC_OK;
+}
+
 WallForceArgs wall_args(const ctc_wall *w, const ctc_dpd_params *p, int n, const float *pos, const float *vel,
                         int stride, float *force, int fstride, float seed, const float *seed_dev) {
     WallForceArgs A;
@@ -256,6 +268,7 @@ WallForceArgs wall_args(const ctc_wall *w, const ctc_dpd_params *p, int n, const
     A.pos = pos; A.vel = vel; A.stride = stride;
     A.force = force; A.fstride = fstride;
     A.seed = seed; A.seed_dev = seed_dev;
+    A.list = w->list; A.count = w->count;
     return A;
 }
 }  // namespace ctc
@@ -277,6 +290,8 @@ extern "C" int ctc_wall_fin(ctc_wall *w) {
     if (!w) return CTC_OK;
     cudaFree(w->pos);
     cudaFree(w->starts);
+    cudaFree(w->list);
+    cudaFree(w->count);
     delete w;
     return CTC_OK;
 }
@@ -305,6 +320,8 @@ extern "C" int ctc_wall_update_vel(ctc_wall *w, float t) {
 extern "C" int ctc_wall_force_seeded(ctc_wall *w, const ctc_dpd_params *p, int n, const float *pp, float seed,
                                      float *ff, void *stream) {
     if (!w || !p || n < 0 || (n > 0 && (!pp || !ff))) return fail(CTC_ERR_ARG, "ctc_wall_force: bad arguments");
+    int rc = wall_scratch(w, n);
+    if (rc) return rc;
     WallForceArgs A = wall_args(w, p, n, pp, pp + 3, 6, ff, 3, seed, nullptr);
     CUDA_TRY(wall_force_launch(A, (cudaStream_t)stream));
     return CTC_OK;

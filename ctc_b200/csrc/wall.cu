@@ -287,45 +287,100 @@ cudaError_t sdf_eval_launch(const SdfView &S, int n, const float *pp, int stride
 // that is not far from the wall walks, in each of its three z-planes, three
 // rows of three cells of the wall cell list around its (clamped) cell; the
 // pair key is mean0var1ii(seed, aid, bid), the wall particle moving with the
-// wall velocity.  One thread per particle; each plane's sum is added to the
-// force in plane order (the reference's three threads add theirs atomically).
+// wall velocity.
+//
+// Two kernels.  k_wall_near lists the particles that are not far from the
+// wall (a few per cent in a channel: one field load each for the rest);
+// k_wall_pairs gives each listed particle four lanes of a warp, lanes 0-2 one
+// z-plane each as the reference's three threads do, and the group's first
+// lane adds the three plane sums to the force in plane order (the reference
+// adds them atomically, in an unspecified order).  The list's order does not
+// matter: every particle's force is its own.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_wall_force(WallForceArgs A) {
+__global__ void __launch_bounds__(256) k_wall_near(WallForceArgs A) {
     const int aid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (aid >= A.n || (A.nptr && aid >= __ldg(A.nptr))) return;
-    const float *p = A.pos + (size_t)A.stride * aid, *v = A.vel + (size_t)A.stride * aid;
-    const float4 pa = make_float4(p[0], p[1], p[2], 0), va = make_float4(v[0], v[1], v[2], 0);
-    if (sdf_far(A.sdf, pa.x, pa.y, pa.z)) return;
+    bool near = false;
+    if (aid < A.n && !(A.nptr && aid >= __ldg(A.nptr))) {
+        const float *p = A.pos + (size_t)A.stride * aid;
+        near = !sdf_far(A.sdf, p[0], p[1], p[2]);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, near);
+    if (!m) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(A.count, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (near) A.list[base + __popc(m & ((1u << lane) - 1))] = aid;
+}
+
+__global__ void __launch_bounds__(128) k_wall_pairs(WallForceArgs A) {
+    const int q = threadIdx.x & 3;                      // z-plane of this lane (3: none)
+    const int cnt = __ldg(A.count);
     const float seed = A.seed_dev ? __ldg(A.seed_dev) : A.seed;
     const int xc = A.L.x + 2 * WALL_M, yc = A.L.y + 2 * WALL_M, zc = A.L.z + 2 * WALL_M;
-    int xb = (int)(pa.x + xc / 2), yb = (int)(pa.y + yc / 2), zb = (int)(pa.z + zc / 2);
-    xb = min(xc - 2, max(1, xb));
-    yb = min(yc - 2, max(1, yb));
-    zb = min(zc - 2, max(1, zb));
-    float *o = A.force + (size_t)A.fstride * aid;
-    float f0 = o[0], f1 = o[1], f2 = o[2];
-    for (int zp = 0; zp < 3; zp++) {
+    const int groups = gridDim.x * (blockDim.x >> 2);
+    // uniform trip count over the warp: the shuffles below take all lanes
+    const int first = blockIdx.x * (blockDim.x >> 2) + (threadIdx.x >> 2);
+    const int ntrip = (cnt + groups - 1) / groups;
+    for (int t = 0; t < ntrip; t++) {
+        const int k = first + t * groups;
+        const bool live = k < cnt;
         float3 acc = make_float3(0, 0, 0);
-        const int cid0 = xb - 1 + xc * (yb - 1 + yc * (zb - 1 + zp));
-        for (int row = 0; row < 3; row++) {
-            const int cid = cid0 + row * xc;
-            const int b0 = __ldg(A.wstart + cid), b1 = __ldg(A.wstart + cid + 3);
-            for (int bid = b0; bid < b1; bid++) {
-                const float4 pb = __ldg(A.wpos + bid);
-                const float3 wv = wvel_at(A.wv, make_float3(pb.x, pb.y, pb.z));
-                const float rnd = mean0var1ii(seed, aid, bid);
-                float3 f;
-                if (dpd_force(A.par, pa, va, pb, make_float4(wv.x, wv.y, wv.z, 0), rnd, f)) {
-                    acc.x += f.x; acc.y += f.y; acc.z += f.z;
+        int aid = 0;
+        if (live) {
+            aid = __ldg(A.list + k);
+            const float *p = A.pos + (size_t)A.stride * aid, *v = A.vel + (size_t)A.stride * aid;
+            const float4 pa = make_float4(p[0], p[1], p[2], 0), va = make_float4(v[0], v[1], v[2], 0);
+            if (q < 3) {
+                int xb = (int)(pa.x + xc / 2), yb = (int)(pa.y + yc / 2), zb = (int)(pa.z + zc / 2);
+                xb = min(xc - 2, max(1, xb));
+                yb = min(yc - 2, max(1, yb));
+                zb = min(zc - 2, max(1, zb));
+                const int cid0 = xb - 1 + xc * (yb - 1 + yc * (zb - 1 + q));
+                for (int row = 0; row < 3; row++) {
+                    const int cid = cid0 + row * xc;
+                    const int b0 = __ldg(A.wstart + cid), b1 = __ldg(A.wstart + cid + 3);
+                    for (int bid = b0; bid < b1; bid++) {
+                        const float4 pb = __ldg(A.wpos + bid);
+                        // the cutoff first (the pair force's own r^2): key and
+                        // wall velocity only for the pairs that interact
+                        if (dist2(pa.x - pb.x, pa.y - pb.y, pa.z - pb.z) >= 1) continue;
+                        const float3 wv = wvel_at(A.wv, make_float3(pb.x, pb.y, pb.z));
+                        const float rnd = mean0var1ii(seed, aid, bid);
+                        float3 f;
+                        if (dpd_force(A.par, pa, va, pb, make_float4(wv.x, wv.y, wv.z, 0), rnd, f)) {
+                            acc.x += f.x; acc.y += f.y; acc.z += f.z;
+                        }
+                    }
                 }
             }
         }
-        f0 += acc.x; f1 += acc.y; f2 += acc.z;
+        // the group's lane 0 takes the plane sums of lanes 1 and 2
+        const float p1x = __shfl_down_sync(0xffffffffu, acc.x, 1), p1y = __shfl_down_sync(0xffffffffu, acc.y, 1);
+        const float p1z = __shfl_down_sync(0xffffffffu, acc.z, 1);
+        const float p2x = __shfl_down_sync(0xffffffffu, acc.x, 2), p2y = __shfl_down_sync(0xffffffffu, acc.y, 2);
+        const float p2z = __shfl_down_sync(0xffffffffu, acc.z, 2);
+        if (live && q == 0) {
+            float *o = A.force + (size_t)A.fstride * aid;
+            float f0 = o[0], f1 = o[1], f2 = o[2];
+            f0 += acc.x; f1 += acc.y; f2 += acc.z;
+            f0 += p1x; f1 += p1y; f2 += p1z;
+            f0 += p2x; f1 += p2y; f2 += p2z;
+            o[0] = f0; o[1] = f1; o[2] = f2;
+        }
     }
-    o[0] = f0; o[1] = f1; o[2] = f2;
 }
+
 cudaError_t wall_force_launch(const WallForceArgs &A, cudaStream_t st) {
-    if (A.n > 0 && A.wn > 0) k_wall_force<<<ceil_div(A.n, 128), 128, 0, st>>>(A);
+    if (A.n <= 0 || A.wn <= 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(A.count, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    k_wall_near<<<ceil_div(A.n, 256), 256, 0, st>>>(A);
+    // one group of four lanes per eighth of the particles: one pass when at
+    // most one in eight is near the wall (a channel: a few per cent), a loop
+    // otherwise
+    const int blocks = ceil_div(A.n, 256);
+    k_wall_pairs<<<blocks, 128, 0, st>>>(A);
     return cudaGetLastError();
 }
 

@@ -66,6 +66,7 @@ struct WallForceArgs {
     int fstride;
     float seed;
     const float *seed_dev;   // when set, the seed is read here
+    int *list, *count;       // scratch: n ints and a counter (the particles near the wall)
 };
 cudaError_t wall_force_launch(const WallForceArgs &A, cudaStream_t st);
 
@@ -95,6 +96,7 @@ struct ctc_wall {
     ctc::Kiss rnd;              // the ticket's generator, rnd_ini(42, 42, 42, 42)
     ctc_wvel vel;
     ctc::WvelView step;
+    int *list, *count, list_cap;   // scratch of the wall forces: particles near the wall
 };
 
 namespace ctc {
@@ -105,6 +107,8 @@ bool wvel_ok(const ctc_wvel *p);
 int wall_build(const ctc_sdf *sdf, int n, float *pp, int *n_out, ctc_wall *w, cudaStream_t st);
 // the cell list of the wall particles wall (x y z), and the wall of a restart template base/wall.pp/templ
 int wall_cells(const ctc_sdf *sdf, const std::vector<float> &wall, ctc_wall *w);
+// the wall forces' scratch for n particles (allocates; outside graph capture)
+int wall_scratch(ctc_wall *w, int n);
 int wall_from_templ(const ctc_sdf *sdf, const char *base, ctc_wall *w);
 WallForceArgs wall_args(const ctc_wall *w, const ctc_dpd_params *p, int n, const float *pos, const float *vel,
                         int stride, float *force, int fstride, float seed, const float *seed_dev);

@@ -305,3 +305,41 @@ def test_wall_restart_template(tmp_path):
     a.close()
     b.close()
     assert C.device_error() == 0
+
+
+def test_sim_walls_with_membranes():
+    """A cell in the channel between the plates: the wall forces (FSI
+    parameters) and the repulsion act on its vertices (the module's forces
+    on the same state), the membranes set after the walls are covered, and
+    after some steps no vertex is inside the wall."""
+    import ctc_b200 as C
+    from ctc_b200 import mesh
+    L = (16, 16, 16)
+    path = os.path.join(SDF, "wall.dat")
+    q = oracle.Sdf(*oracle.sdf_read(path), L)
+    sdf = C.Sdf(L, path=path)
+    X, F = mesh.rbc_template()
+    pv = np.zeros((len(X), 6), np.float32)
+    pv[:, :3] = X
+    pv[:, 2] += 4.2                        # its top within the plate's reach
+    s = q.eval(pv)
+    assert (s < -0.5).all() and (s > -1.4).sum() > 10
+    A, V = mesh.area_volume(X, F)
+    par = systems.rbc_params(A, V)
+    dpd = systems.dpd_params()
+    fsi = C.DpdParams(0.0, 8.0, dpd[2], 0.25)
+    sim = C.Sim(L, 10 * 16 ** 3, C.DpdParams(*dpd), mass=1.0, dt=systems.DT)
+    sim.set_solvent(_solvent(L, 23, q=q))
+    sim.set_walls(sdf, C.wvel("cste"), lam=4.0)
+    sim.set_membranes(pv, F, len(X), par, fsi, mass=systems.RBC_MASS)
+    # the module's forces on these vertices: some near the plate feel it
+    w = C.Wall(sdf, np.zeros((0, 6), np.float32))
+    fw = torch.zeros((len(pv), 3), device="cuda")
+    w.repulse(4.0, dev(pv), fw)
+    assert (fw.abs().sum(1) > 0).sum().item() > 10
+    sim.step(20)
+    gv = sim.get_membranes()
+    assert np.isfinite(gv).all()
+    assert (q.eval(gv) < 0).all()
+    assert C.device_error() == 0
+    sim.close()
