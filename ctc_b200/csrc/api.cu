@@ -296,6 +296,8 @@ struct ctc_sim {
     float wall_lambda;                     // membranes' wall repulsion (0: none)
     Kiss wall_host;                        // host mirror of the wall ticket's generator
     long nstep;                            // steps taken (the wall velocity's clock)
+    float *stage;                          // AoS staging of uploads and downloads (grows, kept)
+    size_t stage_cap;                      // its floats
     // the step as CUDA graphs (one from each ping-pong buffer) on an own stream
     bool use_graph;
     cudaGraphExec_t gexec[2];
@@ -389,6 +391,7 @@ extern "C" int ctc_sim_destroy(ctc_sim *s) {
     for (int b = 0; b < 2; b++) { cudaFree(s->pos[b]); cudaFree(s->vel[b]); }
     cudaFree(s->force); cudaFree(s->counts); cudaFree(s->starts); cudaFree(s->count0); cudaFree(s->fss);
     if (s->wall) ctc_wall_fin(s->wall);
+    cudaFree(s->stage);
     cudaFree(s->scratch); cudaFree(s->trunk_dev); cudaFree(s->seeds_dev); cudaFree(s->diag_scratch);
     cudaFree(s->cnt_scratch);
     cudaFree(s->diag_out);
@@ -401,22 +404,36 @@ extern "C" int ctc_sim_destroy(ctc_sim *s) {
     return CTC_OK;
 }
 
+// the staging buffer for nfloat floats (allocated once, grown when needed;
+// every user synchronises its stream before returning)
+static int sim_stage(ctc_sim *s, size_t nfloat, float **p) {
+    if (nfloat > s->stage_cap) {
+        cudaFree(s->stage);
+        s->stage = nullptr;
+        s->stage_cap = 0;
+        CUDA_TRY(cudaMalloc(&s->stage, sizeof(float) * nfloat));
+        s->stage_cap = nfloat;
+    }
+    *p = s->stage;
+    return CTC_OK;
+}
+
 static int sim_set(ctc_sim *s, int n, const float *pp, bool host, cudaStream_t st) {
     if (!s || n < 0 || (n > 0 && !pp)) return fail(CTC_ERR_ARG, "ctc_sim_set_solvent: bad arguments");
     if (n > s->cfg.maxp) return fail(CTC_ERR_CAPACITY, "ctc_sim_set_solvent: %d > capacity %d", n, s->cfg.maxp);
     const float *src = pp;
-    float *tmp = nullptr;
     if (host && n > 0) {
-        CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 6 * (size_t)n, st));
+        float *tmp = nullptr;
+        int rc = sim_stage(s, 6 * (size_t)s->cfg.maxp, &tmp);
+        if (rc) return rc;
         CUDA_TRY(cudaMemcpyAsync(tmp, pp, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice, st));
         src = tmp;
     }
     s->cur = 0;
-    sim_drop_graphs(s);                  // the grids follow the particle count
+    if (n != s->n_host) sim_drop_graphs(s);   // the grids follow the particle count
     CUDA_TRY(aos_to_soa(n, src, s->pos[0], s->vel[0], st));
     CUDA_TRY(cudaMemcpyAsync(s->count0, &n, sizeof(int), cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    if (tmp) CUDA_TRY(cudaFreeAsync(tmp, st));
     s->n_host = n;
     s->built = false;
     return CTC_OK;
@@ -463,15 +480,15 @@ extern "C" int ctc_sim_set_membranes(ctc_sim *s, int nc, int nv, int nt, const i
         CUDA_TRY(cudaMemcpy(s->vperm, perm.data(), sizeof(int) * nv, cudaMemcpyHostToDevice));
     }
     int n = (int)nvt;
-    float *tmp = nullptr;
     if (n > 0) {
-        CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 6 * nvt, st));
+        float *tmp = nullptr;
+        int rs = sim_stage(s, 6 * nvt, &tmp);
+        if (rs) return rs;
         CUDA_TRY(cudaMemcpyAsync(tmp, pp, sizeof(float) * 6 * nvt, cudaMemcpyHostToDevice, st));
         CUDA_TRY(aos_to_soa(n, tmp, s->mpos, s->mvel, st));
     }
     CUDA_TRY(cudaMemcpyAsync(s->mcount, &n, sizeof(int), cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    if (tmp) CUDA_TRY(cudaFreeAsync(tmp, st));
     s->mnc = nc; s->mnv = nv;
     int rcc = sim_cnt_alloc(s);
     if (rcc) return rcc;
@@ -571,10 +588,10 @@ extern "C" int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream) {
     size_t nvt = (size_t)s->mnc * s->mnv;
     if (nvt == 0) return CTC_OK;
     float *tmp = nullptr;
-    CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 6 * nvt, st));
+    int rc = sim_stage(s, 6 * nvt, &tmp);
+    if (rc) return rc;
     CUDA_TRY(soa_to_aos(nullptr, (int)nvt, s->mpos, s->mvel, tmp, st));
     CUDA_TRY(cudaMemcpyAsync(pp, tmp, sizeof(float) * 6 * nvt, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaFreeAsync(tmp, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     return CTC_OK;
 }
@@ -875,12 +892,12 @@ extern "C" int ctc_sim_get_solvent(ctc_sim *s, float *pp, int *n, void *stream) 
     int cnt = 0;
     int rc = ctc_sim_count(s, &cnt, stream);
     if (rc) return rc;
-    float *tmp = nullptr;
     if (cnt > 0) {
-        CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 6 * (size_t)cnt, st));
+        float *tmp = nullptr;
+        rc = sim_stage(s, 6 * (size_t)std::max(cnt, s->cfg.maxp), &tmp);
+        if (rc) return rc;
         CUDA_TRY(soa_to_aos(nullptr, cnt, s->pos[s->cur], s->vel[s->cur], tmp, st));
         CUDA_TRY(cudaMemcpyAsync(pp, tmp, sizeof(float) * 6 * (size_t)cnt, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaFreeAsync(tmp, st));
         CUDA_TRY(cudaStreamSynchronize(st));
     }
     if (n) *n = cnt;
