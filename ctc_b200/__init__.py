@@ -365,6 +365,15 @@ class Sdf:
     def label(self, pp, out, stream=None):
         check(lib().ctc_sdf_label(self.h, int(pp.shape[0]), _ptr(pp), _ptr(out), _stream(stream)))
 
+    def who_stays(self, pp, nv):
+        """sdf_who_stays: indices of the cells of pp (device (nc*nv, 6)) with
+        every vertex in the bulk."""
+        nc = int(pp.shape[0]) // int(nv)
+        stay = (C.c_int * max(nc, 1))()
+        ns = C.c_int(0)
+        check(lib().ctc_sdf_who_stays(self.h, nc, int(nv), _ptr(pp), stay, C.byref(ns)))
+        return np.array(stay[:ns.value], np.int64)
+
 
 class Wall:
     """wall_gen_quants + wall_gen_ticket (src/wall): freezes the solvent
@@ -535,6 +544,10 @@ class Sim:
         v = v if v is not None else wvel("cste")
         check(lib().ctc_sim_set_walls(self.h, sdf.h, C.byref(v), float(lam), _stream(stream)))
         self._sdf = sdf                  # the field outlives the walls
+        nc, nv = C.c_int(0), C.c_int(0)  # membranes inside the wall were removed
+        check(lib().ctc_sim_membrane_count(self.h, C.byref(nc), C.byref(nv)))
+        if getattr(self, "mnv", 0):
+            self.mnc = nc.value
 
     def set_walls_strt(self, sdf, base, v=None, lam=0.0):
         """Walls from the restart template base/wall.pp/templ (the solvent as it is)."""

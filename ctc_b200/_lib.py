@@ -96,6 +96,8 @@ SIGNATURES = {
     "ctc_sim_set_membrane_noise": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_sim_set_bending": (C.c_int, [vp, C.c_int]),
     "ctc_sim_set_walls": (C.c_int, [vp, vp, C.POINTER(Wvel), C.c_float, vp]),
+    "ctc_sim_membrane_count": (C.c_int, [vp, ip, ip]),
+    "ctc_sdf_who_stays": (C.c_int, [vp, C.c_int, C.c_int, vp, ip, ip]),
     "ctc_sim_set_walls_strt": (C.c_int, [vp, vp, C.c_char_p, C.POINTER(Wvel), C.c_float]),
     "ctc_sim_wall_strt_dump_templ": (C.c_int, [vp, C.c_char_p]),
     "ctc_wall_strt_dump_templ": (C.c_int, [vp, C.c_char_p]),

@@ -532,7 +532,39 @@ extern "C" int ctc_sim_set_walls(ctc_sim *s, const ctc_sdf *sdf, const ctc_wvel 
     if (rc) return rc;
     kiss_ini(&s->wall_host, 42, 42, 42, 42);
     CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 30, s->wall_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
-    return sim_set(s, n_out, pp.data(), true, st);
+    rc = sim_set(s, n_out, pp.data(), true, st);
+    if (rc) return rc;
+    // objects_remove_from_wall (src/sim/objects/imp/gen.h:24-55): the cells
+    // with a vertex outside the bulk leave, the others keep their order
+    const int nvt = s->mnc * s->mnv;
+    if (nvt > 0) {
+        std::vector<float> mv(6 * (size_t)nvt);
+        rc = ctc_sim_get_membranes(s, mv.data(), stream);
+        if (rc) return rc;
+        float *dm = nullptr;
+        rc = sim_stage(s, 6 * (size_t)nvt, &dm);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpy(dm, mv.data(), sizeof(float) * mv.size(), cudaMemcpyHostToDevice));
+        std::vector<int> stay((size_t)s->mnc);
+        int ns = 0;
+        rc = ctc_sdf_who_stays(sdf, s->mnc, s->mnv, dm, stay.data(), &ns);
+        if (rc) return rc;
+        if (ns < s->mnc) {
+            for (int c = 0; c < ns; c++)
+                memmove(mv.data() + 6 * (size_t)c * s->mnv, mv.data() + 6 * (size_t)stay[c] * s->mnv,
+                        sizeof(float) * 6 * s->mnv);
+            const int n2 = ns * s->mnv;
+            if (n2 > 0) {
+                CUDA_TRY(cudaMemcpy(dm, mv.data(), sizeof(float) * 6 * (size_t)n2, cudaMemcpyHostToDevice));
+                CUDA_TRY(aos_to_soa(n2, dm, s->mpos, s->mvel, st));
+            }
+            CUDA_TRY(cudaMemcpyAsync(s->mcount, &n2, sizeof(int), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaStreamSynchronize(st));
+            s->mnc = ns;
+            sim_drop_graphs(s);
+        }
+    }
+    return CTC_OK;
 }
 
 extern "C" int ctc_sim_set_walls_strt(ctc_sim *s, const ctc_sdf *sdf, const char *base, const ctc_wvel *v,
@@ -579,6 +611,13 @@ extern "C" int ctc_sim_set_membrane_noise(ctc_sim *s, int enable, unsigned seed)
         kiss_ini(&s->noise_host, (int)seed, 0x2545f491, 0x6c078965, 0x1b873593);
         CUDA_TRY(cudaMemcpy(s->trunk_dev + 4 * 29, s->noise_host.s, sizeof(unsigned) * 4, cudaMemcpyHostToDevice));
     }
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_membrane_count(const ctc_sim *s, int *nc, int *nv) {
+    if (!s || !nc || !nv) return fail(CTC_ERR_ARG, "ctc_sim_membrane_count: bad arguments");
+    *nc = s->mnc;
+    *nv = s->mnv;
     return CTC_OK;
 }
 

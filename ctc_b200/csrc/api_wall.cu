@@ -383,3 +383,26 @@ extern "C" int ctc_wall_strt_ini(const ctc_sdf *sdf, const char *base, ctc_wall 
     *pw = w;
     return CTC_OK;
 }
+
+// sdf_who_stays (src/wall/sdf/imp/split.h:30-56): the cells (nc of nv vertices
+// pp [dev, AoS]) whose vertices are all in the bulk, in order: stay[*ns]
+extern "C" int ctc_sdf_who_stays(const ctc_sdf *s, int nc, int nv, const float *pp, int *stay, int *ns) {
+    if (!s || nc < 0 || nv <= 0 || (nc > 0 && (!pp || !stay)) || !ns)
+        return fail(CTC_ERR_ARG, "ctc_sdf_who_stays: bad arguments");
+    *ns = 0;
+    if (nc == 0) return CTC_OK;
+    const size_t n = (size_t)nc * nv;
+    int *dl = nullptr;
+    CUDA_TRY(cudaMalloc(&dl, sizeof(int) * n));
+    CUDA_TRY(sdf_label_launch(sdf_view(s), (int)n, pp, 6, dl, 0));
+    std::vector<int> lab(n);
+    cudaError_t e = cudaMemcpy(lab.data(), dl, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    cudaFree(dl);
+    CUDA_TRY(e);
+    for (int c = 0; c < nc; c++) {
+        int v = 0;
+        while (v < nv && lab[(size_t)c * nv + v] == 0) v++;
+        if (v == nv) stay[(*ns)++] = c;
+    }
+    return CTC_OK;
+}

@@ -263,6 +263,9 @@ int ctc_sdf_texture(const ctc_sdf *s, int *T, float *o, float *sp, float *thr, f
  * 0 bulk (s < 0), 1 wall (0 <= s <= 2), 2 deep (s > 2) */
 int ctc_sdf_eval(const ctc_sdf *s, int n, const float *pp, float *out, void *stream);
 int ctc_sdf_label(const ctc_sdf *s, int n, const float *pp, int *labels, void *stream);
+/* sdf_who_stays: of nc cells of nv vertices pp [dev, AoS], the ones whose
+ * vertices are all in the bulk, in order: stay [host, nc ints], *ns of them */
+int ctc_sdf_who_stays(const ctc_sdf *s, int nc, int nv, const float *pp, int *stay, int *ns);
 
 /* wall velocity (wvel_set_cste / _shear / _shear_sin / _hs) */
 #define CTC_WVEL_CSTE 0
@@ -369,7 +372,8 @@ int ctc_sim_set_membrane_noise(ctc_sim *s, int enable, unsigned seed);
 int ctc_sim_set_bending(ctc_sim *s, int mode);
 /* walls in the step (src/sim/walls, src/sim/imp/{force,update}.h): the
  * current solvent freezes against the field sdf (borrowed: it must outlive
- * the walls; same box), the bulk particles stay; from the next step on the
+ * the walls; same box), the bulk particles stay, and membranes with a vertex
+ * outside the bulk are removed (objects_remove_from_wall); from the next step on the
  * wall forces act on the solvent and, with the FSI parameters, on the
  * membranes (plus the repulsion lambda if non-zero), and both bounce back
  * from the walls after the update; v is the wall velocity (its clock starts
@@ -382,6 +386,8 @@ int ctc_sim_set_walls_strt(ctc_sim *s, const ctc_sdf *sdf, const char *base, con
 int ctc_sim_wall_strt_dump_templ(ctc_sim *s, const char *base);
 /* download the membrane vertices [host, AoS, nc * nv] */
 int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream);
+/* the membranes' cell count (cells leave when walls are set) and vertices per cell */
+int ctc_sim_membrane_count(const ctc_sim *s, int *nc, int *nv);
 /* download the cell-sorted solvent [host, AoS, capacity maxp] */
 int ctc_sim_get_solvent(ctc_sim *s, float *pp, int *n, void *stream);
 /* total momentum (3), kinetic temperature, count -- FP64 reductions on the

@@ -343,3 +343,36 @@ def test_sim_walls_with_membranes():
     assert (q.eval(gv) < 0).all()
     assert C.device_error() == 0
     sim.close()
+
+
+def test_cells_in_the_wall_are_removed():
+    """objects_remove_from_wall: of two cells, the one that crosses a plate
+    leaves when the walls are set; sdf_who_stays names the other."""
+    import ctc_b200 as C
+    from ctc_b200 import mesh
+    L = (16, 16, 16)
+    path = os.path.join(SDF, "wall.dat")
+    q = oracle.Sdf(*oracle.sdf_read(path), L)
+    sdf = C.Sdf(L, path=path)
+    X, F = mesh.rbc_template()
+    nv = len(X)
+    pv = np.zeros((2 * nv, 6), np.float32)
+    pv[:nv, :3] = X
+    pv[nv:, :3] = X
+    pv[nv:, 2] += 6.5                     # through the upper plate
+    s = q.eval(pv)
+    assert (s[:nv] < 0).all() and (s[nv:] >= 0).any()
+    assert list(sdf.who_stays(dev(pv), nv)) == [0]
+    A, V = mesh.area_volume(X, F)
+    dpd = systems.dpd_params()
+    sim = C.Sim(L, 10 * 16 ** 3, C.DpdParams(*dpd), mass=1.0, dt=systems.DT)
+    sim.set_solvent(_solvent(L, 29, q=q))
+    sim.set_membranes(pv, F, nv, systems.rbc_params(A, V), C.DpdParams(0.0, 8.0, dpd[2], 0.25),
+                      mass=systems.RBC_MASS)
+    sim.set_walls(sdf, C.wvel("cste"))
+    assert sim.mnc == 1
+    gv = sim.get_membranes()
+    assert np.array_equal(gv, pv[:nv])
+    sim.step(3)
+    assert C.device_error() == 0
+    sim.close()
