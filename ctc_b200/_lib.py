@@ -102,6 +102,7 @@ SIGNATURES = {
     "ctc_sim_wall_strt_dump_templ": (C.c_int, [vp, C.c_char_p]),
     "ctc_wall_strt_dump_templ": (C.c_int, [vp, C.c_char_p]),
     "ctc_wall_strt_ini": (C.c_int, [vp, C.c_char_p, C.POINTER(vp)]),
+    "ctc_wall_ini_particles": (C.c_int, [vp, C.c_int, vp, C.POINTER(vp)]),
     "ctc_bop_write": (C.c_int, [C.c_char_p, C.c_long, C.c_int, C.c_char_p, vp]),
     "ctc_bop_read": (C.c_int, [C.c_char_p, C.c_long, C.POINTER(C.c_long), ip, ip, vp]),
     "ctc_restart_write_pp": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_long, vp]),

@@ -39,6 +39,10 @@
 #include <stdio.h>
 #include <limits.h>
 #include "io/restart/imp.h"
+#include "coords/imp.h"
+#include "wall/imp.h"
+#include "wall/sdf/imp.h"
+#include "wall/wvel/imp.h"
 #include "utils/error.h"
 
 #include "ctc_b200.h"
@@ -251,3 +255,238 @@ void restart_read_ii(MPI_Comm, const char *base, const char *code, int id, int *
     CTC(ctc_restart_read_ii(base, code, id, LONG_MAX, &m, ii));
     *n = (int)m;
 }
+
+// ---- walls (src/wall/imp.h, src/wall/sdf/imp.h, src/wall/wvel/imp.h), one rank --
+struct Sdf {
+    int3 L;
+    ctc_sdf *h;
+    ctc_wall *bw;            // a wall without particles: bounce-back and repulsion need the field only
+};
+struct WallTicket {
+    ctc_wall *h;             // built on the first wall_force (it brings the field)
+    const Sdf *sdf;
+};
+struct Wvel { ctc_wvel v; };
+struct WvelStep { ctc_wvel v; float t; };
+struct WallRepulsePrm { float l; };
+
+void sdf_ini(int3 L, Sdf **s) {
+    *s = new Sdf;
+    (*s)->L = L;
+    (*s)->h = NULL;
+    (*s)->bw = NULL;
+}
+
+void sdf_fin(Sdf *s) {
+    if (s->bw) CTC(ctc_wall_fin(s->bw));
+    if (s->h) CTC(ctc_sdf_fin(s->h));
+    delete s;
+}
+
+// the field file sdf.dat of the working directory, as the reference reads it
+void sdf_gen(const Coords *c, MPI_Comm, bool dump, Sdf *s) {
+    if (dump) ERR("ctc_b200: dumping the field (HDF5) is not supported");
+    const int3 L = subdomain(c);
+    if (L.x != s->L.x || L.y != s->L.y || L.z != s->L.z) ERR("ctc_b200: sdf_gen: box differs from sdf_ini's");
+    if (s->h) CTC(ctc_sdf_fin(s->h));
+    CTC(ctc_sdf_ini("sdf.dat", L.x, L.y, L.z, &s->h));
+    int n_out = 0;
+    if (s->bw) CTC(ctc_wall_fin(s->bw));
+    CTC(ctc_wall_ini(s->h, 0, NULL, &n_out, &s->bw));
+}
+
+// labels on the device, split on the host: the bulk stays in s_pp [dev], the
+// wall particles go to w_pp [host]
+void sdf_bulk_wall(const Sdf *s, int *s_n, Particle *s_pp, int *w_n, Particle *w_pp) {
+    const int n = *s_n;
+    int *lab_dev = NULL;
+    std::vector<int> lab(n > 0 ? n : 1);
+    std::vector<Particle> hst(n > 0 ? n : 1);
+    if (n > 0) {
+        if (cudaMalloc((void**)&lab_dev, sizeof(int) * n) != cudaSuccess) ERR("ctc_b200: sdf_bulk_wall: no memory");
+        CTC(ctc_sdf_label(s->h, n, reinterpret_cast<const float*>(s_pp), lab_dev, NULL));
+        cudaMemcpy(lab.data(), lab_dev, sizeof(int) * n, cudaMemcpyDeviceToHost);
+        cudaMemcpy(hst.data(), s_pp, sizeof(Particle) * n, cudaMemcpyDeviceToHost);
+        cudaFree(lab_dev);
+    }
+    int is = 0, iw = 0;
+    for (int i = 0; i < n; i++) {
+        if (lab[i] == 0) hst[is++] = hst[i];
+        else if (lab[i] == 1) w_pp[iw++] = hst[i];
+    }
+    if (is > 0) cudaMemcpy(s_pp, hst.data(), sizeof(Particle) * is, cudaMemcpyHostToDevice);
+    *s_n = is;
+    *w_n = iw;
+}
+
+int sdf_who_stays(const Sdf *s, int n, const Particle *pp, int nc, int nv, int *stay) {
+    if (n != nc * nv) ERR("ctc_b200: sdf_who_stays: %d particles for %d x %d", n, nc, nv);
+    int ns = 0;
+    CTC(ctc_sdf_who_stays(s->h, nc, nv, reinterpret_cast<const float*>(pp), stay, &ns));
+    return ns;
+}
+
+void sdf_bounce(float dt, const WvelStep *wv, const Coords *, const Sdf *s, int n, Particle *pp) {
+    CTC(ctc_wall_set_vel(s->bw, &wv->v));
+    CTC(ctc_wall_update_vel(s->bw, wv->t));
+    CTC(ctc_wall_bounce(s->bw, dt, n, reinterpret_cast<float*>(pp), NULL));
+}
+
+void wvel_ini(Wvel **w) { *w = new Wvel; memset(&(*w)->v, 0, sizeof((*w)->v)); }
+void wvel_fin(Wvel *w) { delete w; }
+void wvel_step_ini(WvelStep **w) { *w = new WvelStep; memset(&(*w)->v, 0, sizeof((*w)->v)); (*w)->t = 0; }
+void wvel_step_fin(WvelStep *w) { delete w; }
+
+void wvel_set_cste(float3 u, Wvel *w) {
+    memset(&w->v, 0, sizeof(w->v));
+    w->v.type = CTC_WVEL_CSTE;
+    w->v.u[0] = u.x; w->v.u[1] = u.y; w->v.u[2] = u.z;
+}
+
+void wvel_set_shear(float gdot, int vdir, int gdir, int half, Wvel *w) {
+    memset(&w->v, 0, sizeof(w->v));
+    w->v.type = CTC_WVEL_SHEAR;
+    w->v.gdot = gdot; w->v.vdir = vdir; w->v.gdir = gdir; w->v.half = half;
+}
+
+void wvel_set_shear_sin(float gdot, int vdir, int gdir, int half, float om, Wvel *w) {
+    wvel_set_shear(gdot, vdir, gdir, half, w);
+    w->v.type = CTC_WVEL_SHEAR_SIN;
+    w->v.w = om;
+}
+
+void wvel_set_hs(float u, float h, Wvel *w) {
+    memset(&w->v, 0, sizeof(w->v));
+    w->v.type = CTC_WVEL_HS;
+    w->v.u[0] = u; w->v.h = h;
+}
+
+void wvel_get_step(float t, const Wvel *w, WvelStep *s) {
+    s->v = w->v;
+    s->t = t;
+}
+
+int wvel_get_type(const WvelStep *s) {     // the step's kind: WALL_VEL_V_CSTE, _SHEAR, _HS
+    return s->v.type == CTC_WVEL_CSTE ? WALL_VEL_V_CSTE : s->v.type == CTC_WVEL_HS ? WALL_VEL_V_HS : WALL_VEL_V_SHEAR;
+}
+
+void wall_ini_quants(int3 L, WallQuants *q) {
+    q->n = 0;
+    q->pp = NULL;
+    q->L = L;
+}
+
+void wall_fin_quants(WallQuants *q) {
+    cudaFree(q->pp);
+    q->pp = NULL;
+    q->n = 0;
+}
+
+void wall_ini_ticket(int3, WallTicket **t) {
+    *t = new WallTicket;
+    (*t)->h = NULL;
+    (*t)->sdf = NULL;
+}
+
+void wall_fin_ticket(WallTicket *t) {
+    if (t->h) CTC(ctc_wall_fin(t->h));
+    delete t;
+}
+
+// freeze (o_pp [dev]) and the periodic images in the margin: the frozen
+// particles as float4 x y z 0, cell-sorted, into q
+void wall_gen_quants(MPI_Comm, int, int maxn, const Sdf *s, int *o_n, Particle *o_pp, WallQuants *q) {
+    const int n = *o_n;
+    std::vector<Particle> hst(n > 0 ? n : 1);
+    if (n > 0) cudaMemcpy(hst.data(), o_pp, sizeof(Particle) * n, cudaMemcpyDeviceToHost);
+    ctc_wall *w = NULL;
+    int n_out = 0, nw = 0;
+    CTC(ctc_wall_ini(s->h, n, reinterpret_cast<float*>(hst.data()), &n_out, &w));
+    if (n_out > 0) cudaMemcpy(o_pp, hst.data(), sizeof(Particle) * n_out, cudaMemcpyHostToDevice);
+    *o_n = n_out;
+    CTC(ctc_wall_particles(w, &nw, NULL, NULL));
+    if (nw > maxn) ERR("Too many particles for wall : %d / %d\n", nw, maxn);
+    std::vector<float4> p4(nw > 0 ? nw : 1);
+    CTC(ctc_wall_particles(w, &nw, reinterpret_cast<float*>(p4.data()), NULL));
+    CTC(ctc_wall_fin(w));
+    cudaFree(q->pp);
+    q->pp = NULL;
+    if (nw > 0) {
+        if (cudaMalloc((void**)&q->pp, sizeof(float4) * nw) != cudaSuccess) ERR("ctc_b200: wall_gen_quants: no memory");
+        cudaMemcpy(q->pp, p4.data(), sizeof(float4) * nw, cudaMemcpyHostToDevice);
+    }
+    q->n = nw;
+}
+
+void wall_gen_ticket(const WallQuants *, WallTicket *t) {
+    if (t->h) CTC(ctc_wall_fin(t->h));
+    t->h = NULL;
+    t->sdf = NULL;
+}
+
+static void ticket_for(const Sdf *s, const WallQuants *q, const WallTicket *t0) {
+    WallTicket *t = const_cast<WallTicket*>(t0);
+    if (t->h && t->sdf == s) return;
+    if (t->h) CTC(ctc_wall_fin(t->h));
+    std::vector<float4> p4(q->n > 0 ? q->n : 1);
+    if (q->n > 0) cudaMemcpy(p4.data(), q->pp, sizeof(float4) * q->n, cudaMemcpyDeviceToHost);
+    CTC(ctc_wall_ini_particles(s->h, q->n, reinterpret_cast<const float*>(p4.data()), &t->h));
+    t->sdf = s;
+}
+
+void wall_strt_quants(MPI_Comm, const char *base, int maxn, WallQuants *q) {
+    long n = 0;
+    CTC(ctc_restart_read_pp(base, "wall.pp", CTC_RESTART_TEMPL, 0, &n, NULL));
+    if (n > maxn) ERR("ctc_b200: wall template of %ld particles > %d", n, maxn);
+    std::vector<Particle> pp(n > 0 ? n : 1);
+    CTC(ctc_restart_read_pp(base, "wall.pp", CTC_RESTART_TEMPL, n, &n, reinterpret_cast<float*>(pp.data())));
+    std::vector<float4> p4(n > 0 ? n : 1);
+    for (long i = 0; i < n; i++) p4[i] = make_float4(pp[i].r[0], pp[i].r[1], pp[i].r[2], 0);
+    cudaFree(q->pp);
+    q->pp = NULL;
+    if (n > 0) {
+        if (cudaMalloc((void**)&q->pp, sizeof(float4) * n) != cudaSuccess) ERR("ctc_b200: wall_strt_quants: no memory");
+        cudaMemcpy(q->pp, p4.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+    }
+    q->n = (int)n;
+}
+
+void wall_strt_dump_templ(MPI_Comm, const char *base, const WallQuants *q) {
+    std::vector<float4> p4(q->n > 0 ? q->n : 1);
+    if (q->n > 0) cudaMemcpy(p4.data(), q->pp, sizeof(float4) * q->n, cudaMemcpyDeviceToHost);
+    std::vector<Particle> pp(q->n > 0 ? q->n : 1);
+    for (int i = 0; i < q->n; i++) {
+        Particle p = {{p4[i].x, p4[i].y, p4[i].z}, {0, 0, 0}};
+        pp[i] = p;
+    }
+    CTC(ctc_restart_write_pp(base, "wall.pp", CTC_RESTART_TEMPL, q->n, reinterpret_cast<const float*>(pp.data())));
+}
+
+void wall_force(const PairParams *par, const WvelStep *wv, const Coords *, const Sdf *s, const WallQuants *q,
+                const WallTicket *t, int n, const PaArray *a, const FoArray *f) {
+    if (a->colors) ERR("ctc_b200: coloured solvent is not supported");
+    if (f->stress) ERR("ctc_b200: stresses are not supported");
+    ticket_for(s, q, t);
+    PairDPD p;
+    pair_get_view_dpd(par, &p);
+    const ctc_dpd_params d = {p.a, p.g, p.s, p.spow};
+    CTC(ctc_wall_set_vel(t->h, &wv->v));
+    CTC(ctc_wall_update_vel(t->h, wv->t));
+    CTC(ctc_wall_force(t->h, &d, n, a->pp, f->ff, NULL));
+}
+
+void wall_force_adhesion(const PairParams *, const WvelStep *, const Coords *, const Sdf *, const WallQuants *,
+                         const WallTicket *, int, const PaArray *, const FoArray *) {
+    ERR("ctc_b200: wall adhesion is not supported");
+}
+
+void wall_repulse(const Sdf *s, const WallRepulsePrm *wr, long n, const PaArray *a, const FoArray *f) {
+    CTC(ctc_wall_repulse(s->bw, wr->l, (int)n, a->pp, f->ff, NULL));
+}
+
+void wall_repulse_prm_ini(float lambda, WallRepulsePrm **wr) {
+    *wr = new WallRepulsePrm;
+    (*wr)->l = lambda;
+}
+
+void wall_repulse_prm_fin(WallRepulsePrm *wr) { delete wr; }

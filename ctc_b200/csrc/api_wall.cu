@@ -406,3 +406,20 @@ extern "C" int ctc_sdf_who_stays(const ctc_sdf *s, int nc, int nv, const float *
     }
     return CTC_OK;
 }
+
+// wall_gen_ticket from given wall particles: pos4 [host] x y z (w ignored), n of them
+extern "C" int ctc_wall_ini_particles(const ctc_sdf *sdf, int n, const float *pos4, ctc_wall **pw) {
+    if (!sdf || n < 0 || (n > 0 && !pos4) || !pw) return fail(CTC_ERR_ARG, "ctc_wall_ini_particles: bad arguments");
+    std::vector<float> wall(3 * (size_t)n);
+    for (int i = 0; i < n; i++)
+        for (int c = 0; c < 3; c++) wall[3 * (size_t)i + c] = pos4[4 * (size_t)i + c];
+    ctc_wall *w = new ctc_wall();
+    int rc = wall_cells(sdf, wall, w);
+    if (rc) {
+        cudaFree(w->pos); cudaFree(w->starts);
+        delete w;
+        return rc;
+    }
+    *pw = w;
+    return CTC_OK;
+}

@@ -308,6 +308,8 @@ int ctc_wall_repulse(ctc_wall *w, float lambda, int n, const float *pp, float *f
  * particles as the restart template base/wall.pp/templ (positions, zero
  * velocities), and a wall built from such a template */
 int ctc_wall_strt_dump_templ(const ctc_wall *w, const char *base);
+/* wall_gen_ticket alone: a wall from n given particles pos4 [host, x y z w] */
+int ctc_wall_ini_particles(const ctc_sdf *s, int n, const float *pos4, ctc_wall **w);
 int ctc_wall_strt_ini(const ctc_sdf *s, const char *base, ctc_wall **w);
 
 /* ---- time update: replaces src/scheme/move/imp.h:5-6, scheme/force ------- */

@@ -12,7 +12,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 OBJ = os.path.join(ROOT, "ctc_b200", "compat", "_build", "udx_compat.o")
 
 # the declarations of src/clist/imp.h, src/fluforces/imp.h (bulk),
-# src/rbc/force/imp.h, src/scheme/move/imp.h and src/io/restart/imp.h (the
+# src/rbc/force/imp.h, src/scheme/move/imp.h, src/io/restart/imp.h and the
+# walls' src/wall/imp.h, src/wall/sdf/imp.h, src/wall/wvel/imp.h (the
 # MPI_Comm of the compile check is its stand-in type), as the C++ compiler
 # names them
 EXPECTED = [
@@ -43,6 +44,35 @@ EXPECTED = [
     "restart_write_ii(ctc_compat_check_comm*, char const*, char const*, int, long, int const*)",
     "restart_read_pp(ctc_compat_check_comm*, char const*, char const*, int, int*, Particle*)",
     "restart_read_ii(ctc_compat_check_comm*, char const*, char const*, int, int*, int*)",
+    "sdf_ini(int3, Sdf**)",
+    "sdf_fin(Sdf*)",
+    "sdf_gen(Coords const*, ctc_compat_check_comm*, bool, Sdf*)",
+    "sdf_bulk_wall(Sdf const*, int*, Particle*, int*, Particle*)",
+    "sdf_who_stays(Sdf const*, int, Particle const*, int, int, int*)",
+    "sdf_bounce(float, WvelStep const*, Coords const*, Sdf const*, int, Particle*)",
+    "wvel_ini(Wvel**)",
+    "wvel_fin(Wvel*)",
+    "wvel_step_ini(WvelStep**)",
+    "wvel_step_fin(WvelStep*)",
+    "wvel_set_cste(float3, Wvel*)",
+    "wvel_set_shear(float, int, int, int, Wvel*)",
+    "wvel_set_shear_sin(float, int, int, int, float, Wvel*)",
+    "wvel_set_hs(float, float, Wvel*)",
+    "wvel_get_step(float, Wvel const*, WvelStep*)",
+    "wvel_get_type(WvelStep const*)",
+    "wall_ini_quants(int3, WallQuants*)",
+    "wall_ini_ticket(int3, WallTicket**)",
+    "wall_fin_quants(WallQuants*)",
+    "wall_fin_ticket(WallTicket*)",
+    "wall_gen_quants(ctc_compat_check_comm*, int, int, Sdf const*, int*, Particle*, WallQuants*)",
+    "wall_gen_ticket(WallQuants const*, WallTicket*)",
+    "wall_strt_quants(ctc_compat_check_comm*, char const*, int, WallQuants*)",
+    "wall_strt_dump_templ(ctc_compat_check_comm*, char const*, WallQuants const*)",
+    "wall_force(PairParams const*, WvelStep const*, Coords const*, Sdf const*, WallQuants const*, WallTicket const*, "
+    "int, PaArray const*, FoArray const*)",
+    "wall_repulse(Sdf const*, WallRepulsePrm const*, long, PaArray const*, FoArray const*)",
+    "wall_repulse_prm_ini(float, WallRepulsePrm**)",
+    "wall_repulse_prm_fin(WallRepulsePrm*)",
 ]
 
 
