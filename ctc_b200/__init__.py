@@ -409,6 +409,15 @@ class Wall:
         check(lib().ctc_wall_strt_dump_templ(self.h, str(base).encode()))
 
     @classmethod
+    def from_particles(cls, sdf, pos4):
+        """wall_gen_ticket alone: a wall from given particles pos4 (host (n, 4))."""
+        pos4 = np.ascontiguousarray(pos4, np.float32).reshape(-1, 4)
+        w = cls.__new__(cls)
+        w.sdf, w.h, w.bulk = sdf, C.c_void_p(), None
+        check(lib().ctc_wall_ini_particles(sdf.h, len(pos4), _vp(pos4), C.byref(w.h)))
+        return w
+
+    @classmethod
     def strt(cls, sdf, base):
         """A wall from the restart template base/wall.pp/templ."""
         w = cls.__new__(cls)

@@ -291,6 +291,11 @@ def test_wall_restart_template(tmp_path):
     w2 = C.Wall.strt(sdf, tmp_path)
     pos2, st2 = w2.particles()
     assert np.array_equal(pos, pos2) and np.array_equal(st, st2)
+    # a wall from the particles themselves, in another order: the same cell list
+    w3 = C.Wall.from_particles(sdf, pos[::-1])
+    pos3, st3 = w3.particles()
+    assert np.array_equal(st, st3)
+    assert np.array_equal(np.sort(pos3.view(np.complex128).ravel()), np.sort(pos.view(np.complex128).ravel()))
     dpd = systems.dpd_params()
     a = C.Sim(L, len(pp), C.DpdParams(*dpd), mass=1.0, dt=systems.DT, bodyf=(0.1, 0.0, 0.0))
     a.set_solvent(pp)
