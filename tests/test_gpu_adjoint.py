@@ -144,7 +144,7 @@ def test_autograd_wrapper_matches_direct_backward():
     r.set_positions(pp[:, :3], pv[:, :3])
     l2 = r.forward(4, 2)
     g = r.backward()
-    assert abs(float(loss) - l2) <= 1e-6 * max(1.0, abs(l2))
+    assert abs(float(loss.detach()) - l2) <= 1e-6 * max(1.0, abs(l2))
     np.testing.assert_allclose(th.grad.numpy(), g["theta"], rtol=1e-4, atol=1e-10)
     np.testing.assert_allclose(xv.grad.numpy(), g["gxv"], rtol=1e-3, atol=1e-6 * np.abs(g["gxv"]).max())
     assert xs.grad.shape == xs.shape
