@@ -382,3 +382,44 @@ def test_cells_in_the_wall_are_removed():
     sim.step(3)
     assert C.device_error() == 0
     sim.close()
+
+
+def test_sim_everything_together_graph_and_direct():
+    """Walls, membranes with contact, the membrane random force and
+    Juelicher bending in one step: graph replay follows the direct
+    launches, nothing enters the wall, no kernel records a failure."""
+    import ctc_b200 as C
+    from ctc_b200 import mesh
+    L = (16, 16, 16)
+    path = os.path.join(SDF, "wall.dat")
+    q = oracle.Sdf(*oracle.sdf_read(path), L)
+    sdf = C.Sdf(L, path=path)
+    X, F = mesh.rbc_template()
+    nv = len(X)
+    pv = np.zeros((2 * nv, 6), np.float32)
+    pv[:nv, :3] = X + (-3.0, 0.0, -1.5)
+    pv[nv:, :3] = X + (3.0, 0.0, 1.5)
+    A, V = mesh.area_volume(X, F)
+    dpd = systems.dpd_params()
+    ps = _solvent(L, 31, q=q)
+    out = []
+    for graph in (False, True):
+        sim = C.Sim(L, len(ps), C.DpdParams(*dpd), mass=1.0, dt=systems.DT, bodyf=(0.2, 0.0, 0.0),
+                    rng=C.CTC_RNG_STABLE)
+        sim.set_solvent(ps)
+        sim.set_membranes(pv, F, nv, systems.rbc_params(A, V), C.DpdParams(0.0, 8.0, dpd[2], 0.25),
+                          mass=systems.RBC_MASS)
+        sim.set_walls(sdf, C.wvel("shear", gdot=1.0, vdir=0, gdir=2), lam=2.0)
+        sim.set_contact(C.DpdLjParams(dpd[0], dpd[1], dpd[2], 0.25, 0.3, 0.44))
+        sim.set_membrane_noise(True, seed=5)
+        sim.set_bending("juelicher")
+        sim.set_graph(graph)
+        sim.step(20)
+        gs, gv = sim.get_solvent(), sim.get_membranes()
+        assert np.isfinite(gs).all() and np.isfinite(gv).all()
+        assert (q.eval(gs) < 0).all() and (q.eval(gv) < 0).all()
+        out.append((gs, gv))
+        sim.close()
+    assert np.abs(out[0][0] - out[1][0]).max() < 1e-3
+    assert np.abs(out[0][1] - out[1][1]).max() < 1e-3
+    assert C.device_error() == 0
