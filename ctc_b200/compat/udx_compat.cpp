@@ -225,6 +225,18 @@ void rbc_force_apply(RbcForce *f, const RbcParams *par, float dt, const RbcQuant
                             NULL));
 }
 
+// the reference's own statistics entry point returns these placeholders
+// (src/rbc/force/imp/stat.h:1-3)
+void rbc_force_stat(float *pArea, float *pVolume) {
+    *pArea = 1.0;
+    *pVolume = 1.0;
+}
+
+// stress-free reference lengths (src/rbc/shape) are not part of this build
+void rbc_force_set_stressfree(const char *fname, RbcForce *) {
+    ERR("ctc_b200: stress-free membranes (%s) are not supported; use rbc_force_set_stressful", fname);
+}
+
 // ---- update (src/scheme/move/imp.h) -------------------------------------------
 void scheme_move_apply(float dt, float mass, int n, const Force *ff, Particle *pp) {
     CTC(ctc_scheme_move_apply(dt, mass, n, reinterpret_cast<const float*>(ff), reinterpret_cast<float*>(pp), NULL));

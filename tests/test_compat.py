@@ -38,6 +38,8 @@ EXPECTED = [
     "rbc_force_set_rnd1(int, RbcForce*)",
     "rbc_force_set_bending(MeshRead const*, char const*, RbcForce*)",
     "rbc_force_apply(RbcForce*, RbcParams const*, float, RbcQuants const*, Force*)",
+    "rbc_force_stat(float*, float*)",
+    "rbc_force_set_stressfree(char const*, RbcForce*)",
     "scheme_move_apply(float, float, int, Force const*, Particle*)",
     "scheme_move_clear_vel(int, Particle*)",
     "restart_write_pp(ctc_compat_check_comm*, char const*, char const*, int, long, Particle const*)",
