@@ -92,6 +92,7 @@ def lib():
             "orc_rbc_forces": (None, [C.c_int] * 5 + [i32p, i32p, f32p, f64p, RbcParams, f32p]),
             "orc_rbc_forces_f64": (None, [C.c_int] * 4 + [i32p, i32p, f32p, f64p, RbcParams, f64p]),
             "orc_kantor_energy": (C.c_double, [C.c_int, C.c_int, i32p, i32p, f32p, C.c_double, C.c_double]),
+            "orc_kantor_vertex_energy": (None, [C.c_int, C.c_int, i32p, i32p, f32p, C.c_double, C.c_double, f64p]),
             "orc_move": (None, [C.c_float, C.c_float, C.c_int, f32p, f32p]),
             "orc_body_force": (None, [C.c_float, f32p, C.c_int, f32p]),
             "orc_wrap": (None, [C.c_int] * 4 + [f32p]),
@@ -324,6 +325,15 @@ def rbc_forces(tri, nv, pp, params, av=None, mode=0, f64=False):
 def kantor_energy(tri, nv, pp, kb, phi_deg=0.0):
     md, a0, a1 = adj_build(tri, nv)
     return lib().orc_kantor_energy(nv, md, a0, a1, _pp(pp), kb, phi_deg)
+
+
+def kantor_vertex_energy(tri, nv, pp, kb, phi_deg=0.0):
+    """Per vertex, the mean over its edges of kb (1 - cos(theta - phi)) with
+    the Kantor force's dihedral angle."""
+    md, a0, a1 = adj_build(tri, nv)
+    ev = np.zeros(nv, np.float64)
+    lib().orc_kantor_vertex_energy(nv, md, a0, a1, _pp(pp), kb, phi_deg, ev)
+    return ev
 
 
 # ---- update --------------------------------------------------------------------

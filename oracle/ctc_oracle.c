@@ -1070,6 +1070,33 @@ double orc_kantor_energy(int nv, int md, const int *adj0, const int *adj1, const
     return 0.5 * e;
 }
 
+/* per vertex: the mean over its edges of kb (1 - cos(theta - phi)), theta
+ * the dihedral angle of the Kantor force above.  The ring slot (i0, j) holds
+ * the dihedral across the ring edge (m[1], m[2]) opposite to i0; every edge
+ * is seen from its two opposite vertices, so each sighting gives half of the
+ * edge's term to each end (the edge-to-vertex average of src/mesh/scatter). */
+void orc_kantor_vertex_energy(int nv, int md, const int *adj0, const int *adj1, const float *pp, double kb,
+                              double phi_deg, double *ev) {
+    int i, m[5], *deg = (int*)calloc((size_t)nv, sizeof(int));
+    double phi = phi_deg / 180.0 * M_PI;
+    for (i = 0; i < nv; i++) ev[i] = 0;
+    for (i = 0; i < nv * md; i++) {
+        d3 a, b, c, d, k, n;
+        double ct, st, th;
+        if (!adj_map(md, nv, i, adj0, adj1, m)) continue;
+        a = pos(pp, m[0]); b = pos(pp, m[2]); c = pos(pp, m[1]); d = pos(pp, m[4]);
+        k = crs(sub(a, b), sub(a, c)); n = crs(sub(b, d), sub(b, c));
+        ct = dot3(k, n) / sqrt(dot3(k, k) * dot3(n, n));
+        st = dot3(crs(k, n), sub(b, c)) / sqrt(dot3(k, k) * dot3(n, n) * dot3(sub(b, c), sub(b, c)));
+        th = atan2(st, ct);
+        ev[m[1]] += 0.5 * kb * (1 - cos(th - phi));
+        ev[m[2]] += 0.5 * kb * (1 - cos(th - phi));
+        deg[i / md]++;                         /* a vertex has as many slots as edges */
+    }
+    for (i = 0; i < nv; i++) ev[i] /= deg[i];
+    free(deg);
+}
+
 /* ========================================================================= */
 /* update                                                                    */
 /* ========================================================================= */

@@ -124,6 +124,8 @@ double orc_kantor_energy(int nv, int md, const int *adj0, const int *adj1, const
 /* Juelicher bending (src/rbc/force/bending/juelicher, kb = 1 and H0 = -1/2 as
  * the reference hard-codes them) of nc cells of one template: the forces
  * f + fad of juelicher_apply in double, added to ff (3 per vertex) */
+void orc_kantor_vertex_energy(int nv, int md, const int *adj0, const int *adj1, const float *pp, double kb,
+                              double phi_deg, double *ev);
 void orc_juelicher_forces(int nc, int nv, int nt, const int *tri, const float *pp, double *ff);
 
 /* ---- update (src/scheme/move, src/scheme/force) --------------------------- */

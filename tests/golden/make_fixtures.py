@@ -38,6 +38,8 @@ COPIES = {
     "clist.ref.clist.t2.txt": "src/test_data/clist.ref.clist.t2.txt",
     "rnd.ref.rnd.t0.txt": "src/test_data/rnd.ref.rnd.t0.txt",
     "pair.ref.pair.0.txt": "src/test_data/pair.ref.pair.0.txt",
+    "eng.ref.mesh.eng_kantor.txt": "src/test_data/eng.ref.mesh.eng_kantor.txt",
+    "rbc.2562.off": "src/data/cells/rbc/sc/2562.off",
     "pair.in.2.txt": "src/data/pair/2",
     "av.ref.rbc.u.area_volume.dev.0.txt": "src/test_data/av.ref.rbc.u.area_volume.dev.0.txt",
     "rbc.1986.off": "src/data/cells/rbc/1986.off",

@@ -110,3 +110,21 @@ def test_area_volume_1986():
     # prints as the golden line, a sequential float sum is within 2e-6
     assert "%g %g" % (av64[0], av64[1]) == "%g %g" % tuple(ref)
     assert np.allclose(av32, av64, rtol=2e-6)
+
+
+def test_kantor_angles_eng_kantor():
+    """src/test_data/eng.ref.mesh.eng_kantor.txt (src/test/mesh/eng_kantor:
+    the 2562-vertex sphere, kb = 1, angle0 = 0): per vertex, the mean over
+    its edges of the mesh tool's 2 kb (1 - cos theta)
+    (src/mesh/eng_kantor/imp/main.h:22-33, edge-to-vertex average of
+    src/mesh/scatter).  The oracle's Kantor dihedral angles reproduce it to
+    the file's six printed digits, which pins the angle the bending force
+    differentiates."""
+    V, F = mesh.read_off(os.path.join(GOLDEN, "rbc.2562.off"))
+    pp = np.zeros((len(V), 6), np.float32)
+    pp[:, :3] = V
+    ev = 2 * oracle.kantor_vertex_energy(F, len(V), pp, 1.0)
+    g = np.loadtxt(os.path.join(GOLDEN, "eng.ref.mesh.eng_kantor.txt"))
+    assert g.shape == (len(V), 4)
+    assert np.abs(ev - g[:, 3]).max() <= 5e-6 * np.abs(g[:, 3]).max()
+    assert (np.abs(ev - g[:, 3]) <= 1e-5 * np.abs(g[:, 3]) + 1e-12).all()
