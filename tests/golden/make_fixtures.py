@@ -6,7 +6,8 @@ Run it from the repository root where the reference tree is available:
 
 It writes two kinds of files:
 
-* inputs restated here: the clist test particles of src/test/clist/{0,1,2}/main
+* inputs restated here: the clist and bulk test particles of
+  src/test/clist/{0,1,2}/main and src/test/bulk/{0,1}/main
   made the way pre/units/gen_random.cpp makes them (drand48 from its
   unseeded glibc state, ``L*(-0.5f + 0.9999f*drand48())`` in double, stored as
   float, printed with ``%f``).  When ``oracle/_ref/gen_random`` (the reference
@@ -32,6 +33,12 @@ CLIST_CASES = {
     "t2": ((20, 6, 8), 64),
 }
 
+# src/test/bulk/{0,1}/main: gen_random box and N (the bulk box is the same)
+BULK_CASES = {
+    "t0": ((4, 4, 4), 64),
+    "t1": ((4, 4, 4), 640),
+}
+
 COPIES = {
     "clist.ref.clist.t0.txt": "src/test_data/clist.ref.clist.t0.txt",
     "clist.ref.clist.t1.txt": "src/test_data/clist.ref.clist.t1.txt",
@@ -39,6 +46,8 @@ COPIES = {
     "rnd.ref.rnd.t0.txt": "src/test_data/rnd.ref.rnd.t0.txt",
     "pair.ref.pair.0.txt": "src/test_data/pair.ref.pair.0.txt",
     "eng.ref.mesh.eng_kantor.txt": "src/test_data/eng.ref.mesh.eng_kantor.txt",
+    "ff.ref.bulk.t0.txt": "src/test_data/ff.ref.bulk.t0.txt",
+    "ff.ref.bulk.t1.txt": "src/test_data/ff.ref.bulk.t1.txt",
     "rbc.2562.off": "src/data/cells/rbc/sc/2562.off",
     "pair.in.2.txt": "src/data/pair/2",
     "av.ref.rbc.u.area_volume.dev.0.txt": "src/test_data/av.ref.rbc.u.area_volume.dev.0.txt",
@@ -70,9 +79,11 @@ def gen_random(X, Y, Z, n):
 
 
 def main(ref):
-    for name, ((X, Y, Z), n) in CLIST_CASES.items():
+    cases = [("clist", name, c) for name, c in CLIST_CASES.items()] + \
+        [("bulk", name, c) for name, c in BULK_CASES.items()]
+    for kind, name, ((X, Y, Z), n) in cases:
         txt = gen_random(X, Y, Z, n)
-        path = os.path.join(HERE, "clist.in.%s.txt" % name)
+        path = os.path.join(HERE, "%s.in.%s.txt" % (kind, name))
         with open(path, "w") as f:
             f.write(txt)
         exe = os.path.join(ROOT, "oracle", "_ref", "gen_random")
@@ -81,7 +92,7 @@ def main(ref):
                                  text=True, check=True).stdout
             if out != txt:
                 raise SystemExit("gen_random restatement differs from the reference for " + name)
-            print("%s: identical to the reference generator" % name)
+            print("%s %s: identical to the reference generator" % (kind, name))
     for dst, src in COPIES.items():
         shutil.copyfile(os.path.join(ref, src), os.path.join(HERE, dst))
     print("fixtures written to", HERE)

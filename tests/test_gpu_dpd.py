@@ -289,3 +289,19 @@ def test_sim_step_forces_vs_modules(L):
     err = np.abs(f - ref).max(1) / np.maximum(fn, 0.1 * fn.mean())
     assert err.max() < 1e-5, err.max()
     assert C.device_error() == 0
+
+
+@pytest.mark.parametrize("case", ["t0", "t1"])
+def test_bulk_kernel_golden(case):
+    """The reference's own bulk test output (ff.ref.bulk.{t0,t1}, kBT = 0):
+    this build's cell lists and bulk kernel on the same particles."""
+    import ctc_b200 as C
+    from .test_oracle_golden import BULK_DPD, bulk_golden, match_bulk
+    pp, g = bulk_golden(case)
+    L = (4, 4, 4)
+    out, starts, counts, ids = C.Clist(L, len(pp)).build(torch.as_tensor(pp, device="cuda"))
+    ff = torch.zeros((len(pp), 3), device="cuda")
+    C.FluForces(L, len(pp)).apply_seeded(C.DpdParams(*BULK_DPD), out, starts, counts,
+                                        np.zeros(27, np.float32), ff, which=1)
+    assert match_bulk(out.cpu().numpy(), ff.cpu().numpy(), g) < 1e-5
+    assert C.device_error() == 0

@@ -128,3 +128,42 @@ def test_kantor_angles_eng_kantor():
     assert g.shape == (len(V), 4)
     assert np.abs(ev - g[:, 3]).max() <= 5e-6 * np.abs(g[:, 3]).max()
     assert (np.abs(ev - g[:, 3]) <= 1e-5 * np.abs(g[:, 3]) + 1e-12).all()
+
+
+# src/test/bulk/{0,1}/main: u/bulk on gen_random particles in a 4^3 box, kBT = 0
+# (no random force), a = 2.6666667, g = 8, spow = 0.25 (conf.cfg); the output
+# is the sorted particles and their bulk forces, scaled by uscale and sorted as
+# text lines
+BULK_GOLDEN = {"t0": 1e4, "t1": 1e2}
+BULK_DPD = (2.6666667, 8.0, 0.0, 0.25)
+
+
+def bulk_golden(case):
+    """(input particles, golden rows (x y z vx vy vz fx fy fz))."""
+    pp = np.loadtxt(os.path.join(GOLDEN, "bulk.in.%s.txt" % case), dtype=np.float32)
+    g = np.loadtxt(os.path.join(GOLDEN, "ff.ref.bulk.%s.txt" % case)) / BULK_GOLDEN[case]
+    return pp, g
+
+
+def match_bulk(ppout, ff, g):
+    """Per golden row, the relative force error of the particle at its position
+    (floored at 0.1 x the mean force)."""
+    mags = np.abs(g[:, 6:9]).max(1)
+    err = []
+    for row, m in zip(g, mags):
+        d = np.abs(ppout[:, :3] - row[:3]).sum(1)
+        k = int(d.argmin())
+        assert d[k] < 1e-3
+        err.append(np.abs(ff[k] - row[6:9]).max() / max(m, 0.1 * mags.mean()))
+    return max(err)
+
+
+@pytest.mark.parametrize("case", ["t0", "t1"])
+def test_bulk_forces_golden(case):
+    """ff.ref.bulk.{t0,t1}: the oracle's bulk forces to the file's digits."""
+    pp, g = bulk_golden(case)
+    L = (4, 4, 4)
+    counts, starts, order, ppout = oracle.clist_build(L, pp)
+    assert len(ppout) == len(g)
+    ff = oracle.dpd_bulk(L, ppout, starts, BULK_DPD, 0.0)
+    assert match_bulk(ppout, ff, g) < 1e-5
