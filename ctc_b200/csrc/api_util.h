@@ -72,6 +72,17 @@ inline void halo_trunk_ini(int fid, Kiss *k) {
     kiss_ini(k, 390 + seed, seed + 615, 12309, 23094);
 }
 
+// a temporary device buffer freed on every return path
+template <typename T>
+struct DevTmp {
+    T *p = nullptr;
+    DevTmp() = default;
+    DevTmp(const DevTmp &) = delete;
+    DevTmp &operator=(const DevTmp &) = delete;
+    ~DevTmp() { if (p) cudaFree(p); }
+    cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * n); }
+};
+
 inline bool box_ok(int LX, int LY, int LZ) { return LX >= 3 && LY >= 3 && LZ >= 3; }
 
 inline void dpd_args_common(DpdArgs *A, int3 L, const ctc_dpd_params *p) {

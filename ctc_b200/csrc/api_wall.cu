@@ -167,16 +167,14 @@ bool wvel_ok(const ctc_wvel *p) {
 int wall_build(const ctc_sdf *sdf, int n, float *pp, int *n_out, ctc_wall *w, cudaStream_t st) {
     std::vector<int> lab(n > 0 ? n : 1);
     if (n > 0) {
-        float *dpp = nullptr;
-        int *dl = nullptr;
-        CUDA_TRY(cudaMalloc(&dpp, sizeof(float) * 6 * (size_t)n));
-        CUDA_TRY(cudaMalloc(&dl, sizeof(int) * (size_t)n));
-        CUDA_TRY(cudaMemcpyAsync(dpp, pp, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice, st));
-        CUDA_TRY(sdf_label_launch(sdf_view(sdf), n, dpp, 6, dl, st));
-        CUDA_TRY(cudaMemcpyAsync(lab.data(), dl, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
+        DevTmp<float> dpp;
+        DevTmp<int> dl;
+        CUDA_TRY(dpp.alloc(6 * (size_t)n));
+        CUDA_TRY(dl.alloc((size_t)n));
+        CUDA_TRY(cudaMemcpyAsync(dpp.p, pp, sizeof(float) * 6 * (size_t)n, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(sdf_label_launch(sdf_view(sdf), n, dpp.p, 6, dl.p, st));
+        CUDA_TRY(cudaMemcpyAsync(lab.data(), dl.p, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaStreamSynchronize(st));
-        cudaFree(dpp);
-        cudaFree(dl);
     }
     std::vector<float> wall;   // x y z of the frozen particles
     int k = 0;
@@ -392,13 +390,13 @@ extern "C" int ctc_sdf_who_stays(const ctc_sdf *s, int nc, int nv, const float *
     *ns = 0;
     if (nc == 0) return CTC_OK;
     const size_t n = (size_t)nc * nv;
-    int *dl = nullptr;
-    CUDA_TRY(cudaMalloc(&dl, sizeof(int) * n));
-    CUDA_TRY(sdf_label_launch(sdf_view(s), (int)n, pp, 6, dl, 0));
+    // runs on the legacy default stream and synchronises with it (the
+    // reference's sdf_who_stays runs on its default stream too)
+    DevTmp<int> dl;
+    CUDA_TRY(dl.alloc(n));
+    CUDA_TRY(sdf_label_launch(sdf_view(s), (int)n, pp, 6, dl.p, 0));
     std::vector<int> lab(n);
-    cudaError_t e = cudaMemcpy(lab.data(), dl, sizeof(int) * n, cudaMemcpyDeviceToHost);
-    cudaFree(dl);
-    CUDA_TRY(e);
+    CUDA_TRY(cudaMemcpy(lab.data(), dl.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
     for (int c = 0; c < nc; c++) {
         int v = 0;
         while (v < nv && lab[(size_t)c * nv + v] == 0) v++;

@@ -10,6 +10,8 @@
 // an unspecified order; here the order is fixed: particles that stayed in the
 // box first, then those that re-entered through a periodic face, each group by
 // ascending input index -- one of the orders the reference can produce.
+// clist_noalloc.cu restates count/scan/place/gather for AoS input and a fixed
+// scratch array: a change of these semantics here must be made there too.
 #include "common.cuh"
 
 namespace ctc {

@@ -1,13 +1,16 @@
 // Cell-list build that allocates no device memory.
 //
 // Some callers cannot call cudaMalloc at the point where they need cell
-// lists: code that runs inside a host callback or an allocator hook (where
-// CUDA allocation is not allowed), host code that must not touch a
-// caching allocator it does not own, or a long-running service that forbids
-// allocation on its steady-state path so that it cannot fail or fragment
-// memory mid-run.  ctc_clist_build_noalloc serves them: the caller passes
-// its inputs and outputs, and the scratch the build needs lives in one
+// lists: code that runs inside an allocator hook (a pluggable allocator that
+// must not re-enter the allocator it implements), host code that must not
+// touch a caching allocator it does not own, or a long-running service that
+// forbids allocation on its steady-state path so that it cannot fail or
+// fragment memory mid-run.  ctc_clist_build_noalloc serves them: the caller
+// passes its inputs and outputs, and the scratch the build needs lives in one
 // file-scope device array of fixed size, allocated with the library image.
+// The call itself enqueues one cudaMemsetAsync and six kernel launches on
+// `stream`; like every CUDA call it must not be made from inside a stream
+// callback or a host function launched with cudaLaunchHostFunc.
 //
 // Limits and rules:
 //   - at most CTC_CLIST_NOALLOC_MAXP particles and CTC_CLIST_NOALLOC_MAXC cells per
@@ -18,12 +21,21 @@
 //     whose work overlaps on the GPU (other streams, other host threads on
 //     the same device) race on it and must be serialised by the caller;
 //   - the first call on a device looks up the array's device address (with
-//     that device current); make that first call before any stream capture.
+//     that device current) and keeps it for the life of the process; make that
+//     first call before any stream capture.  A cudaDeviceReset of the device
+//     unloads the library image there, so the kept address goes stale: a
+//     process that resets a device must not call this entry point on it again.
 //
 // The kernels follow the cell-list semantics of the reference
 // (src/clist/dev/main.h:6-101): cell index in double, particles outside the
-// box dropped, and within a cell the input order (as clist.cu).
+// box dropped, and within a cell the input order.  They restate the
+// count/scan/place/gather kernels of clist.cu for AoS input and a fixed
+// scratch; a change of semantics there (inside test, cell index, order in a
+// cell) must be made here too -- tests/test_zz_no_alloc.py compares the two
+// bit for bit.
 #include <cuda_runtime.h>
+
+#include <atomic>
 
 #include "api_util.h"
 #include "common.cuh"
@@ -143,7 +155,9 @@ __global__ void k_gather(int nc, const Scratch *S, const int *__restrict__ start
 }
 
 constexpr int MAX_DEVICES = 64;
-static Scratch *g_ptr[MAX_DEVICES];   // device address of g_scratch, per device
+// device address of g_scratch, per device; host threads that make their first
+// call on a device at the same time both look it up and store the same value
+static std::atomic<Scratch *> g_ptr[MAX_DEVICES];
 
 }  // namespace noalloc
 }  // namespace ctc
@@ -164,14 +178,13 @@ extern "C" int ctc_clist_build_noalloc(int LX, int LY, int LZ, int n, const floa
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= MAX_DEVICES) return fail(CTC_ERR_ARG, "ctc_clist_build_noalloc: device %d", dev);
-    if (!g_ptr[dev]) {   // one-time set-up on this device: the array's device address
-        Scratch *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress((void**)&p, g_scratch);
-        if (e != cudaSuccess || !p)
+    Scratch *S = g_ptr[dev].load(std::memory_order_acquire);
+    if (!S) {   // one-time set-up on this device: the array's device address
+        cudaError_t e = cudaGetSymbolAddress((void**)&S, g_scratch);
+        if (e != cudaSuccess || !S)
             return fail(CTC_ERR_CUDA, "ctc_clist_build_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-        g_ptr[dev] = p;
+        g_ptr[dev].store(S, std::memory_order_release);
     }
-    Scratch *S = g_ptr[dev];
     cudaStream_t st = (cudaStream_t)stream;
     int3 L = make_int3(LX, LY, LZ);
     int nb = (int)((nc + SCAN_TILE - 1) / SCAN_TILE);

@@ -94,10 +94,12 @@ int ctc_clist_get(const ctc_clist *c, const int **starts, const int **counts, co
 
 /* ---- cell lists without device allocation ------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
- * where they need cell lists -- code running inside a host callback or an
- * allocator hook, where CUDA allocation is not allowed, or a service whose
+ * where they need cell lists -- code running inside an allocator hook, which
+ * must not re-enter the allocator it implements, or a service whose
  * steady-state path must not allocate so that it cannot fail or fragment
- * memory mid-run.  Same result as ctc_clist_build: pp [dev, AoS, n] in,
+ * memory mid-run.  It enqueues a memset and kernel launches on `stream`, so
+ * like any CUDA call it cannot be made from a stream callback or a host
+ * function.  Same result as ctc_clist_build: pp [dev, AoS, n] in,
  * ppout [dev, AoS], starts [dev, LX*LY*LZ + 1], counts [dev, LX*LY*LZ] and
  * ids [dev, may be NULL] out.  Its scratch is one fixed 3 MiB device array
  * of the library (held on every GPU that loads it until exit), so a call
@@ -105,7 +107,8 @@ int ctc_clist_get(const ctc_clist *c, const int **starts, const int **counts, co
  * cells (CTC_ERR_CAPACITY otherwise).  All calls share that array: calls
  * whose work overlaps on the GPU race and must be serialised by the caller.
  * The first call on a device looks up the array's address with that device
- * current; make it before any stream capture. */
+ * current and keeps it; make it before any stream capture, and make no call
+ * on a device after a cudaDeviceReset of it. */
 #define CTC_CLIST_NOALLOC_MAXP 262144
 #define CTC_CLIST_NOALLOC_MAXC 1048576
 int ctc_clist_build_noalloc(int LX, int LY, int LZ, int n, const float *pp, float *ppout, int *starts,
@@ -264,7 +267,9 @@ int ctc_sdf_texture(const ctc_sdf *s, int *T, float *o, float *sp, float *thr, f
 int ctc_sdf_eval(const ctc_sdf *s, int n, const float *pp, float *out, void *stream);
 int ctc_sdf_label(const ctc_sdf *s, int n, const float *pp, int *labels, void *stream);
 /* sdf_who_stays: of nc cells of nv vertices pp [dev, AoS], the ones whose
- * vertices are all in the bulk, in order: stay [host, nc ints], *ns of them */
+ * vertices are all in the bulk, in order: stay [host, nc ints], *ns of them.
+ * Runs on the legacy default stream and synchronises with it, as the
+ * reference's (src/wall/sdf/imp/split.h:30-56). */
 int ctc_sdf_who_stays(const ctc_sdf *s, int nc, int nv, const float *pp, int *stay, int *ns);
 
 /* wall velocity (wvel_set_cste / _shear / _shear_sin / _hs) */

@@ -5,7 +5,10 @@
 # reference sources into this repository.
 #
 #   make -f oracle/ref.mk REF=/path/to/reference
-REF     ?= /root/reference
+# the reference tree: $(CTC_REFERENCE) when set, else its usual place in the
+# build container
+CTC_REFERENCE ?= /root/reference
+REF     ?= $(CTC_REFERENCE)
 OUT     := oracle/_ref
 CXX     := g++
 NVCC    ?= nvcc

@@ -1,12 +1,15 @@
 """The cell-list build that allocates no device memory (ctc_clist_build_noalloc).
 
 It exists for callers that cannot call cudaMalloc where they build cell lists
-(host callbacks or allocator hooks, where CUDA allocation is not allowed, or a
+(an allocator hook, which must not re-enter the allocator it implements, or a
 service that must not allocate on its steady-state path).  It must give
 exactly the result of the allocating entry point (ctc_clist_build): cell
 counts, starts, the sorted particles and the input index of each, bit for bit
--- also on a second call in a row, which finds the shared scratch array holding
-the first call's leftovers.  This file is named so that pytest collects it last.
+-- also on the calls after the first, which find the shared scratch array
+holding the previous call's leftovers: a larger call after a smaller one, then
+a smaller one after it, in both particles and cells, so that stale slots
+beyond the current sizes are left in the array.  This file is named so that
+pytest collects it last.
 """
 import ctypes as C
 
@@ -41,8 +44,9 @@ def _allocating(L, pp):
     return out.cpu().numpy(), starts.cpu().numpy(), counts.cpu().numpy(), ids.cpu().numpy()
 
 
-def test_noalloc_matches_allocating_build_twice():
-    cases = [((12, 10, 8), 1), ((16, 16, 8), 2)]        # two calls in a row, different sizes
+def test_noalloc_matches_allocating_build_in_a_row():
+    # three calls in a row: larger, then smaller in particles and cells
+    cases = [((12, 10, 8), 1), ((16, 16, 8), 2), ((10, 6, 8), 3)]
     for L, seed in cases:
         pp = systems.solvent(L, seed=seed)
         extra = systems.solvent(L, n=50, seed=seed + 10)
