@@ -187,8 +187,10 @@ int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const flo
             f->calls++;
         }
     }
-    CUDA_TRY(membrane_launch(A, st));
+    // bending_apply before the triangle forces, as rbc_force_apply
+    // (src/rbc/force/imp/forces.h:53)
     if (f->bending == 2) CUDA_TRY(juelicher_launch(A, f->jl_av, f->jl_lt, f->jl_curva, st));
+    CUDA_TRY(membrane_launch(A, st));
     return CTC_OK;
 }
 }  // namespace ctc

@@ -8,8 +8,9 @@
 //                src/rbc/force/bending/kantor/dev/main.h:23-66 +
 //                src/mesh/force/kantor0/dev.h:28-131.
 // One thread per vertex walks its md ring slots over the fixed-valence
-// adjacency table (src/rbc/adj/dev.h:2-31), sums every contribution in double
-// and adds it to the vertex force once: no atomics.  The float steps of the
+// adjacency table (src/rbc/adj/dev.h:2-31), computes each slot's contribution
+// in double and adds it to the vertex's float force in the reference's order
+// (bending slots, then triangle slots): no atomics.  The float steps of the
 // reference -- sqrtf of the squared spring length, powf of the POW term -- are
 // kept as float operations, as the reference computes them.
 #include "common.cuh"
@@ -128,6 +129,34 @@ __device__ __forceinline__ D3 dih(double cphi, double sphi, double kb, D3 a, D3 
     }
 }
 
+// adj_get_map0 (src/rbc/adj/dev.h:2-31): ring slot j of the vertex whose
+// table row starts at k; false for an empty slot
+__device__ __forceinline__ bool ring_slot(const MembraneArgs &A, int k, int j, int off, int &i1, int &i2, int &i3,
+                                          int &i4) {
+    const int md = A.md;
+    i1 = __ldg(A.adj0 + k + j);
+    if (i1 == -1) return false;
+    i2 = __ldg(A.adj0 + k + (j + 1) % md);
+    if (i2 == -1) { i2 = __ldg(A.adj0 + k); i3 = __ldg(A.adj0 + k + 1); }
+    else { i3 = __ldg(A.adj0 + k + (j + 2) % md); if (i3 == -1) i3 = __ldg(A.adj0 + k); }
+    i4 = __ldg(A.adj1 + k + j);
+    i1 += off; i2 += off; i3 += off; i4 += off;
+    return true;
+}
+
+__device__ __forceinline__ void add_slot(float3 &acc, D3 f) {
+    acc.x += (float)f.x;
+    acc.y += (float)f.y;
+    acc.z += (float)f.z;
+}
+
+// Each ring slot's contribution is computed in FP64 and added to the vertex's
+// float force in the reference's order: what the force array holds (the FSI
+// forces, in the step), then the bending partial of every slot
+// (bending_apply runs first, src/rbc/force/imp/forces.h:53), then the
+// triangle + viscous (+ random) partial of every slot -- each partial rounded
+// to float as the reference's per-slot atomicAdd does, so that vertices whose
+// slot contributions cancel round as the reference's do.
 __global__ void k_membrane(MembraneArgs A) {
     int pid = blockIdx.x * blockDim.x + threadIdx.x;
     if (pid >= A.nc * A.nv) return;
@@ -135,10 +164,22 @@ __global__ void k_membrane(MembraneArgs A) {
     const int rbc = pid / nv, k = (pid % nv) * md, off = rbc * nv;
     const RbcPar P = A.par;
     const D3 r0 = ld_pos(A.pos, A.stride, pid), v0 = ld_vel(A.vel, A.stride, pid);
-    const double Acell = A.av[2 * rbc], Vcell = A.av[2 * rbc + 1];
-    const double phi = (double)P.phi / 180.0 * M_PI;
-    const double cphi = cos(phi), sphi = sin(phi), kb = P.kb;
-    D3 fb = mk(0, 0, 0), ft = mk(0, 0, 0);
+    // the cell's area and volume, reduced in FP64, enter as the floats the
+    // reference keeps them in (float *av, src/rbc/force/area_volume/imp/main.h:38-51)
+    const double Acell = (float)A.av[2 * rbc], Vcell = (float)A.av[2 * rbc + 1];
+    float *o = A.force + (size_t)A.fstride * pid;
+    float3 acc = make_float3(o[0], o[1], o[2]);
+    int i1, i2, i3, i4;
+    if (A.bending) {   // kantor_dev::force, one dih_a + dih_b partial per slot
+        const double phi = (double)P.phi / 180.0 * M_PI;
+        const double cphi = cos(phi), sphi = sin(phi), kb = P.kb;
+        for (int j = 0; j < md; j++) {
+            if (!ring_slot(A, k, j, off, i1, i2, i3, i4)) continue;
+            D3 r1 = ld_pos(A.pos, A.stride, i1), r2 = ld_pos(A.pos, A.stride, i2);
+            D3 r3 = ld_pos(A.pos, A.stride, i3), r4 = ld_pos(A.pos, A.stride, i4);
+            add_slot(acc, dih<1>(cphi, sphi, kb, r0, r2, r1, r4, A.err) + dih<2>(cphi, sphi, kb, r1, r0, r2, r3, A.err));
+        }
+    }
     // membrane random force (src/rbc/force/dev/common.h:93-108): the
     // magnitude's float square root as the reference's frnd0
     unsigned nkey = 0;
@@ -147,19 +188,10 @@ __global__ void k_membrane(MembraneArgs A) {
         nkey = A.noise_seed_dev ? __float_as_uint(__ldg(A.noise_seed_dev)) : A.noise_key;
         f0n = (double)sqrtf((float)(2.0 * (double)P.gammaC * (double)P.kBT / A.dt));
     }
-    for (int j = 0; j < md; j++) {
-        // adj_get_map0, src/rbc/adj/dev.h:2-31
-        int i1 = __ldg(A.adj0 + k + j);
-        if (i1 == -1) continue;
-        int i2 = __ldg(A.adj0 + k + (j + 1) % md), i3;
-        if (i2 == -1) { i2 = __ldg(A.adj0 + k); i3 = __ldg(A.adj0 + k + 1); }
-        else { i3 = __ldg(A.adj0 + k + (j + 2) % md); if (i3 == -1) i3 = __ldg(A.adj0 + k); }
-        int i4 = __ldg(A.adj1 + k + j);
-        i1 += off; i2 += off; i3 += off; i4 += off;
+    for (int j = 0; j < md; j++) {   // rbc_force_dev::force, adj_tris per slot
+        if (!ring_slot(A, k, j, off, i1, i2, i3, i4)) continue;
         D3 r1 = ld_pos(A.pos, A.stride, i1), r2 = ld_pos(A.pos, A.stride, i2);
-        D3 r3 = ld_pos(A.pos, A.stride, i3), r4 = ld_pos(A.pos, A.stride, i4);
-        if (A.bending) fb = fb + dih<1>(cphi, sphi, kb, r0, r2, r1, r4, A.err) + dih<2>(cphi, sphi, kb, r1, r0, r2, r3, A.err);
-        ft = ft + ftri(P, r0, r1, r2, A.l0, A.a0, Acell, Vcell);
+        D3 ft = ftri(P, r0, r1, r2, A.l0, A.a0, Acell, Vcell);
         ft = ft + fvisc(P, r0, r1, v0, ld_vel(A.vel, A.stride, i1));
         if (A.noise) {   // the edge (pid, i1): one normal number for both directions
             const int a = pid - off, b = i1 - off;
@@ -169,12 +201,11 @@ __global__ void k_membrane(MembraneArgs A) {
             const double r = (double)sqrtf((float)dot(dr, dr));
             if (r > 0.0) ft = ft + (f0n * normal_from(w) / r) * dr;
         }
+        add_slot(acc, ft);
     }
-    D3 f = fb + ft;
-    float *o = A.force + (size_t)A.fstride * pid;
-    o[0] += (float)f.x;
-    o[1] += (float)f.y;
-    o[2] += (float)f.z;
+    o[0] = acc.x;
+    o[1] = acc.y;
+    o[2] = acc.z;
 }
 
 // ---------------------------------------------------------------------------

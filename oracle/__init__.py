@@ -303,8 +303,10 @@ def area_volume(tri, nv, pp, f32=False):
     return av.reshape(nc, 2)
 
 
-def rbc_forces(tri, nv, pp, params, av=None, mode=0, f64=False):
-    """Internal membrane forces; params is a dict of RbcParams fields."""
+def rbc_forces(tri, nv, pp, params, av=None, mode=0, f64=False, ff=None):
+    """Internal membrane forces; params is a dict of RbcParams fields.  With ff
+    (float32 (n, 3)) the float path adds them onto a copy of ff, slot by slot,
+    as the reference's atomics add them onto the force array it is given."""
     tri4 = _tri4(tri)
     pp = _pp(pp)
     md, a0, a1 = adj_build(tri4, nv)
@@ -317,7 +319,7 @@ def rbc_forces(tri, nv, pp, params, av=None, mode=0, f64=False):
         ff = np.zeros((len(pp), 3), np.float64)
         lib().orc_rbc_forces_f64(nc, nv, md, len(tri4), a0, a1, pp, av, par, ff)
     else:
-        ff = np.zeros((len(pp), 3), np.float32)
+        ff = np.zeros((len(pp), 3), np.float32) if ff is None else np.array(ff, np.float32).reshape(-1, 3)
         lib().orc_rbc_forces(mode, nc, nv, md, len(tri4), a0, a1, pp, av, par, ff)
     return ff
 
@@ -441,11 +443,13 @@ def rbc_step(L, ps, pv, tri, nv, dpd, fsi, rbcpar, seeds27, fsi_seeds, bodyf, dt
     fs = body_force(fs, ms, a)
     fv = body_force(fv, mv, a)
     ps = move(ps, fs, dt, ms)
+    # bending first, then the triangle forces, onto the forces already there
+    # (src/sim/objects/imp/main.h:40-48, src/rbc/force/imp/forces.h:53)
     if bending == "juelicher":
-        fv = fv + rbc_forces(tri, nv, pv, dict(rbcpar, kb=0.0), mode=0)
-        fv = (fv + juelicher_forces(tri, nv, pv)).astype(np.float32)
+        fv = fv + juelicher_forces(tri, nv, pv).astype(np.float32)   # the double sum rounded, then added
+        fv = rbc_forces(tri, nv, pv, dict(rbcpar, kb=0.0), mode=0, ff=fv)
     else:
-        fv = fv + rbc_forces(tri, nv, pv, rbcpar, mode=0)
+        fv = rbc_forces(tri, nv, pv, rbcpar, mode=0, ff=fv)
     pv = move(pv, fv, dt, mv)
     return ps, pv
 

@@ -1011,7 +1011,11 @@ static void rbc_slot(int mode, int nv, int md, int i, const int *adj0, const int
     f = addv(dih(1, phi, kb, r0, r2, r1, r4), dih(2, phi, kb, r1, r0, r2, r3));
     fb[0] = f.x; fb[1] = f.y; fb[2] = f.z;
     /* triangle + viscous, src/rbc/force/dev/main.h:23-46 */
-    f = ftri(mode, p, r0, r1, r2, l0, a0, av[2 * rbc], av[2 * rbc + 1]);
+    /* the reference keeps the cell's area and volume as floats (float *av,
+     * src/rbc/force/area_volume/imp/main.h:38-51); mode 1 (all double) keeps
+     * them exact */
+    if (mode == 1) f = ftri(mode, p, r0, r1, r2, l0, a0, av[2 * rbc], av[2 * rbc + 1]);
+    else f = ftri(mode, p, r0, r1, r2, l0, a0, (double)(float)av[2 * rbc], (double)(float)av[2 * rbc + 1]);
     f = addv(f, fvisc(p, r0, r1, vel(pp, m[0]), vel(pp, m[1])));
     ft[0] = f.x; ft[1] = f.y; ft[2] = f.z;
 }

@@ -209,3 +209,205 @@ class RefSdf:
         import torch
         torch.cuda.synchronize()
         assert self.lib.refwall_repulse(self.h, float(lam), int(pp.shape[0]), _p(pp), _p(ff)) == 0
+
+
+# ---- membranes, FSI and contact (oracle/refkern/refobj.cu) --------------------
+_RBC_FIELDS = ("gammaC", "gammaT", "kBT", "kb", "phi", "ks", "x0", "mpow", "ka", "kd", "kv", "totArea", "totVolume")
+
+
+def _rbc_par(par):
+    import numpy as np
+    return np.array([par[k] for k in _RBC_FIELDS], np.float32)
+
+
+def _osig(L):
+    vp, i, f = C.c_void_p, C.c_int, C.c_float
+    L.refkern_area_volume.argtypes = [i, i, i, vp, vp, vp]
+    L.refkern_rbc_force.argtypes = [vp, f, i, i, i, vp, vp, vp, f, f, vp, vp]
+    L.refkern_kantor.argtypes = [vp, i, i, i, vp, vp, vp, vp]
+    L.refkern_fsi_bulk.argtypes = [f] * 4 + [i] * 4 + [vp, i, vp, vp, f, vp, vp]
+    L.refkern_fsi_halo.argtypes = [f] * 4 + [i] * 3 + [vp, vp, i, vp, vp, f, vp, vp]
+    L.refkern_cnt_bulk.argtypes = [vp, i, i, i, i, vp, vp, vp, f, vp]
+    L.refkern_cnt_halo.argtypes = [vp, i, i, i, vp, vp, i, vp, vp, vp, f, vp, vp]
+
+
+def _olib():
+    L_ = lib()
+    _osig(L_)
+    return L_
+
+
+def _tri4(tri):
+    import numpy as np
+    tri = np.asarray(tri)[:, :3]
+    t4 = np.zeros((len(tri), 4), np.int32)
+    t4[:, :3] = tri
+    return t4
+
+
+def area_volume(tri, nv, pp):
+    """area_volume_compute of the reference (float, atomics): (nc, 2) float32
+    [torch, device] of the cells pp (torch (nc*nv, 6) AoS)."""
+    import torch
+    t4 = torch.as_tensor(_tri4(tri), device=pp.device)
+    nc = int(pp.shape[0]) // nv
+    av = torch.zeros(2 * nc, dtype=torch.float32, device=pp.device)
+    torch.cuda.synchronize()
+    assert _olib().refkern_area_volume(nc, nv, len(t4), _p(pp), _p(t4), _p(av)) == 0
+    return av.view(nc, 2)
+
+
+def stressful(nt, totArea):
+    """rbc_force_set_stressful (src/rbc/force/imp/main.h:50-59): a0 = totArea /
+    nt in float, l0 = sqrt(4 a0 / sqrt(3)) in double, stored as float."""
+    import numpy as np
+    a0 = np.float32(np.float32(totArea) / np.float32(nt))
+    l0 = np.float32(np.sqrt(np.float64(a0) * 4.0 / np.sqrt(3.0)))
+    return float(l0), float(a0)
+
+
+def rbc_force(par, dt, tri, nv, adj0, adj1, md, pp, av, ff):
+    """rbc_force_dev::force (stress-ful, no random force) of the cells pp
+    (torch (nc*nv, 6)) with the per-cell av (torch float32 (nc, 2)); adds to ff
+    (torch (nc*nv, 3)).  adj0/adj1: the ring tables (torch int32, device)."""
+    import torch
+    l0, a0 = stressful(len(tri), par["totArea"])
+    q = _rbc_par(par)                                   # host: the kernel takes the view by value
+    nc = int(pp.shape[0]) // nv
+    torch.cuda.synchronize()
+    assert _olib().refkern_rbc_force(q.ctypes.data_as(C.c_void_p), float(dt), md, nv, nc, _p(pp), _p(adj0), _p(adj1), l0, a0,
+                                     _p(av.contiguous()), _p(ff)) == 0
+
+
+def kantor(par, nv, adj0, adj1, md, pp, ff):
+    """kantor_dev::force of the cells pp; adds to ff."""
+    import torch
+    q = _rbc_par(par)                                   # host: the kernel takes the view by value
+    nc = int(pp.shape[0]) // nv
+    torch.cuda.synchronize()
+    assert _olib().refkern_kantor(q.ctypes.data_as(C.c_void_p), md, nv, nc, _p(pp), _p(adj0), _p(adj1), _p(ff)) == 0
+
+
+def fsi_bulk(dpd, L, pv, ps, starts, seed, fv, fs):
+    """fsi_dev::bulk: vertices pv against the cell-sorted solvent ps (torch
+    AoS) with cell starts; adds to fv and fs."""
+    import torch
+    torch.cuda.synchronize()
+    assert _olib().refkern_fsi_bulk(*[float(x) for x in dpd], *L, int(pv.shape[0]), _p(pv), int(ps.shape[0]),
+                                    _p(ps), _p(starts), float(seed), _p(fv), _p(fs)) == 0
+
+
+def images(L, pv_host):
+    """The object halo's image list in receive order (the oracle's restatement
+    of src/exch/map/dev.h, ascending vertex order in a fragment): counts per
+    fragment, the vertex of each image and the image positions (AoS, shifted by
+    -d(fid) L as the exchange unpacks them)."""
+    import numpy as np
+    from . import fsi_halo_images, frag_dir, frag_anti
+    frag, vert = fsi_halo_images(L, pv_host)
+    slot = np.array([frag_anti(int(f)) for f in frag], np.int64)
+    counts = np.bincount(slot, minlength=26).astype(np.int32) if len(frag) else np.zeros(26, np.int32)
+    img = np.array(pv_host, np.float32)[vert].copy()
+    dirs = np.array([frag_dir(f) for f in range(26)], np.float32)
+    if len(frag):
+        img[:, :3] -= dirs[frag] * np.asarray(L, np.float32)
+    # images sent in fragment fid arrive in receive slot anti(fid), slot after slot
+    assert len(frag) == 0 or np.all(np.diff(slot) >= 0)
+    return counts, vert, img
+
+
+def fsi_halo(dpd, L, pv_host, ps, starts, seed, fv, fs):
+    """fsi_dev::halo on the images of the vertices pv_host [host]; the image
+    forces go back to their vertices in fv (as eobj unpack_ff); adds to fs."""
+    import numpy as np
+    import torch
+    counts, vert, img = images(L, pv_host)
+    if len(vert) == 0:
+        return 0
+    dev = ps.device
+    c26 = np.ascontiguousarray(counts, np.int32)
+    pimg = torch.as_tensor(img, device=dev)
+    fimg = torch.zeros((len(img), 3), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    assert _olib().refkern_fsi_halo(*[float(x) for x in dpd], *L, c26.ctypes.data_as(C.c_void_p), _p(pimg),
+                                    int(ps.shape[0]), _p(ps), _p(starts), float(seed), _p(fimg), _p(fs)) == 0
+    fv.index_add_(0, torch.as_tensor(vert.astype(np.int64), device=dev), fimg)
+    return len(vert)
+
+
+def vertex_cells(L, pv_host):
+    """The vertex cell list of cnt_build_cells (project = true): starts (nc+1)
+    and ids (the clist map codes, object 0: the vertex index) [host int32]."""
+    import numpy as np
+    from . import clist_build
+    counts, starts, order, _ = clist_build(L, pv_host, project=True)
+    return np.ascontiguousarray(starts, np.int32), np.ascontiguousarray(order, np.int32)
+
+
+def cnt(p, L, pv_host, seed_bulk, seed_halo, fv):
+    """cnt_dev::bulk then cnt_dev::halo of one object type on the vertices
+    pv_host [host]; adds to fv (torch (nv, 3)), image forces returned to their
+    vertices."""
+    import numpy as np
+    import torch
+    dev = fv.device
+    starts, ids = vertex_cells(L, pv_host)
+    pv = torch.as_tensor(np.ascontiguousarray(pv_host, np.float32), device=dev)
+    st, ii = torch.as_tensor(starts, device=dev), torch.as_tensor(ids, device=dev)
+    lj = np.ascontiguousarray(p, np.float32)            # host: the kernel takes PairDPDLJ by value
+    ljp = lj.ctypes.data_as(C.c_void_p)
+    lib_ = _olib()
+    torch.cuda.synchronize()
+    assert lib_.refkern_cnt_bulk(ljp, *L, int(pv.shape[0]), _p(pv), _p(st), _p(ii), float(seed_bulk), _p(fv)) == 0
+    counts, vert, img = images(L, pv_host)
+    if len(vert) == 0:
+        return
+    c26 = np.ascontiguousarray(counts, np.int32)
+    pimg = torch.as_tensor(img, device=dev)
+    fimg = torch.zeros((len(img), 3), dtype=torch.float32, device=dev)
+    assert lib_.refkern_cnt_halo(ljp, *L, c26.ctypes.data_as(C.c_void_p), _p(pimg), int(pv.shape[0]), _p(pv),
+                                 _p(st), _p(ii), float(seed_halo), _p(fimg), _p(fv)) == 0
+    fv.index_add_(0, torch.as_tensor(vert.astype(np.int64), device=dev), fimg)
+
+
+# ---- the reference's host membrane pieces (oracle/_ref/librefhost.so) ---------
+HOST_PATH = os.path.join(_HERE, "_ref", "librefhost.so")
+_hlib = None
+
+
+def host_available():
+    return os.path.exists(HOST_PATH)
+
+
+def hlib():
+    global _hlib
+    if _hlib is None:
+        L_ = C.CDLL(HOST_PATH)
+        vp, i = C.c_void_p, C.c_int
+        L_.refhost_adj.argtypes = [i, i, i, vp, vp, vp]
+        L_.refhost_kantor.argtypes = [C.c_double, C.c_double, i, i, i, vp, i, vp, vp]
+        _hlib = L_
+    return _hlib
+
+
+def host_adj(tri, nv, md):
+    """adj_ini of the reference (src/rbc/adj/imp/ini.h): adj0, adj1 [md nv]."""
+    import numpy as np
+    t4 = _tri4(tri)
+    a0 = np.zeros(md * nv, np.int32)
+    a1 = np.zeros(md * nv, np.int32)
+    assert hlib().refhost_adj(md, len(t4), nv, t4.ctypes.data_as(C.c_void_p), a0.ctypes.data_as(C.c_void_p),
+                              a1.ctypes.data_as(C.c_void_p)) == 0
+    return a0, a1
+
+
+def host_kantor(tri, nv, md, pp, kb, phi_deg=0.0):
+    """The Kantor forces of the cells pp [host (nc*nv, 6)] from the reference's
+    host build of its dihedral forces (FP64): (nc*nv, 3) float64."""
+    import numpy as np
+    t4 = _tri4(tri)
+    pp = np.ascontiguousarray(pp, np.float32)
+    ff = np.zeros((len(pp), 3), np.float64)
+    assert hlib().refhost_kantor(float(phi_deg), float(kb), md, len(t4), nv, t4.ctypes.data_as(C.c_void_p),
+                                 len(pp) // nv, pp.ctypes.data_as(C.c_void_p), ff.ctypes.data_as(C.c_void_p)) == 0
+    return ff

@@ -53,6 +53,9 @@ COPIES = {
     "av.ref.rbc.u.area_volume.dev.0.txt": "src/test_data/av.ref.rbc.u.area_volume.dev.0.txt",
     "rbc.1986.off": "src/data/cells/rbc/1986.off",
     "rbc.642.off": "src/data/cells/rbc/642.off",
+    # the disabled rbc.u.simple test's output: positions and forces x 0.1
+    # (its pipe through uscale 0.1) of two 642-vertex cells
+    "forces.ref.rbc.u.simple.txt": "src/test_data/forces.ref.rbc.u.simple.txt",
 }
 
 

@@ -76,3 +76,35 @@ def test_juelicher_oracle_invariants():
     f2 = oracle.juelicher_forces(F, len(V), two)
     assert np.abs(f2[:len(V)] - f).max() < 1e-12 * scale
     assert 1e-6 < np.abs(f.sum(0)).max() / np.abs(f).sum() < 1e-2
+
+
+def test_rbc_simple_file_not_determined_by_its_inputs():
+    """The reference's disabled rbc.u.simple output (src/test/rbc/u/simple: two
+    642-vertex cells, the template moved by the whole-number shifts of its
+    initial condition data/ic/two and the 16^3 box; positions and forces
+    printed x 0.1 through uscale 0.1).  Rebuilt from the template, the inputs
+    equal the printed positions to their digits.  On them the oracle gives
+    both cells the same forces (to 1e-3 of the largest: the volume term sees
+    absolute positions); the file's two cells differ by almost 3 % -- more
+    than the oracle differs from either of them -- so the file's forces are not
+    a function of its inputs, and the oracle stays within 5 % of them."""
+    import os
+    from ctc_b200 import mesh
+    from .conftest import GOLDEN
+    d = np.loadtxt(os.path.join(GOLDEN, "forces.ref.rbc.u.simple.txt")) * 10.0
+    V, F = mesh.read_off(os.path.join(GOLDEN, "rbc.642.off"))
+    nv = len(V)
+    pp = np.zeros((len(d), 6), np.float32)
+    pp[:nv, :3] = V.astype(np.float32) + np.float32(-8)
+    pp[nv:, :3] = V.astype(np.float32) + np.array([-7, -6, -5], np.float32)
+    assert np.abs(pp[:, :3] - d[:, :3]).max() < 1e-4           # to the printed digits
+    A, Vol = mesh.area_volume(V, F)
+    par = dict(gammaC=30.0, gammaT=90.0, kBT=0.0444, kb=17.78, phi=6.97, ks=14.8, x0=0.5, mpow=2.0, ka=2450.0,
+               kd=100.0, kv=3750.0, totArea=A, totVolume=Vol)
+    f = oracle.rbc_forces(F, nv, pp, par, f64=True)
+    ff = d[:, 3:]
+    fmax = np.abs(ff).max()
+    assert np.abs(f[:nv] - f[nv:]).max() / fmax < 1e-3
+    file_cells = np.abs(ff[:nv] - ff[nv:]).max() / fmax
+    assert file_cells > 2e-2
+    assert np.abs(f - ff).max() / fmax < min(0.05, file_cells)
