@@ -78,37 +78,37 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def bulk_profile_figure(key):
-    """A per-particle figure of one k_dpd_bulk launch from the committed ncu
-    summary (a line "key: X"), or None."""
-    p = os.path.join(ROOT, "profiles", "k_dpd_bulk_p64.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.strip().startswith(key + ":"):
-            return float(line.split(":")[1])
-    return None
+# Per-launch figures of k_dpd_bulk from ncu captures, keyed by the launch
+# shape the autotuner picks (threads per block, candidate loads in flight per
+# lane): warp instructions and DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum) per target particle.  Each entry names the ncu summary
+# under profiles/ it was read from; a shape without an entry has no figures
+# (the line then says so instead of borrowing another instantiation's).
+BULK_NCU = {
+    (256, 4): {"warp_inst_per_particle": 247.6, "dram_bytes_per_particle": 55.80,
+               "source": "profiles/k_dpd_bulk_p64.md: k_dpd_bulk<0,false,256,4,0>, 64^3 box"},
+}
 
 
-def issue_roofline(n, bulk_ms, clk):
+def bulk_ncu(shape):
+    return BULK_NCU.get(tuple(shape))
+
+
+def issue_roofline(n, bulk_ms, clk, shape):
     """Instruction-issue fraction of k_dpd_bulk, the bound it runs into:
-    warp instructions per particle (ncu capture) x particles / the launch's
-    CUDA-event time, against 148 SMs x 4 schedulers x one warp instruction per
-    cycle at the SM clock sampled during the timed region."""
-    ipp = bulk_profile_figure("warp_instructions_per_particle")
-    if not ipp:
-        return None
+    warp instructions per particle (ncu capture of the same launch shape) x
+    particles / the launch's CUDA-event time, against 148 SMs x 4 schedulers x
+    one warp instruction per cycle at the SM clock sampled during the timed
+    region."""
+    fig = bulk_ncu(shape)
+    if not fig:
+        return {"frac": None, "note": "no ncu capture of k_dpd_bulk with %d threads x %d loads" % tuple(shape)}
+    ipp = fig["warp_inst_per_particle"]
     mhz = (clk or {}).get("sm_mhz") or 1965.0
     achieved = ipp * n / (bulk_ms * 1e-3)
     peak = 148 * 4 * mhz * 1e6
     return {"achieved_warp_inst_per_s": achieved, "peak_warp_inst_per_s": peak, "frac": achieved / peak,
-            "warp_inst_per_particle": ipp, "sm_mhz": mhz,
-            "note": "instructions per particle from profiles/k_dpd_bulk_p64.md (ncu, 64^3 box)"}
-
-
-def bulk_traffic_per_particle():
-    """DRAM bytes per particle of one k_dpd_bulk launch (ncu capture)."""
-    return bulk_profile_figure("traffic_bytes_per_particle")
+            "warp_inst_per_particle": ipp, "sm_mhz": mhz, "shape": list(shape), "source": fig["source"]}
 
 
 class Clocks:
@@ -358,7 +358,9 @@ def run_ours(args, cfg, world, rank, local):
     hbm, peak_kind = peaks()
     bulk_ms = phases["bulk"]
     achieved = PAIR_BYTES * n / (bulk_ms * 1e-3) / 1e9
-    traffic = bulk_traffic_per_particle()
+    shape = (tuned[0], tuned[1])
+    fig = bulk_ncu(shape)
+    traffic = fig["dram_bytes_per_particle"] if fig else None
     # seeds, 6 cell-list kernels, fragment starts, 2 halo packing kernels, bulk, halo, update; with
     # membranes also cell wrap, FSI seeds, 4 image-list kernels, FSI, area/volume, membrane forces,
     # vertex update; contact adds its seeds, 6 vertex cell-list kernels and the pair kernel
@@ -382,6 +384,8 @@ def run_ours(args, cfg, world, rank, local):
         "roofline": {"bound": "hbm", "kernel": "k_dpd_bulk", "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic * n if traffic else None,
+                     "traffic_source": fig["source"] if fig else
+                     "no ncu capture of k_dpd_bulk with %d threads x %d loads" % shape,
                      "peak_kind": peak_kind + " (copy bandwidth)",
                      "algorithmic_bytes_per_particle": PAIR_BYTES,
                      "fp32": {"achieved_tflops": PAIR_FLOP * n / (bulk_ms * 1e-3) / 1e12,
@@ -389,7 +393,7 @@ def run_ours(args, cfg, world, rank, local):
                               "frac": PAIR_FLOP * n / (bulk_ms * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS,
                               "note": "~%d flop per particle (100 per accepted half-pair, 20.94 half-pairs)"
                                       % PAIR_FLOP},
-                     "issue": issue_roofline(n, bulk_ms, clk)},
+                     "issue": issue_roofline(n, bulk_ms, clk, shape)},
         "e2e": {"value": e2e_value, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": state_bytes / args.steps,
                 "d2h_bytes_per_step": 40 + state_bytes / args.steps},

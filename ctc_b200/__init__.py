@@ -537,6 +537,12 @@ class Sim:
         check(lib().ctc_sim_tune(self.h, int(reps), ch, _stream(stream)))
         return tuple(ch)
 
+    def set_tune(self, choice):
+        """Launch shapes of the pair kernels (bulk threads, bulk loads in
+        flight, halo threads, halo loads), as tune() returns them."""
+        ch = (C.c_int * 4)(*[int(x) for x in choice])
+        check(lib().ctc_sim_set_tune(self.h, ch))
+
     def set_membrane_noise(self, enable=True, seed=0):
         """The membrane random force (rbc_force_set_rnd1) from the next step on."""
         check(lib().ctc_sim_set_membrane_noise(self.h, int(bool(enable)), int(seed) & 0xffffffff))
@@ -608,6 +614,35 @@ class Sim:
         s = (C.c_float * 27)()
         check(lib().ctc_sim_next_seeds(self.h, s))
         return np.array(s[:], np.float32)
+
+    def forces(self):
+        """Copies of the last step's force arrays: the solvent's (cell-sorted,
+        (n, 3)) and the membrane vertices' ((nc*nv, 3), empty without
+        membranes), as device tensors."""
+        torch = _torch()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        fp = C.c_void_p()
+        check(lib().ctc_sim_state(self.h, None, None, C.byref(fp), None))
+        n = int(self.get_count())
+        fs = _wrap_dev(fp.value, 4 * n, torch.float32, dev).reshape(n, 4)[:, :3].contiguous()
+        nc, nv = C.c_int(0), C.c_int(0)
+        check(lib().ctc_sim_membrane_count(self.h, C.byref(nc), C.byref(nv)))
+        nvt = nc.value * nv.value
+        fv = torch.zeros((0, 3), dtype=torch.float32, device=dev)
+        if nvt > 0:
+            mp = C.c_void_p()
+            check(lib().ctc_sim_membrane_state(self.h, None, None, C.byref(mp)))
+            fv = _wrap_dev(mp.value, 4 * nvt, torch.float32, dev).reshape(nvt, 4)[:, :3].contiguous()
+        return fs, fv
+
+    def get_count(self):
+        """Solvent particles in the box (device count of the last build)."""
+        st = C.c_void_p()
+        check(lib().ctc_sim_state(self.h, None, None, None, C.byref(st)))
+        torch = _torch()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        nc = self.L[0] * self.L[1] * self.L[2]
+        return int(_wrap_dev(st.value + 4 * nc, 1, torch.int32, dev).item())
 
     def profile(self, enable=True):
         """Record per-phase CUDA events on every following step."""

@@ -79,6 +79,8 @@ SIGNATURES = {
     "ctc_fluforces_halo_apply": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, vp, vp, vp, vp]),
     "ctc_fluforces_apply_seeded": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, vp, vp, fp, C.c_int,
                                              C.c_int, vp, vp]),
+    "ctc_fluforces_halo_frags": (C.c_int, [vp, vp, ip, vp, vp, vp, vp, vp, vp]),
+    "ctc_fluforces_halo_frags_seeded": (C.c_int, [vp, vp, ip, vp, vp, vp, vp, fp, vp, vp]),
     "ctc_rbc_force_ini": (C.c_int, [C.c_int, C.c_int, vp, C.c_int, C.POINTER(vp)]),
     "ctc_rbc_force_fin": (C.c_int, [vp]),
     "ctc_rbc_force_md": (C.c_int, [vp, ip]),
@@ -130,11 +132,14 @@ SIGNATURES = {
     "ctc_wall_repulse": (C.c_int, [vp, C.c_float, C.c_int, vp, vp, vp]),
     "ctc_rbc_force_set_rnd": (C.c_int, [vp, C.c_int, C.c_uint]),
     "ctc_sim_tune": (C.c_int, [vp, C.c_int, ip, vp]),
+    "ctc_sim_set_tune": (C.c_int, [vp, ip]),
     "ctc_fsi_ini": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]),
     "ctc_fsi_fin": (C.c_int, [vp]),
     "ctc_fsi_apply": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, C.c_int, vp, vp, vp, vp, vp, vp]),
     "ctc_fsi_apply_seeded": (C.c_int, [vp, C.POINTER(DpdParams), C.c_int, vp, C.c_int, vp, vp, vp, C.c_float,
                                        C.c_float, C.c_int, vp, vp, vp]),
+    "ctc_fsi_pairs": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, C.c_float, vp, vp, vp]),
+    "ctc_fsi_next_seed": (C.c_int, [vp, fp]),
     "ctc_scheme_move_apply": (C.c_int, [C.c_float, C.c_float, C.c_int, vp, vp, vp]),
     "ctc_scheme_move_clear_vel": (C.c_int, [C.c_int, vp, vp]),
     "ctc_bforce_apply_cste": (C.c_int, [C.c_float, fp, C.c_int, vp, vp]),
@@ -150,6 +155,7 @@ SIGNATURES = {
     "ctc_sim_get_solvent": (C.c_int, [vp, vp, ip, vp]),
     "ctc_sim_diag": (C.c_int, [vp, C.POINTER(C.c_double), vp]),
     "ctc_sim_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+    "ctc_sim_membrane_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
     "ctc_sim_next_seeds": (C.c_int, [vp, fp]),
     "ctc_sim_profile": (C.c_int, [vp, C.c_int]),
     "ctc_sim_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), ip]),

@@ -2,6 +2,7 @@
 // the reference's clist / fluforces / scheme modules, and the fast-path
 // plain-DPD system.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -225,6 +226,42 @@ extern "C" int ctc_fluforces_halo_apply(ctc_fluforces *f, const ctc_dpd_params *
     for (int i = 0; i < 26; i++) seeds[1 + i] = kiss_get(&f->halo[i]);  // halo_prepare draws all 26
     if (n <= 0) return CTC_OK;
     return ctc_fluforces_apply_seeded(f, p, n, pp, starts, counts, seeds, 2, CTC_RNG_REFERENCE, ff, stream);
+}
+
+extern "C" int ctc_fluforces_halo_frags_seeded(ctc_fluforces *f, const ctc_dpd_params *p, const int *ln,
+                                               const float *const *lpp, const int *const *lii,
+                                               const float *const *rpp, const int *const *rstart,
+                                               const float *seeds26, float *ff, void *stream) {
+    if (!f || !p || !ln || !seeds26) return fail(CTC_ERR_ARG, "ctc_fluforces_halo_frags: bad arguments");
+    HaloFrags H;
+    memset(&H, 0, sizeof(H));
+    long tot = 0;
+    for (int i = 0; i < 26; i++) {
+        if (ln[i] < 0 || (ln[i] > 0 && (!lpp || !lii || !rpp || !rstart || !lpp[i] || !lii[i] || !rstart[i] || !ff)))
+            return fail(CTC_ERR_ARG, "ctc_fluforces_halo_frags: fragment %d: bad arguments", i);
+        H.loff[i] = (int)tot;
+        tot += ln[i];
+        if (ln[i] > 0) {
+            H.lpp[i] = lpp[i]; H.lii[i] = lii[i]; H.rpp[i] = rpp[i]; H.rstart[i] = rstart[i];
+        }
+        H.seeds[i] = seeds26[i];
+    }
+    if (tot > INT_MAX) return fail(CTC_ERR_CAPACITY, "ctc_fluforces_halo_frags: %ld boundary particles", tot);
+    H.loff[26] = (int)tot;
+    H.masks = halo_masks();
+    DpdPar P;
+    P.a = p->a; P.g = p->g; P.s = p->s; P.spow = p->spow;
+    CUDA_TRY(halo_frags_launch(f->L, P, H, ff, 3, dev_err_ptr(), (cudaStream_t)stream));
+    return CTC_OK;
+}
+
+extern "C" int ctc_fluforces_halo_frags(ctc_fluforces *f, const ctc_dpd_params *p, const int *ln,
+                                        const float *const *lpp, const int *const *lii, const float *const *rpp,
+                                        const int *const *rstart, float *ff, void *stream) {
+    if (!f) return fail(CTC_ERR_ARG, "null module");
+    float seeds[26];
+    for (int i = 0; i < 26; i++) seeds[i] = kiss_get(&f->halo[i]);   // halo_prepare draws all 26
+    return ctc_fluforces_halo_frags_seeded(f, p, ln, lpp, lii, rpp, rstart, seeds, ff, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -834,6 +871,21 @@ extern "C" int ctc_sim_step(ctc_sim *s, int nsteps, void *stream) {
 
 // times the pair kernels (bulk, halo) of every launch shape on the cell
 // lists of the current state, without advancing it, and keeps the fastest
+extern "C" int ctc_sim_set_tune(ctc_sim *s, const int *choice) {
+    if (!s || !choice) return fail(CTC_ERR_ARG, "ctc_sim_set_tune: bad arguments");
+    DpdTune t;
+    t.bulk_threads = choice[0]; t.bulk_unroll = choice[1]; t.halo_threads = choice[2]; t.halo_unroll = choice[3];
+    bool ok_t = false, ok_u = false, ok_h = false, ok_hu = false;
+    for (int v : DPD_TUNE_BULK_T) ok_t |= v == t.bulk_threads;
+    for (int v : DPD_TUNE_BULK_U) ok_u |= v == t.bulk_unroll;
+    for (int v : DPD_TUNE_HALO_T) ok_h |= v == t.halo_threads;
+    for (int v : DPD_TUNE_HALO_U) ok_hu |= v == t.halo_unroll;
+    if (!ok_t || !ok_u || !ok_h || !ok_hu) return fail(CTC_ERR_ARG, "ctc_sim_set_tune: unknown launch shape");
+    sim_drop_graphs(s);
+    s->tune = t;
+    return CTC_OK;
+}
+
 extern "C" int ctc_sim_tune(ctc_sim *s, int reps, int *choice, void *stream) {
     if (!s || reps <= 0) return fail(CTC_ERR_ARG, "ctc_sim_tune: bad arguments");
     if (!s->built) return fail(CTC_ERR_ARG, "ctc_sim_tune: step once first");
@@ -959,6 +1011,14 @@ extern "C" int ctc_sim_state(ctc_sim *s, float **pos, float **vel, float **force
     if (vel) *vel = (float*)s->vel[s->cur];
     if (force) *force = (float*)s->force;
     if (starts) *starts = s->starts;
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_membrane_state(ctc_sim *s, float **pos, float **vel, float **force) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sim_membrane_state: null");
+    if (pos) *pos = (float*)s->mpos;
+    if (vel) *vel = (float*)s->mvel;
+    if (force) *force = (float*)s->mforce;
     return CTC_OK;
 }
 

@@ -315,6 +315,33 @@ extern "C" int ctc_fsi_apply(ctc_fsi *f, const ctc_dpd_params *p, int nv, const 
     return ctc_fsi_apply_seeded(f, p, nv, pv, ns, ps, starts, counts, sb, sh, CTC_RNG_REFERENCE, fv, fs, stream);
 }
 
+extern "C" int ctc_fsi_next_seed(ctc_fsi *f, float *seed) {
+    if (!f || !seed) return fail(CTC_ERR_ARG, "ctc_fsi_next_seed: bad arguments");
+    *seed = kiss_get4(&f->trunk);
+    return CTC_OK;
+}
+
+extern "C" int ctc_fsi_pairs(ctc_fsi *f, const ctc_dpd_params *p, int n, const float *pv, int ns, const float *ps,
+                             const int *starts, const int *counts, float seed, float *fv, float *fs, void *stream) {
+    if (!f || !p || n < 0 || ns < 0 || (n > 0 && (!pv || !fv)) || (ns > 0 && (!ps || !starts || !fs)))
+        return fail(CTC_ERR_ARG, "ctc_fsi_pairs: bad arguments");
+    if (n > f->maxv || ns > f->maxs) return fail(CTC_ERR_CAPACITY, "fsi: %d particles / %d solvent over capacity", n, ns);
+    if (n == 0 || ns == 0) return CTC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(aos_to_soa(ns, ps, f->spos, f->svel, st));
+    FsiArgs A;
+    memset(&A, 0, sizeof(A));
+    A.L = f->L; A.nv = n; A.pv = pv; A.vv = pv + 3; A.pstride = 6;
+    A.spos = f->spos; A.svel = f->svel; A.starts = starts; A.counts = counts;
+    A.fv = fv; A.fstride = 3; A.fs = fs; A.sstride = 3;
+    A.par.a = p->a; A.par.g = p->g; A.par.s = p->s; A.par.spow = p->spow;
+    A.seed_bulk = seed;
+    A.err = dev_err_ptr();
+    A.no_wrap = 1;
+    CUDA_TRY(fsi_launch(A, CTC_RNG_REFERENCE, st));
+    return CTC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // membrane-membrane contact (src/cnt/imp.h)
 // ---------------------------------------------------------------------------

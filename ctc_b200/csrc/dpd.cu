@@ -429,6 +429,73 @@ __device__ __forceinline__ void halo_run(const DpdArgs &A, const int ia, const u
     if (qn > 0) process(qn);
 }
 
+// halo pairs from exchanged fragments (the reference's data model of
+// fhalo_dev::apply, src/fluforces/halo/dev/main.h + map.h): one (fragment,
+// local particle) per thread over all 26 fragments; the remote window is
+// r2map's (rows of `cols` consecutive fragment cells, `jump` apart) on the
+// unshifted local position, the local particle then moved into the remote
+// frame by -d L; only the local particle takes the force
+__global__ void k_dpd_halo_frags(int3 L, DpdPar P, const __grid_constant__ HaloFrags H, float *ff, int fstride,
+                                 int *err) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= H.loff[26]) return;
+    int fid = 0;
+    while (fid < 25 && H.loff[fid + 1] <= t) fid++;
+    const int i = t - H.loff[fid];
+    const float *a = H.lpp[fid] + 6 * (size_t)i;
+    float4 pa = make_float4(a[0], a[1], a[2], 0.0f);
+    const float4 va = make_float4(a[3], a[4], a[5], 0.0f);
+    const int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
+    const int xc = dx == 0 ? L.x : 1, yc = dy == 0 ? L.y : 1, zc = dz == 0 ? L.z : 1;
+    int xs = 1, ys = 1, zs = 1, l, id = 0;
+    if (dz == 0) { r2size_dev(pa.z, zc, L.z, l, zs); id += l; }
+    id *= yc;
+    if (dy == 0) { r2size_dev(pa.y, yc, L.y, l, ys); id += l; }
+    id *= xc;
+    if (dx == 0) { r2size_dev(pa.x, xc, L.x, l, xs); id += l; }
+    int rows, cols, jump;
+    const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+    if (nz == 1) {
+        if (dx) { rows = zs; cols = ys; jump = yc; }
+        else if (dy) { rows = zs; cols = xs; jump = xc; }
+        else { rows = ys; cols = xs; jump = xc; }
+    } else if (nz == 2) {
+        rows = jump = 1;
+        cols = max(xs, max(ys, zs));
+    } else {
+        rows = cols = jump = 1;
+    }
+    const int ncf = xc * yc * zc;                         // remote fragment cells
+    pa.x -= (float)(dx * L.x);
+    pa.y -= (float)(dy * L.y);
+    pa.z -= (float)(dz * L.z);
+    const bool mask = (H.masks >> fid) & 1u;
+    const float seed = H.seeds[fid];
+    const float *rpp = H.rpp[fid];
+    const int *rs = H.rstart[fid];
+    float3 acc = make_float3(0.0f, 0.0f, 0.0f);
+    for (int r = 0; r < rows; r++) {
+        const int c0 = id + r * jump;
+        if (c0 < 0 || c0 + cols > ncf) { set_error(err, DEV_BAD_PARTICLE); continue; }
+        const int j0 = __ldg(rs + c0), j1 = __ldg(rs + c0 + cols);
+        for (int j = j0; j < j1; j++) {
+            const float *b = rpp + 6 * (size_t)j;
+            const float4 pb = make_float4(b[0], b[1], b[2], 0.0f), vb = make_float4(b[3], b[4], b[5], 0.0f);
+            const float rnd = mean0var1uu(seed, mask ? (unsigned)i : (unsigned)j, mask ? (unsigned)j : (unsigned)i);
+            float3 f;
+            if (dpd_force(P, pa, va, pb, vb, rnd, f)) { acc.x += f.x; acc.y += f.y; acc.z += f.z; }
+        }
+    }
+    red_force(ff, fstride, __ldg(H.lii[fid] + i), 1.0f, acc);
+}
+
+cudaError_t halo_frags_launch(int3 L, const DpdPar &P, const HaloFrags &H, float *ff, int fstride, int *err,
+                              cudaStream_t st) {
+    const int n = H.loff[26];
+    if (n > 0) k_dpd_halo_frags<<<ceil_div(n, 128), 128, 0, st>>>(L, P, H, ff, fstride, err);
+    return cudaGetLastError();
+}
+
 // one local particle per thread, every fragment of its cell
 template <int RNG, bool BATCH, int T, int MODE = 0>
 __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs A) {

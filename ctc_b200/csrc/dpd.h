@@ -70,6 +70,25 @@ cudaError_t halo_pack_boxes_launch(const DpdArgs &A, const int *coff, int nseg, 
 // nseg = 26 (one box) or 26 nbox (A.B)
 cudaError_t halo_packed_launch(const DpdArgs &A, const int *pack, const int *pack_off, int cap, int rng_mode,
                                cudaStream_t st, int nseg = 26, const DpdTune &tune = DpdTune());
+// halo pairs from exchanged fragments (fluforces_halo_prepare/apply,
+// src/fluforces/halo): for fragment fid, the local boundary particles
+// lpp[fid] (AoS, 6 floats, ln = loff[fid+1] - loff[fid] of them, packed as the
+// exchange packs them) whose forces go to ff[lii[fid][i]], and the remote
+// fragment received from direction fid: particles rpp[fid] (AoS) and its
+// fragment-cell starts rstart[fid] (the neighbour's boundary layer, cells
+// x-fastest); keys mean0var1uu(seeds[fid], mask ? i : j, mask ? j : i) of the
+// two fragment-local indices
+struct HaloFrags {
+    const float *lpp[26];
+    const int *lii[26];
+    const float *rpp[26];
+    const int *rstart[26];
+    int loff[27];
+    float seeds[26];
+    unsigned masks;
+};
+cudaError_t halo_frags_launch(int3 L, const DpdPar &P, const HaloFrags &H, float *ff, int fstride, int *err,
+                              cudaStream_t st);
 // vector-Jacobian product of the bulk (which & 1) and halo (which & 2) pair
 // forces, stable keys, one box
 cudaError_t dpd_vjp_launch(const DpdArgs &A, int nmax, cudaStream_t st);

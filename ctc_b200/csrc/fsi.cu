@@ -438,11 +438,12 @@ __global__ void __launch_bounds__(FSIQ_T) k_fsi_q(const __grid_constant__ FsiArg
                 const int wx = gx < 0 ? -1 : (gx >= L.x ? 1 : 0);
                 const int wy = gy < 0 ? -1 : (gy >= L.y ? 1 : 0);
                 const int wz = gz < 0 ? -1 : (gz >= L.z ? 1 : 0);
+                if (A.no_wrap && (wx | wy | wz)) continue;
                 gx -= wx * L.x; gy -= wy * L.y; gz -= wz * L.z;
                 if (gx < 0 || gx + ncell > L.x || gy < 0 || gy >= L.y || gz < 0 || gz >= L.z) continue;
                 const int cid = gx + L.x * (gy + L.y * gz);
                 j = __ldg(starts + cid);
-                e = ncell == 3 ? __ldg(starts + cid + 3) : j + __ldg(counts + cid);
+                e = ncell == 3 ? __ldg(starts + cid + 3) : (counts ? j + __ldg(counts + cid) : __ldg(starts + cid + 1));
                 halo = (wx | wy | wz) != 0;
                 a = pa;
                 aid = (unsigned)vk;

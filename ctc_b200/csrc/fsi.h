@@ -33,6 +33,10 @@ struct FsiArgs {
     // each walked in a spatially coherent order of the template); null: t
     const int *vperm;
     int vperm_n;
+    // the cells of the box only, no periodic wrap (fsi_dev::bulk's map,
+    // src/fsi/dev/map/bulk.h): the pair pass of ctc_fsi_pairs over vertices or
+    // over images the caller lists
+    int no_wrap;
 };
 
 // ints of the count buffer of fsi_images_launch: 26 per box with B.nbox > 0;

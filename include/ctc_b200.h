@@ -131,6 +131,25 @@ int ctc_fluforces_bulk_apply(ctc_fluforces *f, const ctc_dpd_params *p, int n, c
  * fragment seeds and adds the forces of the pairs across the periodic faces */
 int ctc_fluforces_halo_apply(ctc_fluforces *f, const ctc_dpd_params *p, int n, const float *pp,
                              const int *starts, const int *counts, float *ff, void *stream);
+/* fluforces_halo_prepare + fluforces_halo_apply (src/fluforces/imp/main.h:23-37,
+ * src/fluforces/halo/imp/main.h:49-101) on the fragments of the exchange
+ * (flu::LFrag26, flu::RFrag26 of src/flu/type.h): for fragment fid, ln[fid]
+ * local boundary particles lpp[fid] [dev, AoS, packed as the exchange packs
+ * them] whose forces are added to ff[lii[fid][i]] [dev, AoS], against the
+ * remote fragment received from direction fid -- particles rpp[fid] [dev,
+ * AoS] and its fragment-cell starts rstart[fid] [dev, cells + 1] -- with
+ * the local particle moved by -d(fid) L; lpp, lii, rpp, rstart are host
+ * arrays of 26 device pointers.  Draws the 26 fragment seeds from the
+ * module's trunks; keys mean0var1uu(seed, mask ? i : j, mask ? j : i) of the
+ * fragment-local indices.  Works for any source of the remote fragments: a
+ * periodic box's own boundary layer, or a neighbouring rank's. */
+int ctc_fluforces_halo_frags(ctc_fluforces *f, const ctc_dpd_params *p, const int *ln, const float *const *lpp,
+                             const int *const *lii, const float *const *rpp, const int *const *rstart, float *ff,
+                             void *stream);
+/* the same with explicit seeds [host, 26] */
+int ctc_fluforces_halo_frags_seeded(ctc_fluforces *f, const ctc_dpd_params *p, const int *ln,
+                                    const float *const *lpp, const int *const *lii, const float *const *rpp,
+                                    const int *const *rstart, const float *seeds26, float *ff, void *stream);
 /* both in one launch with explicit seeds: seeds[0] bulk, seeds[1 + fid]
  * fragment fid [host]; which: 1 bulk, 2 halo, 3 both; rng: CTC_RNG_* */
 int ctc_fluforces_apply_seeded(ctc_fluforces *f, const ctc_dpd_params *p, int n, const float *pp,
@@ -183,6 +202,20 @@ int ctc_fsi_apply(ctc_fsi *f, const ctc_dpd_params *p, int nv, const float *pv, 
 int ctc_fsi_apply_seeded(ctc_fsi *f, const ctc_dpd_params *p, int nv, const float *pv, int ns, const float *ps,
                          const int *starts, const int *counts, float seed_bulk, float seed_halo, int rng,
                          float *fv, float *fs, void *stream);
+
+/* fsi_bulk of one object type (src/fsi/imp/bulk.h:1-42), or fsi_halo of its
+ * periodic images (src/fsi/imp/halo.h:1-33): the n particles pv [dev, AoS] --
+ * the vertices, or the images the object exchange delivered, packed fragment
+ * after fragment -- against the ns cell-sorted solvent particles ps [dev,
+ * AoS] with their cell starts (starts[LX*LY*LZ] = ns) and counts (may be NULL:
+ * taken from starts), in the cells of the box only (the map of
+ * src/fsi/dev/map/bulk.h, no periodic wrap), keys mean0var1uu(seed, index in
+ * pv, solvent index); forces accumulated into fv [dev, AoS, n] and, as
+ * reactions, fs [dev, AoS, ns] */
+int ctc_fsi_pairs(ctc_fsi *f, const ctc_dpd_params *p, int n, const float *pv, int ns, const float *ps,
+                  const int *starts, const int *counts, float seed, float *fv, float *fs, void *stream);
+/* the next draw of the module's trunk (rnd_get of src/fsi/imp/{bulk,halo}.h) */
+int ctc_fsi_next_seed(ctc_fsi *f, float *seed);
 
 /* ---- membrane-membrane contact: replaces src/cnt/imp.h ------------------- */
 /* PairDPDLJ {a, g, s, spow, ljs, lje} (src/pair/type.h:22-25): DPD plus a
@@ -354,6 +387,9 @@ int ctc_sim_set_graph(ctc_sim *s, int enable);
  * (as ctc_batch_tune) reps times on the current state without advancing it
  * (after at least one step), keeps the fastest; choice [host, 4] or NULL */
 int ctc_sim_tune(ctc_sim *s, int reps, int *choice, void *stream);
+/* sets the launch shapes of the pair kernels directly (choice as ctc_sim_tune
+ * returns it); CTC_ERR_ARG for a shape the tuner does not offer */
+int ctc_sim_set_tune(ctc_sim *s, const int *choice);
 /* number of solvent particles (synchronises the stream) */
 int ctc_sim_count(ctc_sim *s, int *n, void *stream);
 /* red-blood-cell membranes of the system: nc cells of one template (nv
@@ -400,8 +436,13 @@ int ctc_sim_get_solvent(ctc_sim *s, float *pp, int *n, void *stream);
 /* total momentum (3), kinetic temperature, count -- FP64 reductions on the
  * device (replaces diag_part_apply, src/io/diag/part/imp/main.h:37-68) */
 int ctc_sim_diag(ctc_sim *s, double *out5, void *stream);
-/* device pointers of the current state (cell-sorted float4 SoA) */
+/* device pointers of the current state (cell-sorted float4 SoA); force holds
+ * the last step's solvent forces (pairs, walls, FSI reactions) */
 int ctc_sim_state(ctc_sim *s, float **pos, float **vel, float **force, const int **starts);
+/* device pointers of the membranes' state (float4 SoA, cell c vertex v at
+ * c*nv + v); force holds the last step's vertex forces (walls, FSI, contact,
+ * internal) */
+int ctc_sim_membrane_state(ctc_sim *s, float **pos, float **vel, float **force);
 /* current bulk seed and 26 halo seeds of the next step [host, 27 floats] */
 int ctc_sim_next_seeds(const ctc_sim *s, float *seeds27);
 /* per-phase device timing: when enabled every step records CUDA events on

@@ -305,3 +305,43 @@ def test_bulk_kernel_golden(case):
                                         np.zeros(27, np.float32), ff, which=1)
     assert match_bulk(out.cpu().numpy(), ff.cpu().numpy(), g) < 1e-5
     assert C.device_error() == 0
+
+
+ALL_SHAPES = [(bt, bu, ht, hu) for bt in (128, 256) for bu in (2, 4, 8) for ht in (64, 128, 256) for hu in (2, 4)]
+
+
+def test_sim_every_launch_shape_vs_modules():
+    """Every launch shape the autotuner can pick for the fused step's pair
+    kernels (bulk threads x loads in flight, halo threads x loads in flight;
+    the C2 bench's 128 x 8 among them) gives the module entry points' forces
+    within 1e-5 on the same state and seeds."""
+    C = ctc()
+    L = (16, 12, 10)
+    pp = systems.solvent(L, seed=95)
+    n = len(pp)
+    dpd = C.DpdParams(*systems.dpd_params())
+    out, starts, counts, ids = C.Clist(L, n).build(dev(pp))
+    sim = C.Sim(L, n, dpd)
+    for shape in ALL_SHAPES:
+        sim.set_solvent(pp)
+        sim.set_tune(shape)
+        seeds = sim.next_seeds()
+        sim.step(1)
+        f = sim.forces()[0].cpu().numpy()
+        ff = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        C.FluForces(L, n).apply_seeded(dpd, out, starts, counts, seeds, ff, which=3)
+        ref = ff.cpu().numpy()
+        fn = np.abs(ref).max(1)
+        err = np.abs(f - ref).max(1) / np.maximum(fn, 0.1 * fn.mean())
+        assert err.max() < 1e-5, (shape, err.max())
+    assert C.device_error() == 0
+    sim.close()
+
+
+def test_sim_set_tune_rejects_unknown_shape():
+    C = ctc()
+    from ctc_b200 import _lib
+    sim = C.Sim((8, 8, 8), 5120, C.DpdParams(*systems.dpd_params()))
+    with pytest.raises(_lib.CtcError):
+        sim.set_tune((96, 4, 128, 2))
+    sim.close()

@@ -94,3 +94,89 @@ def test_sim_tune_leaves_state():
     assert np.array_equal(out[0][1], out[1][1])
     assert np.abs(out[0][0] - out[1][0]).max() < 1e-4
     assert C.device_error() == 0
+
+
+def _rel_err(f, ref):
+    f = np.asarray(f, np.float64).reshape(-1, 3)
+    ref = np.asarray(ref, np.float64).reshape(-1, 3)
+    mag = np.abs(ref).max(1)
+    act = mag[mag > 0]
+    floor = 0.1 * act.mean() if len(act) else 1.0
+    return float((np.abs(f - ref).max(1) / np.maximum(mag, floor)).max())
+
+
+@pytest.mark.parametrize("case", ["membranes", "contact", "walls"])
+def test_fused_step_forces_vs_modules(case):
+    """The force arrays of one fused step -- the solvent's (bulk + halo pairs,
+    wall forces, FSI reactions) and the vertices' (wall forces and repulsion,
+    FSI, contact, internal membrane forces on top) -- against the module entry
+    points composed in the reference's order on the same state and seeds
+    (each module held to the reference's own kernels at 1e-5): within 1e-5
+    relative, max-norm per particle, so that no force term of the fused step
+    can be dropped or doubled unseen."""
+    import os
+
+    import ctc_b200 as C
+    from .test_gpu_wall import SDF
+    L = (16, 16, 16)
+    dpd = systems.dpd_params()
+    fsi = C.DpdParams(0.0, 8.0, dpd[2], 0.25)
+    cnt = C.DpdLjParams(2.6666667, 8.0, dpd[2], 0.25, 0.3, 0.44)
+    ps0 = systems.solvent(L, seed=101)
+    pv, tri, par = systems.rbc_system(L, 2, seed=102)
+    nv = len(pv) // 2
+    sim = C.Sim(L, len(ps0), C.DpdParams(*dpd), mass=1.0, dt=systems.DT)
+    sim.set_solvent(ps0)
+    lam = 3.0
+    if case == "walls":
+        from ctc_b200 import mesh
+        sdf = C.Sdf(L, path=os.path.join(SDF, "wall.dat"))
+        wall = C.Wall(sdf, ps0)                           # the same freezing as the step's
+        ps = wall.bulk
+        sim.set_walls(sdf, C.wvel("cste"), lam=lam)
+        assert np.array_equal(sim.get_solvent(), ps)
+        X, F = mesh.rbc_template()                        # one cell in the channel, near a plate
+        pv = np.zeros((len(X), 6), np.float32)
+        pv[:, :3] = X
+        pv[:, 2] += 4.2
+        pv[:, 3:] = np.random.default_rng(103).normal(0, 0.3, (len(X), 3))
+        tri, nv = F, len(X)
+        A, V = mesh.area_volume(X, F)
+        par = systems.rbc_params(A, V)
+    else:
+        ps = ps0
+        pv[:nv, 0] += L[0] / 2 - pv[:nv, 0].max() + 1.0  # one cell across the +x face
+        pv = oracle.rbc_wrap(L, pv, nv)                   # as the step's objects_distribute leaves it
+    sim.set_membranes(pv, tri, nv, par, fsi, mass=systems.RBC_MASS)
+    if case == "contact":
+        pv[nv:, 2] = pv[:nv, 2] + 0.5                     # the second cell on top of the first
+        pv[nv:, :2] = pv[:nv, :2]
+        pv = oracle.rbc_wrap(L, pv, nv)
+        sim.set_membranes(pv, tri, nv, par, fsi, mass=systems.RBC_MASS)
+        sim.set_contact(cnt)
+    seeds = sim.next_seeds()
+    kf = oracle.Kiss(1908, 1409, 290, 12968)
+    kc = oracle.Kiss(7119, 187, 18278, 15674)
+    kw = oracle.Kiss(42, 42, 42, 42)
+    sim.step(1)
+    fs_step, fv_step = sim.forces()
+    # the module entry points on the step's input state
+    out, starts, counts, ids = C.Clist(L, len(ps)).build(torch.as_tensor(ps, device="cuda"))
+    fs = torch.zeros((len(ps), 3), device="cuda")
+    fv = torch.zeros((len(pv), 3), device="cuda")
+    P = torch.as_tensor(pv, device="cuda")
+    C.FluForces(L, len(ps)).apply_seeded(C.DpdParams(*dpd), out, starts, counts, seeds, fs, which=3)
+    if case == "walls":
+        wall.force(C.DpdParams(*dpd), out, fs, seed=kw.get())
+        wall.force(fsi, P, fv, seed=kw.get())
+        wall.repulse(lam, P, fv)
+    C.Fsi(L, len(pv), len(ps)).apply_seeded(fsi, P, out, starts, counts, kf.get(), kf.get(), fv, fs)
+    if case == "contact":
+        C.Contact(L, len(pv)).apply_seeded(cnt, P, kc.get(), kc.get(), fv)
+    C.RbcForce(tri, nv, len(pv) // nv).apply(C.RbcParams(**par), P, fv)
+    torch.cuda.synchronize()
+    assert C.device_error() == 0
+    assert fv.abs().max().item() > 1.0 and fs.abs().max().item() > 1.0
+    assert _rel_err(fs_step.cpu().numpy(), fs.cpu().numpy()) < 1e-5
+    assert _rel_err(fv_step.cpu().numpy(), fv.cpu().numpy()) < 1e-5
+    sim.close()
