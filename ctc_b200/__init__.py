@@ -132,6 +132,22 @@ class FluForces:
         check(lib().ctc_fluforces_apply_seeded(self.h, C.byref(params), int(pp.shape[0]), _ptr(pp), _ptr(starts),
                                                _ptr(counts), sd, int(which), int(rng), _ptr(ff), _stream(stream)))
 
+    def halo_frags(self, params, lpp, lii, rpp, rstart, ff, seeds26=None, stream=None):
+        """fluforces_halo_prepare + _apply on exchanged fragments: lists of 26
+        device tensors -- local fragment particles lpp[f] (n, 6), their indices
+        lii[f] into ff, remote fragment particles rpp[f] (m, 6) and its cell
+        starts rstart[f]; seeds26 None draws the module's trunks."""
+        def ptrs(ts):
+            return (C.c_void_p * 26)(*[t.data_ptr() if t is not None and t.numel() else None for t in ts])
+        ln = (C.c_int * 26)(*[int(t.shape[0]) for t in lpp])
+        keep = (ptrs(lpp), ptrs(lii), ptrs(rpp), ptrs(rstart))
+        if seeds26 is None:
+            check(lib().ctc_fluforces_halo_frags(self.h, C.byref(params), ln, *keep, _ptr(ff), _stream(stream)))
+        else:
+            sd = (C.c_float * 26)(*[float(x) for x in np.asarray(seeds26, np.float32).reshape(-1)[:26]])
+            check(lib().ctc_fluforces_halo_frags_seeded(self.h, C.byref(params), ln, *keep, sd, _ptr(ff),
+                                                        _stream(stream)))
+
 
 def RbcParams(**kw):
     """RbcParams_v (src/rbc/params/imp.h:3-9) from keyword fields."""
@@ -203,6 +219,19 @@ class Fsi:
         check(lib().ctc_fsi_apply_seeded(self.h, C.byref(params), int(pv.shape[0]), _ptr(pv), int(ps.shape[0]),
                                          _ptr(ps), _ptr(starts), _ptr(counts), float(seed_bulk), float(seed_halo),
                                          int(rng), _ptr(fv), _ptr(fs), _stream(stream)))
+
+    def pairs(self, params, pv, ps, starts, counts, seed, fv, fs, stream=None):
+        """fsi_bulk of the vertices pv, or fsi_halo of the images pv listed by
+        the object exchange: the cells of the box only, keys (seed, index in pv,
+        solvent index)."""
+        check(lib().ctc_fsi_pairs(self.h, C.byref(params), int(pv.shape[0]), _ptr(pv), int(ps.shape[0]), _ptr(ps),
+                                  _ptr(starts), _ptr(counts) if counts is not None else None, float(seed), _ptr(fv),
+                                  _ptr(fs), _stream(stream)))
+
+    def next_seed(self):
+        s = C.c_float(0)
+        check(lib().ctc_fsi_next_seed(self.h, C.byref(s)))
+        return s.value
 
 
 class Contact:

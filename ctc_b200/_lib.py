@@ -81,6 +81,7 @@ SIGNATURES = {
                                              C.c_int, vp, vp]),
     "ctc_fluforces_halo_frags": (C.c_int, [vp, vp, ip, vp, vp, vp, vp, vp, vp]),
     "ctc_fluforces_halo_frags_seeded": (C.c_int, [vp, vp, ip, vp, vp, vp, vp, fp, vp, vp]),
+    "ctc_fluforces_set_cart": (C.c_int, [vp, ip, ip, C.c_int, ip]),
     "ctc_rbc_force_ini": (C.c_int, [C.c_int, C.c_int, vp, C.c_int, C.POINTER(vp)]),
     "ctc_rbc_force_fin": (C.c_int, [vp]),
     "ctc_rbc_force_md": (C.c_int, [vp, ip]),
@@ -140,6 +141,7 @@ SIGNATURES = {
                                        C.c_float, C.c_int, vp, vp, vp]),
     "ctc_fsi_pairs": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, vp, vp, vp, C.c_float, vp, vp, vp]),
     "ctc_fsi_next_seed": (C.c_int, [vp, fp]),
+    "ctc_fsi_set_rank": (C.c_int, [vp, C.c_int]),
     "ctc_scheme_move_apply": (C.c_int, [C.c_float, C.c_float, C.c_int, vp, vp, vp]),
     "ctc_scheme_move_clear_vel": (C.c_int, [C.c_int, vp, vp]),
     "ctc_bforce_apply_cste": (C.c_int, [C.c_float, fp, C.c_int, vp, vp]),

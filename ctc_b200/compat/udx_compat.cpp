@@ -2,23 +2,32 @@
 // on the C ABI of include/ctc_b200.h, for a uDeviceX build that links
 // libctc_b200 in place of these modules so that its callers (src/sim, the
 // u/* drivers) relink unchanged.  It is compiled inside the reference's build,
-// with the reference's headers on the include path (see Makefile here).
+// with the reference's headers on the include path (see Makefile here);
+// ctc_b200/compat/udx_drive.cpp runs the step through it.
 //
-// Covered: the single-array cell lists (src/clist/imp.h: clist_ini / _fin /
-// _ini_map / _fin_map / clists_get_* / clist_get_ids / clist_build), the
-// bulk solvent forces (src/fluforces/imp.h: fluforces_bulk_*), the membrane
-// forces (src/rbc/force/imp.h: rbc_force_ini / _fin / _set_stressful /
-// _set_bending / _set_rnd0 / _set_rnd1 / _apply) and the update
-// (src/scheme/move/imp.h).
-// Not covered: entry points whose arguments come from the multi-rank
-// exchange (clist_subindex* / clist_build_map / clist_gather_* of the
-// redistribution, fluforces_halo_* over exchanged fragments, fsi_* over
-// wrapped object arrays); for one periodic box per GPU the whole step of
-// ctc_sim_* (or ctc_fluforces_halo_apply, ctc_fsi_apply) replaces them.
+// Covered:
+//   - pair parameters (src/pair/imp.h: pair_ini / _fin / _set_dpd / _set_lj /
+//     _set_adhesion / _set_conf / _compute_dpd_sigma / _get_view_*);
+//   - the single-array cell lists (src/clist/imp.h: clist_ini / _fin /
+//     _ini_map / _fin_map / clists_get_* / clist_get_ids / clist_build);
+//   - the solvent forces (src/fluforces/imp.h: fluforces_bulk_* and
+//     fluforces_halo_* on the exchange's fragments, any cart);
+//   - the solvent-membrane forces (src/fsi/imp.h: fsi_ini / _fin /
+//     _bind_solvent / _bulk / _halo on the object exchange's images);
+//   - the membrane forces (src/rbc/force/imp.h: rbc_force_ini / _fin /
+//     _set_stressful / _set_bending / _set_rnd0 / _set_rnd1 / _apply / _stat)
+//     and the cells' area and volume (src/rbc/force/area_volume/imp.h);
+//   - the body force (src/scheme/force/imp.h: constant or none) and the update
+//     (src/scheme/move/imp.h);
+//   - restart files and walls (below).
+// Not covered: the cell lists of the multi-rank redistribution
+// (clist_subindex* / clist_build_map / clist_gather_*), coloured solvent,
+// stresses, the body forces other than constant.
 #include <sys/types.h>
 #include <vector_types.h>
 #include <vector_functions.h>
 
+#include <stdio.h>
 #include <mpi.h>
 
 #include "inc/def.h"
@@ -35,7 +44,11 @@
 #include "rbc/type.h"
 #include "rbc/params/imp.h"
 #include "rbc/force/imp.h"
+#include "rbc/force/area_volume/imp.h"
 #include "scheme/move/imp.h"
+#include "scheme/force/imp.h"
+#include "fsi/imp.h"
+#include "conf/imp.h"
 #include <stdio.h>
 #include <limits.h>
 #include "io/restart/imp.h"
@@ -47,10 +60,125 @@
 
 #include "ctc_b200.h"
 
+#include <math.h>
 #include <string.h>
 #include <vector>
 
 #define CTC(call) do { if ((call) != CTC_OK) ERR("ctc_b200: %s", ctc_last_error()); } while (0)
+
+// ---- pair parameters (src/pair/imp.h) ------------------------------------------
+// the reference's PairParams (src/pair/imp/type.h): colours' a, gamma, sigma,
+// the weight exponent, Lennard-Jones and adhesion constants
+struct PairParams {
+    bool dpd, lj, adhesion;
+    int ncolors;
+    float a[MAX_PAR], g[MAX_PAR], s[MAX_PAR], spow;
+    float ljs, lje, k1, k2;
+};
+
+static int pair_npar(int ncol) { return ncol * (ncol + 1) / 2; }
+
+void pair_ini(PairParams **p) {
+    *p = new PairParams();
+}
+
+void pair_fin(PairParams *p) { delete p; }
+
+void pair_set_dpd(int ncol, const float a[], const float g[], float spow, PairParams *p) {
+    if (ncol <= 0 || ncol > N_COLOR) ERR("ctc_b200: pair_set_dpd: %d colours", ncol);
+    p->dpd = true;
+    p->ncolors = ncol;
+    for (int i = 0; i < pair_npar(ncol); i++) { p->a[i] = a[i]; p->g[i] = g[i]; }
+    p->spow = spow;
+}
+
+void pair_set_lj(float sigma, float eps, PairParams *p) {
+    p->lj = true;
+    p->ljs = sigma;
+    p->lje = eps;
+}
+
+void pair_set_adhesion(float k1, float k2, PairParams *p) {
+    p->adhesion = true;
+    p->k1 = k1;
+    p->k2 = k2;
+}
+
+// the keys of src/pair/conf.cpp
+void pair_set_conf(const Config *c, const char *ns, PairParams *p) {
+    int dpd, lj, adh;
+    conf_lookup_bool_ns(c, ns, "dpd", &dpd);
+    conf_lookup_bool_ns(c, ns, "lj", &lj);
+    conf_lookup_bool_ns(c, ns, "adhesion", &adh);
+    if (dpd) {
+        int na, ng;
+        float a[MAX_PAR], g[MAX_PAR], spow;
+        conf_lookup_vfloat_ns(c, ns, "a", MAX_PAR, &na, a);
+        conf_lookup_vfloat_ns(c, ns, "g", MAX_PAR, &ng, g);
+        conf_lookup_float_ns(c, ns, "spow", &spow);
+        if (na != ng) ERR("%s.a and %s.g must have the same length: %d / %d", ns, ns, na, ng);
+        pair_set_dpd(((int)lround(sqrt(1.0 + 8.0 * na)) - 1) / 2, a, g, spow, p);
+    }
+    if (lj) {
+        float ls, le;
+        conf_lookup_float_ns(c, ns, "ljs", &ls);
+        conf_lookup_float_ns(c, ns, "lje", &le);
+        pair_set_lj(ls, le, p);
+    }
+    if (adh) {
+        float k1, k2;
+        conf_lookup_float_ns(c, ns, "k1", &k1);
+        conf_lookup_float_ns(c, ns, "k2", &k2);
+        pair_set_adhesion(k1, k2, p);
+    }
+}
+
+// sigma = sqrt(2 kBT gamma / dt), the expression of src/pair/imp/main.h:54-62
+void pair_compute_dpd_sigma(float kBT, float dt, PairParams *p) {
+    if (!p->dpd) ERR("Must have dpd parameters");
+    for (int i = 0; i < pair_npar(p->ncolors); i++) p->s[i] = sqrt(2 * kBT * p->g[i] / dt);
+}
+
+void pair_get_view_dpd(const PairParams *p, PairDPD *v) {
+    if (!p->dpd) ERR("Must have dpd parameters");
+    v->a = p->a[0]; v->g = p->g[0]; v->s = p->s[0]; v->spow = p->spow;
+}
+
+void pair_get_view_dpd_color(const PairParams *p, PairDPDC *v) {
+    if (!p->dpd) ERR("Must have dpd parameters");
+    v->ncolors = p->ncolors;
+    for (int i = 0; i < pair_npar(p->ncolors); i++) { v->a[i] = p->a[i]; v->g[i] = p->g[i]; v->s[i] = p->s[i]; }
+    v->spow = p->spow;
+}
+
+void pair_get_view_dpd_mirrored(const PairParams *p, PairDPDCM *v) {
+    if (!p->dpd) ERR("Must have dpd parameters");
+    v->ncolors = p->ncolors;
+    for (int i = 0; i < p->ncolors; i++) {     // the i-i pairs
+        const int j = (i + 1) * (i + 2) / 2 - 1;
+        v->a[i] = p->a[j]; v->g[i] = p->g[j]; v->s[i] = p->s[j];
+    }
+    v->spow = p->spow;
+}
+
+void pair_get_view_dpd_lj(const PairParams *p, PairDPDLJ *v) {
+    if (!p->dpd) ERR("Must have dpd parameters");
+    if (!p->lj) ERR("Must have lj parameters");
+    v->a = p->a[0]; v->g = p->g[0]; v->s = p->s[0]; v->spow = p->spow;
+    v->ljs = p->ljs; v->lje = p->lje;
+}
+
+void pair_get_view_adhesion(const PairParams *p, PairAdhesion *v) {
+    if (!p->adhesion) ERR("Must have adhesion parameters");
+    v->k1 = p->k1; v->k2 = p->k2;
+}
+
+static ctc_dpd_params dpd_of(const PairParams *par) {
+    PairDPD p;
+    pair_get_view_dpd(par, &p);
+    const ctc_dpd_params q = {p.a, p.g, p.s, p.spow};
+    return q;
+}
 
 // ---- cell lists (src/clist/imp.h) ---------------------------------------------
 struct Clist {
@@ -142,10 +270,59 @@ void fluforces_bulk_prepare(int n, const PaArray *a, FluForcesBulk *b) {
 void fluforces_bulk_apply(const PairParams *par, int n, const FluForcesBulk *b, const int *start, const int *count,
                           const FoArray *ff) {
     if (ff->stress) ERR("ctc_b200: stresses are not supported");
-    PairDPD p;
-    pair_get_view_dpd(par, &p);
-    const ctc_dpd_params q = {p.a, p.g, p.s, p.spow};
+    const ctc_dpd_params q = dpd_of(par);
     CTC(ctc_fluforces_bulk_apply(b->h, &q, n, b->pp, start, count, ff->ff, NULL));
+}
+
+// the halo on the fragments of the exchange (LFrag26 / RFrag26 of
+// src/flu/type.h): prepare keeps them, apply computes the pairs with the
+// trunks and masks set up for this rank of the cart
+struct FluForcesHalo {
+    ctc_fluforces *h;
+    flu::LFrag26 lf;
+    flu::RFrag26 rf;
+};
+
+void fluforces_halo_ini(MPI_Comm cart, int3 L, FluForcesHalo **hd) {
+    *hd = new FluForcesHalo;
+    CTC(ctc_fluforces_ini(L.x, L.y, L.z, 0, &(*hd)->h));
+    int dims[3], periods[3], coords[3], rank, nbr[26];
+    MPI_Cart_get(cart, 3, dims, periods, coords);
+    MPI_Cart_rank(cart, coords, &rank);
+    for (int fid = 0; fid < 26; fid++) {       // src/frag/dev.h:19-21
+        const int d[3] = {(fid + 2) % 3 - 1, (fid / 3 + 2) % 3 - 1, (fid / 9 + 2) % 3 - 1};
+        int cn[3];
+        for (int c = 0; c < 3; c++) cn[c] = (coords[c] + d[c] + dims[c]) % dims[c];
+        MPI_Cart_rank(cart, cn, &nbr[fid]);
+    }
+    CTC(ctc_fluforces_set_cart((*hd)->h, dims, coords, rank, nbr));
+}
+
+void fluforces_halo_fin(FluForcesHalo *h) {
+    CTC(ctc_fluforces_fin(h->h));
+    delete h;
+}
+
+void fluforces_halo_prepare(flu::LFrag26 lfrags, flu::RFrag26 rfrags, FluForcesHalo *h) {
+    h->lf = lfrags;
+    h->rf = rfrags;
+}
+
+void fluforces_halo_apply(const PairParams *par, const FluForcesHalo *h, const FoArray *ff) {
+    if (ff->stress) ERR("ctc_b200: stresses are not supported");
+    const ctc_dpd_params q = dpd_of(par);
+    int ln[26];
+    const float *lpp[26], *rpp[26];
+    const int *lii[26], *rst[26];
+    for (int i = 0; i < 26; i++) {
+        if (h->lf.d[i].parray.colors || h->rf.d[i].parray.colors) ERR("ctc_b200: coloured solvent is not supported");
+        ln[i] = h->lf.d[i].n;
+        lpp[i] = h->lf.d[i].parray.pp;
+        lii[i] = h->lf.d[i].ii;
+        rpp[i] = h->rf.d[i].parray.pp;
+        rst[i] = h->rf.d[i].start;
+    }
+    CTC(ctc_fluforces_halo_frags(h->h, &q, ln, lpp, lii, rpp, rst, ff->ff, NULL));
 }
 
 // ---- membrane forces (src/rbc/force/imp.h) ------------------------------------
@@ -235,6 +412,204 @@ void rbc_force_stat(float *pArea, float *pVolume) {
 // stress-free reference lengths (src/rbc/shape) are not part of this build
 void rbc_force_set_stressfree(const char *fname, RbcForce *) {
     ERR("ctc_b200: stress-free membranes (%s) are not supported; use rbc_force_set_stressful", fname);
+}
+
+// ---- cells' area and volume (src/rbc/force/area_volume/imp.h) -----------------
+// reduced in FP64 on the device, handed out as the reference's floats
+struct AreaVolume {
+    ctc_rbc_force *h;
+    int max_cell;
+    double *av64;            // [dev, 2 max_cell]
+    float *av;               // [dev, 2 max_cell]
+    std::vector<float> hst;
+    std::vector<double> tmp;
+    int nc;
+};
+
+void area_volume_ini(int nv, int nt, const int4 *tt, int max_cell, AreaVolume **pq) {
+    std::vector<int> tri(3 * (size_t)nt);
+    for (int t = 0; t < nt; t++) { tri[3 * t] = tt[t].x; tri[3 * t + 1] = tt[t].y; tri[3 * t + 2] = tt[t].z; }
+    AreaVolume *q = new AreaVolume;
+    CTC(ctc_rbc_force_ini(nv, nt, tri.data(), max_cell, &q->h));
+    q->max_cell = max_cell;
+    q->nc = 0;
+    if (cudaMalloc((void**)&q->av64, sizeof(double) * 2 * (max_cell > 0 ? max_cell : 1)) != cudaSuccess ||
+        cudaMalloc((void**)&q->av, sizeof(float) * 2 * (max_cell > 0 ? max_cell : 1)) != cudaSuccess)
+        ERR("ctc_b200: area_volume_ini: no device memory");
+    q->hst.assign(2 * (size_t)(max_cell > 0 ? max_cell : 1), 0.0f);
+    q->tmp.assign(2 * (size_t)(max_cell > 0 ? max_cell : 1), 0.0);
+    *pq = q;
+}
+
+void area_volume_fin(AreaVolume *q) {
+    CTC(ctc_rbc_force_fin(q->h));
+    cudaFree(q->av64);
+    cudaFree(q->av);
+    delete q;
+}
+
+void area_volume_compute(AreaVolume *q, int nc, const Particle *pp, float **av) {
+    if (nc > q->max_cell) ERR("nc=%d > max_cell=%d", nc, q->max_cell);
+    q->nc = nc;
+    if (nc > 0) {
+        CTC(ctc_rbc_area_volume(q->h, nc, reinterpret_cast<const float*>(pp), q->av64, NULL));
+        cudaMemcpy(q->tmp.data(), q->av64, sizeof(double) * 2 * nc, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < 2 * nc; i++) q->hst[i] = (float)q->tmp[i];
+        cudaMemcpy(q->av, q->hst.data(), sizeof(float) * 2 * nc, cudaMemcpyHostToDevice);
+    }
+    *av = q->av;
+}
+
+void area_volume_host(AreaVolume *q, float **av) {
+    *av = q->hst.data();
+}
+
+// ---- solvent-membrane forces (src/fsi/imp.h) ----------------------------------
+// fsi_bulk: the pairs of each object type's vertices; fsi_halo: those of the
+// images the object exchange delivered, gathered fragment after fragment into
+// one array and their forces added back.  One module holds the trunk (drawn
+// per fsi_bulk type and per fsi_halo type, src/fsi/imp/{bulk,halo}.h); the
+// working one grows with the arrays.
+struct Fsi {
+    int3 L;
+    ctc_fsi *trunk, *work;
+    int cap_v, cap_s;
+    PaArray pa;
+    Force *ff;
+    int n;
+    const int *starts;
+    Particle *img;
+    Force *fimg;
+    int img_cap;
+};
+
+static void fsi_reserve(Fsi *f, int nv, int ns) {
+    if (f->work && nv <= f->cap_v && ns <= f->cap_s) return;
+    if (f->work) CTC(ctc_fsi_fin(f->work));
+    f->cap_v = nv > f->cap_v ? nv : f->cap_v;
+    f->cap_s = ns > f->cap_s ? ns : f->cap_s;
+    CTC(ctc_fsi_ini(f->L.x, f->L.y, f->L.z, f->cap_v, f->cap_s, &f->work));
+}
+
+void fsi_ini(int rank, int3 L, Fsi **pf) {
+    Fsi *f = new Fsi();
+    f->L = L;
+    CTC(ctc_fsi_ini(L.x, L.y, L.z, 0, 0, &f->trunk));
+    CTC(ctc_fsi_set_rank(f->trunk, rank));
+    *pf = f;
+}
+
+void fsi_fin(Fsi *f) {
+    CTC(ctc_fsi_fin(f->trunk));
+    if (f->work) CTC(ctc_fsi_fin(f->work));
+    cudaFree(f->img);
+    cudaFree(f->fimg);
+    delete f;
+}
+
+void fsi_bind_solvent(PaArray pa, Force *ff, int n, const int *starts, Fsi *f) {
+    if (pa.colors) ERR("ctc_b200: coloured solvent is not supported");
+    f->pa = pa;
+    f->ff = ff;
+    f->n = n;
+    f->starts = starts;
+}
+
+void fsi_bulk(Fsi *f, int nw, const PairParams **prms, PaWrap *pw, FoWrap *fw) {
+    for (int i = 0; i < nw; i++) {
+        if (!prms[i]) continue;
+        float seed;
+        CTC(ctc_fsi_next_seed(f->trunk, &seed));
+        fsi_reserve(f, pw[i].n, f->n);
+        const ctc_dpd_params q = dpd_of(prms[i]);
+        CTC(ctc_fsi_pairs(f->work, &q, pw[i].n, reinterpret_cast<const float*>(pw[i].pp), f->n, f->pa.pp, f->starts,
+                          NULL, seed, reinterpret_cast<float*>(fw[i].ff), reinterpret_cast<float*>(f->ff), NULL));
+    }
+}
+
+void fsi_halo(Fsi *f, int nw, const PairParams **prms, Pap26 all_pp, Fop26 all_ff, const int *all_counts) {
+    int start[26] = {0};
+    for (int i = 0; i < nw; i++) {
+        const int *counts = all_counts + 26 * i;
+        int n = 0;
+        for (int j = 0; j < 26; j++) n += counts[j];
+        if (prms[i]) {
+            float seed;
+            CTC(ctc_fsi_next_seed(f->trunk, &seed));
+            if (n > f->img_cap) {
+                cudaFree(f->img);
+                cudaFree(f->fimg);
+                if (cudaMalloc((void**)&f->img, sizeof(Particle) * n) != cudaSuccess ||
+                    cudaMalloc((void**)&f->fimg, sizeof(Force) * n) != cudaSuccess)
+                    ERR("ctc_b200: fsi_halo: no device memory");
+                f->img_cap = n;
+            }
+            int k = 0;
+            for (int j = 0; j < 26; j++) {      // this type's images of fragment j
+                if (counts[j] > 0) {
+                    cudaMemcpy(f->img + k, all_pp.d[j] + start[j], sizeof(Particle) * counts[j],
+                               cudaMemcpyDeviceToDevice);
+                    cudaMemcpy(f->fimg + k, all_ff.d[j] + start[j], sizeof(Force) * counts[j],
+                               cudaMemcpyDeviceToDevice);
+                }
+                k += counts[j];
+            }
+            fsi_reserve(f, n, f->n);
+            const ctc_dpd_params q = dpd_of(prms[i]);
+            CTC(ctc_fsi_pairs(f->work, &q, n, reinterpret_cast<const float*>(f->img), f->n, f->pa.pp, f->starts, NULL,
+                              seed, reinterpret_cast<float*>(f->fimg), reinterpret_cast<float*>(f->ff), NULL));
+            k = 0;
+            for (int j = 0; j < 26; j++) {
+                if (counts[j] > 0)
+                    cudaMemcpy(all_ff.d[j] + start[j], f->fimg + k, sizeof(Force) * counts[j],
+                               cudaMemcpyDeviceToDevice);
+                k += counts[j];
+            }
+        }
+        for (int j = 0; j < 26; j++) start[j] += counts[j];
+    }
+}
+
+// ---- body force (src/scheme/force/imp.h): constant or none --------------------
+struct BForce {
+    int type;                // 0 none, 1 constant
+    float a[3];
+};
+
+void bforce_ini(BForce **p) { *p = new BForce(); }
+void bforce_fin(BForce *p) { delete p; }
+void bforce_set_none(BForce *p) { p->type = 0; }
+void bforce_set_cste(float3 f, BForce *p) {
+    p->type = 1;
+    p->a[0] = f.x; p->a[1] = f.y; p->a[2] = f.z;
+}
+void bforce_set_dp(float, BForce *) { ERR("ctc_b200: body force \"double_poiseuille\" is not supported"); }
+void bforce_set_shear(float, BForce *) { ERR("ctc_b200: body force \"shear\" is not supported"); }
+void bforce_set_rol(float, BForce *) { ERR("ctc_b200: body force \"four_roller\" is not supported"); }
+void bforce_set_rad(float, BForce *) { ERR("ctc_b200: body force \"rad\" is not supported"); }
+
+// the keys of src/scheme/force/conf.cpp for the supported types
+void bforce_set_conf(const Config *c, BForce *p) {
+    const char *type;
+    conf_lookup_string(c, "bforce.type", &type);
+    if (!strcmp(type, "none")) bforce_set_none(p);
+    else if (!strcmp(type, "constant")) {
+        float3 f;
+        conf_lookup_float3(c, "bforce.f", &f);
+        bforce_set_cste(f, p);
+    } else {
+        ERR("ctc_b200: body force \"%s\" is not supported (none, constant)", type);
+    }
+}
+
+void bforce_adjust(float3 f, BForce *p) {
+    if (p->type == 1) { p->a[0] = f.x; p->a[1] = f.y; p->a[2] = f.z; }
+    else if (p->type != 0) ERR("not implemented");
+}
+
+void bforce_apply(const Coords *, float mass, const BForce *bf, int n, const Particle *, Force *ff) {
+    if (bf->type == 0) return;
+    CTC(ctc_bforce_apply_cste(mass, bf->a, n, reinterpret_cast<float*>(ff), NULL));
 }
 
 // ---- update (src/scheme/move/imp.h) -------------------------------------------

@@ -161,6 +161,7 @@ struct ctc_fluforces {
     int *fss;
     Off27 off;
     Kiss bulk, halo[26];
+    unsigned masks;        // bit fid: the RNG key order of fragment fid (fluforces_halo_ini)
 };
 
 extern "C" int ctc_fluforces_ini(int LX, int LY, int LZ, int maxp, ctc_fluforces **pf) {
@@ -175,7 +176,40 @@ extern "C" int ctc_fluforces_ini(int LX, int LY, int LZ, int maxp, ctc_fluforces
     CUDA_TRY(cudaMalloc(&f->fss, sizeof(int) * (size_t)f->off.d[26]));
     kiss_ini(&f->bulk, 0, 0, 0, 0);                 // src/fluforces/imp/ini.h:6
     for (int i = 0; i < 26; i++) halo_trunk_ini(i, &f->halo[i]);
+    f->masks = halo_masks();
     *pf = f;
+    return CTC_OK;
+}
+
+// get_interrank_infos (src/fluforces/imp/ini.h:22-59) for fragment fid of the
+// rank at coords of a dims cart whose neighbour in direction d(fid) is rank
+// nbr: the trunk seeds (a base from the two ranks' coordinates and the
+// direction's offset), and the mask: the lower rank takes its own index
+// first, one rank alone the lower of the fragment and its anti-fragment
+extern "C" int ctc_fluforces_set_cart(ctc_fluforces *f, const int *dims, const int *coords, int rank,
+                                      const int *nbr) {
+    if (!f || !dims || !coords || !nbr) return fail(CTC_ERR_ARG, "ctc_fluforces_set_cart: bad arguments");
+    for (int c = 0; c < 3; c++)
+        if (dims[c] <= 0 || coords[c] < 0 || coords[c] >= dims[c])
+            return fail(CTC_ERR_ARG, "ctc_fluforces_set_cart: coords %d of dims %d", coords[c], dims[c]);
+    unsigned masks = 0;
+    for (int fid = 0; fid < 26; fid++) {
+        const int d[3] = {frag_i2dx(fid), frag_i2dy(fid), frag_i2dz(fid)};
+        int indx[3];
+        for (int c = 0; c < 3; c++) {
+            const int cn = (coords[c] + d[c] + dims[c]) % dims[c];
+            indx[c] = std::min(coords[c], cn) * dims[c] + std::max(coords[c], cn);
+        }
+        const int base = indx[0] + dims[0] * dims[0] * (indx[1] + dims[1] * dims[1] * indx[2]);
+        const int plus = (d[0] + d[1] + d[2] > 0) || ((d[0] + d[1] + d[2] == 0) && (d[0] > 0)) ||
+                         ((d[0] == 0) && (d[1] > 0)) || (d[1] == 0 && d[2] > 0);
+        const int sg = 2 * plus - 1;
+        const int seed = base + (1 + sg * d[0]) + 3 * ((1 + sg * d[1]) + 3 * (1 + sg * d[2]));
+        kiss_ini(&f->halo[fid], 390 + seed, seed + 615, 12309, 23094);
+        const bool m = nbr[fid] != rank ? std::min(nbr[fid], rank) == rank : std::min(fid, frag_anti(fid)) == fid;
+        if (m) masks |= 1u << fid;
+    }
+    f->masks = masks;
     return CTC_OK;
 }
 
@@ -248,7 +282,7 @@ extern "C" int ctc_fluforces_halo_frags_seeded(ctc_fluforces *f, const ctc_dpd_p
     }
     if (tot > INT_MAX) return fail(CTC_ERR_CAPACITY, "ctc_fluforces_halo_frags: %ld boundary particles", tot);
     H.loff[26] = (int)tot;
-    H.masks = halo_masks();
+    H.masks = f->masks;
     DpdPar P;
     P.a = p->a; P.g = p->g; P.s = p->s; P.spow = p->spow;
     CUDA_TRY(halo_frags_launch(f->L, P, H, ff, 3, dev_err_ptr(), (cudaStream_t)stream));

@@ -315,6 +315,14 @@ extern "C" int ctc_fsi_apply(ctc_fsi *f, const ctc_dpd_params *p, int nv, const 
     return ctc_fsi_apply_seeded(f, p, nv, pv, ns, ps, starts, counts, sb, sh, CTC_RNG_REFERENCE, fv, fs, stream);
 }
 
+extern "C" int ctc_fsi_set_rank(ctc_fsi *f, int rank) {
+    if (!f) return fail(CTC_ERR_ARG, "ctc_fsi_set_rank: null");
+    // fsi_ini, src/fsi/imp/main.h:7: rnd_ini(1908 - rank, 1409 + rank, 290, 12968)
+    f->trunk.s[0] = (unsigned)(1908 - rank); f->trunk.s[1] = (unsigned)(1409 + rank);
+    f->trunk.s[2] = 290; f->trunk.s[3] = 12968;
+    return CTC_OK;
+}
+
 extern "C" int ctc_fsi_next_seed(ctc_fsi *f, float *seed) {
     if (!f || !seed) return fail(CTC_ERR_ARG, "ctc_fsi_next_seed: bad arguments");
     *seed = kiss_get4(&f->trunk);

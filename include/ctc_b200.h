@@ -146,6 +146,11 @@ int ctc_fluforces_halo_apply(ctc_fluforces *f, const ctc_dpd_params *p, int n, c
 int ctc_fluforces_halo_frags(ctc_fluforces *f, const ctc_dpd_params *p, const int *ln, const float *const *lpp,
                              const int *const *lii, const float *const *rpp, const int *const *rstart, float *ff,
                              void *stream);
+/* fluforces_halo_ini's per-rank set-up (src/fluforces/imp/ini.h:22-59) for
+ * the rank at coords[3] of a periodic dims[3] cart whose neighbour in
+ * direction fid is rank nbr[fid]: the 26 fragment trunks' seeds and the key
+ * masks; ctc_fluforces_ini sets up the one-rank cart (dims 1 1 1) */
+int ctc_fluforces_set_cart(ctc_fluforces *f, const int *dims, const int *coords, int rank, const int *nbr);
 /* the same with explicit seeds [host, 26] */
 int ctc_fluforces_halo_frags_seeded(ctc_fluforces *f, const ctc_dpd_params *p, const int *ln,
                                     const float *const *lpp, const int *const *lii, const float *const *rpp,
@@ -216,6 +221,9 @@ int ctc_fsi_pairs(ctc_fsi *f, const ctc_dpd_params *p, int n, const float *pv, i
                   const int *starts, const int *counts, float seed, float *fv, float *fs, void *stream);
 /* the next draw of the module's trunk (rnd_get of src/fsi/imp/{bulk,halo}.h) */
 int ctc_fsi_next_seed(ctc_fsi *f, float *seed);
+/* fsi_ini of rank `rank` (src/fsi/imp/main.h:7): reseeds the module's trunk
+ * rnd_ini(1908 - rank, 1409 + rank, 290, 12968); ctc_fsi_ini seeds rank 0's */
+int ctc_fsi_set_rank(ctc_fsi *f, int rank);
 
 /* ---- membrane-membrane contact: replaces src/cnt/imp.h ------------------- */
 /* PairDPDLJ {a, g, s, spow, ljs, lje} (src/pair/type.h:22-25): DPD plus a

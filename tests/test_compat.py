@@ -11,12 +11,46 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 OBJ = os.path.join(ROOT, "ctc_b200", "compat", "_build", "udx_compat.o")
 
-# the declarations of src/clist/imp.h, src/fluforces/imp.h (bulk),
-# src/rbc/force/imp.h, src/scheme/move/imp.h, src/io/restart/imp.h and the
+# the declarations of src/pair/imp.h, src/clist/imp.h, src/fluforces/imp.h
+# (bulk and halo), src/fsi/imp.h, src/rbc/force/imp.h,
+# src/rbc/force/area_volume/imp.h, src/scheme/force/imp.h,
+# src/scheme/move/imp.h, src/io/restart/imp.h and the
 # walls' src/wall/imp.h, src/wall/sdf/imp.h, src/wall/wvel/imp.h (the
 # MPI_Comm of the compile check is its stand-in type), as the C++ compiler
 # names them
 EXPECTED = [
+    "pair_ini(PairParams**)",
+    "pair_fin(PairParams*)",
+    "pair_set_dpd(int, float const*, float const*, float, PairParams*)",
+    "pair_set_lj(float, float, PairParams*)",
+    "pair_set_adhesion(float, float, PairParams*)",
+    "pair_set_conf(Config const*, char const*, PairParams*)",
+    "pair_compute_dpd_sigma(float, float, PairParams*)",
+    "pair_get_view_dpd(PairParams const*, PairDPD*)",
+    "pair_get_view_dpd_color(PairParams const*, PairDPDC*)",
+    "pair_get_view_dpd_mirrored(PairParams const*, PairDPDCM*)",
+    "pair_get_view_dpd_lj(PairParams const*, PairDPDLJ*)",
+    "pair_get_view_adhesion(PairParams const*, PairAdhesion*)",
+    "fluforces_halo_ini(ctc_compat_check_comm*, int3, FluForcesHalo**)",
+    "fluforces_halo_fin(FluForcesHalo*)",
+    "fluforces_halo_prepare(Sarray<flu::LFrag, 26>, Sarray<flu::RFrag, 26>, FluForcesHalo*)",
+    "fluforces_halo_apply(PairParams const*, FluForcesHalo const*, FoArray const*)",
+    "fsi_ini(int, int3, Fsi**)",
+    "fsi_fin(Fsi*)",
+    "fsi_bind_solvent(PaArray, Force*, int, int const*, Fsi*)",
+    "fsi_bulk(Fsi*, int, PairParams const**, PaWrap*, FoWrap*)",
+    "fsi_halo(Fsi*, int, PairParams const**, Sarray<Particle*, 26>, Sarray<Force*, 26>, int const*)",
+    "area_volume_ini(int, int, int4 const*, int, AreaVolume**)",
+    "area_volume_fin(AreaVolume*)",
+    "area_volume_compute(AreaVolume*, int, Particle const*, float**)",
+    "area_volume_host(AreaVolume*, float**)",
+    "bforce_ini(BForce**)",
+    "bforce_fin(BForce*)",
+    "bforce_set_none(BForce*)",
+    "bforce_set_cste(float3, BForce*)",
+    "bforce_set_conf(Config const*, BForce*)",
+    "bforce_adjust(float3, BForce*)",
+    "bforce_apply(Coords const*, float, BForce const*, int, Particle const*, Force*)",
     "clist_ini(int, int, int, Clist**)",
     "clist_fin(Clist*)",
     "clist_ini_map(int, int, Clist const*, ClistMap**)",

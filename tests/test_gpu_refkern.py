@@ -116,3 +116,65 @@ def test_bulk_kernel_faster_than_reference_kernel():
     t_ours = timed(lambda: ff.apply_seeded(C.DpdParams(*dpd), P, S, N, seeds, out, which=1))
     print("bulk 64^3: reference kernel %.3f ms, this build %.3f ms" % (t_ref, t_ours))
     assert t_ours < t_ref, (t_ours, t_ref)
+
+
+def _frag_lists(L, ps, starts, counts):
+    """The exchanged fragments of a periodic box with itself as neighbour:
+    fragment fid's local boundary particles (packed, with their sorted
+    indices) and, as its remote fragment, the anti-fragment's packed particles
+    and fragment-cell starts."""
+    fr = refkern.fragments(L, starts, counts)
+    P = dev(ps)
+    lpp, lii, rpp, rst = [], [], [], []
+    for fid in range(26):
+        ii, _ = fr[fid]
+        ia, ss = fr[oracle.frag_anti(fid)]
+        lpp.append(P[torch.as_tensor(ii.astype(np.int64), device="cuda")].contiguous())
+        lii.append(dev(ii))
+        rpp.append(P[torch.as_tensor(ia.astype(np.int64), device="cuda")].contiguous())
+        rst.append(dev(ss))
+    return lpp, lii, rpp, rst
+
+
+@pytest.mark.parametrize("L", [(8, 8, 8), (16, 12, 10), (6, 6, 6)])
+def test_halo_from_exchanged_fragments_vs_reference_kernel(L):
+    """fluforces_halo_prepare + _apply on the exchange's fragments
+    (ctc_fluforces_halo_frags: the reference's LFrag26 / RFrag26 data) against
+    the reference's own halo kernel on the same fragments and seeds, and
+    against the module's halo from the cell lists: within 1e-5."""
+    import ctc_b200 as C
+    ps, starts, counts = _sorted(L, 21)
+    dpd = systems.dpd_params()
+    seeds = np.random.default_rng(22).random(27).astype(np.float32)
+    lpp, lii, rpp, rst = _frag_lists(L, ps, starts, counts)
+    ours = torch.zeros((len(ps), 3), device="cuda")
+    C.FluForces(L, len(ps)).halo_frags(C.DpdParams(*dpd), lpp, lii, rpp, rst, ours, seeds26=seeds[1:])
+    ref = torch.zeros((len(ps), 3), device="cuda")
+    refkern.halo(dpd, L, dev(ps), starts, counts, seeds[1:], ref)
+    e = _errs(ours.cpu().numpy(), ref.cpu().numpy())
+    assert e.max() < 1e-5, e.max()
+    mod = torch.zeros((len(ps), 3), device="cuda")
+    C.FluForces(L, len(ps)).apply_seeded(C.DpdParams(*dpd), dev(ps), dev(starts), dev(counts), seeds, mod, which=2)
+    assert _errs(ours.cpu().numpy(), mod.cpu().numpy()).max() < 1e-5
+    assert C.device_error() == 0
+
+
+def test_halo_from_fragments_draws_the_reference_trunks():
+    """Without explicit seeds the 26 fragment seeds come from the module's
+    trunks (src/fluforces/imp/ini.h:22-59), one draw each per call."""
+    import ctc_b200 as C
+    L = (8, 8, 8)
+    ps, starts, counts = _sorted(L, 23)
+    dpd = systems.dpd_params()
+    lpp, lii, rpp, rst = _frag_lists(L, ps, starts, counts)
+    mod = C.FluForces(L, len(ps))
+    kh = [oracle.Kiss.halo(f) for f in range(26)]
+    for _ in range(2):
+        seeds = np.array([k.get() for k in kh], np.float32)
+        ours = torch.zeros((len(ps), 3), device="cuda")
+        mod.halo_frags(C.DpdParams(*dpd), lpp, lii, rpp, rst, ours)
+        ref = torch.zeros((len(ps), 3), device="cuda")
+        mod2 = C.FluForces(L, len(ps))
+        mod2.halo_frags(C.DpdParams(*dpd), lpp, lii, rpp, rst, ref, seeds26=seeds)
+        # particles of edge and corner cells take one atomic add per fragment
+        assert _errs(ours.cpu().numpy(), ref.cpu().numpy()).max() < 1e-6

@@ -269,3 +269,41 @@ def test_reference_kernel_on_rbc_simple_inputs():
     file_cells = np.abs(f_file[:nv] - f_file[nv:]).max() / np.abs(f_file).max()
     assert file_cells > 2e-2, file_cells
     assert np.abs(ref - f_file).max() / np.abs(f_file).max() < file_cells
+
+
+@pytest.mark.parametrize("L", [(16, 16, 16), (12, 10, 14)])
+def test_fsi_pairs_bulk_and_images_vs_reference_kernels(L):
+    """ctc_fsi_pairs, the entry point behind the drop-in fsi_bulk / fsi_halo:
+    on the vertices with the bulk seed it is fsi_dev::bulk, on the images the
+    object exchange lists (fragment after fragment, shifted) with the halo seed
+    it is fsi_dev::halo -- both sides of the forces within 1e-5 of the
+    reference's kernels; together they equal the module's fsi (images built on
+    the device)."""
+    import ctc_b200 as C
+    ps, counts, starts, pv = _fsi_case(L, 15)
+    dpd = (0.0, 8.0, systems.dpd_params()[2], 0.25)
+    sb, sh = 0.375, 0.875
+    P, S, St, N = dev(pv), dev(ps), dev(starts), dev(counts)
+    cnt, vert, img = refkern.images(L, pv)
+    mod = C.Fsi(L, max(len(pv), len(img)), len(ps))
+    fv = torch.zeros((len(pv), 3), device="cuda")
+    fs = torch.zeros((len(ps), 3), device="cuda")
+    mod.pairs(C.DpdParams(*dpd), P, S, St, N, sb, fv, fs)
+    rv = torch.zeros_like(fv)
+    rs = torch.zeros_like(fs)
+    refkern.fsi_bulk(dpd, L, P, S, St, sb, rv, rs)
+    assert rel_err(fv.cpu().numpy(), rv.cpu().numpy()) < TOL
+    assert rel_err(fs.cpu().numpy(), rs.cpu().numpy()) < TOL
+    # the images (counts may be omitted: taken from the starts)
+    fi = torch.zeros((len(img), 3), device="cuda")
+    mod.pairs(C.DpdParams(*dpd), dev(img), S, St, None, sh, fi, fs)
+    fv.index_add_(0, torch.as_tensor(vert.astype(np.int64), device="cuda"), fi)
+    assert refkern.fsi_halo(dpd, L, pv, S, St, sh, rv, rs) > 0
+    assert rel_err(fv.cpu().numpy(), rv.cpu().numpy()) < TOL
+    assert rel_err(fs.cpu().numpy(), rs.cpu().numpy()) < TOL
+    whole_v = torch.zeros_like(fv)
+    whole_s = torch.zeros_like(fs)
+    C.Fsi(L, len(pv), len(ps)).apply_seeded(C.DpdParams(*dpd), P, S, St, N, sb, sh, whole_v, whole_s)
+    assert rel_err(fv.cpu().numpy(), whole_v.cpu().numpy()) < TOL
+    assert rel_err(fs.cpu().numpy(), whole_s.cpu().numpy()) < TOL
+    assert C.device_error() == 0
