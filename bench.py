@@ -80,13 +80,21 @@ def peaks():
 
 # Per-launch figures of k_dpd_bulk from ncu captures, keyed by the launch
 # shape the autotuner picks (threads per block, candidate loads in flight per
-# lane): warp instructions and DRAM bytes (dram__bytes_read.sum +
+# lane, candidate rows staged in shared memory): warp instructions and DRAM bytes (dram__bytes_read.sum +
 # dram__bytes_write.sum) per target particle.  Each entry names the ncu summary
 # under profiles/ it was read from; a shape without an entry has no figures
 # (the line then says so instead of borrowing another instantiation's).
 BULK_NCU = {
-    (256, 4): {"warp_inst_per_particle": 247.6, "dram_bytes_per_particle": 55.80,
-               "source": "profiles/k_dpd_bulk_p64.md: k_dpd_bulk<0,false,256,4,0>, 64^3 box"},
+    (256, 4, 2): {"warp_inst_per_particle": 239.0, "dram_bytes_per_particle": 56.05,
+                  "source": "profiles/k_dpd_bulk_p64.md: k_dpd_bulk<0,0,256,4,0,0,1>, 64^3 box, ncu --set full"},
+    (128, 4, 2): {"warp_inst_per_particle": 239.0, "dram_bytes_per_particle": 57.67,
+                  "source": "profiles/k_dpd_bulk_p64.md: k_dpd_bulk<0,0,128,4,0,0,1>, 64^3 box"},
+    (128, 4, 0): {"warp_inst_per_particle": 223.2, "dram_bytes_per_particle": 56.72,
+                  "source": "profiles/k_dpd_bulk_p64.md: k_dpd_bulk<0,0,128,4,0,0,0>, 64^3 box"},
+    (256, 4, 0): {"warp_inst_per_particle": 223.2, "dram_bytes_per_particle": 56.51,
+                  "source": "profiles/k_dpd_bulk_p64.md: k_dpd_bulk<0,0,256,4,0,0,0>, 64^3 box"},
+    (128, 4, 1): {"warp_inst_per_particle": 238.0, "dram_bytes_per_particle": 55.99,
+                  "source": "profiles/k_dpd_bulk_p64.md: k_dpd_bulk<0,0,128,4,0,1,0>, 64^3 box"},
 }
 
 
@@ -102,7 +110,7 @@ def issue_roofline(n, bulk_ms, clk, shape):
     region."""
     fig = bulk_ncu(shape)
     if not fig:
-        return {"frac": None, "note": "no ncu capture of k_dpd_bulk with %d threads x %d loads" % tuple(shape)}
+        return {"frac": None, "note": "no ncu capture of k_dpd_bulk with %d threads x %d loads, staged %d" % tuple(shape)}
     ipp = fig["warp_inst_per_particle"]
     mhz = (clk or {}).get("sm_mhz") or 1965.0
     achieved = ipp * n / (bulk_ms * 1e-3)
@@ -300,7 +308,11 @@ def run_ours(args, cfg, world, rank, local):
     # launch shapes tuned on the first step's state; the step replayed as CUDA
     # graphs (captured during the warm-up)
     sim.step(1)
-    tuned = sim.tune(reps=2)
+    if args.shape:
+        tuned = tuple(int(x) for x in args.shape.split(",")) + (0,) * (5 - len(args.shape.split(",")))
+        sim.set_tune(tuned)
+    else:
+        tuned = sim.tune(reps=2)
     sim.set_graph(True)
     sim.step(max(args.warmup - 1, 1))
     torch.cuda.synchronize()
@@ -358,7 +370,7 @@ def run_ours(args, cfg, world, rank, local):
     hbm, peak_kind = peaks()
     bulk_ms = phases["bulk"]
     achieved = PAIR_BYTES * n / (bulk_ms * 1e-3) / 1e9
-    shape = (tuned[0], tuned[1])
+    shape = (tuned[0], tuned[1], tuned[4])
     fig = bulk_ncu(shape)
     traffic = fig["dram_bytes_per_particle"] if fig else None
     # seeds, 6 cell-list kernels, fragment starts, 2 halo packing kernels, bulk, halo, update; with
@@ -375,8 +387,9 @@ def run_ours(args, cfg, world, rank, local):
         "config": {"workload": cfg["name"], "particles_per_gpu": n, "membrane_vertices_per_gpu": nvt,
                    "box": list(L), "rho": 10,
                    "rng": "reference keys", "parallelism": "replicas" if world > 1 else "1 GPU",
-                   "tuned_shape": {"bulk_threads": tuned[0], "bulk_unroll": tuned[1], "halo_threads": tuned[2],
-                                   "halo_unroll": tuned[3]},
+                   "tuned_shape": {"bulk_threads": tuned[0], "bulk_unroll": tuned[1], "bulk_variant": tuned[4],
+                                   "halo_threads": tuned[2], "halo_unroll": tuned[3],
+                                   "from": "--shape" if args.shape else "autotuner"},
                    "graph": True,
                    "l2": "inputs larger than L2 (state %.2f GB per buffer)" % (32e-9 * n)},
         "gpu_launches": launches * args.steps,
@@ -385,7 +398,7 @@ def run_ours(args, cfg, world, rank, local):
                      "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic * n if traffic else None,
                      "traffic_source": fig["source"] if fig else
-                     "no ncu capture of k_dpd_bulk with %d threads x %d loads" % shape,
+                     "no ncu capture of k_dpd_bulk with %d threads x %d loads, staged %d" % shape,
                      "peak_kind": peak_kind + " (copy bandwidth)",
                      "algorithmic_bytes_per_particle": PAIR_BYTES,
                      "fp32": {"achieved_tflops": PAIR_FLOP * n / (bulk_ms * 1e-3) / 1e12,
@@ -624,6 +637,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--shape", default="",
+                    help="pair-kernel launch shape instead of tuning: bulk threads,bulk loads,halo threads,halo loads"
+                         "[,bulk variant] (single-box configurations)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
     world, rank, local = dist_init()

@@ -561,15 +561,18 @@ class Sim:
 
     def tune(self, reps=3, stream=None):
         """Autotune the pair kernels' launch shapes on the current state (after
-        a step); returns (bulk threads, bulk unroll, halo threads, halo unroll)."""
-        ch = (C.c_int * 4)()
+        a step); returns (bulk threads, bulk unroll, halo threads, halo unroll,
+        bulk staging)."""
+        ch = (C.c_int * 5)()
         check(lib().ctc_sim_tune(self.h, int(reps), ch, _stream(stream)))
         return tuple(ch)
 
     def set_tune(self, choice):
         """Launch shapes of the pair kernels (bulk threads, bulk loads in
-        flight, halo threads, halo loads), as tune() returns them."""
-        ch = (C.c_int * 4)(*[int(x) for x in choice])
+        flight, halo threads, halo loads[, bulk staging = 0]), as tune()
+        returns them."""
+        choice = tuple(int(x) for x in choice) + (0,) * (5 - len(choice))
+        ch = (C.c_int * 5)(*choice)
         check(lib().ctc_sim_set_tune(self.h, ch))
 
     def set_membrane_noise(self, enable=True, seed=0):

@@ -909,12 +909,16 @@ extern "C" int ctc_sim_set_tune(ctc_sim *s, const int *choice) {
     if (!s || !choice) return fail(CTC_ERR_ARG, "ctc_sim_set_tune: bad arguments");
     DpdTune t;
     t.bulk_threads = choice[0]; t.bulk_unroll = choice[1]; t.halo_threads = choice[2]; t.halo_unroll = choice[3];
+    t.bulk_stage = choice[4];
     bool ok_t = false, ok_u = false, ok_h = false, ok_hu = false;
     for (int v : DPD_TUNE_BULK_T) ok_t |= v == t.bulk_threads;
     for (int v : DPD_TUNE_BULK_U) ok_u |= v == t.bulk_unroll;
     for (int v : DPD_TUNE_HALO_T) ok_h |= v == t.halo_threads;
     for (int v : DPD_TUNE_HALO_U) ok_hu |= v == t.halo_unroll;
-    if (!ok_t || !ok_u || !ok_h || !ok_hu) return fail(CTC_ERR_ARG, "ctc_sim_set_tune: unknown launch shape");
+    const bool ok_s = t.bulk_stage == 0 ||
+                      (t.bulk_stage == 1 && t.bulk_threads == 128 && t.bulk_unroll >= 4 && s->cfg.rng == CTC_RNG_REFERENCE) ||
+                      (t.bulk_stage == 2 && s->cfg.rng == CTC_RNG_REFERENCE);
+    if (!ok_t || !ok_u || !ok_h || !ok_hu || !ok_s) return fail(CTC_ERR_ARG, "ctc_sim_set_tune: unknown launch shape");
     sim_drop_graphs(s);
     s->tune = t;
     return CTC_OK;
@@ -961,14 +965,23 @@ extern "C" int ctc_sim_tune(ctc_sim *s, int reps, int *choice, void *stream) {
     float best_ms = 1e30f;
     int rc = CTC_OK;
     for (int ti = 0; ti < 2 && !rc; ti++)
-        for (int ui = 0; ui < 3 && !rc; ui++) {
-            DpdTune t = best;
-            t.bulk_threads = DPD_TUNE_BULK_T[ti];
-            t.bulk_unroll = DPD_TUNE_BULK_U[ui];
-            float ms = 0;
-            rc = time_it(1, t, ms);
-            if (!rc && ms < best_ms) { best_ms = ms; best.bulk_threads = t.bulk_threads; best.bulk_unroll = t.bulk_unroll; }
-        }
+        for (int ui = 0; ui < 3 && !rc; ui++)
+            for (int sg = 0; sg < 3 && !rc; sg++) {
+                DpdTune t = best;
+                t.bulk_threads = DPD_TUNE_BULK_T[ti];
+                t.bulk_unroll = DPD_TUNE_BULK_U[ui];
+                t.bulk_stage = sg;
+                if (sg && s->cfg.rng != CTC_RNG_REFERENCE) continue;
+                if (sg == 1 && (t.bulk_unroll < 4 || t.bulk_threads != 128)) continue;
+                float ms = 0;
+                rc = time_it(1, t, ms);
+                if (!rc && ms < best_ms) {
+                    best_ms = ms;
+                    best.bulk_threads = t.bulk_threads;
+                    best.bulk_unroll = t.bulk_unroll;
+                    best.bulk_stage = t.bulk_stage;
+                }
+            }
     best_ms = 1e30f;
     for (int hi = 0; hi < 3 && !rc; hi++)
         for (int ui = 0; ui < 2 && !rc; ui++) {
@@ -985,12 +998,14 @@ extern "C" int ctc_sim_tune(ctc_sim *s, int reps, int *choice, void *stream) {
     // the state pos[cur] is untouched; the next step rebuilds the cell lists
     // and clears the forces as usual
     if (best.bulk_threads != s->tune.bulk_threads || best.bulk_unroll != s->tune.bulk_unroll ||
-        best.halo_threads != s->tune.halo_threads || best.halo_unroll != s->tune.halo_unroll)
+        best.halo_threads != s->tune.halo_threads || best.halo_unroll != s->tune.halo_unroll ||
+        best.bulk_stage != s->tune.bulk_stage)
         sim_drop_graphs(s);
     s->tune = best;
     if (choice) {
         choice[0] = best.bulk_threads; choice[1] = best.bulk_unroll;
         choice[2] = best.halo_threads; choice[3] = best.halo_unroll;
+        choice[4] = best.bulk_stage;
     }
     return CTC_OK;
 }

@@ -17,6 +17,7 @@ enum DevErr : int {
     DEV_PAIR_QUEUE = 2,        // internal queue misuse (never expected)
     DEV_BAD_PARTICLE = 3,      // NaN / out-of-range position after the wrap
     DEV_CELL_OVERFLOW = 4,     // more particles in one cell than the kernel supports
+    DEV_WAIT_TIMEOUT = 5,      // a bounded wait (an mbarrier of staged copies) gave up
 };
 
 __device__ __forceinline__ void set_error(int *err, int code) {

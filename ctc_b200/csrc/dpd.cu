@@ -22,6 +22,8 @@
 // aid/bid as src/exch/flu packs them and the per-fragment seeds and masks of
 // src/fluforces/imp/ini.h:11-59.  Stable keys (rng_mode 1):
 // mean0var1uu(seed, max(id), min(id)) of the particles' global ids.
+#include <type_traits>
+
 #include "common.cuh"
 #include "dpd.h"
 
@@ -41,9 +43,61 @@ __device__ __forceinline__ int frag_index(int3 L, const int *fss_fid, int fid, i
     return __ldg(fss_fid + hci) + off;
 }
 
-// queue records: (ia, ib), and the box in batched launches
+// ---------------------------------------------------------------------------
+// 1-D bulk copies global -> this CTA's shared memory, completed on an mbarrier
+// (cp.async.bulk, no multicast: the source is this GPU's own memory)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bytes: a multiple of 16; both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// waits for phase 0 of bar at most `limit` polls; false when it gave up
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned limit) {
+    for (unsigned it = 0; it < limit; it++)
+        if (mbar_try_wait(bar, 0)) return true;
+    return false;
+}
+
+// per-block staging of the bulk kernel's five half-stencil rows: the block's
+// targets are consecutive in the cell-sorted order, so each row offset (dz,
+// dy) maps the whole block onto one contiguous span of candidates
+constexpr int STG_CAP = 256;           // float4 positions staged per row offset
+struct BulkStage {
+    float4 pos[5][STG_CAP];
+    int lo[5], hi[5];                  // the span's candidates [lo, hi)
+    int wlo[8][5], whi[8][5];          // per-warp cell bounds of the rows
+    unsigned long long bar;
+    int ok;                            // 1: every row staged, 0: read from global
+};
+
+// queue records: (ia, ib), and the box in batched launches; REGP records:
+// (target's lane in the warp << 27 | ib, the candidate's position x y z)
 template <bool BATCH> struct BulkRec { uint2 v; };
 template <> struct BulkRec<true> { uint4 v; };
+struct BulkRecP { uint4 v; };
 
 // ---------------------------------------------------------------------------
 // bulk pairs: the reference's traversal (one target particle per thread, the
@@ -85,13 +139,25 @@ __device__ __forceinline__ void vjp_par(const DpdArgs &A, float da, float dg) {
 
 // T threads per block, UNROLL candidate loads in flight per lane; MODE 0
 // accumulates the forces, MODE 1 their vector-Jacobian product
-template <int RNG, bool BATCH, int T, int UNROLL, int MODE = 0>
-__global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs A) {
+// STAGE (one box, forces, T <= 256): the block's five candidate spans are
+// first copied into shared memory with bulk copies, and the filter reads them
+// there (a span longer than STG_CAP, or a wait that gives up, sends the block
+// to global loads)
+// REGP: the pair's data without scattered loads where it is at hand -- the
+// target's position and velocity come from its own lane of the warp by
+// shuffles (the queue only holds the warp's targets), the candidate's
+// position rides in the queue record from the filter; only the candidate's
+// velocity is loaded (one box, forces, reference keys)
+template <int RNG, bool BATCH, int T, int UNROLL, int MODE = 0, bool STAGE = false, bool REGP = false>
+__global__ void __launch_bounds__(T, STAGE ? 1024 / T : 1) k_dpd_bulk(const __grid_constant__ DpdArgs A) {
     constexpr int W = T / 32;
+    static_assert(!STAGE || (!BATCH && MODE == 0 && W <= 8), "staging: one box, forces, at most 8 warps");
+    static_assert(!REGP || (RNG == 0 && !BATCH && MODE == 0 && !STAGE), "REGP: one box, forces");
     // ring of accepted pairs per warp, drained every DR pushes: at most
     // 31 + 32 DR records wait (RQ a power of two above that)
     constexpr int DR = UNROLL < 4 ? UNROLL : 4, RQ = 256;
-    __shared__ BulkRec<BATCH> queue[W][RQ];
+    using Rec = typename std::conditional<REGP, BulkRecP, BulkRec<BATCH>>::type;
+    __shared__ Rec queue[W][RQ];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ia = blockIdx.x * T + threadIdx.x;
     int3 L = A.L;
@@ -110,23 +176,103 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
     const bool act = ia < n;
     const float *seeds = A.seeds_dev ? A.seeds_dev : A.seeds;
     const DpdPar P = A.par;
-    BulkRec<BATCH> *q = queue[warp];
+    Rec *q = queue[warp];
     unsigned head = 0, tail = 0;                    // ring positions (wrap at RQ)
     float acc_a = 0.0f, acc_g = 0.0f;               // MODE 1: parameter cotangents
 
-    float4 pa = make_float4(0, 0, 0, 0);
+    float4 pa = make_float4(0, 0, 0, 0), va = make_float4(0, 0, 0, 0);
+    const int ia0 = blockIdx.x * T + warp * 32;     // the warp's first target
     int cx = 0, cy = 0, cz = 0;
     if (act) {
         pa = __ldg(A.pos + ia);
+        if constexpr (REGP) va = __ldg(A.vel + ia);
         // get_cid (src/fluforces/bulk/dev/main.h:11-17): float, truncated
         cx = (int)(pa.x + (float)(L.x / 2));
         cy = (int)(pa.y + (float)(L.y / 2));
         cz = (int)(pa.z + (float)(L.z / 2));
     }
 
+    // ---- staging: the block's candidate spans into shared memory ----
+    __shared__ typename std::conditional<STAGE, BulkStage, int>::type stage_mem;
+    bool staged = false;
+    if constexpr (STAGE) {
+        BulkStage &S = stage_mem;
+        const int nc = L.x * L.y * L.z;
+        // the cell range of every row this target walks (none for rows
+        // outside the box), reduced over the warp, then over the block
+        for (int r = 0; r < 5; r++) {
+            const int dz = r < 3 ? -1 : 0, dy = r < 3 ? r - 1 : (r == 3 ? -1 : 0);
+            const int bz = cz + dz, by = cy + dy;
+            int c0 = 0x7fffffff, c1 = -1;
+            if (act && bz >= 0 && bz < L.z && by >= 0 && by < L.y) {
+                const int enddx = (dz == 0 && dy == 0) ? 0 : 1;
+                const int cid0 = L.x * (by + L.y * bz);
+                c0 = cid0 + max(0, cx - 1);
+                c1 = cid0 + 1 + min(L.x - 1, cx + enddx);
+            }
+            c0 = __reduce_min_sync(0xffffffffu, c0);
+            c1 = __reduce_max_sync(0xffffffffu, c1);
+            if (lane == 0) { S.wlo[warp][r] = c0; S.whi[warp][r] = c1; }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int ok = 1;
+            unsigned bytes = 0;
+            for (int r = 0; r < 5; r++) {
+                int c0 = 0x7fffffff, c1 = -1;
+                for (int w = 0; w < W; w++) { c0 = min(c0, S.wlo[w][r]); c1 = max(c1, S.whi[w][r]); }
+                int lo = 0, hi = 0;
+                if (c1 > c0) {
+                    lo = __ldg(starts + max(c0, 0));
+                    hi = __ldg(starts + min(c1, nc));
+                }
+                if (hi - lo > STG_CAP) ok = 0;
+                S.lo[r] = lo;
+                S.hi[r] = hi;
+                bytes += 16u * (unsigned)max(hi - lo, 0);
+            }
+            S.ok = ok;
+            if (ok) {
+                mbar_init(&S.bar, 1);
+                mbar_arrive_expect_tx(&S.bar, bytes);
+                for (int r = 0; r < 5; r++)
+                    if (S.hi[r] > S.lo[r])
+                        bulk_g2s(S.pos[r], A.pos + S.lo[r], 16u * (unsigned)(S.hi[r] - S.lo[r]), &S.bar);
+            }
+        }
+        __syncthreads();
+        if (S.ok) {
+            staged = mbar_wait_bounded(&S.bar, 1u << 22);
+            if (!staged) set_error(A.err, DEV_WAIT_TIMEOUT);
+            staged = __all_sync(0xffffffffu, staged);
+        }
+    }
+
     auto process = [&](int m) {
+        if constexpr (REGP) {
+            const uint4 rec = lane < m ? q[(head + lane) & (RQ - 1)].v : make_uint4(0u, 0u, 0u, 0u);
+            const int il = (int)(rec.x >> 27), j = (int)(rec.x & 0x7ffffffu);
+            // every lane shuffles (the target's lane il holds its position and velocity)
+            const float4 p1 = make_float4(__shfl_sync(0xffffffffu, pa.x, il), __shfl_sync(0xffffffffu, pa.y, il),
+                                          __shfl_sync(0xffffffffu, pa.z, il), 0.0f);
+            const float4 v1 = make_float4(__shfl_sync(0xffffffffu, va.x, il), __shfl_sync(0xffffffffu, va.y, il),
+                                          __shfl_sync(0xffffffffu, va.z, il), 0.0f);
+            if (lane < m) {
+                const int i = ia0 + il;
+                const float4 p2 = make_float4(__uint_as_float(rec.y), __uint_as_float(rec.z), __uint_as_float(rec.w),
+                                              0.0f);
+                const float rnd = mean0var1ii(seeds[0], i, j);   // i > j: the reference's (ia, ib)
+                float3 f;
+                if (dpd_force(P, p1, v1, p2, __ldg(A.vel + j), rnd, f)) {
+                    red_force(A.out, A.out_stride, i, 1.0f, f);
+                    red_force(A.out, A.out_stride, j, -1.0f, f);
+                }
+            }
+            __syncwarp();
+            return;
+        }
         if (lane < m) {
-            const BulkRec<BATCH> rec = q[(head + lane) & (RQ - 1)];
+            const Rec rec = q[(head + lane) & (RQ - 1)];
             const int i = (int)rec.v.x, j = (int)rec.v.y;
             float4 p1 = __ldg(A.pos + i), p2 = __ldg(A.pos + j);
             float4 v1 = __ldg(A.vel + i), v2 = __ldg(A.vel + j);
@@ -164,11 +310,14 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
         __syncwarp();
     };
 
-    auto push = [&](bool ok, int cand) {
+    auto push = [&](bool ok, int cand, const float4 &pbu) {
         const unsigned bal = __ballot_sync(0xffffffffu, ok);
         if (ok) {
-            BulkRec<BATCH> &e = q[(tail + __popc(bal & ((1u << lane) - 1u))) & (RQ - 1)];
-            if constexpr (BATCH) e.v = make_uint4((unsigned)ia, (unsigned)cand, (unsigned)box, 0u);
+            Rec &e = q[(tail + __popc(bal & ((1u << lane) - 1u))) & (RQ - 1)];
+            if constexpr (REGP)
+                e.v = make_uint4(((unsigned)(ia - ia0) << 27) | (unsigned)cand, __float_as_uint(pbu.x),
+                                 __float_as_uint(pbu.y), __float_as_uint(pbu.z));
+            else if constexpr (BATCH) e.v = make_uint4((unsigned)ia, (unsigned)cand, (unsigned)box, 0u);
             else e.v = make_uint2((unsigned)ia, (unsigned)cand);
         }
         tail += __popc(bal);
@@ -185,10 +334,12 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
     // -1..0 for the own row.  Every round a lane tests the next UNROLL
     // candidates of its row at once (independent loads in flight).
     int r = 0, ib = 0, be = 0;
+    int soff = 0;                // STAGE: candidate ib of the current row at stage_mem.pos[0][soff + ib]
     for (;;) {
         if (act) {
             while (ib >= be && r < 5) {
                 const int dz = r < 3 ? -1 : 0, dy = r < 3 ? r - 1 : (r == 3 ? -1 : 0);
+                if constexpr (STAGE) soff = r * STG_CAP - stage_mem.lo[r];
                 r++;
                 const int bz = cz + dz, by = cy + dy;
                 if (bz < 0 || bz >= L.z || by < 0 || by >= L.y) continue;
@@ -202,14 +353,21 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
         const bool have = act && ib < be;
         if (!__any_sync(0xffffffffu, have)) break;
         float4 pb[UNROLL];
+        if (STAGE && staged) {
+            const float4 *S0 = reinterpret_cast<const float4*>(&stage_mem) + soff;
 #pragma unroll
-        for (int u = 0; u < UNROLL; u++)
-            if (have && ib + u < be) pb[u] = __ldg(A.pos + ib + u);
+            for (int u = 0; u < UNROLL; u++)
+                if (have && ib + u < be) pb[u] = S0[ib + u];
+        } else {
+#pragma unroll
+            for (int u = 0; u < UNROLL; u++)
+                if (have && ib + u < be) pb[u] = __ldg(A.pos + ib + u);
+        }
 #pragma unroll
         for (int u = 0; u < UNROLL; u++) {
             const bool v = have && ib + u < be;
             const bool ok = v && dist2(pa.x - pb[u].x, pa.y - pb[u].y, pa.z - pb[u].z) <= 1.0f;   // cutoff_range
-            push(ok, ib + u);
+            push(ok, ib + u, pb[u]);
             if ((u + 1) % DR == 0) drain();
         }
         if (have) ib = min(ib + UNROLL, be);
@@ -217,6 +375,10 @@ __global__ void __launch_bounds__(T) k_dpd_bulk(const __grid_constant__ DpdArgs 
     __syncwarp();
     if (tail != head) process((int)(tail - head));
     if constexpr (MODE == 1) vjp_par(A, acc_a, acc_g);
+    if constexpr (STAGE) {
+        // a block whose wait gave up keeps its shared memory until the copies land
+        if (stage_mem.ok && !staged) mbar_wait_bounded(&stage_mem.bar, 1u << 22);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -765,6 +927,19 @@ cudaError_t frag_starts_boxes_launch(const Boxes &B, const int *counts, int *fss
 
 template <int RNG, bool BATCH>
 static void launch_bulk(const DpdArgs &A, int nmax, const DpdTune &t, cudaStream_t st) {
+    // the variants (DpdTune::bulk_stage): 1 candidate rows staged in shared
+    // memory, 2 the pairs' data from the target's lane and the queue record
+    if constexpr (RNG == 0 && !BATCH) {
+#define CTC_BULKV(TT, UU, V)                                                                  \
+    if (t.bulk_stage == V && t.bulk_threads == TT && t.bulk_unroll == UU) {                 \
+        k_dpd_bulk<0, false, TT, UU, 0, V == 1, V == 2><<<ceil_div(nmax, TT), TT, 0, st>>>(A); \
+        return;                                                                             \
+    }
+        CTC_BULKV(128, 4, 1) CTC_BULKV(128, 8, 1)
+        CTC_BULKV(128, 2, 2) CTC_BULKV(128, 4, 2) CTC_BULKV(128, 8, 2)
+        CTC_BULKV(256, 2, 2) CTC_BULKV(256, 4, 2) CTC_BULKV(256, 8, 2)
+    }
+#undef CTC_BULKV
     // every (threads, unroll) shape of DPD_TUNE_BULK_* for the reference keys;
     // the stable-key variant exists in the default shape only
 #define CTC_BULK(TT, UU)                                                             \
@@ -772,11 +947,12 @@ static void launch_bulk(const DpdArgs &A, int nmax, const DpdTune &t, cudaStream
         k_dpd_bulk<RNG, BATCH, TT, UU><<<ceil_div(nmax, TT), TT, 0, st>>>(A);        \
         return;                                                                      \
     }
-    if (RNG == 0) {
+    if (RNG == 0 && t.bulk_stage == 0) {
         CTC_BULK(128, 2) CTC_BULK(128, 4) CTC_BULK(128, 8)
         CTC_BULK(256, 2) CTC_BULK(256, 8)
     }
 #undef CTC_BULK
+
     k_dpd_bulk<RNG, BATCH, 256, 4><<<ceil_div(nmax, 256), 256, 0, st>>>(A);
 }
 

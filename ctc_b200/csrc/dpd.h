@@ -43,6 +43,8 @@ struct DpdTune {
     int bulk_unroll = 4;      // candidate loads in flight per lane: 2, 4 or 8
     int halo_threads = 128;   // 64, 128 or 256
     int halo_unroll = 2;      // halo candidate loads in flight per lane: 2 or 4
+    int bulk_stage = 0;       // bulk variant: 1 candidate rows staged in shared memory (128 threads x 4 or
+                              // 8 loads), 2 the pairs' data from the target's lane and the queue record
 };
 constexpr int DPD_TUNE_BULK_T[2] = {128, 256};
 constexpr int DPD_TUNE_BULK_U[3] = {2, 4, 8};

@@ -392,11 +392,16 @@ int ctc_sim_step(ctc_sim *s, int nsteps, void *stream);
  * steps run directly; 0: direct launches */
 int ctc_sim_set_graph(ctc_sim *s, int enable);
 /* autotuner: times every launch shape of the bulk and halo pair kernels
- * (as ctc_batch_tune) reps times on the current state without advancing it
- * (after at least one step), keeps the fastest; choice [host, 4] or NULL */
+ * (as ctc_batch_tune, and two variants of the bulk kernel: 1 its candidate
+ * rows staged in shared memory by bulk copies (128 threads x 4 or 8 loads),
+ * 2 the pairs' data taken from the target's lane and the queue record instead
+ * of scattered loads (any shape)) reps times on the current state without
+ * advancing it (after at least one step), keeps the fastest; choice [host,
+ * 5] = bulk threads, bulk unroll, halo threads, halo unroll, bulk variant
+ * (0..2), or NULL */
 int ctc_sim_tune(ctc_sim *s, int reps, int *choice, void *stream);
-/* sets the launch shapes of the pair kernels directly (choice as ctc_sim_tune
- * returns it); CTC_ERR_ARG for a shape the tuner does not offer */
+/* sets the launch shapes of the pair kernels directly (choice [host, 5] as
+ * ctc_sim_tune returns it); CTC_ERR_ARG for a shape the tuner does not offer */
 int ctc_sim_set_tune(ctc_sim *s, const int *choice);
 /* number of solvent particles (synchronises the stream) */
 int ctc_sim_count(ctc_sim *s, int *n, void *stream);

@@ -307,14 +307,17 @@ def test_bulk_kernel_golden(case):
     assert C.device_error() == 0
 
 
-ALL_SHAPES = [(bt, bu, ht, hu) for bt in (128, 256) for bu in (2, 4, 8) for ht in (64, 128, 256) for hu in (2, 4)]
+ALL_SHAPES = [(bt, bu, ht, hu, 0) for bt in (128, 256) for bu in (2, 4, 8) for ht in (64, 128, 256) for hu in (2, 4)] + \
+    [(128, bu, 128, 2, 1) for bu in (4, 8)] + [(bt, bu, 128, 2, 2) for bt in (128, 256) for bu in (2, 4, 8)]
 
 
 def test_sim_every_launch_shape_vs_modules():
     """Every launch shape the autotuner can pick for the fused step's pair
-    kernels (bulk threads x loads in flight, halo threads x loads in flight;
-    the C2 bench's 128 x 8 among them) gives the module entry points' forces
-    within 1e-5 on the same state and seeds."""
+    kernels (bulk threads x loads in flight, halo threads x loads in flight,
+    the bulk kernel's variants: candidate rows staged in shared memory, the
+    pair data taken from the target's lane and the queue record; the C2
+    bench's shapes among them) gives the module entry points' forces within 1e-5 on the same
+    state and seeds."""
     C = ctc()
     L = (16, 12, 10)
     pp = systems.solvent(L, seed=95)
@@ -344,4 +347,8 @@ def test_sim_set_tune_rejects_unknown_shape():
     sim = C.Sim((8, 8, 8), 5120, C.DpdParams(*systems.dpd_params()))
     with pytest.raises(_lib.CtcError):
         sim.set_tune((96, 4, 128, 2))
+    with pytest.raises(_lib.CtcError):
+        sim.set_tune((256, 4, 128, 2, 1))          # staging only at 128 threads
+    with pytest.raises(_lib.CtcError):
+        sim.set_tune((128, 2, 128, 2, 1))          # staging takes 4 or 8 loads
     sim.close()

@@ -85,7 +85,7 @@ def test_sim_tune_leaves_state():
         sim.step(1)
         if tune:
             shape = sim.tune(reps=1)
-            assert len(shape) == 4 and shape[0] in (128, 256) and shape[1] in (2, 4, 8)
+            assert len(shape) == 5 and shape[0] in (128, 256) and shape[1] in (2, 4, 8) and shape[4] in (0, 1, 2)
             assert shape[2] in (64, 128, 256) and shape[3] in (2, 4)
         seeds = sim.next_seeds()
         sim.step(2)
