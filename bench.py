@@ -1,6 +1,6 @@
 """Benchmark of the per-step particle hot path.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5|p64]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5|c2d|p64]
 
 Default (c2): one "step" = wrap + cell-list rebuild, bulk + periodic-halo DPD
 forces with the reference's pair RNG keys, constant body force, update -- the
@@ -59,6 +59,13 @@ CONFIGS = {
     "c4": dict(adjoint=True, L=(32, 32, 32), rbc=20, K=20, kck=5, bodyf=(0.0, 0.0, 0.0),
                name="C4 adjoint 32x32x32 rho=10 (327,680 solvent) + 20 RBC, loss = mean vertex x-velocity "
                     "after 20 steps, checkpoints every 5"),
+    # the C2 box decomposed over a periodic 2 x 2 x 2 cart (src/distr/flu +
+    # src/exch/flu): on one GPU the eight subdomains run as emulated ranks whose
+    # bags move by device copies; under torchrun each rank holds one subdomain of
+    # the C2 size and the bags move over NCCL
+    "c2d": dict(decomposed=True, L=(96, 48, 48), dims=(2, 2, 2), bodyf=(0.01, 0.0, 0.0), steps=200,
+                name="C2 192x96x96 rho=10 (17,694,720 particles), body force 0.01 x, decomposed into 2x2x2 "
+                     "subdomains of 96x48x48 with migration and halo exchange"),
     "c5": dict(batch=True, nbox=512, bodyf=(0.0, 0.0, 0.0), steps=100,
                name="C5 512 periodic boxes, edges uniform in 8..24, rho=10, one RBC in every 4th box"),
 }
@@ -424,6 +431,101 @@ def run_ours(args, cfg, world, rank, local):
 
 
 # ---------------------------------------------------------------------------
+# the decomposed solvent: ranks of a periodic cart with migration and halo
+# exchange (ctc_sub_*, ctc_b200/exch.py)
+# ---------------------------------------------------------------------------
+def run_decomposed(args, cfg, world, rank, local):
+    import torch
+
+    import ctc_b200 as ctc
+    from ctc_b200 import exch, systems
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world == 1:
+        dims, L = cfg["dims"], cfg["L"]
+        cart = exch.Cart(dims)
+        mine = list(range(cart.size))
+        transport = exch.LocalTransport(cart)
+        par = "%dx%dx%d cart emulated on 1 GPU (bags moved by device copies)" % dims
+    else:
+        import torch.distributed as dist
+        dims = {2: (2, 1, 1), 4: (2, 2, 1), 8: (2, 2, 2)}.get(world, (world, 1, 1))
+        L = tuple(d * l for d, l in zip(cfg["dims"], cfg["L"]))     # the C2 box per rank
+        cart = exch.Cart(dims)
+        mine = [rank]
+        group = dist.new_group(backend="nccl")
+        transport = exch.DistTransport(cart, rank, group, device=dev)
+        par = "%dx%dx%d cart, one subdomain per GPU (bags over NCCL)" % dims
+    dpd = ctc.DpdParams(*systems.dpd_params())
+    subs = []
+    for r in mine:
+        pp = systems.solvent(L, seed=2 + r)
+        n = len(pp)
+        sub = exch.SubDomain(L, cart, r, int(1.05 * n) + 4096, dpd, dt=systems.DT, bodyf=cfg["bodyf"], device=dev)
+        sub.set_solvent(pp, np.arange(r * n, (r + 1) * n, dtype=np.int32))
+        subs.append(sub)
+    for _ in range(args.warmup):
+        exch.step(subs, transport)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        exch.step(subs, transport)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier(world)
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    assert ctc.device_error() == 0, "device error during the timed steps"
+    # a few more steps with events between the phases (on the main stream)
+    phase = np.zeros(4)
+    for _ in range(3):
+        m = []
+        s0 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        exch.step(subs, transport, marks=m)
+        torch.cuda.synchronize()
+        ev = [s0] + m
+        phase += [ev[k].elapsed_time(ev[k + 1]) for k in range(4)]
+    phase /= 3
+    n_all = allsum(world, sum(s.count() for s in subs))
+    ms_max = allmax(world, ms)
+    # bytes each step moves between ranks: the last step's migration and halo records
+    moved = 0
+    for s in subs:
+        s.distr_pack()
+        s.exch_pack()
+        moved += 32 * (sum(s.distr_counts()) + sum(s.exch_counts()))
+    moved = allsum(world, moved)
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": n_all * args.steps / (ms_max * 1e-3), "unit": "particle-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform solvent, Maxwellian velocities)",
+        "config": {"workload": cfg["name"] if world == 1 else
+                   "C2 192x96x96 per GPU decomposed over %d GPUs" % world,
+                   "subdomain": list(L), "dims": list(dims), "particles": int(n_all), "rng": "reference keys",
+                   "parallelism": par, "l2": "inputs larger than L2"},
+        "host_ms_per_step": 1e3 * wall / args.steps,
+        "phase_ms": {"migration": phase[0], "cell_lists": phase[1], "pack_bulk_halo_exchange": phase[2],
+                     "halo_update": phase[3]},
+        "exchange_bytes_per_step": moved,
+    }
+    if clk:
+        line["clocks"] = clk
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # batched boxes: all boxes per launch (graph-replayed, autotuned) against one
 # single-box system per box stepped one after another
 # ---------------------------------------------------------------------------
@@ -649,6 +751,8 @@ def main():
         run_batch(args, cfg, world, rank, local)
     elif cfg.get("adjoint"):
         run_adjoint(args, cfg, world, rank, local)
+    elif cfg.get("decomposed"):
+        run_decomposed(args, cfg, world, rank, local)
     else:
         run_ours(args, cfg, world, rank, local)
     if world > 1:

@@ -132,6 +132,13 @@ class FluForces:
         check(lib().ctc_fluforces_apply_seeded(self.h, C.byref(params), int(pp.shape[0]), _ptr(pp), _ptr(starts),
                                                _ptr(counts), sd, int(which), int(rng), _ptr(ff), _stream(stream)))
 
+    def set_cart(self, dims, coords, rank, nbr):
+        """fluforces_halo_ini's per-rank set-up (src/fluforces/imp/ini.h:22-59):
+        the fragment trunks and key masks of the rank at coords of a periodic
+        dims cart whose neighbour in direction f is rank nbr[f]."""
+        check(lib().ctc_fluforces_set_cart(self.h, (C.c_int * 3)(*dims), (C.c_int * 3)(*coords), int(rank),
+                                           (C.c_int * 26)(*nbr)))
+
     def halo_frags(self, params, lpp, lii, rpp, rstart, ff, seeds26=None, stream=None):
         """fluforces_halo_prepare + _apply on exchanged fragments: lists of 26
         device tensors -- local fragment particles lpp[f] (n, 6), their indices

@@ -49,6 +49,11 @@ class SimConfig(C.Structure):
                 ("bodyf", C.c_float * 3), ("rng", C.c_int)]
 
 
+class SubConfig(C.Structure):
+    _fields_ = [("sim", SimConfig), ("dims", C.c_int * 3), ("coords", C.c_int * 3), ("rank", C.c_int),
+                ("nbr", C.c_int * 26), ("maxd", C.c_float)]
+
+
 class BatchConfig(C.Structure):
     _fields_ = [("nbox", C.c_int), ("L", C.POINTER(C.c_int)), ("n", C.POINTER(C.c_int)), ("dpd", DpdParams),
                 ("mass", C.c_float), ("dt", C.c_float), ("bodyf", C.c_float * 3), ("rng", C.c_int)]
@@ -161,6 +166,21 @@ SIGNATURES = {
     "ctc_sim_next_seeds": (C.c_int, [vp, fp]),
     "ctc_sim_profile": (C.c_int, [vp, C.c_int]),
     "ctc_sim_profile_read": (C.c_int, [vp, C.POINTER(C.c_double), ip]),
+    "ctc_sub_create": (C.c_int, [C.POINTER(SubConfig), C.POINTER(vp)]),
+    "ctc_sub_destroy": (C.c_int, [vp]),
+    "ctc_sub_set_solvent": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, vp]),
+    "ctc_sub_distr_pack": (C.c_int, [vp, vp]),
+    "ctc_sub_distr_counts": (C.c_int, [vp, ip]),
+    "ctc_sub_distr_unpack": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_exch_pack": (C.c_int, [vp, vp]),
+    "ctc_sub_exch_counts": (C.c_int, [vp, ip]),
+    "ctc_sub_bulk": (C.c_int, [vp, vp]),
+    "ctc_sub_halo_update": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_bags": (C.c_int, [vp, C.c_int, C.POINTER(vp), C.POINTER(vp), ip]),
+    "ctc_sub_count": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
+    "ctc_sub_seeds": (C.c_int, [vp, fp]),
+    "ctc_sub_masks": (C.c_int, [vp, C.POINTER(C.c_uint)]),
     "ctc_batch_create": (C.c_int, [C.POINTER(BatchConfig), C.POINTER(vp)]),
     "ctc_batch_destroy": (C.c_int, [vp]),
     "ctc_batch_set_solvent": (C.c_int, [vp, vp, vp]),

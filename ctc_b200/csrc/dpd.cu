@@ -658,6 +658,82 @@ cudaError_t halo_frags_launch(int3 L, const DpdPar &P, const HaloFrags &H, float
     return cudaGetLastError();
 }
 
+// the same pairs on the bags of a subdomain's exchange (records of two
+// float4: position with the id bits in w, velocity): one (fragment, local
+// particle) per thread; RNG 0 the fragment-local keys above, RNG 1 the
+// stable keys of the two ids under seeds[0] of the bulk
+template <int RNG>
+__global__ void k_dpd_halo_bags(int3 L, DpdPar P, const __grid_constant__ HaloBags H, float4 *ff, int *err) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= H.loff[26]) return;
+    int fid = 0;
+    while (fid < 25 && H.loff[fid + 1] <= t) fid++;
+    const int i = t - H.loff[fid];
+    float4 pa = __ldg(H.lbag + 2 * (size_t)t);
+    const float4 va = __ldg(H.lbag + 2 * (size_t)t + 1);
+    const int dx = frag_i2dx(fid), dy = frag_i2dy(fid), dz = frag_i2dz(fid);
+    const int xc = dx == 0 ? L.x : 1, yc = dy == 0 ? L.y : 1, zc = dz == 0 ? L.z : 1;
+    int xs = 1, ys = 1, zs = 1, l, id = 0;
+    if (dz == 0) { r2size_dev(pa.z, zc, L.z, l, zs); id += l; }
+    id *= yc;
+    if (dy == 0) { r2size_dev(pa.y, yc, L.y, l, ys); id += l; }
+    id *= xc;
+    if (dx == 0) { r2size_dev(pa.x, xc, L.x, l, xs); id += l; }
+    int rows, cols, jump;
+    const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+    if (nz == 1) {
+        if (dx) { rows = zs; cols = ys; jump = yc; }
+        else if (dy) { rows = zs; cols = xs; jump = xc; }
+        else { rows = ys; cols = xs; jump = xc; }
+    } else if (nz == 2) {
+        rows = jump = 1;
+        cols = max(xs, max(ys, zs));
+    } else {
+        rows = cols = jump = 1;
+    }
+    const int ncf = xc * yc * zc;
+    pa.x -= (float)(dx * L.x);
+    pa.y -= (float)(dy * L.y);
+    pa.z -= (float)(dz * L.z);
+    const bool mask = (H.masks >> fid) & 1u;
+    const float seed = RNG == 1 ? H.seed0 : H.seeds[fid];
+    const unsigned ga = (unsigned)__float_as_int(pa.w);
+    const float4 *rb = H.rbag + 2 * (size_t)H.roff[fid];
+    const int *rs = H.rstart + H.soff[fid];
+    float3 acc = make_float3(0.0f, 0.0f, 0.0f);
+    for (int r = 0; r < rows; r++) {
+        const int c0 = id + r * jump;
+        if (c0 < 0 || c0 + cols > ncf) { set_error(err, DEV_BAD_PARTICLE); continue; }
+        // the starts come from another rank: clip them to the records received
+        const int j0 = max(__ldg(rs + c0), 0), j1 = min(__ldg(rs + c0 + cols), H.rn[fid]);
+        for (int j = j0; j < j1; j++) {
+            const float4 pb = __ldg(rb + 2 * (size_t)j);
+            // the force's own r^2 (the same contraction): no key for a pair out of range
+            if (!(dist2(pa.x - pb.x, pa.y - pb.y, pa.z - pb.z) < 1.0f)) continue;
+            const float4 vb = __ldg(rb + 2 * (size_t)j + 1);
+            float rnd;
+            if (RNG == 1) {
+                const unsigned gb = (unsigned)__float_as_int(pb.w);
+                rnd = mean0var1uu(seed, max(ga, gb), min(ga, gb));
+            } else {
+                rnd = mean0var1uu(seed, mask ? (unsigned)i : (unsigned)j, mask ? (unsigned)j : (unsigned)i);
+            }
+            float3 f;
+            if (dpd_force(P, pa, va, pb, vb, rnd, f)) { acc.x += f.x; acc.y += f.y; acc.z += f.z; }
+        }
+    }
+    red_force((float*)ff, 4, __ldg(H.lii + t), 1.0f, acc);
+}
+
+cudaError_t halo_bags_launch(int3 L, const DpdPar &P, const HaloBags &H, int rng_mode, float4 *ff, int *err,
+                             cudaStream_t st) {
+    const int n = H.loff[26];
+    if (n <= 0) return cudaSuccess;
+    if (rng_mode == CTC_RNG_STABLE) k_dpd_halo_bags<1><<<ceil_div(n, 128), 128, 0, st>>>(L, P, H, ff, err);
+    else k_dpd_halo_bags<0><<<ceil_div(n, 128), 128, 0, st>>>(L, P, H, ff, err);
+    return cudaGetLastError();
+}
+
 // one local particle per thread, every fragment of its cell
 template <int RNG, bool BATCH, int T, int MODE = 0>
 __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs A) {

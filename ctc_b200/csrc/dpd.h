@@ -91,6 +91,24 @@ struct HaloFrags {
 };
 cudaError_t halo_frags_launch(int3 L, const DpdPar &P, const HaloFrags &H, float *ff, int fstride, int *err,
                               cudaStream_t st);
+// the same pairs on a subdomain's exchange bags: records of two float4
+// (position, id bits in w; velocity).  Local fragment f's i-th record is
+// lbag[2 (loff[f] + i)] and its particle index lii[loff[f] + i]; the bag
+// received from direction f holds rn[f] records from rbag[2 roff[f]] and its
+// fragment-cell starts from rstart[soff[f]]; forces into ff (float4)
+struct HaloBags {
+    const float4 *lbag;
+    const int *lii;
+    const float4 *rbag;
+    const int *rstart;
+    int loff[27];
+    int roff[26], rn[26], soff[26];
+    float seeds[26];        // reference keys: the fragment trunks' seeds
+    float seed0;            // stable keys: the bulk seed
+    unsigned masks;
+};
+cudaError_t halo_bags_launch(int3 L, const DpdPar &P, const HaloBags &H, int rng_mode, float4 *ff, int *err,
+                             cudaStream_t st);
 // vector-Jacobian product of the bulk (which & 1) and halo (which & 2) pair
 // forces, stable keys, one box
 cudaError_t dpd_vjp_launch(const DpdArgs &A, int nmax, cudaStream_t st);

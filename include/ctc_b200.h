@@ -469,6 +469,70 @@ int ctc_sim_next_seeds(const ctc_sim *s, float *seeds27);
 int ctc_sim_profile(ctc_sim *s, int enable);
 int ctc_sim_profile_read(ctc_sim *s, double *ms, int *steps);
 
+/* ---- one rank's subdomain of a decomposed periodic domain ----------------
+ * Replaces the solvent's migration (src/distr/flu/imp.h:6-35: dflu_build_map,
+ * dflu_pack, dflu_download, dflu_unpack, dflu_bulk/halo/gather), its halo
+ * exchange (src/exch/flu/imp.h:5-43: eflu_compute_map, eflu_pack,
+ * eflu_download_data, eflu_unpack, eflu_get_local/remote_frags) and the
+ * host-staged communication between them (src/comm/imp.h:52-63).  The bags
+ * stay in device memory: the caller's transport moves this rank's send bag
+ * for direction f (ctc_sub_bags) into the receive bag anti(f) of rank nbr[f]
+ * -- NCCL send/recv, or device copies when the ranks share a process.  A
+ * step (the reference's distribute_flu + forces_dpd + update_solvent,
+ * src/sim/imp/{distr,force,update}.h) is
+ *   distr_pack -> distr_counts -> exchange kind 0 -> distr_unpack ->
+ *   exch_pack -> bulk -> exch_counts -> exchange kinds 1 and 2 -> halo_update. */
+typedef struct ctc_sub ctc_sub;
+typedef struct {
+    ctc_sim_config sim;      /* subdomain box (LX, LY, LZ), capacity and physics */
+    int dims[3];             /* the periodic cart */
+    int coords[3];           /* this rank's place in it */
+    int rank;
+    int nbr[26];             /* rank of the neighbour in direction f (src/frag ids) */
+    float maxd;              /* maxdensity: bag capacities, as frag_hst::estimates */
+} ctc_sub_config;
+int ctc_sub_create(const ctc_sub_config *cfg, ctc_sub **s);
+int ctc_sub_destroy(ctc_sub *s);
+/* n particles pp [AoS] in subdomain coordinates and their global ids [n, or
+ * NULL for 0..n-1], both host (host = 1) or device (host = 0) arrays */
+int ctc_sub_set_solvent(ctc_sub *s, int n, const float *pp, const int *ids, int host, void *stream);
+/* dflu_build_map + dflu_pack: the particles that left into the 26 migration
+ * send bags; their counts start for the host */
+int ctc_sub_distr_pack(ctc_sub *s, void *stream);
+/* dflu_download: waits for those counts [host, 26], checks the capacities */
+int ctc_sub_distr_counts(ctc_sub *s, int *counts);
+/* dflu_unpack + dflu_bulk/halo/gather: rcounts [host, 26] received records,
+ * shifted into the subdomain and appended; cell lists of the whole */
+int ctc_sub_distr_unpack(ctc_sub *s, const int *rcounts, void *stream);
+/* eflu_compute_map + eflu_pack: the 26 boundary layers' particles and
+ * fragment-cell starts into the halo send bags; their counts start for the
+ * host */
+int ctc_sub_exch_pack(ctc_sub *s, void *stream);
+/* eflu_download_data: waits for those counts [host, 26], checks the capacities */
+int ctc_sub_exch_counts(ctc_sub *s, int *counts);
+/* fluforces_bulk_apply: clears the forces and adds the pairs inside, on the
+ * object's own stream after the work on `stream`, so that it runs while the
+ * halo bags travel */
+int ctc_sub_bulk(ctc_sub *s, void *stream);
+/* fluforces_halo_apply on the received bags (rcounts [host, 26]), body force
+ * and scheme_move_apply: ends the step */
+int ctc_sub_halo_update(ctc_sub *s, const int *rcounts, void *stream);
+/* exchange buffers [device addresses, 26 each]: kind 0 migration records, 1
+ * halo records (2 float4 each: position with the id bits in w, velocity), 2
+ * halo fragment-cell starts (ints, fixed sizes cap[f]); send[f] the last
+ * pack's bag for direction f, recv[f] where the bag from direction f goes,
+ * cap[f] its capacity in elements */
+int ctc_sub_bags(const ctc_sub *s, int kind, void **send, void **recv, int *cap);
+/* the number of particles (synchronises) */
+int ctc_sub_count(ctc_sub *s, int *n, void *stream);
+/* device pointers of the state: cell-sorted float4 positions (ids in w),
+ * velocities, the last step's forces, cell starts */
+int ctc_sub_state(ctc_sub *s, float **pos, float **vel, float **force, const int **starts);
+/* this step's seeds [host, 27]: [0] bulk, [1 + f] fragment f's trunk */
+int ctc_sub_seeds(ctc_sub *s, float *seeds27);
+/* the key masks of the rank's fragments (bit f) */
+int ctc_sub_masks(const ctc_sub *s, unsigned *masks);
+
 /* ---- many independent boxes per launch ----------------------------------
  * No single counterpart in the reference (it runs one domain per MPI rank);
  * each box is the periodic system a ctc_sim of its size would be -- its own
