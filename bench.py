@@ -578,30 +578,42 @@ def run_batch(args, cfg, world, rank, local):
     e2e_s = allmax(world, time.perf_counter() - t0)
     b.close()
 
-    # one launch per box: a single-box system per box, stepped box after box
+    # one system per box, stepped box after box: each tuned on its own state
+    # (ctc_sim_tune) and replayed as CUDA graphs, as the batched arm is; and
+    # the same without tuning and graphs (every kernel launched directly)
     pb_steps = max(1, min(args.steps, 5))
-    sims, o, ov = [], 0, 0
-    for k in range(len(n)):
-        s = ctc.Sim(tuple(L[k]), int(n[k]), dpd, mass=1.0, dt=systems.DT, bodyf=cfg["bodyf"])
-        s.set_solvent(pp[o:o + n[k]])
-        o += int(n[k])
-        if cells[k]:
-            s.set_membranes(pv[ov:ov + 642 * cells[k]], tri, 642, par, fsi, mass=systems.RBC_MASS)
-            ov += 642 * int(cells[k])
-        sims.append(s)
-    for s in sims:
-        s.step(1)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(pb_steps):
+
+    def per_box(tuned):
+        sims, o, ov = [], 0, 0
+        for k in range(len(n)):
+            s = ctc.Sim(tuple(L[k]), int(n[k]), dpd, mass=1.0, dt=systems.DT, bodyf=cfg["bodyf"])
+            s.set_solvent(pp[o:o + n[k]])
+            o += int(n[k])
+            if cells[k]:
+                s.set_membranes(pv[ov:ov + 642 * cells[k]], tri, 642, par, fsi, mass=systems.RBC_MASS)
+                ov += 642 * int(cells[k])
+            sims.append(s)
         for s in sims:
             s.step(1)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    pb_ms = allmax(world, e0.elapsed_time(e1))
-    for s in sims:
-        s.close()
-    pb_value = allsum(world, (ntot + nvt) * pb_steps) / (pb_ms * 1e-3)
+            if tuned:
+                s.tune(reps=2)
+                s.set_graph(True)
+        for s in sims:          # graph capture on the first replayed steps
+            s.step(2)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(pb_steps):
+            for s in sims:
+                s.step(1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = allmax(world, e0.elapsed_time(e1))
+        for s in sims:
+            s.close()
+        return allsum(world, (ntot + nvt) * pb_steps) / (ms * 1e-3), ms / pb_steps
+
+    pb_value, pb_ms_step = per_box(True)
+    pb_direct_value, pb_direct_ms = per_box(False)
     if rank != 0:
         return
     hbm, peak_kind = peaks()
@@ -625,9 +637,12 @@ def run_batch(args, cfg, world, rank, local):
         # for all boxes
         "gpu_launches": 22 * args.steps,
         "per_box": {"value": pb_value, "unit": "particle-steps/s", "steps": pb_steps,
-                    "ms_per_step": pb_ms / pb_steps,
-                    "launches_per_step": int(13 * len(n) + 9 * int(cells.sum())),
-                    "note": "one single-box system per box, stepped box after box on one stream"},
+                    "ms_per_step": pb_ms_step, "graph_launches_per_step": int(len(n)),
+                    "note": "one single-box system per box, stepped box after box on one stream, each "
+                            "autotuned (ctc_sim_tune) and replayed as a CUDA graph"},
+        "per_box_direct": {"value": pb_direct_value, "unit": "particle-steps/s", "ms_per_step": pb_direct_ms,
+                           "launches_per_step": int(13 * len(n) + 9 * int(cells.sum())),
+                           "note": "the same without tuning or graphs: every kernel launched directly"},
         "batched_over_per_box": value / pb_value,
         "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind + " (copy bandwidth)",

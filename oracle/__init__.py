@@ -91,6 +91,11 @@ def lib():
             "orc_area_volume_f32": (None, [C.c_int] * 3 + [i32p, f32p, f32p]),
             "orc_rbc_forces": (None, [C.c_int] * 5 + [i32p, i32p, f32p, f64p, RbcParams, f32p]),
             "orc_rbc_forces_f64": (None, [C.c_int] * 4 + [i32p, i32p, f32p, f64p, RbcParams, f64p]),
+            "orc_area_volume_d": (None, [C.c_int] * 3 + [i32p, f64p, f64p]),
+            "orc_rbc_forces_d": (None, [C.c_int] * 4 + [i32p, i32p, f64p, f64p, RbcParams, f64p]),
+            "orc_rollout_forces_d": (None, [C.c_int] * 4 + [f64p, i32p, f64p, C.c_float, C.c_int, f64p, f64p,
+                                                            C.c_float] + [C.c_int] * 4
+                                     + [i32p, i32p, i32p, RbcParams, f64p, f64p]),
             "orc_kantor_energy": (C.c_double, [C.c_int, C.c_int, i32p, i32p, f32p, C.c_double, C.c_double]),
             "orc_kantor_vertex_energy": (None, [C.c_int, C.c_int, i32p, i32p, f32p, C.c_double, C.c_double, f64p]),
             "orc_move": (None, [C.c_float, C.c_float, C.c_int, f32p, f32p]),
@@ -322,6 +327,31 @@ def rbc_forces(tri, nv, pp, params, av=None, mode=0, f64=False, ff=None):
         ff = np.zeros((len(pp), 3), np.float32) if ff is None else np.array(ff, np.float32).reshape(-1, 3)
         lib().orc_rbc_forces(mode, nc, nv, md, len(tri4), a0, a1, pp, av, par, ff)
     return ff
+
+
+def rollout_forces_f64(L, pp, ids, dpd, seed, pv=None, fsi=None, fseed=0.0, tri=None, nv=0, params=None):
+    """FP64 forces of one step of the differentiable rollout (stable keys):
+    solvent pairs, FSI and membrane forces from double positions; returns
+    (F (n, 3), Fv (nvt, 3)).  A test reference for the adjoint's gradients."""
+    pp = np.ascontiguousarray(pp, np.float64).reshape(-1, 6)
+    ids = np.ascontiguousarray(ids, np.int32)
+    F = np.zeros((len(pp), 3))
+    if pv is None:
+        pv, nc, md, a0, a1, tri4 = np.zeros((0, 6)), 0, 0, np.zeros(1, np.int32), np.zeros(1, np.int32), \
+            np.zeros(4, np.int32)
+        fsi, params = (0.0, 0.0, 0.0, 1.0), dict(gammaC=0, gammaT=0, kBT=0, kb=0, phi=0, ks=0, x0=0.5, mpow=2,
+                                                  ka=0, kd=0, kv=0, totArea=1, totVolume=1)
+        ntri = 0
+    else:
+        pv = np.ascontiguousarray(pv, np.float64).reshape(-1, 6)
+        tri4 = _tri4(tri)
+        md, a0, a1 = adj_build(tri4, nv)
+        nc, ntri = len(pv) // nv, len(tri4)
+    Fv = np.zeros((len(pv), 3))
+    lib().orc_rollout_forces_d(*L, len(pp), pp, ids, np.asarray(dpd, np.float64), float(seed), len(pv), pv,
+                               np.asarray(fsi, np.float64), float(fseed), nc, nv, md, ntri, a0, a1, tri4,
+                               RbcParams(**params), F, Fv)
+    return F, Fv
 
 
 def kantor_energy(tri, nv, pp, kb, phi_deg=0.0):

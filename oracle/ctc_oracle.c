@@ -1183,3 +1183,183 @@ void orc_diag(int n, const float *pp, double mass, double out[5]) {
     out[3] = n > 0 ? ke / (3.0 * n) : 0;
     out[4] = n;
 }
+
+/* ---------------------------------------------------------------------------
+ * FP64 forces of the differentiable rollout's step with stable keys (a test
+ * reference for the adjoint's gradients, not a restatement of a reference
+ * kernel): every input in double, the pair sets by minimum image through
+ * unit cells, the same pair force, keys and membrane formulas as above.
+ *   solvent: phi(r, e.dv) e with rnd = mean0var1uu(seed, max(id), min(id));
+ *   FSI (vertex k, solvent j): rnd = mean0var1uu(fseed, k, id_j), +f on the
+ *   vertex, -f on the solvent;
+ *   membranes: rbc_slot's double path (bending, triangle, viscous) on double
+ *   positions, the cells' area and volume in double.
+ * ------------------------------------------------------------------------- */
+static d3 posd(const double *pp, int i) { return mk(pp[6 * i], pp[6 * i + 1], pp[6 * i + 2]); }
+static d3 veld(const double *pp, int i) { return mk(pp[6 * i + 3], pp[6 * i + 4], pp[6 * i + 5]); }
+
+void orc_area_volume_d(int nc, int nv, int nt, const int *tri, const double *pp, double *av) {
+    int c, t;
+    for (c = 0; c < nc; c++) {
+        double A = 0, V = 0;
+        for (t = 0; t < nt; t++) {
+            d3 r0 = posd(pp, tri[4 * t] + c * nv), r1 = posd(pp, tri[4 * t + 1] + c * nv),
+               r2 = posd(pp, tri[4 * t + 2] + c * nv);
+            d3 n = crs(sub(r1, r0), sub(r2, r0));
+            A += 0.5 * sqrt(dot3(n, n));
+            V += ((r0.x * r1.y - r0.y * r1.x) * r2.z + (r0.z * r1.x - r0.x * r1.z) * r2.y +
+                  (r0.y * r1.z - r0.z * r1.y) * r2.x) / 6.0;
+        }
+        av[2 * c] = A; av[2 * c + 1] = V;
+    }
+}
+
+/* the membranes' internal forces (rbc_slot, mode 1) on double positions */
+void orc_rbc_forces_d(int nc, int nv, int md, int nt, const int *adj0, const int *adj1, const double *pp,
+                      const double *av, orc_rbc_params p, double *ff) {
+    int i, n = nc * nv * md;
+    double l0, a0;
+    stressful(nt, p.totArea, &l0, &a0);
+    for (i = 0; i < n; i++) {
+        int m[5], rbc;
+        d3 r0, r1, r2, r3, r4, f;
+        double phi;
+        if (!adj_map(md, nv, i, adj0, adj1, m)) continue;
+        rbc = m[0] / nv;
+        r0 = posd(pp, m[0]); r1 = posd(pp, m[1]); r2 = posd(pp, m[2]); r3 = posd(pp, m[3]); r4 = posd(pp, m[4]);
+        phi = p.phi / 180.0 * M_PI;
+        f = addv(dih(1, phi, p.kb, r0, r2, r1, r4), dih(2, phi, p.kb, r1, r0, r2, r3));
+        f = addv(f, ftri(1, &p, r0, r1, r2, l0, a0, av[2 * rbc], av[2 * rbc + 1]));
+        f = addv(f, fvisc(&p, r0, r1, veld(pp, m[0]), veld(pp, m[1])));
+        ff[3 * (i / md)] += f.x; ff[3 * (i / md) + 1] += f.y; ff[3 * (i / md) + 2] += f.z;
+    }
+}
+
+/* the DPD pair force in double: phi e for r^2 in [1e-6, 1) */
+static int pair_d(const double *d, const double *dv, double a, double g, double s, double spow, double rnd,
+                  double f[3]) {
+    double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2], r, e[3], ev, w, wr, phi;
+    if (r2 >= 1.0 || r2 < 1e-6) return 0;
+    r = sqrt(r2);
+    e[0] = d[0] / r; e[1] = d[1] / r; e[2] = d[2] / r;
+    ev = e[0] * dv[0] + e[1] * dv[1] + e[2] * dv[2];
+    w = 1.0 - r;
+    wr = pow(w, spow);
+    phi = (-g * wr * ev + s * rnd) * wr + a * w;
+    f[0] = phi * e[0]; f[1] = phi * e[1]; f[2] = phi * e[2];
+    return 1;
+}
+
+static void min_image(const int L[3], double *d) {
+    int c;
+    for (c = 0; c < 3; c++) d[c] -= L[c] * floor(d[c] / L[c] + 0.5);
+}
+
+/* unit-cell lists of n particles (double AoS, inside [-L/2, L/2) after a wrap) */
+static void cells_d(const int L[3], int n, const double *pp, int *start, int *order) {
+    int nc = L[0] * L[1] * L[2], i, *cnt = calloc(nc + 1, sizeof(int)), *cid = malloc(sizeof(int) * (n > 0 ? n : 1));
+    for (i = 0; i < n; i++) {
+        int c, k[3];
+        for (c = 0; c < 3; c++) {
+            double x = pp[6 * i + c] + L[c] / 2;   /* -(L/2) for even L */
+            x -= L[c] * floor(x / L[c]);
+            k[c] = (int)x;
+            if (k[c] >= L[c]) k[c] = L[c] - 1;
+        }
+        cid[i] = k[0] + L[0] * (k[1] + L[1] * k[2]);
+        cnt[cid[i] + 1]++;
+    }
+    for (i = 0; i < nc; i++) cnt[i + 1] += cnt[i];
+    memcpy(start, cnt, sizeof(int) * (nc + 1));
+    for (i = 0; i < n; i++) order[cnt[cid[i]]++] = i;
+    free(cnt); free(cid);
+}
+
+void orc_rollout_forces_d(int LX, int LY, int LZ, int n, const double *pp, const int *ids, const double dpd[4],
+                          float seed, int nvt, const double *pv, const double fsi[4], float fseed,
+                          int nc, int nv, int md, int nt, const int *adj0, const int *adj1, const int *tri,
+                          orc_rbc_params p, double *F, double *Fv) {
+    const int L[3] = {LX, LY, LZ};
+    int ncell = LX * LY * LZ, *start = malloc(sizeof(int) * (ncell + 1)), *order = malloc(sizeof(int) * (n > 0 ? n : 1));
+    int i;
+    cells_d(L, n, pp, start, order);
+    /* solvent pairs: each particle against the 27 cells around it, every
+     * pair once (j > i), -f onto the other side */
+    _Pragma("omp parallel for schedule(dynamic, 256)")
+    for (i = 0; i < n; i++) {
+        int c, k[3], dx, dy, dz;
+        double acc[3] = {0, 0, 0};
+        for (c = 0; c < 3; c++) {
+            double x = pp[6 * i + c] + L[c] / 2;
+            x -= L[c] * floor(x / L[c]);
+            k[c] = (int)x;
+            if (k[c] >= L[c]) k[c] = L[c] - 1;
+        }
+        for (dz = -1; dz <= 1; dz++)
+            for (dy = -1; dy <= 1; dy++)
+                for (dx = -1; dx <= 1; dx++) {
+                    int q[3] = {k[0] + dx, k[1] + dy, k[2] + dz}, cc, s;
+                    for (c = 0; c < 3; c++) q[c] = (q[c] + L[c]) % L[c];
+                    cc = q[0] + L[0] * (q[1] + L[1] * q[2]);
+                    for (s = start[cc]; s < start[cc + 1]; s++) {
+                        int j = order[s];
+                        double d[3], dv[3], f[3], rnd, r2;
+                        uint32_t gi = (uint32_t)ids[i], gj = (uint32_t)ids[j];
+                        if (j <= i) continue;
+                        for (c = 0; c < 3; c++) {
+                            d[c] = pp[6 * i + c] - pp[6 * j + c];
+                            if (d[c] > 0.5 * L[c]) d[c] -= L[c];
+                            else if (d[c] < -0.5 * L[c]) d[c] += L[c];
+                        }
+                        r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                        if (r2 >= 1.0) continue;
+                        for (c = 0; c < 3; c++) dv[c] = pp[6 * i + 3 + c] - pp[6 * j + 3 + c];
+                        rnd = orc_mean0var1uu(seed, gi > gj ? gi : gj, gi > gj ? gj : gi);
+                        if (pair_d(d, dv, dpd[0], dpd[1], dpd[2], dpd[3], rnd, f))
+                            for (c = 0; c < 3; c++) {
+                                acc[c] += f[c];
+                                _Pragma("omp atomic")
+                                F[3 * j + c] -= f[c];
+                            }
+                    }
+                }
+        for (c = 0; c < 3; c++) {
+            _Pragma("omp atomic")
+            F[3 * i + c] += acc[c];
+        }
+    }
+    /* FSI: vertex k against the solvent of the 27 cells around it */
+    for (i = 0; i < nvt; i++) {
+        int c, k[3], dx, dy, dz;
+        for (c = 0; c < 3; c++) {
+            double x = pv[6 * i + c] + L[c] / 2;
+            x -= L[c] * floor(x / L[c]);
+            k[c] = (int)x;
+            if (k[c] >= L[c]) k[c] = L[c] - 1;
+        }
+        for (dz = -1; dz <= 1; dz++)
+            for (dy = -1; dy <= 1; dy++)
+                for (dx = -1; dx <= 1; dx++) {
+                    int q[3] = {k[0] + dx, k[1] + dy, k[2] + dz}, cc, s;
+                    for (c = 0; c < 3; c++) q[c] = (q[c] + L[c]) % L[c];
+                    cc = q[0] + L[0] * (q[1] + L[1] * q[2]);
+                    for (s = start[cc]; s < start[cc + 1]; s++) {
+                        int j = order[s];
+                        double d[3], dv[3], f[3], rnd;
+                        for (c = 0; c < 3; c++) { d[c] = pv[6 * i + c] - pp[6 * j + c]; dv[c] = pv[6 * i + 3 + c] - pp[6 * j + 3 + c]; }
+                        min_image(L, d);
+                        if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] >= 1.0) continue;
+                        rnd = orc_mean0var1uu(fseed, (uint32_t)i, (uint32_t)ids[j]);
+                        if (pair_d(d, dv, fsi[0], fsi[1], fsi[2], fsi[3], rnd, f))
+                            for (c = 0; c < 3; c++) { Fv[3 * i + c] += f[c]; F[3 * j + c] -= f[c]; }
+                    }
+                }
+    }
+    if (nc > 0) {
+        double *av = malloc(sizeof(double) * 2 * nc);
+        orc_area_volume_d(nc, nv, nt, tri, pv, av);
+        orc_rbc_forces_d(nc, nv, md, nt, adj0, adj1, pv, av, p, Fv);
+        free(av);
+    }
+    free(start); free(order);
+}

@@ -116,6 +116,15 @@ void orc_rbc_forces(int mode, int nc, int nv, int md, int nt, const int *adj0, c
                     const float *pp, const double *av, orc_rbc_params p, float *ff);
 void orc_rbc_forces_f64(int nc, int nv, int md, int nt, const int *adj0, const int *adj1,
                         const float *pp, const double *av, orc_rbc_params p, double *ff);
+/* the same from double positions, and the FP64 forces of a step of the
+ * differentiable rollout (stable keys; a test reference for its gradients) */
+void orc_area_volume_d(int nc, int nv, int nt, const int *tri, const double *pp, double *av);
+void orc_rbc_forces_d(int nc, int nv, int md, int nt, const int *adj0, const int *adj1, const double *pp,
+                      const double *av, orc_rbc_params p, double *ff);
+void orc_rollout_forces_d(int LX, int LY, int LZ, int n, const double *pp, const int *ids, const double dpd[4],
+                          float seed, int nvt, const double *pv, const double fsi[4], float fseed,
+                          int nc, int nv, int md, int nt, const int *adj0, const int *adj1, const int *tri,
+                          orc_rbc_params p, double *F, double *Fv);
 /* Kantor energy per edge summed per vertex is not on the path; the
  * dihedral angle of every (vertex, slot) is exposed for known answers */
 double orc_kantor_energy(int nv, int md, const int *adj0, const int *adj1, const float *pp,

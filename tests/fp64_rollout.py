@@ -72,3 +72,54 @@ def step_seeds(K):
     """The solvent seeds of K steps: the trunk seeded (0, 0, 0, 0), once a step."""
     k = oracle.Kiss(0, 0, 0, 0)
     return [k.get() for _ in range(K)]
+
+
+def full_seeds(K):
+    """Per step: the solvent seed (trunk (0, 0, 0, 0), once a step) and the
+    FSI seed (trunk rnd_ini(1908, 1409, 290, 12968), the first of its two
+    draws a step; with stable keys the bulk seed keys every FSI pair)."""
+    kb, kf = oracle.Kiss(0, 0, 0, 0), oracle.Kiss(1908, 1409, 290, 12968)
+    out = []
+    for _ in range(K):
+        s = kb.get()
+        f = kf.get()
+        kf.get()
+        out.append((s, f))
+    return out
+
+
+def _rbc_wrap(L, pv, nv):
+    """A cell whose bounding-box centre left [-L/2, L/2) re-enters whole."""
+    lo = -(L // 2)
+    for c in range(len(pv) // nv):
+        q = pv[c * nv:(c + 1) * nv]
+        r = 0.5 * (q[:, :3].min(0) + q[:, :3].max(0))
+        d = -1 + (r >= lo).astype(int) + (r >= lo + L).astype(int)
+        q[:, :3] -= d * L
+
+
+def full_rollout(L, pp, pv, tri, nv, theta, rbc, fsi, K, seeds, spow=0.25, kBT=0.0444, dt=5e-4, mass=1.0,
+                 mmass=0.5):
+    """Solvent + membranes, K steps in double with stable keys, the step of
+    the device rollout: wrap, solvent pairs (a, gamma = theta[:2], sigma from
+    gamma), FSI, membrane forces (ks, kb = theta[2:]), then both updates.
+    Returns the final solvent (AoS, by particle id) and vertices (AoS)."""
+    Li = np.asarray(L, np.int64)
+    Lf = Li.astype(np.float64)
+    lo = -(Li // 2).astype(np.float64)
+    x = np.array(pp, np.float64)
+    xv = np.array(pv, np.float64)
+    ids = np.arange(len(x), dtype=np.int32)
+    a, g, ks, kb = (float(t) for t in theta)
+    s = np.sqrt(2.0 * kBT * g / dt)
+    par = dict(rbc, ks=ks, kb=kb)
+    for t in range(K):
+        x[:, :3] = lo + np.mod(x[:, :3] - lo, Lf)
+        _rbc_wrap(Li, xv, nv)
+        F, Fv = oracle.rollout_forces_f64(tuple(int(l) for l in Li), x, ids, (a, g, s, spow), seeds[t][0], xv, fsi,
+                                          seeds[t][1], tri, nv, par)
+        x[:, 3:] += F / mass * dt
+        x[:, :3] += x[:, 3:] * dt
+        xv[:, 3:] += Fv / mmass * dt
+        xv[:, :3] += xv[:, 3:] * dt
+    return x, xv

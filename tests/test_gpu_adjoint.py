@@ -149,3 +149,107 @@ def test_autograd_wrapper_matches_direct_backward():
     np.testing.assert_allclose(xv.grad.numpy(), g["gxv"], rtol=1e-3, atol=1e-6 * np.abs(g["gxv"]).max())
     assert xs.grad.shape == xs.shape
     r.close()
+
+
+def _fp64_reference_check(L, ncell, K, kck, seed, spow, params=(0, 1, 2, 3), nvert=3, nsolv=2, hs=(1e-6,),
+                          label=""):
+    """The adjoint's gradient of the configuration's loss (mean x-velocity of
+    the vertices after K steps) against central differences of the FP64 host
+    rollout (tests/fp64_rollout.full_rollout: the same dynamics in double,
+    stable keys) with steps hs -- for the parameters listed and the initial
+    positions of the nvert vertices and nsolv solvent particles with the
+    largest gradients.  Returns {component: (adjoint, [differences per h])}."""
+    from ctc_b200.adjoint import Rollout
+    from tests import fp64_rollout as R
+    pp = systems.solvent(L, seed=seed)
+    pv, tri, par = systems.rbc_system(L, ncell, seed=seed + 1)
+    dpd = list(systems.dpd_params())
+    dpd[3] = spow
+    fsi = (0.0, 8.0, dpd[2], dpd[3])
+    r = Rollout(L, pp, dpd, systems.KBT, systems.DT, pv=pv, tri=tri, rbc=par, fsi=fsi, mmass=systems.RBC_MASS)
+    theta = np.array([systems.A_DPD, systems.GAMMA, par["ks"], par["kb"]])
+    r.set_params(theta)
+    r.forward(K, kck)
+    g = r.backward()
+    r.close()
+    seeds = R.full_seeds(K)
+    f32 = lambda x: float(np.float32(x))
+    kw = dict(spow=f32(spow), kBT=f32(systems.KBT), dt=f32(systems.DT), mmass=f32(systems.RBC_MASS))
+
+    def loss(th, pp_=pp, pv_=pv):
+        _, xv = R.full_rollout(L, pp_, pv_, tri, 642, th, par, fsi, K, seeds, **kw)
+        return float(xv[:, 3].mean())
+
+    out = {}
+    for k in params:
+        fds = []
+        for hr in hs:
+            h = hr * max(1.0, abs(theta[k]))
+            if k >= 2:
+                # ks and kb reach the membrane forces as floats (RbcParams):
+                # a step of whole float ulps, so that theta +- h is exact
+                u = float(np.spacing(np.float32(theta[k])))
+                h = u * max(1.0, np.round(h / u))
+            tp, tm = theta.copy(), theta.copy()
+            tp[k] += h
+            tm[k] -= h
+            fds.append((loss(tp) - loss(tm)) / (2 * h))
+        out[("a", "gamma", "ks", "kb")[k]] = (float(g["theta"][k]), fds)
+    for which, arr, gk, cnt in (("vertex", pv, g["gxv"], nvert), ("solvent", pp, g["gx"], nsolv)):
+        for f in np.argsort(np.abs(gk).ravel())[::-1][:cnt]:
+            i, c = divmod(int(f), 3)
+            fds = []
+            for h in hs:
+                ap, am = arr.astype(np.float64), arr.astype(np.float64)
+                ap[i, c] += h
+                am[i, c] -= h
+                if which == "vertex":
+                    fds.append((loss(theta, pp, ap) - loss(theta, pp, am)) / (2 * h))
+                else:
+                    fds.append((loss(theta, ap, pv) - loss(theta, am, pv)) / (2 * h))
+            out["%s %d.%d" % (which, i, c)] = (float(gk[i, c]), fds)
+    print(label, {k: "adj %.7e fd %s rel %.2e" % (a, ["%.7e" % x for x in f], abs(a - f[0]) / abs(f[0]))
+                  for k, (a, f) in out.items()})
+    return out
+
+
+def test_adjoint_vs_fp64_reference_smooth_weight():
+    """Solvent + one red blood cell in a 12^3 box, K = 4, checkpoints every
+    2, the pair weight (1 - r)^1: every parameter and the largest position
+    gradients within 1e-4 of the FP64 reference (measured: 1e-6 .. 7e-5)."""
+    out = _fp64_reference_check((12, 12, 12), 1, 4, 2, seed=61, spow=1.0, label="spow 1")
+    for k, (a, f) in out.items():
+        assert abs(a - f[0]) <= 1e-4 * abs(f[0]), (k, a, f)
+
+
+def test_adjoint_vs_fp64_reference_configuration_weight():
+    """The same system with the configurations' weight (1 - r)^0.25.  The
+    force then has an unbounded slope at the cutoff, and a gradient
+    component that a pair close to the cutoff carries is not resolved by
+    finite differences of any step: the FP64 differences at steps 1e-6 and
+    1e-7 still differ by up to a few percent (the position components with
+    the largest gradients are exactly those).  Measured bound: every
+    component lies within twice the spread of the two differences plus 2e-4
+    of the value; the parameters, whose differences do converge, within 2e-3
+    (measured: a 1.1e-3, gamma 7e-4, ks and kb 1.2e-4 -- the FP32 positions
+    of pairs within ~1e-6 of the cutoff, where the slope (1 - r)^-0.75 is
+    steep, differ from the FP64 ones by rounding, and so do their
+    contributions; with the smooth weight above the same code agrees to
+    7e-5)."""
+    out = _fp64_reference_check((12, 12, 12), 1, 4, 2, seed=61, spow=0.25, hs=(1e-6, 1e-7), label="spow 0.25")
+    for k, (a, (f1, f2)) in out.items():
+        assert abs(a - f2) <= 2 * abs(f1 - f2) + 2e-4 * abs(f2), (k, a, f1, f2)
+        if k in ("a", "gamma", "ks", "kb"):
+            assert abs(a - f2) <= 2e-3 * abs(f2), (k, a, f1, f2)
+
+
+def test_c4_configuration_gradients_vs_fp64_reference():
+    """The C4 configuration itself -- 32^3 at density 10 with 20 cells, K =
+    20, checkpoints every 5 -- with the smooth pair weight (1 - r)^1 (the
+    kernels take the exponent as a parameter, the code is the same): the four
+    parameters and the largest vertex and solvent position gradients within
+    1e-4 of the FP64 reference (each FP64 rollout of this size takes seconds
+    on the host).  Measured: the parameters 1e-5 .. 6e-5, the positions 4e-6."""
+    out = _fp64_reference_check((32, 32, 32), 20, 20, 5, seed=71, spow=1.0, nvert=1, nsolv=1, label="C4")
+    for k, (a, f) in out.items():
+        assert abs(a - f[0]) <= 1e-4 * abs(f[0]), (k, a, f)
