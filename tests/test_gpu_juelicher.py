@@ -74,16 +74,39 @@ def test_juelicher_vs_oracle(template, noise):
     assert err < 1e-6
 
 
+def _dev_juelicher(C, F, nv, pp, par):
+    mod = C.RbcForce(F, nv, 4)
+    mod.set_bending("juelicher")
+    ff = torch.zeros((len(pp), 3), device="cuda")
+    mod.apply(C.RbcParams(**_only_bending(par)), dev(pp), ff)
+    return ff.cpu().numpy()
+
+
 @pytest.mark.skipif(not refkern.available(), reason="oracle/_ref/librefkern.so not built")
 @pytest.mark.parametrize("template", ["642.off", "evans-fung"])
 def test_juelicher_vs_reference_kernels(template):
+    """The reference's nine kernels sum their per-triangle and per-edge
+    terms in float with atomics, in an order that changes from run to run;
+    this build gathers per vertex in double.  Measured against the FP64
+    oracle: this build 6e-8, the reference's kernels 1.2e-5 and 2.4e-5 (the
+    two templates); two runs of the reference's kernels on the same input
+    differ from each other by 1.4e-5 and 2.0e-5.  The gap between the two
+    builds is the reference's own float accumulation, which varies from run
+    to run by more than 1e-5: no build can reproduce it more closely, so the
+    bar is 5e-5 here and this build is held to 1e-6 of the oracle."""
     import ctc_b200 as C
     pp, F, nv, par = _cells(4, 6, template)
     fr = torch.zeros((len(pp), 3), device="cuda")
     refkern.juelicher(F, nv, dev(pp), fr)
     ref = fr.cpu().numpy()
+    fr2 = torch.zeros((len(pp), 3), device="cuda")
+    refkern.juelicher(F, nv, dev(pp), fr2)
+    e_runs = rel_err(fr2.cpu().numpy(), ref)
     orc = oracle.juelicher_forces(F, nv, pp)
     e_orc = rel_err(ref, orc)
+    e_me = rel_err(_dev_juelicher(C, F, nv, pp, par), orc)
+    print("juelicher reference kernels: run to run", e_runs, "vs FP64 oracle", e_orc, "; this build vs oracle", e_me)
+    assert e_me < 1e-6 and e_me < e_orc
     mod = C.RbcForce(F, nv, 4)
     mod.set_bending("juelicher")
     ff = torch.zeros((len(pp), 3), device="cuda")
