@@ -565,6 +565,20 @@ def run_batch(args, cfg, world, rank, local):
     total = allsum(world, (ntot + nvt) * args.steps)
     value = total / (ms_max * 1e-3)
 
+    # the same steps as ONE persistent launch each (grid-wide barriers between
+    # the stages), replayed as a graph of that one launch
+    b.set_persistent(True)
+    b.step(2)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    assert ctc.device_error() == 0, "device error during the persistent steps"
+    p_ms = allmax(world, e0.elapsed_time(e1))
+    p_blocks = b.persistent_grid()
+    b.set_persistent(False)
+
     # end to end through the public API: host state in, K steps, host state out
     barrier(world)
     torch.cuda.synchronize()
@@ -643,6 +657,10 @@ def run_batch(args, cfg, world, rank, local):
         "per_box_direct": {"value": pb_direct_value, "unit": "particle-steps/s", "ms_per_step": pb_direct_ms,
                            "launches_per_step": int(13 * len(n) + 9 * int(cells.sum())),
                            "note": "the same without tuning or graphs: every kernel launched directly"},
+        "persistent": {"value": total / (p_ms * 1e-3), "unit": "particle-steps/s", "ms_per_step": p_ms / args.steps,
+                       "launches_per_step": 1, "blocks": p_blocks,
+                       "note": "every stage of the step in one cooperative launch, 12 grid-wide barriers, "
+                               "256 threads x 2 loads (bulk and halo), replayed as a one-node graph"},
         "batched_over_per_box": value / pb_value,
         "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind + " (copy bandwidth)",

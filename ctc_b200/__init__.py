@@ -752,6 +752,24 @@ class Batch:
     def set_graph(self, enable=True):
         check(lib().ctc_batch_set_graph(self.h, int(bool(enable))))
 
+    def set_persistent(self, enable=True):
+        """Each step as one persistent cooperative launch (grid-wide barriers
+        between its stages) instead of one launch per stage."""
+        check(lib().ctc_batch_set_persistent(self.h, int(bool(enable))))
+
+    def persistent_check(self, barrier, stream=None):
+        """One persistent step in which block 0 never arrives at `barrier`:
+        returns the launch's blocks; the device error word then holds
+        CTC_DEV_WAIT_TIMEOUT (the state is undefined)."""
+        blocks = C.c_int(0)
+        check(lib().ctc_batch_persistent_check(self.h, int(barrier), C.byref(blocks), _stream(stream)))
+        return blocks.value
+
+    def persistent_grid(self):
+        blocks = C.c_int(0)
+        check(lib().ctc_batch_persistent_grid(self.h, C.byref(blocks)))
+        return blocks.value
+
     def tune(self, reps=3, stream=None):
         """Autotune the pair kernels' launch shapes on the current state;
         returns (bulk threads, bulk unroll, halo threads, halo unroll)."""

@@ -6,8 +6,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libctc_b200.so")
 
-SOURCES = ["api.cu", "api_adjoint.cu", "api_batch.cu", "api_objects.cu", "clist.cu", "clist_noalloc.cu", "cnt.cu", "dpd.cu", "fsi.cu", "integrate.cu", "io_ply.cu", "io_bop.cu", "wall.cu", "api_wall.cu", "exch.cu",
-           "membrane.cu", "membrane_vjp.cu"]
+# kernels.cu compiles clist.cu, dpd.cu, fsi.cu, integrate.cu and membrane.cu
+# as one translation unit, with the persistent batched step built from their
+# kernel bodies
+SOURCES = ["api.cu", "api_adjoint.cu", "api_batch.cu", "api_objects.cu", "kernels.cu", "clist_noalloc.cu", "cnt.cu",
+           "io_ply.cu", "io_bop.cu", "wall.cu", "api_wall.cu", "exch.cu", "membrane_vjp.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -9,6 +9,10 @@
 // fragment-cell starts and FSI image lists.  The particles and cells of the
 // boxes are concatenated; a box keeps its particle range for good because
 // its particles only re-enter through its own periodic faces.
+//
+// ctc_batch_set_persistent switches the step to ONE persistent cooperative
+// launch (kernels.cu: k_batch_persistent) that runs the same stages with
+// grid-wide barriers between them.
 #include <algorithm>
 #include <cstdio>
 #include <vector>
@@ -19,6 +23,7 @@
 #include "fsi.h"
 #include "integrate.h"
 #include "membrane.h"
+#include "persist.h"
 
 using namespace ctc;
 
@@ -61,6 +66,10 @@ struct ctc_batch {
     cudaStream_t own = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};   // one step from buffer 0, one from buffer 1
+    // the step as one persistent launch (ctc_batch_set_persistent)
+    bool persistent = false;
+    GridBar *bar = nullptr;
+    int grid = 0;                                    // its blocks at the last launch
 };
 
 static void drop_graphs(ctc_batch *b) {
@@ -87,6 +96,7 @@ extern "C" int ctc_batch_destroy(ctc_batch *b) {
     cudaFree(b->scratch); cudaFree(b->trunk); cudaFree(b->ftrunk); cudaFree(b->seeds); cudaFree(b->fseeds);
     cudaFree(b->d_tab); cudaFree(b->d_L);
     cudaFree(b->pack); cudaFree(b->pack_off); cudaFree(b->coff);
+    cudaFree(b->bar);
     if (b->ev_in) cudaEventDestroy(b->ev_in);
     if (b->ev_out) cudaEventDestroy(b->ev_out);
     if (b->own) cudaStreamDestroy(b->own);
@@ -283,8 +293,78 @@ extern "C" int ctc_batch_set_membranes(ctc_batch *b, const int *cells, int nv, i
     return CTC_OK;
 }
 
+// the persistent step's arguments: the same buffers and stages as below
+static int persist_args(ctc_batch *b, PersistArgs *P, int hold) {
+    const int src = b->cur, dst = 1 - b->cur;
+    memset(P, 0, sizeof(*P));
+    P->B = b->B;
+    P->nbox = b->nbox; P->ntot = b->ntot; P->nctot = b->nctot;
+    P->pos_src = b->pos[src]; P->vel_src = b->vel[src];
+    P->pos = b->pos[dst]; P->vel = b->vel[dst]; P->force = b->force;
+    P->counts = b->counts; P->starts = b->starts; P->ntot_dev = b->ntot_dev;
+    P->w = b->w;
+    P->trunk = b->trunk; P->seeds = b->seeds;
+    dpd_args_common(&P->A, make_int3(1, 1, 1), &b->dpd);
+    P->A.pos = b->pos[dst]; P->A.vel = b->vel[dst]; P->A.starts = b->starts; P->A.counts = b->counts;
+    P->A.out = (float*)b->force; P->A.out_stride = 4;
+    P->A.seeds_dev = b->seeds;
+    P->A.fss = b->fss;
+    P->A.err = dev_err_ptr();
+    P->A.B = b->B;
+    P->A.which = 1;
+    P->fss = b->fss;
+    P->coff = b->coff; P->pack = b->pack; P->pack_off = b->pack_off;
+    P->pack_cap = b->pack_cap; P->ncells_frag = b->ncells_frag;
+    const int nvt = b->mnc * b->mnv;
+    if (nvt > 0) {
+        P->mnc = b->mnc; P->mnv = b->mnv;
+        P->mpos = b->mpos; P->mvel = b->mvel; P->mforce = b->mforce; P->mcount = b->mcount;
+        P->ftrunk = b->ftrunk; P->fseeds = b->fseeds;
+        P->fmask = b->fmask; P->frank = b->frank; P->fcount = b->fcount; P->fimg = b->fimg;
+        FsiArgs &F = P->F;     // as fsi_forces sets it up
+        F.L = make_int3(1, 1, 1); F.nv = nvt; F.pv = (const float*)b->mpos; F.vv = (const float*)b->mvel;
+        F.pstride = 4;
+        F.spos = b->pos[dst]; F.svel = b->vel[dst]; F.starts = b->starts; F.counts = b->counts;
+        F.fv = (float*)b->mforce; F.fstride = 4; F.fs = (float*)b->force; F.sstride = 4;
+        F.par.a = b->fsi.a; F.par.g = b->fsi.g; F.par.s = b->fsi.s; F.par.spow = b->fsi.spow;
+        F.seeds_dev = b->fseeds;
+        F.img_rank = b->frank; F.img_start = b->fimg;
+        F.err = dev_err_ptr();
+        F.B = b->B;
+        if (b->vperm && b->mnv > 0) { F.vperm = b->vperm; F.vperm_n = b->mnv; }
+        int rc = membrane_args(b->rbc, &P->M);
+        if (rc) return rc;
+        membrane_args_par(&P->M, &b->mpar, membrane_nt(b->rbc));
+        P->M.nc = b->mnc;
+        P->M.pos = (const float*)b->mpos; P->M.vel = (const float*)b->mvel; P->M.stride = 4;
+        P->M.force = (float*)b->mforce; P->M.fstride = 4;
+        P->M.av = membrane_av(b->rbc);
+        P->nt = membrane_nt(b->rbc);
+        P->tri = membrane_tri(b->rbc);
+        P->av = membrane_av(b->rbc);
+    }
+    P->dt = b->dt; P->mass = b->mass; P->mmass = b->mmass;
+    P->bodyf = b->bodyf;
+    P->rng = b->rng;
+    P->bar = b->bar;
+    P->err = dev_err_ptr();
+    P->hold = hold;
+    return CTC_OK;
+}
+
+static int batch_step_persistent(ctc_batch *b, cudaStream_t st, int hold) {
+    if (!dev_err_ptr()) return fail(CTC_ERR_CUDA, "ctc_batch_step: device error word unavailable");
+    PersistArgs P;
+    int rc = persist_args(b, &P, hold);
+    if (rc) return rc;
+    CUDA_TRY(batch_persistent_launch(P, st, &b->grid));
+    b->cur = 1 - b->cur;
+    return CTC_OK;
+}
+
 // one step of every box, the order of ctc_sim_step
 static int batch_step1(ctc_batch *b, cudaStream_t st) {
+    if (b->persistent) return batch_step_persistent(b, st, -1);
     const int src = b->cur, dst = 1 - b->cur;
     CUDA_TRY(draw_seeds_launch(b->trunk, 27 * b->nbox, b->seeds, st));
     CUDA_TRY(clist_launch(make_int3(1, 1, 1), b->ntot, nullptr, b->pos[src], b->vel[src], 1, b->counts, b->starts,
@@ -370,6 +450,48 @@ extern "C" int ctc_batch_step(ctc_batch *b, int nsteps, void *stream) {
     }
     CUDA_TRY(cudaEventRecord(b->ev_out, b->own));
     CUDA_TRY(cudaStreamWaitEvent(st, b->ev_out, 0));
+    return CTC_OK;
+}
+
+// the step as one persistent cooperative launch (1) or as one launch per
+// stage (0); the membranes' bending must be Kantor or none, without their
+// random force
+extern "C" int ctc_batch_set_persistent(ctc_batch *b, int enable) {
+    if (!b) return fail(CTC_ERR_ARG, "ctc_batch_set_persistent: null");
+    if (enable && b->rbc) {
+        MembraneArgs M;
+        int rc = membrane_args(b->rbc, &M);
+        if (rc) return rc;
+        if (M.bending > 1 || membrane_noise(b->rbc))
+            return fail(CTC_ERR_ARG, "ctc_batch_set_persistent: Juelicher bending or membrane noise not in the "
+                                     "persistent step");
+    }
+    if (enable && !b->bar) {
+        CUDA_TRY(cudaMalloc(&b->bar, sizeof(GridBar)));
+        CUDA_TRY(cudaMemset(b->bar, 0, sizeof(GridBar)));
+    }
+    drop_graphs(b);
+    b->persistent = enable != 0;
+    return CTC_OK;
+}
+
+// one persistent step in which block 0 never arrives at barrier `barrier`:
+// the other blocks' bounded waits must end it with CTC_DEV_WAIT_TIMEOUT in
+// the device error word (read with ctc_device_error) instead of hanging the
+// device; the state is left undefined.  blocks [host]: the launch's blocks.
+extern "C" int ctc_batch_persistent_check(ctc_batch *b, int barrier, int *blocks, void *stream) {
+    if (!b || barrier < 0 || barrier > 11) return fail(CTC_ERR_ARG, "ctc_batch_persistent_check: bad arguments");
+    if (!b->persistent || !b->loaded)
+        return fail(CTC_ERR_ARG, "ctc_batch_persistent_check: persistent mode and a loaded state first");
+    int rc = batch_step_persistent(b, (cudaStream_t)stream, barrier);
+    if (blocks) *blocks = b->grid;
+    return rc;
+}
+
+// blocks of the last persistent launch [host]
+extern "C" int ctc_batch_persistent_grid(const ctc_batch *b, int *blocks) {
+    if (!b || !blocks) return fail(CTC_ERR_ARG, "ctc_batch_persistent_grid: bad arguments");
+    *blocks = b->grid;
     return CTC_OK;
 }
 

@@ -160,6 +160,8 @@ void membrane_args_par(MembraneArgs *A, const ctc_rbc_params *p, int nt) {
 
 const int *membrane_tri(const ctc_rbc_force *f) { return f->tri; }
 int membrane_nt(const ctc_rbc_force *f) { return f->nt; }
+double *membrane_av(const ctc_rbc_force *f) { return f->av; }
+int membrane_noise(const ctc_rbc_force *f) { return f->noise ? 1 : 0; }
 
 int membrane_forces(ctc_rbc_force *f, const ctc_rbc_params *p, int nc, const float *pos, const float *vel, int stride,
                     float *force, int fstride, cudaStream_t st, double dt, const float *noise_seed_dev) {

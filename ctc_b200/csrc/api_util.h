@@ -24,6 +24,10 @@ int membrane_args(const ctc_rbc_force *f, MembraneArgs *A);
 void membrane_args_par(MembraneArgs *A, const ctc_rbc_params *p, int nt);
 const int *membrane_tri(const ctc_rbc_force *f);
 int membrane_nt(const ctc_rbc_force *f);
+// the module's area/volume buffer (2 doubles per cell) and whether its random
+// force is on
+double *membrane_av(const ctc_rbc_force *f);
+int membrane_noise(const ctc_rbc_force *f);
 // FSI of nv vertices against the cell-sorted solvent; seeds_dev (2 floats) may replace the seeds;
 // count holds fsi_count_ints(nv, B.nbox) ints; vperm (device, vperm_n ints, may be null): the
 // order in which threads take each cell's vertices

@@ -46,9 +46,12 @@ __device__ __forceinline__ int cell_of(float4 p, int3 L) {
 // pass 1: cell + slot by warp-aggregated atomics
 // (with many boxes, B.nbox > 0: the particle's box gives L and the offset of
 // its cells in the concatenated cell arrays)
-__global__ void k_clist_count(int n, const int *__restrict__ nptr, const float4 *__restrict__ pos, int3 L,
-                              int wrap, int2 *__restrict__ cidslot, int *__restrict__ counts, int *err, Boxes B) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+// (the kernels' bodies take their thread's global index, so that the
+// persistent step of many boxes runs them too; kernels.cu)
+__device__ __forceinline__ void clist_count_at(int i, int n, const int *__restrict__ nptr,
+                                               const float4 *__restrict__ pos, int3 L, int wrap,
+                                               int2 *__restrict__ cidslot, int *__restrict__ counts, int *err,
+                                               const Boxes &B) {
     if (nptr) n = min(n, *nptr);
     int cid = -1;
     bool wrapped = false;
@@ -78,6 +81,11 @@ __global__ void k_clist_count(int n, const int *__restrict__ nptr, const float4 
     } else if (i < n) {
         cidslot[i] = make_int2(-1, 0);
     }
+}
+
+__global__ void k_clist_count(int n, const int *__restrict__ nptr, const float4 *__restrict__ pos, int3 L,
+                              int wrap, int2 *__restrict__ cidslot, int *__restrict__ counts, int *err, Boxes B) {
+    clist_count_at(blockIdx.x * blockDim.x + threadIdx.x, n, nptr, pos, L, wrap, cidslot, counts, err, B);
 }
 
 // exclusive scan, pass 1: 4096 counts per block
@@ -148,9 +156,9 @@ __global__ void k_scan_add(int nc, int *__restrict__ starts, const int *__restri
 }
 
 // pass 2: place keys at start + slot
-__global__ void k_clist_place(int n, const int *__restrict__ nptr, const int2 *__restrict__ cidslot,
-                              const int *__restrict__ starts, unsigned *__restrict__ keys) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void clist_place_at(int i, int n, const int *__restrict__ nptr,
+                                               const int2 *__restrict__ cidslot, const int *__restrict__ starts,
+                                               unsigned *__restrict__ keys) {
     if (nptr) n = min(n, *nptr);
     if (i >= n) return;
     int2 cs = cidslot[i];
@@ -159,12 +167,18 @@ __global__ void k_clist_place(int n, const int *__restrict__ nptr, const int2 *_
     keys[starts[cs.x] + (cs.y & 0x7fffffff)] = wrapped | (unsigned)i;
 }
 
+__global__ void k_clist_place(int n, const int *__restrict__ nptr, const int2 *__restrict__ cidslot,
+                              const int *__restrict__ starts, unsigned *__restrict__ keys) {
+    clist_place_at(blockIdx.x * blockDim.x + threadIdx.x, n, nptr, cidslot, starts, keys);
+}
+
 // pass 3: rank inside the cell by key, gather the particle, write it sorted
-__global__ void k_clist_gather(int nc, const unsigned *__restrict__ keys, const int2 *__restrict__ cidslot,
-                               const int *__restrict__ starts, const float4 *__restrict__ pos_in,
-                               const float4 *__restrict__ vel_in, int3 L, int wrap, float4 *__restrict__ pos_out,
-                               float4 *__restrict__ vel_out, int *__restrict__ order, Boxes B) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void clist_gather_at(int k, int nc, const unsigned *__restrict__ keys,
+                                                const int2 *__restrict__ cidslot, const int *__restrict__ starts,
+                                                const float4 *__restrict__ pos_in, const float4 *__restrict__ vel_in,
+                                                int3 L, int wrap, float4 *__restrict__ pos_out,
+                                                float4 *__restrict__ vel_out, int *__restrict__ order,
+                                                const Boxes &B) {
     int total = __ldg(starts + nc);
     if (k >= total) return;
     // a box keeps its particle range: the input index's box is the output's
@@ -182,6 +196,14 @@ __global__ void k_clist_gather(int nc, const unsigned *__restrict__ keys, const 
     pos_out[out] = p;
     vel_out[out] = __ldg(vel_in + i);
     if (order) order[out] = i;
+}
+
+__global__ void k_clist_gather(int nc, const unsigned *__restrict__ keys, const int2 *__restrict__ cidslot,
+                               const int *__restrict__ starts, const float4 *__restrict__ pos_in,
+                               const float4 *__restrict__ vel_in, int3 L, int wrap, float4 *__restrict__ pos_out,
+                               float4 *__restrict__ vel_out, int *__restrict__ order, Boxes B) {
+    clist_gather_at(blockIdx.x * blockDim.x + threadIdx.x, nc, keys, cidslot, starts, pos_in, vel_in, L, wrap, pos_out,
+                    vel_out, order, B);
 }
 
 // AoS Particle {r[3], v[3]} <-> SoA float4 (w of the position = particle id)

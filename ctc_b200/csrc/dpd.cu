@@ -148,18 +148,20 @@ __device__ __forceinline__ void vjp_par(const DpdArgs &A, float da, float dg) {
 // shuffles (the queue only holds the warp's targets), the candidate's
 // position rides in the queue record from the filter; only the candidate's
 // velocity is loaded (one box, forces, reference keys)
+// (the body takes its block's index, so that the persistent step of many
+// boxes runs it too; kernels.cu)
 template <int RNG, bool BATCH, int T, int UNROLL, int MODE = 0, bool STAGE = false, bool REGP = false>
-__global__ void __launch_bounds__(T, STAGE ? 1024 / T : 1) k_dpd_bulk(const __grid_constant__ DpdArgs A) {
+__device__ __forceinline__ void dpd_bulk_block(const DpdArgs &A, const int bid) {
     constexpr int W = T / 32;
     static_assert(!STAGE || (!BATCH && MODE == 0 && W <= 8), "staging: one box, forces, at most 8 warps");
     static_assert(!REGP || (RNG == 0 && !BATCH && MODE == 0 && !STAGE), "REGP: one box, forces");
     // ring of accepted pairs per warp, drained every DR pushes: at most
     // 31 + 32 DR records wait (RQ a power of two above that)
-    constexpr int DR = UNROLL < 4 ? UNROLL : 4, RQ = 256;
+    constexpr int DR = UNROLL < 4 ? UNROLL : 4, RQ = DR <= 2 ? 128 : 256;
     using Rec = typename std::conditional<REGP, BulkRecP, BulkRec<BATCH>>::type;
     __shared__ Rec queue[W][RQ];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ia = blockIdx.x * T + threadIdx.x;
+    const int ia = bid * T + threadIdx.x;
     int3 L = A.L;
     const int *starts = A.starts;
     int n, box = 0;
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(T, STAGE ? 1024 / T : 1) k_dpd_bulk(const __gr
     float acc_a = 0.0f, acc_g = 0.0f;               // MODE 1: parameter cotangents
 
     float4 pa = make_float4(0, 0, 0, 0), va = make_float4(0, 0, 0, 0);
-    const int ia0 = blockIdx.x * T + warp * 32;     // the warp's first target
+    const int ia0 = bid * T + warp * 32;            // the warp's first target
     int cx = 0, cy = 0, cz = 0;
     if (act) {
         pa = __ldg(A.pos + ia);
@@ -379,6 +381,11 @@ __global__ void __launch_bounds__(T, STAGE ? 1024 / T : 1) k_dpd_bulk(const __gr
         // a block whose wait gave up keeps its shared memory until the copies land
         if (stage_mem.ok && !staged) mbar_wait_bounded(&stage_mem.bar, 1u << 22);
     }
+}
+
+template <int RNG, bool BATCH, int T, int UNROLL, int MODE = 0, bool STAGE = false, bool REGP = false>
+__global__ void __launch_bounds__(T, STAGE ? 1024 / T : 1) k_dpd_bulk(const __grid_constant__ DpdArgs A) {
+    dpd_bulk_block<RNG, BATCH, T, UNROLL, MODE, STAGE, REGP>(A, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -750,12 +757,13 @@ __global__ void __launch_bounds__(T) k_dpd_halo(const __grid_constant__ DpdArgs 
 // particle) per thread, grid-stride, so no lane idles on an interior particle
 // or walks a fragment loop
 template <int RNG, bool BATCH, int T, int HU>
-__global__ void __launch_bounds__(T) k_dpd_halo_packed(const __grid_constant__ DpdArgs A, const int *__restrict__ pack,
-                                                       const int *__restrict__ pack_off, int nseg, int cap) {
+__device__ __forceinline__ void dpd_halo_packed_blocks(const DpdArgs &A, const int *__restrict__ pack,
+                                                       const int *__restrict__ pack_off, int nseg, int cap,
+                                                       const int bid, const int nblk) {
     __shared__ uint4 queue[T / 32][QCAP];
     float acc_a = 0.0f, acc_g = 0.0f;
     const int total = min(__ldg(pack_off + nseg), cap);
-    for (int base = blockIdx.x * T; base < total; base += gridDim.x * T) {
+    for (int base = bid * T; base < total; base += nblk * T) {
         const int t = base + threadIdx.x;
         int ia = 0x7fffffff, aid = 0;
         unsigned only = 0;
@@ -769,15 +777,23 @@ __global__ void __launch_bounds__(T) k_dpd_halo_packed(const __grid_constant__ D
     }
 }
 
+template <int RNG, bool BATCH, int T, int HU>
+__global__ void __launch_bounds__(T) k_dpd_halo_packed(const __grid_constant__ DpdArgs A, const int *__restrict__ pack,
+                                                       const int *__restrict__ pack_off, int nseg, int cap) {
+    dpd_halo_packed_blocks<RNG, BATCH, T, HU>(A, pack, pack_off, nseg, cap, blockIdx.x, gridDim.x);
+}
+
 // batched boxes: pack_off over the 26 fragments of every box (coff: prefix of
 // the segments' fragment cells), one block
-__global__ void __launch_bounds__(1024) k_halo_pack_off_boxes(Boxes B, const int *__restrict__ fss,
-                                                              const int *__restrict__ coff, int nseg,
-                                                              int *__restrict__ pack_off) {
+template <int T>
+__device__ __forceinline__ void halo_pack_off_boxes_block(const Boxes &B, const int *__restrict__ fss,
+                                                          const int *__restrict__ coff, int nseg,
+                                                          int *__restrict__ pack_off) {
+    constexpr int NW = T / 32;
     __shared__ int sh[32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int carry = 0;
-    for (int s0 = 0; s0 < nseg; s0 += 1024) {
+    for (int s0 = 0; s0 < nseg; s0 += T) {
         const int s = s0 + threadIdx.x;
         int v = 0;
         if (s < nseg) {
@@ -792,26 +808,33 @@ __global__ void __launch_bounds__(1024) k_halo_pack_off_boxes(Boxes B, const int
         if (lane == 31) sh[w] = x;
         __syncthreads();
         if (w == 0) {
-            int t = sh[lane];
+            int t = lane < NW ? sh[lane] : 0;
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, t, o);
                 if (lane >= o) t += y;
             }
-            sh[lane] = t;
+            if (lane < NW) sh[lane] = t;
         }
         __syncthreads();
         if (s < nseg) pack_off[s] = carry + x - v + (w > 0 ? sh[w - 1] : 0);
-        carry += sh[31];
+        carry += sh[NW - 1];
         __syncthreads();
     }
     if (threadIdx.x == 0) pack_off[nseg] = carry;
 }
 
+__global__ void __launch_bounds__(1024) k_halo_pack_off_boxes(Boxes B, const int *__restrict__ fss,
+                                                              const int *__restrict__ coff, int nseg,
+                                                              int *__restrict__ pack_off) {
+    halo_pack_off_boxes_block<1024>(B, fss, coff, nseg, pack_off);
+}
+
 // batched boxes: one fragment cell per thread, its particles into the pack
-__global__ void k_halo_pack_boxes(Boxes B, const int *__restrict__ starts, const int *__restrict__ counts,
-                                  const int *__restrict__ fss, const int *__restrict__ coff, int nseg,
-                                  const int *__restrict__ pack_off, int cap, int *__restrict__ pack, int *err) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void halo_pack_boxes_at(int g, const Boxes &B, const int *__restrict__ starts,
+                                                   const int *__restrict__ counts, const int *__restrict__ fss,
+                                                   const int *__restrict__ coff, int nseg,
+                                                   const int *__restrict__ pack_off, int cap, int *__restrict__ pack,
+                                                   int *err) {
     if (g >= __ldg(coff + nseg)) return;
     const int seg = box_find(coff, nseg, g);
     const int b = seg / 26, f = seg % 26, hci = g - __ldg(coff + seg);
@@ -827,6 +850,13 @@ __global__ void k_halo_pack_boxes(Boxes B, const int *__restrict__ starts, const
         if (base + o < cap) pack[base + o] = s0 + o;
         else set_error(err, DEV_CELL_OVERFLOW);
     }
+}
+
+__global__ void k_halo_pack_boxes(Boxes B, const int *__restrict__ starts, const int *__restrict__ counts,
+                                  const int *__restrict__ fss, const int *__restrict__ coff, int nseg,
+                                  const int *__restrict__ pack_off, int cap, int *__restrict__ pack, int *err) {
+    halo_pack_boxes_at(blockIdx.x * blockDim.x + threadIdx.x, B, starts, counts, fss, coff, nseg, pack_off, cap, pack,
+                       err);
 }
 
 // pack_off[f] = boundary particles of the fragments before f (fss holds each
@@ -873,14 +903,12 @@ __global__ void k_halo_pack(int3 L, const int *__restrict__ starts, const int *_
 constexpr int FS_ITEMS = 8;
 
 template <int FS_T>
-__global__ void __launch_bounds__(FS_T) k_frag_starts(int3 L, const int *__restrict__ counts, int *__restrict__ fss,
-                                                      Off27 off, Boxes B) {
+__device__ __forceinline__ void frag_starts_block(const int fid, const int box, int3 L, const int *__restrict__ counts,
+                                                  int *__restrict__ fss, const Off27 &off, const Boxes &B) {
     constexpr int NW = FS_T / 32;
     __shared__ int sh[NW];
-    const int fid = blockIdx.x;
     int *out = fss + off.d[fid];
     if (B.nbox > 0) {
-        const int box = blockIdx.y;
         L = box_L(B, box);
         counts += __ldg(B.c0 + box);
         out = fss + __ldg(B.fss_tab + 27 * box + fid);
@@ -934,6 +962,12 @@ __global__ void __launch_bounds__(FS_T) k_frag_starts(int3 L, const int *__restr
         __syncthreads();
     }
     if (threadIdx.x == 0) out[nc] = carry;
+}
+
+template <int FS_T>
+__global__ void __launch_bounds__(FS_T) k_frag_starts(int3 L, const int *__restrict__ counts, int *__restrict__ fss,
+                                                      Off27 off, Boxes B) {
+    frag_starts_block<FS_T>(blockIdx.x, blockIdx.y, L, counts, fss, off, B);
 }
 
 __global__ void k_rnd(int n, float seed, const int *__restrict__ u, const int *__restrict__ v, int uu,

@@ -47,25 +47,31 @@ __device__ __forceinline__ unsigned emap_mask(int3 L, float x, float y, float z)
 // (with many boxes, B.nbox > 0, a vertex's box gives L; ranks, counts and
 // list starts are per box: rank[fid * nv + i] counts the box's vertices only,
 // count and img_start hold 26 entries per box)
-__global__ void k_emap(int nv, int3 L, const float *__restrict__ pv, int stride, unsigned *__restrict__ mask,
-                       Boxes B) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+// (bodies with explicit indices, so that the persistent step of many boxes
+// runs them too; kernels.cu)
+__device__ __forceinline__ void emap_at(int i, int nv, int3 L, const float *__restrict__ pv, int stride,
+                                        unsigned *__restrict__ mask, const Boxes &B) {
     if (i >= nv) return;
     if (B.nbox > 0) L = box_L(B, box_find(B.v0, B.nbox, i));
     const float *q = pv + (size_t)stride * i;
     mask[i] = emap_mask(L, q[0], q[1], q[2]);
 }
 
+__global__ void k_emap(int nv, int3 L, const float *__restrict__ pv, int stride, unsigned *__restrict__ mask,
+                       Boxes B) {
+    emap_at(blockIdx.x * blockDim.x + threadIdx.x, nv, L, pv, stride, mask, B);
+}
+
 // per fragment: rank of each member vertex (ascending vertex index) and count
-__global__ void k_emap_rank(int nv, const unsigned *__restrict__ mask, int *__restrict__ rank,
-                            int *__restrict__ count, Boxes B) {
+__device__ __forceinline__ void emap_rank_block(const int fid, const int box, int nv, const unsigned *__restrict__ mask,
+                                                int *__restrict__ rank, int *__restrict__ count, const Boxes &B) {
     __shared__ int sh[32];
-    int fid = blockIdx.x, carry = 0;
+    int carry = 0;
     int i0 = 0, i1 = nv;                 // the box's vertices
     if (B.nbox > 0) {
-        i0 = __ldg(B.v0 + blockIdx.y);
-        i1 = __ldg(B.v0 + blockIdx.y + 1);
-        count += 26 * blockIdx.y;
+        i0 = __ldg(B.v0 + box);
+        i1 = __ldg(B.v0 + box + 1);
+        count += 26 * box;
     }
     for (int b = i0; b < i1; b += blockDim.x) {
         int i = b + threadIdx.x;
@@ -93,6 +99,11 @@ __global__ void k_emap_rank(int nv, const unsigned *__restrict__ mask, int *__re
         __syncthreads();
     }
     if (threadIdx.x == 0) count[fid] = carry;
+}
+
+__global__ void k_emap_rank(int nv, const unsigned *__restrict__ mask, int *__restrict__ rank,
+                            int *__restrict__ count, Boxes B) {
+    emap_rank_block(blockIdx.x, blockIdx.y, nv, mask, rank, count, B);
 }
 
 // one box, in parallel: EMAP_T vertices per block.  Pass 1 (k_emap_count):
@@ -185,14 +196,19 @@ __global__ void __launch_bounds__(EMAP_T) k_emap_rank_par(int nv, const unsigned
 }
 
 // img_start[fid] = start of receive slot anti(fid) in the concatenated list
-__global__ void k_emap_starts(const int *__restrict__ count, int *__restrict__ img_start) {
-    count += 26 * blockIdx.x;            // one block per box
-    img_start += 26 * blockIdx.x;
+__device__ __forceinline__ void emap_starts_box(const int box, const int *__restrict__ count,
+                                                int *__restrict__ img_start) {
+    count += 26 * box;
+    img_start += 26 * box;
     if (threadIdx.x == 0) {
         int s = 0, slot_start[26];
         for (int slot = 0; slot < 26; slot++) { slot_start[slot] = s; s += count[frag_anti(slot)]; }
         for (int fid = 0; fid < 26; fid++) img_start[fid] = slot_start[frag_anti(fid)];
     }
+}
+
+__global__ void k_emap_starts(const int *__restrict__ count, int *__restrict__ img_start) {
+    emap_starts_box(blockIdx.x, count, img_start);   // one block per box
 }
 
 // MODE 0: forces; MODE 1: their vector-Jacobian product
@@ -318,13 +334,13 @@ __device__ __forceinline__ void red3(float *out, int stride, int i, float s, flo
     atomicAdd(o + 2, s * f.z);
 }
 
-template <int RNG>
-__global__ void __launch_bounds__(FSIQ_T) k_fsi_q(const __grid_constant__ FsiArgs A) {
-    __shared__ uint4 queue[FSIQ_T / 32][FSIQ_CAP];
+template <int RNG, int T = FSIQ_T>
+__device__ __forceinline__ void fsi_q_block(const FsiArgs &A, const int bid) {
+    __shared__ uint4 queue[T / 32][FSIQ_CAP];
     const int lane = threadIdx.x & 31;
     uint4 *q = queue[threadIdx.x >> 5];
     int qn = 0;
-    const int t = blockIdx.x * FSIQ_T + threadIdx.x;
+    const int t = bid * T + threadIdx.x;
     const bool act = t < A.nv;
     int i = t;                           // the vertex this thread takes
     if (A.vperm && act) i = t - t % A.vperm_n + __ldg(A.vperm + t % A.vperm_n);
@@ -475,6 +491,11 @@ __global__ void __launch_bounds__(FSIQ_T) k_fsi_q(const __grid_constant__ FsiArg
         if (have) j = min(j + U, e);
     }
     if (qn > 0) process(qn);
+}
+
+template <int RNG>
+__global__ void __launch_bounds__(FSIQ_T) k_fsi_q(const __grid_constant__ FsiArgs A) {
+    fsi_q_block<RNG>(A, blockIdx.x);
 }
 
 size_t fsi_count_ints(int nv, int nbox) {

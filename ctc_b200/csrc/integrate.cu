@@ -9,9 +9,9 @@
 namespace ctc {
 
 // cell-sorted SoA state; the particle count is read on the device
-__global__ void k_integrate(const int *__restrict__ nptr, float4 *__restrict__ pos, float4 *__restrict__ vel,
-                            const float4 *__restrict__ force, float dt, float mass, float3 a) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void integrate_at(int i, const int *__restrict__ nptr, float4 *__restrict__ pos,
+                                             float4 *__restrict__ vel, const float4 *__restrict__ force, float dt,
+                                             float mass, float3 a) {
     if (i >= *nptr) return;
     float4 f = force[i], v = vel[i], r = pos[i];
     // f += m*a, then v += f/m*dt, r += v*dt, each a fused multiply-add as compiled
@@ -26,6 +26,11 @@ __global__ void k_integrate(const int *__restrict__ nptr, float4 *__restrict__ p
     r.z = __fmaf_rn(v.z, dt, r.z);
     vel[i] = v;
     pos[i] = r;
+}
+
+__global__ void k_integrate(const int *__restrict__ nptr, float4 *__restrict__ pos, float4 *__restrict__ vel,
+                            const float4 *__restrict__ force, float dt, float mass, float3 a) {
+    integrate_at(blockIdx.x * blockDim.x + threadIdx.x, nptr, pos, vel, force, dt, mass, a);
 }
 
 // reference AoS layout (Particle 6 floats, Force 3 floats)
@@ -112,18 +117,26 @@ __device__ __forceinline__ unsigned kiss_next(unsigned *s) {
     return s[0] + s[1] + s[2];
 }
 
-__global__ void k_draw_seeds(unsigned *__restrict__ state, int ntrunk, float *__restrict__ seeds) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void draw_seeds_at(int k, unsigned *__restrict__ state, int ntrunk,
+                                              float *__restrict__ seeds) {
     if (k < ntrunk) seeds[k] = __fdiv_rn(__uint2float_rn(kiss_next(state + 4 * k)), 4294967296.0f);
+}
+
+__global__ void k_draw_seeds(unsigned *__restrict__ state, int ntrunk, float *__restrict__ seeds) {
+    draw_seeds_at(blockIdx.x * blockDim.x + threadIdx.x, state, ntrunk, seeds);
 }
 
 // `count` successive draws from each of ntrunk trunks (the FSI trunk is drawn
 // twice a step): seeds[count * t + k]
-__global__ void k_draw_seq(unsigned *__restrict__ state, int ntrunk, int count, float *__restrict__ seeds) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void draw_seq_at(int t, unsigned *__restrict__ state, int ntrunk, int count,
+                                            float *__restrict__ seeds) {
     if (t < ntrunk)
         for (int k = 0; k < count; k++)
             seeds[count * t + k] = __fdiv_rn(__uint2float_rn(kiss_next(state + 4 * t)), 4294967296.0f);
+}
+
+__global__ void k_draw_seq(unsigned *__restrict__ state, int ntrunk, int count, float *__restrict__ seeds) {
+    draw_seq_at(blockIdx.x * blockDim.x + threadIdx.x, state, ntrunk, count, seeds);
 }
 
 // adjoint of k_integrate (v' = v + (f + m a) / m dt; x' = x + v' dt): from the

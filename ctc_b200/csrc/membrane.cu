@@ -44,11 +44,11 @@ __device__ __forceinline__ D3 ld_vel(const float *vv, int stride, int i) {
 // ---------------------------------------------------------------------------
 constexpr int AV_T = 256;
 
-__global__ void __launch_bounds__(AV_T) k_area_volume(int nv, int nt, const int *__restrict__ tri,
-                                                      const float *__restrict__ pp, int stride,
-                                                      double *__restrict__ av) {
+// (bodies with the block's cell c, so that the persistent step of many boxes
+// runs them too; kernels.cu)
+__device__ __forceinline__ void area_volume_cell(int c, int nv, int nt, const int *__restrict__ tri,
+                                                 const float *__restrict__ pp, int stride, double *__restrict__ av) {
     __shared__ double sh[2][AV_T / 32];
-    int c = blockIdx.x;
     double A = 0, V = 0;
     for (int t = threadIdx.x; t < nt; t += AV_T) {
         int i0 = __ldg(tri + 3 * t) + c * nv, i1 = __ldg(tri + 3 * t + 1) + c * nv, i2 = __ldg(tri + 3 * t + 2) + c * nv;
@@ -71,6 +71,12 @@ __global__ void __launch_bounds__(AV_T) k_area_volume(int nv, int nt, const int 
         av[2 * c] = a;
         av[2 * c + 1] = v;
     }
+}
+
+__global__ void __launch_bounds__(AV_T) k_area_volume(int nv, int nt, const int *__restrict__ tri,
+                                                      const float *__restrict__ pp, int stride,
+                                                      double *__restrict__ av) {
+    area_volume_cell(blockIdx.x, nv, nt, tri, pp, stride, av);
 }
 
 // ---------------------------------------------------------------------------
@@ -157,8 +163,7 @@ __device__ __forceinline__ void add_slot(float3 &acc, D3 f) {
 // triangle + viscous (+ random) partial of every slot -- each partial rounded
 // to float as the reference's per-slot atomicAdd does, so that vertices whose
 // slot contributions cancel round as the reference's do.
-__global__ void k_membrane(MembraneArgs A) {
-    int pid = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void membrane_at(int pid, const MembraneArgs &A) {
     if (pid >= A.nc * A.nv) return;
     const int md = A.md, nv = A.nv;
     const int rbc = pid / nv, k = (pid % nv) * md, off = rbc * nv;
@@ -207,6 +212,8 @@ __global__ void k_membrane(MembraneArgs A) {
     o[1] = acc.y;
     o[2] = acc.z;
 }
+
+__global__ void k_membrane(MembraneArgs A) { membrane_at(blockIdx.x * blockDim.x + threadIdx.x, A); }
 
 // ---------------------------------------------------------------------------
 // Juelicher bending (src/rbc/force/bending/juelicher, with the reference's
@@ -365,10 +372,10 @@ cudaError_t juelicher_launch(const MembraneArgs &A, double *av, double *lt, doub
 // membrane migration of one periodic rank (src/distr/rbc/dev.h:1-25): a cell
 // whose bounding-box centre left the box [lo, lo + L) moves by -L*d as a whole
 // (with many boxes, B.nbox > 0, the cell's box -- from its first vertex -- gives L)
-__global__ void k_rbc_wrap(int nv, int3 L, float4 *__restrict__ pos, Boxes B) {
+__device__ __forceinline__ void rbc_wrap_cell(int c, int nv, int3 L, float4 *__restrict__ pos, const Boxes &B) {
     __shared__ float lo[3][AV_T / 32], hi[3][AV_T / 32];
     __shared__ float shift[3];
-    const int c = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (B.nbox > 0) L = box_L(B, box_find(B.v0, B.nbox, c * nv));
     float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
     for (int v = threadIdx.x; v < nv; v += AV_T) {
@@ -401,6 +408,10 @@ __global__ void k_rbc_wrap(int nv, int3 L, float4 *__restrict__ pos, Boxes B) {
             x.x += shift[0]; x.y += shift[1]; x.z += shift[2];
             *r = x;
         }
+}
+
+__global__ void k_rbc_wrap(int nv, int3 L, float4 *__restrict__ pos, Boxes B) {
+    rbc_wrap_cell(blockIdx.x, nv, L, pos, B);
 }
 
 cudaError_t rbc_wrap_launch(int nc, int nv, int3 L, float4 *pos, cudaStream_t st, const Boxes &B) {

@@ -38,7 +38,8 @@ enum {
     CTC_DEV_OK = 0,
     CTC_DEV_TILE_OVERFLOW = 1,  /* a pair tile held more particles than its shared memory */
     CTC_DEV_BAD_PARTICLE = 3,   /* a particle was outside the box after the periodic wrap */
-    CTC_DEV_CELL_OVERFLOW = 4
+    CTC_DEV_CELL_OVERFLOW = 4,
+    CTC_DEV_WAIT_TIMEOUT = 5    /* a bounded wait (staged copies, a grid barrier) gave up */
 };
 
 /* random-number keys of the pair noise */
@@ -572,6 +573,21 @@ int ctc_batch_set_graph(ctc_batch *b, int enable);
  * (2, 4) (may be NULL) */
 int ctc_batch_tune(ctc_batch *b, int reps, int *choice, void *stream);
 int ctc_batch_set_tune(ctc_batch *b, const int *choice);
+/* the step as ONE persistent cooperative launch (1) instead of one launch
+ * per stage (0): the same stages in one kernel whose co-resident blocks meet
+ * at grid-wide barriers between dependent stages (bulk 256 threads x 2
+ * loads, halo 256 x 2; the tuner's shapes are not used); every wait at a
+ * barrier gives up after about half a second with CTC_DEV_WAIT_TIMEOUT in the
+ * device error word.  With ctc_batch_set_graph(b, 1) each step is one graph
+ * of that one launch.  Membranes: Kantor bending or none, no random force. */
+int ctc_batch_set_persistent(ctc_batch *b, int enable);
+/* one persistent step in which block 0 never arrives at barrier `barrier`
+ * (0..11): the other blocks' bounded waits end the step with
+ * CTC_DEV_WAIT_TIMEOUT in the device error word instead of hanging the device;
+ * the state is undefined afterwards.  blocks [host]: the launch's blocks */
+int ctc_batch_persistent_check(ctc_batch *b, int barrier, int *blocks, void *stream);
+/* blocks of the last persistent launch [host] */
+int ctc_batch_persistent_grid(const ctc_batch *b, int *blocks);
 /* state [host, AoS]: solvent box after box (cell-sorted within a box),
  * membrane vertices in ctc_batch_set_membranes order */
 int ctc_batch_get_solvent(ctc_batch *b, float *pp, void *stream);

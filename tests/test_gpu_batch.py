@@ -122,3 +122,78 @@ def test_batch_launch_shapes_agree():
             assert np.abs(out[:, :3] - ref[:, :3]).max() < POS_TOL
             assert np.abs(out[:, 3:] - ref[:, 3:]).max() < VEL_TOL
     assert C.device_error() == 0
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_persistent_step_matches_launch_per_stage(graph):
+    """The step as one persistent cooperative launch (grid-wide barriers
+    between its stages, reference keys, membranes with FSI) against the same
+    step as one launch per stage, three steps; with graph=True the step is
+    one graph of that one launch."""
+    import ctc_b200 as C
+    L, solv, cells, mem, tri, par = _boxes(seed=14)
+    dpd = systems.dpd_params()
+    fsi = (0.0, 8.0, dpd[2], 0.25)
+    bodyf = (0.01, 0.0, 0.0)
+    out = []
+    for persistent in (False, True):
+        b = _new_batch(L, solv, cells, mem, tri, par, dpd, fsi, bodyf)
+        b.set_persistent(persistent)
+        b.set_graph(graph and persistent)
+        for _ in range(3):
+            b.step(1)
+            out.append((persistent, b.get_solvent(), b.get_membranes()))
+        if persistent:
+            assert b.persistent_grid() >= 148
+        b.close()
+    assert C.device_error() == 0
+    for k in range(3):
+        (_, s0, v0), (_, s1, v1) = out[k], out[3 + k]
+        assert np.abs(s0[:, :3] - s1[:, :3]).max() < POS_TOL * (k + 1)
+        assert np.abs(s0[:, 3:] - s1[:, 3:]).max() < VEL_TOL
+        assert np.abs(v0[:, :3] - v1[:, :3]).max() < POS_TOL * (k + 1)
+        assert np.abs(v0[:, 3:] - v1[:, 3:]).max() < VEL_TOL
+
+
+def test_persistent_step_stable_keys():
+    """The same with the stable keys (a second instantiation of the kernel)."""
+    import ctc_b200 as C
+    L, solv, cells, mem, tri, par = _boxes(seed=15)
+    dpd = systems.dpd_params()
+    out = []
+    for persistent in (False, True):
+        b = C.Batch(L, [len(p) for p in solv], C.DpdParams(*dpd), dt=systems.DT, rng=C.CTC_RNG_STABLE)
+        b.set_solvent(np.concatenate(solv))
+        b.set_persistent(persistent)
+        b.step(2)
+        out.append(b.get_solvent())
+        b.close()
+    assert np.abs(out[0][:, :3] - out[1][:, :3]).max() < 2 * POS_TOL
+    assert np.abs(out[0][:, 3:] - out[1][:, 3:]).max() < VEL_TOL
+    assert C.device_error() == 0
+
+
+def test_persistent_barrier_wait_gives_up():
+    """A block that never arrives at a grid barrier (a flag nothing sets)
+    must not hang the device: the other blocks give up after their bounded
+    wait, the step ends with CTC_DEV_WAIT_TIMEOUT in the device error word,
+    and the context stays usable -- a fresh batch steps normally after it."""
+    import ctc_b200 as C
+    L, solv, cells, mem, tri, par = _boxes(seed=16)
+    dpd = systems.dpd_params()
+    fsi = (0.0, 8.0, dpd[2], 0.25)
+    b = _new_batch(L, solv, cells, mem, tri, par, dpd, fsi, (0, 0, 0))
+    b.set_persistent(True)
+    b.step(1)
+    assert C.device_error() == 0
+    blocks = b.persistent_check(5)
+    torch.cuda.synchronize()
+    assert blocks >= 148
+    assert C.device_error() == 5          # CTC_DEV_WAIT_TIMEOUT
+    b.close()
+    b = _new_batch(L, solv, cells, mem, tri, par, dpd, fsi, (0, 0, 0))
+    b.set_persistent(True)
+    b.step(2)
+    torch.cuda.synchronize()
+    assert C.device_error() == 0
+    b.close()
