@@ -754,8 +754,9 @@ class Batch:
 
     def set_persistent(self, enable=True):
         """Each step as one persistent cooperative launch (grid-wide barriers
-        between its stages) instead of one launch per stage."""
-        check(lib().ctc_batch_set_persistent(self.h, int(bool(enable))))
+        between its stages) instead of one launch per stage; enable = 2 builds
+        the launch for 2 blocks per SM (more registers) instead of 3."""
+        check(lib().ctc_batch_set_persistent(self.h, int(enable)))
 
     def persistent_check(self, barrier, stream=None):
         """One persistent step in which block 0 never arrives at `barrier`:
@@ -769,6 +770,13 @@ class Batch:
         blocks = C.c_int(0)
         check(lib().ctc_batch_persistent_grid(self.h, C.byref(blocks)))
         return blocks.value
+
+    def persistent_stages(self, enable=True, stream=None):
+        """Record (enable) the persistent step's per-stage times; returns the
+        last step's 12 stage times and their sum (ms) when recording was on."""
+        ms = (C.c_double * 13)()
+        check(lib().ctc_batch_persistent_stages(self.h, int(bool(enable)), ms, _stream(stream)))
+        return list(ms)
 
     def tune(self, reps=3, stream=None):
         """Autotune the pair kernels' launch shapes on the current state;

@@ -193,6 +193,7 @@ SIGNATURES = {
     "ctc_batch_set_persistent": (C.c_int, [vp, C.c_int]),
     "ctc_batch_persistent_check": (C.c_int, [vp, C.c_int, ip, vp]),
     "ctc_batch_persistent_grid": (C.c_int, [vp, ip]),
+    "ctc_batch_persistent_stages": (C.c_int, [vp, C.c_int, C.POINTER(C.c_double), vp]),
     "ctc_batch_get_solvent": (C.c_int, [vp, vp, vp]),
     "ctc_batch_get_membranes": (C.c_int, [vp, vp, vp]),
     "ctc_batch_count": (C.c_int, [vp, ip, ip]),

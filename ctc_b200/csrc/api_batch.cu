@@ -68,8 +68,10 @@ struct ctc_batch {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};   // one step from buffer 0, one from buffer 1
     // the step as one persistent launch (ctc_batch_set_persistent)
     bool persistent = false;
+    int occupancy = 3;                               // of the persistent kernel: 3 or 2 blocks per SM
     GridBar *bar = nullptr;
     int grid = 0;                                    // its blocks at the last launch
+    unsigned long long *stamps = nullptr;            // per-stage clock of block 0 (ctc_batch_persistent_stages)
 };
 
 static void drop_graphs(ctc_batch *b) {
@@ -97,6 +99,7 @@ extern "C" int ctc_batch_destroy(ctc_batch *b) {
     cudaFree(b->d_tab); cudaFree(b->d_L);
     cudaFree(b->pack); cudaFree(b->pack_off); cudaFree(b->coff);
     cudaFree(b->bar);
+    cudaFree(b->stamps);
     if (b->ev_in) cudaEventDestroy(b->ev_in);
     if (b->ev_out) cudaEventDestroy(b->ev_out);
     if (b->own) cudaStreamDestroy(b->own);
@@ -346,9 +349,11 @@ static int persist_args(ctc_batch *b, PersistArgs *P, int hold) {
     P->dt = b->dt; P->mass = b->mass; P->mmass = b->mmass;
     P->bodyf = b->bodyf;
     P->rng = b->rng;
+    P->occupancy = b->occupancy;
     P->bar = b->bar;
     P->err = dev_err_ptr();
     P->hold = hold;
+    P->stamps = b->stamps;
     return CTC_OK;
 }
 
@@ -453,11 +458,12 @@ extern "C" int ctc_batch_step(ctc_batch *b, int nsteps, void *stream) {
     return CTC_OK;
 }
 
-// the step as one persistent cooperative launch (1) or as one launch per
-// stage (0); the membranes' bending must be Kantor or none, without their
+// the step as one persistent cooperative launch (1: its kernel built for 3
+// blocks of 256 threads per SM; 2: for 2, more registers) or as one launch
+// per stage (0); the membranes' bending must be Kantor or none, without their
 // random force
 extern "C" int ctc_batch_set_persistent(ctc_batch *b, int enable) {
-    if (!b) return fail(CTC_ERR_ARG, "ctc_batch_set_persistent: null");
+    if (!b || enable < 0 || enable > 3) return fail(CTC_ERR_ARG, "ctc_batch_set_persistent: bad arguments");
     if (enable && b->rbc) {
         MembraneArgs M;
         int rc = membrane_args(b->rbc, &M);
@@ -472,6 +478,7 @@ extern "C" int ctc_batch_set_persistent(ctc_batch *b, int enable) {
     }
     drop_graphs(b);
     b->persistent = enable != 0;
+    b->occupancy = enable == 2 ? 2 : 3;
     return CTC_OK;
 }
 
@@ -492,6 +499,33 @@ extern "C" int ctc_batch_persistent_check(ctc_batch *b, int barrier, int *blocks
 extern "C" int ctc_batch_persistent_grid(const ctc_batch *b, int *blocks) {
     if (!b || !blocks) return fail(CTC_ERR_ARG, "ctc_batch_persistent_grid: bad arguments");
     *blocks = b->grid;
+    return CTC_OK;
+}
+
+// the stages of one persistent step as block 0 saw them: enable = 1 records
+// from the next step on (drops captured graphs), then ms [host, 13] = the
+// milliseconds of stage k (between barriers k - 1 and k) of the last step;
+// enable = 0 stops recording.  Synchronises the stream.
+extern "C" int ctc_batch_persistent_stages(ctc_batch *b, int enable, double *ms, void *stream) {
+    if (!b) return fail(CTC_ERR_ARG, "ctc_batch_persistent_stages: null");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ms && b->stamps) {
+        unsigned long long t[13];
+        CUDA_TRY(cudaMemcpyAsync(t, b->stamps, sizeof(t), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        for (int k = 0; k < 12; k++) ms[k] = 1e-6 * (double)(t[k + 1] - t[k]);
+        ms[12] = 1e-6 * (double)(t[12] - t[0]);
+    }
+    if (enable && !b->stamps) {
+        CUDA_TRY(cudaMalloc(&b->stamps, sizeof(unsigned long long) * 13));
+        CUDA_TRY(cudaMemset(b->stamps, 0, sizeof(unsigned long long) * 13));
+        drop_graphs(b);
+    } else if (!enable && b->stamps) {
+        CUDA_TRY(cudaStreamSynchronize(st));
+        cudaFree(b->stamps);
+        b->stamps = nullptr;
+        drop_graphs(b);
+    }
     return CTC_OK;
 }
 

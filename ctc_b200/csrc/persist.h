@@ -49,9 +49,11 @@ struct PersistArgs {
     float dt, mass, mmass;
     float3 bodyf;
     int rng;                        // CTC_RNG_REFERENCE or CTC_RNG_STABLE
+    int occupancy;                  // blocks per SM the kernel is built for: 3 (80 registers) or 2 (128)
     GridBar *bar;
     int *err;
     int hold;                       // test hook: block 0 stops before barrier `hold` (-1: never)
+    unsigned long long *stamps;     // optional [13]: block 0's clock (ns) at the start and after each barrier
 };
 
 constexpr int PERSIST_T = 256;     // threads per block of the persistent step

@@ -573,8 +573,10 @@ int ctc_batch_set_graph(ctc_batch *b, int enable);
  * (2, 4) (may be NULL) */
 int ctc_batch_tune(ctc_batch *b, int reps, int *choice, void *stream);
 int ctc_batch_set_tune(ctc_batch *b, const int *choice);
-/* the step as ONE persistent cooperative launch (1) instead of one launch
- * per stage (0): the same stages in one kernel whose co-resident blocks meet
+/* the step as ONE persistent cooperative launch (1: the kernel built for 3
+ * blocks of 256 threads per SM, 80 registers; 2: for 2 blocks, 128
+ * registers) instead of one launch per stage (0): the same stages in one
+ * kernel whose co-resident blocks meet
  * at grid-wide barriers between dependent stages (bulk 256 threads x 2
  * loads, halo 256 x 2; the tuner's shapes are not used); every wait at a
  * barrier gives up after about half a second with CTC_DEV_WAIT_TIMEOUT in the
@@ -588,6 +590,11 @@ int ctc_batch_set_persistent(ctc_batch *b, int enable);
 int ctc_batch_persistent_check(ctc_batch *b, int barrier, int *blocks, void *stream);
 /* blocks of the last persistent launch [host] */
 int ctc_batch_persistent_grid(const ctc_batch *b, int *blocks);
+/* per-stage time of the persistent step as its block 0 saw it: enable = 1
+ * records from the next step on, then ms [host, 13] receives the last step's
+ * 12 stages between barriers (ms[k]: stage k; the last stage, after barrier
+ * 12, is not timed) and ms[12] their sum; enable = 0 stops.  Synchronises */
+int ctc_batch_persistent_stages(ctc_batch *b, int enable, double *ms, void *stream);
 /* state [host, AoS]: solvent box after box (cell-sorted within a box),
  * membrane vertices in ctc_batch_set_membranes order */
 int ctc_batch_get_solvent(ctc_batch *b, float *pp, void *stream);
