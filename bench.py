@@ -535,7 +535,8 @@ def run_batch(args, cfg, world, rank, local):
     import ctc_b200 as ctc
     from ctc_b200 import systems
     torch.cuda.set_device(local)
-    L, n, pp, cells, pv, tri, par = systems.batch_system(nbox=cfg["nbox"], seed=5 + rank)
+    nbox = args.nbox or cfg["nbox"]
+    L, n, pp, cells, pv, tri, par = systems.batch_system(nbox=nbox, seed=5 + rank)
     dpd = ctc.DpdParams(*systems.dpd_params())
     fsi = ctc.DpdParams(0.0, systems.GAMMA, systems.dpd_params()[2], systems.SPOW)
     stream = torch.cuda.current_stream()
@@ -647,7 +648,7 @@ def run_batch(args, cfg, world, rank, local):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded uniform solvent per box, Maxwellian velocities, seeded RBC placement)",
-        "config": {"workload": cfg["name"], "boxes": int(len(n)), "solvent_particles": ntot,
+        "config": {"workload": cfg["name"] if len(n) == cfg["nbox"] else "%d periodic boxes, edges uniform in 8..24, rho=10, one RBC in every 4th box" % len(n), "boxes": int(len(n)), "solvent_particles": ntot,
                    "membrane_vertices": nvt, "cells_with_rbc": int(cells.sum()),
                    "edges": [int(L[:, 0].min()), int(L[:, 0].max())],
                    "parallelism": "replicas" if world > 1 else "1 GPU",
@@ -784,6 +785,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--nbox", type=int, default=0, help="boxes of the batched configuration (c5: 512)")
     ap.add_argument("--shape", default="",
                     help="pair-kernel launch shape instead of tuning: bulk threads,bulk loads,halo threads,halo loads"
                          "[,bulk variant] (single-box configurations)")
