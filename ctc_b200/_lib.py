@@ -178,6 +178,15 @@ SIGNATURES = {
     "ctc_sub_halo_update": (C.c_int, [vp, ip, vp]),
     "ctc_sub_bags": (C.c_int, [vp, C.c_int, C.POINTER(vp), C.POINTER(vp), ip]),
     "ctc_sub_count": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_set_membranes": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int, C.POINTER(RbcParams),
+                                        C.POINTER(DpdParams), C.c_float]),
+    "ctc_sub_mem_distr_pack": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_mem_distr_unpack": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_mem_exch_pack": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_mem_fsi": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_mem_update": (C.c_int, [vp, vp]),
+    "ctc_sub_get_membranes": (C.c_int, [vp, ip, ip, vp, vp, vp]),
+    "ctc_sub_membrane_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
     "ctc_sub_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]),
     "ctc_sub_seeds": (C.c_int, [vp, fp]),
     "ctc_sub_masks": (C.c_int, [vp, C.POINTER(C.c_uint)]),

@@ -21,9 +21,11 @@
 #include <algorithm>
 #include <climits>
 #include <cstdio>
+#include <vector>
 
 #include "api_util.h"
 #include "clist.h"
+#include "fsi.h"
 #include "integrate.h"
 
 using namespace ctc;
@@ -157,6 +159,111 @@ __global__ void k_set_ids(int n, const int *__restrict__ ids, float4 *__restrict
     if (i < n) pos[i].w = __int_as_float(__ldg(ids + i));
 }
 
+// ---- membranes (src/distr/rbc, src/exch/obj) ----------------------------
+// the bin of each cell: where the centre of its bounding box lies (the
+// reference's rule of src/distr/rbc/dev.h, as k_rbc_wrap applies it to one rank)
+__global__ void k_cell_bins(int nv, int3 L, const float4 *__restrict__ pos, int *__restrict__ bins) {
+    __shared__ float lo[3][8], hi[3][8];
+    const int c = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float mn[3] = {1e30f, 1e30f, 1e30f}, mx[3] = {-1e30f, -1e30f, -1e30f};
+    for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+        const float4 r = pos[(size_t)c * nv + v];
+        mn[0] = fminf(mn[0], r.x); mx[0] = fmaxf(mx[0], r.x);
+        mn[1] = fminf(mn[1], r.y); mx[1] = fmaxf(mx[1], r.y);
+        mn[2] = fminf(mn[2], r.z); mx[2] = fmaxf(mx[2], r.z);
+    }
+    for (int k = 0; k < 3; k++)
+        for (int o = 16; o > 0; o >>= 1) {
+            mn[k] = fminf(mn[k], __shfl_down_sync(0xffffffffu, mn[k], o));
+            mx[k] = fmaxf(mx[k], __shfl_down_sync(0xffffffffu, mx[k], o));
+        }
+    if (lane == 0)
+        for (int k = 0; k < 3; k++) { lo[k][w] = mn[k]; hi[k][w] = mx[k]; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float r[3];
+        for (int k = 0; k < 3; k++) {
+            float a = 1e30f, b = -1e30f;
+            for (int q = 0; q < (int)(blockDim.x >> 5); q++) { a = fminf(a, lo[k][q]); b = fmaxf(b, hi[k][q]); }
+            r[k] = 0.5f * (a + b);
+        }
+        bins[c] = distr_bin(L, make_float4(r[0], r[1], r[2], 0.0f));
+    }
+}
+
+// whole cells: cell src[k] of the input into slot dst0 + k of the output,
+// every vertex moved by `shift`; in/out either SoA (pos, vel) or records of
+// two float4 (recs_in / recs_out)
+__global__ void k_cells_copy(int nv, const int *__restrict__ src, int dst0, const float4 *__restrict__ pin,
+                             const float4 *__restrict__ vin, int recs_in, float4 *__restrict__ pout,
+                             float4 *__restrict__ vout, int recs_out, float3 shift) {
+    const int c = blockIdx.y;
+    const int s = __ldg(src + c);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        const size_t i = (size_t)s * nv + v, o = (size_t)(dst0 + c) * nv + v;
+        float4 p = __ldg(recs_in ? pin + 2 * i : pin + i);
+        const float4 u = __ldg(recs_in ? pin + 2 * i + 1 : vin + i);
+        p.x += shift.x; p.y += shift.y; p.z += shift.z;
+        if (recs_out) {
+            pout[2 * o] = p;
+            pout[2 * o + 1] = u;
+        } else {
+            pout[o] = p;
+            vout[o] = u;
+        }
+    }
+}
+
+// the vertices' images into the 26 image bags (vertex i, for fragment f of
+// its mask, at its rank there), with the vertex index beside each image
+__global__ void k_images_pack(int nv, const unsigned *__restrict__ mask, const int *__restrict__ rank,
+                              const int *__restrict__ boff, const float4 *__restrict__ pos,
+                              const float4 *__restrict__ vel, float4 *__restrict__ bags, int *__restrict__ vidx,
+                              int cap_total, int *err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const unsigned m = __ldg(mask + i);
+    if (!m) return;
+    const float4 p = __ldg(pos + i), u = __ldg(vel + i);
+    for (int f = 0; f < 26; f++) {
+        if (!((m >> f) & 1u)) continue;
+        const int t = __ldg(boff + f) + __ldg(rank + (size_t)f * nv + i);
+        if (t < 0 || t >= cap_total) { set_error(err, DEV_CELL_OVERFLOW); continue; }
+        bags[2 * (size_t)t] = p;
+        bags[2 * (size_t)t + 1] = u;
+        vidx[t] = i;
+    }
+}
+
+// the received images (bag j from direction j at rbase[j], rpre its prefix)
+// moved by +d(j) L into contiguous position and velocity arrays
+__global__ void k_images_unpack(int total, int3 L, const float4 *__restrict__ recv,
+                                const __grid_constant__ ArrivalBags R, float4 *__restrict__ ipos,
+                                float4 *__restrict__ ivel) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= total) return;
+    int j = 0;
+    while (j < 25 && R.rpre[j + 1] <= a) j++;
+    const size_t src = (size_t)R.rbase[j] + (size_t)(a - R.rpre[j]);
+    float4 p = __ldg(recv + 2 * src);
+    p.x += (float)(frag_i2dx(j) * L.x);
+    p.y += (float)(frag_i2dy(j) * L.y);
+    p.z += (float)(frag_i2dz(j) * L.z);
+    ipos[a] = p;
+    ivel[a] = __ldg(recv + 2 * src + 1);
+}
+
+// the forces on this rank's images, sent back by the neighbours (bag f at
+// boff[f], in the order of the image bag f), added to the vertices they were
+// images of
+__global__ void k_images_back(int total, const float4 *__restrict__ back, const int *__restrict__ vidx,
+                              float4 *__restrict__ force) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const float4 f = __ldg(back + t);
+    atomicAdd(force + __ldg(vidx + t), make_float4(f.x, f.y, f.z, 0.0f));
+}
+
 // cells of fragment f of an L box (src/frag/imp.cpp ncell)
 static int frag_ncell(int3 L, int f) {
     return (frag_i2dx(f) == 0 ? L.x : 1) * (frag_i2dy(f) == 0 ? L.y : 1) * (frag_i2dz(f) == 0 ? L.z : 1);
@@ -200,6 +307,31 @@ struct ctc_sub {
     // the bulk forces run on their own stream, beside the halo exchange
     cudaStream_t side;
     cudaEvent_t ev_d, ev_x, ev_ready, ev_bulk;
+    // membranes (ctc_sub_set_membranes): mnc cells of mnv vertices, float4 SoA
+    // (w: the vertex's global id = cell id * mnv + vertex), room for maxc cells
+    int mnc, mnv, maxc;
+    float4 *mpos[2], *mvel[2], *mforce;
+    int *mcount;
+    ctc_rbc_force *rbc;
+    ctc_rbc_params mpar;
+    ctc_dpd_params fsi;
+    float mmass;
+    Kiss fsi_trunk;                          // rnd_ini(1908 - rank, 1409 + rank, 290, 12968)
+    Kiss fsi_trunk0;                         // rank 0's: the stable keys' seed, the same on every rank
+    float fseed[2];                          // this step's FSI seeds: bulk, halo
+    int *cbins_dev, *cbins_host, *cidx_dev;  // bins of the cells, the cells' order of the pack (device copy)
+    int ccap;                                // cells per migration bag
+    float4 *csend, *crecv;                   // cell bags (kind 3): records, ccap cells per direction
+    int csend_off[27];                       // host offsets (cells) of the last pack's bags
+    int mstay;                               // cells that stayed
+    // vertex images (kind 4) and the forces sent back for them (kind 5)
+    unsigned *emask;
+    int *erank, *ecount, *eimg;              // fsi_images_launch's buffers
+    int *eoff_dev, *eoff_host;               // image bag offsets of the last pack (27)
+    int icap;                                // images per bag
+    float4 *isend, *irecv, *ipos, *ivel, *iforce, *iback;
+    int *ividx;
+    int irn[27];                             // received images per bag (the last ctc_sub_mem_fsi), prefix at 26
 };
 
 static int sub_check_cfg(const ctc_sub_config *c) {
@@ -226,6 +358,15 @@ extern "C" int ctc_sub_destroy(ctc_sub *s) {
     for (cudaEvent_t e : {s->ev_d, s->ev_x, s->ev_ready, s->ev_bulk})
         if (e) cudaEventDestroy(e);
     if (s->side) cudaStreamDestroy(s->side);
+    for (int b = 0; b < 2; b++) { cudaFree(s->mpos[b]); cudaFree(s->mvel[b]); }
+    cudaFree(s->mforce); cudaFree(s->mcount);
+    if (s->rbc) ctc_rbc_force_fin(s->rbc);
+    cudaFree(s->cbins_dev); cudaFreeHost(s->cbins_host); cudaFree(s->cidx_dev);
+    cudaFree(s->csend); cudaFree(s->crecv);
+    cudaFree(s->emask); cudaFree(s->erank); cudaFree(s->ecount); cudaFree(s->eimg);
+    cudaFree(s->eoff_dev); cudaFreeHost(s->eoff_host);
+    cudaFree(s->isend); cudaFree(s->irecv); cudaFree(s->ipos); cudaFree(s->ivel); cudaFree(s->iforce);
+    cudaFree(s->iback); cudaFree(s->ividx);
     delete s;
     return CTC_OK;
 }
@@ -460,6 +601,10 @@ extern "C" int ctc_sub_exch_pack(ctc_sub *s, void *stream) {
     A.starts = s->starts; A.counts = s->counts; A.fss = s->fss; A.err = dev_err_ptr();
     CUDA_TRY(frag_starts_launch(s->L, s->counts, s->fss, s->off, st));
     CUDA_TRY(halo_pack_launch(A, s->off, s->pack, s->pack_off, s->pack_cap, st));
+    // the step's forces start from zero here, on the caller's stream: the bulk
+    // pairs (own stream) and FSI (caller's stream) then both add to them
+    if (s->n > 0) CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n, st));
+    if (s->mnc > 0) CUDA_TRY(cudaMemsetAsync(s->mforce, 0, sizeof(float4) * (size_t)s->mnc * s->mnv, st));
     k_exch_gather<<<ceil_div(s->pack_cap, 256), 256, 0, st>>>(s->pack_cap, s->pack_off + 26, s->pack, s->pos[0],
                                                                 s->vel[0], s->xsend);
     CUDA_TRY(cudaGetLastError());
@@ -506,8 +651,8 @@ extern "C" int ctc_sub_bulk(ctc_sub *s, void *stream) {
     CUDA_TRY(cudaEventRecord(s->ev_ready, (cudaStream_t)stream));
     CUDA_TRY(cudaStreamWaitEvent(s->side, s->ev_ready, 0));
     cudaStream_t st = s->side;
+    if (!s->packed && !s->xpending) return fail(CTC_ERR_ARG, "ctc_sub_bulk: ctc_sub_exch_pack first");
     sub_draw(s);
-    if (s->n > 0) CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n, st));
     if (s->n > 0) {
         DpdArgs A;
         dpd_args_common(&A, s->L, &s->cfg.sim.dpd);
@@ -563,6 +708,336 @@ extern "C" int ctc_sub_halo_update(ctc_sub *s, const int *rcounts, void *stream)
     return CTC_OK;
 }
 
+// ---- membranes in the subdomain -------------------------------------------
+// nc cells of one template (nv vertices, nt triangles tri [host]) with their
+// vertices pp [host, AoS, subdomain coordinates] and global cell ids [host],
+// room for maxc cells; p, fsi, mass as ctc_sim_set_membranes.  The cells
+// migrate whole (src/distr/rbc), the vertices within 1 of a face go to the
+// neighbours as images for their FSI and get those forces back
+// (src/exch/obj), the internal forces stay on the rank that holds the cell.
+extern "C" int ctc_sub_set_membranes(ctc_sub *s, int nc, int nv, int nt, const int *tri, const float *pp,
+                                     const int *cell_ids, int maxc, const ctc_rbc_params *p,
+                                     const ctc_dpd_params *fsi, float mass) {
+    if (!s || nc < 0 || nv <= 0 || nt <= 0 || !tri || (nc > 0 && (!pp || !cell_ids)) || maxc < nc || maxc <= 0 ||
+        !p || !fsi || !(mass > 0))
+        return fail(CTC_ERR_ARG, "ctc_sub_set_membranes: bad arguments");
+    if (s->mnv) return fail(CTC_ERR_ARG, "ctc_sub_set_membranes: the subdomain has membranes already");
+    if ((long)maxc * nv > (1 << 26)) return fail(CTC_ERR_CAPACITY, "ctc_sub_set_membranes: %d cells too many", maxc);
+    const size_t nvmax = (size_t)maxc * nv;
+    s->mnv = nv;
+    s->maxc = maxc;
+    s->mpar = *p;
+    s->fsi = *fsi;
+    s->mmass = mass;
+    int rc = ctc_rbc_force_ini(nv, nt, tri, maxc, &s->rbc);
+    if (rc) return rc;
+    for (int b = 0; b < 2; b++) {
+        CUDA_TRY(cudaMalloc(&s->mpos[b], sizeof(float4) * nvmax));
+        CUDA_TRY(cudaMalloc(&s->mvel[b], sizeof(float4) * nvmax));
+    }
+    CUDA_TRY(cudaMalloc(&s->mforce, sizeof(float4) * nvmax));
+    CUDA_TRY(cudaMalloc(&s->mcount, sizeof(int)));
+    CUDA_TRY(cudaMalloc(&s->cbins_dev, sizeof(int) * (size_t)maxc));
+    CUDA_TRY(cudaMallocHost(&s->cbins_host, sizeof(int) * (size_t)maxc));
+    CUDA_TRY(cudaMalloc(&s->cidx_dev, sizeof(int) * 2 * (size_t)maxc));
+    // a migration bag holds a quarter of the cells (at least 4); an image bag
+    // every vertex
+    s->ccap = std::max(4, maxc / 4);
+    CUDA_TRY(cudaMalloc(&s->csend, 2 * sizeof(float4) * nvmax));
+    CUDA_TRY(cudaMalloc(&s->crecv, 2 * sizeof(float4) * (size_t)26 * s->ccap * nv));
+    CUDA_TRY(cudaMalloc(&s->emask, sizeof(unsigned) * nvmax));
+    CUDA_TRY(cudaMalloc(&s->erank, sizeof(int) * 26 * nvmax));
+    CUDA_TRY(cudaMalloc(&s->ecount, sizeof(int) * fsi_count_ints((int)nvmax, 0)));
+    CUDA_TRY(cudaMalloc(&s->eimg, sizeof(int) * 26));
+    CUDA_TRY(cudaMalloc(&s->eoff_dev, sizeof(int) * 27));
+    CUDA_TRY(cudaMallocHost(&s->eoff_host, sizeof(int) * 27));
+    s->icap = (int)nvmax;
+    const size_t itot = (size_t)26 * s->icap;
+    CUDA_TRY(cudaMalloc(&s->isend, 2 * sizeof(float4) * itot));
+    CUDA_TRY(cudaMalloc(&s->irecv, 2 * sizeof(float4) * itot));
+    CUDA_TRY(cudaMalloc(&s->ipos, sizeof(float4) * itot));
+    CUDA_TRY(cudaMalloc(&s->ivel, sizeof(float4) * itot));
+    CUDA_TRY(cudaMalloc(&s->iforce, sizeof(float4) * itot));
+    CUDA_TRY(cudaMalloc(&s->iback, sizeof(float4) * itot));
+    CUDA_TRY(cudaMalloc(&s->ividx, sizeof(int) * itot));
+    CUDA_TRY(cudaMemset(s->eoff_dev, 0, sizeof(int) * 27));
+    memset(s->eoff_host, 0, sizeof(int) * 27);
+    // fsi_ini of this rank (src/fsi/imp/main.h:7); the stable keys draw from
+    // rank 0's trunk on every rank, so that a pair's key does not depend on
+    // which rank evaluates it (the undivided box's keys)
+    kiss_ini(&s->fsi_trunk, 1908 - s->cfg.rank, 1409 + s->cfg.rank, 290, 12968);
+    kiss_ini(&s->fsi_trunk0, 1908, 1409, 290, 12968);
+    if (nc > 0) {
+        std::vector<float> tmp((size_t)nc * nv * 8);
+        for (int c = 0; c < nc; c++)
+            for (int v = 0; v < nv; v++) {
+                const float *q = pp + 6 * ((size_t)c * nv + v);
+                float *r = tmp.data() + 8 * ((size_t)c * nv + v);
+                const int id = cell_ids[c] * nv + v;
+                r[0] = q[0]; r[1] = q[1]; r[2] = q[2];
+                memcpy(r + 3, &id, sizeof(int));
+                r[4] = q[3]; r[5] = q[4]; r[6] = q[5]; r[7] = 0.0f;
+            }
+        float4 *rec = nullptr;
+        CUDA_TRY(cudaMalloc(&rec, sizeof(float) * tmp.size()));
+        cudaError_t e = cudaMemcpy(rec, tmp.data(), sizeof(float) * tmp.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) {
+            std::vector<int> idx(nc);
+            for (int c = 0; c < nc; c++) idx[c] = c;
+            e = cudaMemcpy(s->cidx_dev, idx.data(), sizeof(int) * nc, cudaMemcpyHostToDevice);
+        }
+        if (e == cudaSuccess) {
+            k_cells_copy<<<dim3(ceil_div(nv, 256), nc), 256>>>(nv, s->cidx_dev, 0, rec, nullptr, 1, s->mpos[0],
+                                                               s->mvel[0], 0, make_float3(0, 0, 0));
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        cudaFree(rec);
+        if (e != cudaSuccess) return fail(CTC_ERR_CUDA, "ctc_sub_set_membranes: %s", cudaGetErrorString(e));
+    }
+    s->mnc = nc;
+    const int nvt = nc * nv;
+    CUDA_TRY(cudaMemcpy(s->mcount, &nvt, sizeof(int), cudaMemcpyHostToDevice));
+    return CTC_OK;
+}
+
+// distr_rbc (src/distr/rbc/imp): the cells whose bounding-box centre left the
+// subdomain into the 26 cell bags (kind 3, nv records each, in cell order),
+// the others kept in order; counts [host, 26] in cells.  Synchronises.
+extern "C" int ctc_sub_mem_distr_pack(ctc_sub *s, int *counts, void *stream) {
+    if (!s || !counts) return fail(CTC_ERR_ARG, "ctc_sub_mem_distr_pack: bad arguments");
+    for (int f = 0; f < 26; f++) counts[f] = 0;
+    for (int f = 0; f < 27; f++) s->csend_off[f] = 0;
+    s->mstay = s->mnc;
+    if (s->mnc == 0) return CTC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nv = s->mnv, nc = s->mnc;
+    k_cell_bins<<<nc, 256, 0, st>>>(nv, s->L, s->mpos[0], s->cbins_dev);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(s->cbins_host, s->cbins_dev, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<int> order, stay;
+    for (int f = 0; f < 26; f++) {
+        s->csend_off[f] = (int)order.size();
+        for (int c = 0; c < nc; c++)
+            if (s->cbins_host[c] == f) order.push_back(c);
+        counts[f] = (int)order.size() - s->csend_off[f];
+        if (counts[f] > s->ccap)
+            return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_distr_pack: fragment %d: %d cells leaving > capacity %d", f,
+                        counts[f], s->ccap);
+    }
+    s->csend_off[26] = (int)order.size();
+    for (int c = 0; c < nc; c++)
+        if (s->cbins_host[c] == 26) stay.push_back(c);
+    const int nleave = (int)order.size(), nstay = (int)stay.size();
+    order.insert(order.end(), stay.begin(), stay.end());
+    CUDA_TRY(cudaMemcpyAsync(s->cidx_dev, order.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
+    if (nleave > 0)
+        k_cells_copy<<<dim3(ceil_div(nv, 256), nleave), 256, 0, st>>>(nv, s->cidx_dev, 0, s->mpos[0], s->mvel[0], 0,
+                                                                      s->csend, nullptr, 1, make_float3(0, 0, 0));
+    if (nstay > 0)
+        k_cells_copy<<<dim3(ceil_div(nv, 256), nstay), 256, 0, st>>>(nv, s->cidx_dev + nleave, 0, s->mpos[0],
+                                                                     s->mvel[0], 0, s->mpos[1], s->mvel[1], 0,
+                                                                     make_float3(0, 0, 0));
+    CUDA_TRY(cudaGetLastError());
+    // the order array must stay until the copies have read it
+    CUDA_TRY(cudaStreamSynchronize(st));
+    s->mstay = nstay;
+    return CTC_OK;
+}
+
+// the received cells (rcounts [host, 26], bag j from direction j) moved by
+// +d(j) L and appended to the cells that stayed
+extern "C" int ctc_sub_mem_distr_unpack(ctc_sub *s, const int *rcounts, void *stream) {
+    if (!s || !rcounts) return fail(CTC_ERR_ARG, "ctc_sub_mem_distr_unpack: bad arguments");
+    if (!s->mnv) return CTC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nv = s->mnv;
+    long total = s->mstay;
+    for (int j = 0; j < 26; j++) {
+        if (rcounts[j] < 0 || rcounts[j] > s->ccap)
+            return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_distr_unpack: bag %d: %d cells, capacity %d", j, rcounts[j],
+                        s->ccap);
+        total += rcounts[j];
+    }
+    if (total > s->maxc) return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_distr_unpack: %ld cells > %d", total, s->maxc);
+    std::vector<int> idx(std::max(1, s->ccap));
+    for (int k = 0; k < (int)idx.size(); k++) idx[k] = k;
+    CUDA_TRY(cudaMemcpyAsync(s->cidx_dev + s->maxc, idx.data(), sizeof(int) * std::min(s->ccap, s->maxc),
+                             cudaMemcpyHostToDevice, st));
+    int at = s->mstay;
+    for (int j = 0; j < 26; j++) {
+        if (rcounts[j] == 0) continue;
+        const float3 sh = make_float3((float)(frag_i2dx(j) * s->L.x), (float)(frag_i2dy(j) * s->L.y),
+                                      (float)(frag_i2dz(j) * s->L.z));
+        k_cells_copy<<<dim3(ceil_div(nv, 256), rcounts[j]), 256, 0, st>>>(
+            nv, s->cidx_dev + s->maxc, at, s->crecv + 2 * (size_t)j * s->ccap * nv, nullptr, 1, s->mpos[1],
+            s->mvel[1], 0, sh);
+        CUDA_TRY(cudaGetLastError());
+        at += rcounts[j];
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));   // the index array is a host vector
+    std::swap(s->mpos[0], s->mpos[1]);
+    std::swap(s->mvel[0], s->mvel[1]);
+    s->mnc = at;
+    const int nvt = at * nv;
+    CUDA_TRY(cudaMemcpyAsync(s->mcount, &nvt, sizeof(int), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return CTC_OK;
+}
+
+// exch_obj's map and pack (src/exch/obj/imp/{map,pack}.h): every vertex
+// within 1 of a face (or beyond it) into the image bag of each fragment it
+// must reach (kind 4, ascending vertex order); counts [host, 26].  Synchronises.
+extern "C" int ctc_sub_mem_exch_pack(ctc_sub *s, int *counts, void *stream) {
+    if (!s || !counts) return fail(CTC_ERR_ARG, "ctc_sub_mem_exch_pack: bad arguments");
+    for (int f = 0; f < 26; f++) counts[f] = 0;
+    memset(s->eoff_host, 0, sizeof(int) * 27);
+    const int nvt = s->mnc * s->mnv;
+    if (nvt == 0) return CTC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(fsi_images_launch(nvt, s->L, (const float*)s->mpos[0], 4, s->emask, s->erank, s->ecount, s->eimg, st));
+    CUDA_TRY(cudaMemcpyAsync(s->eoff_host, s->ecount, sizeof(int) * 26, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    int o = 0;
+    for (int f = 0; f < 26; f++) {
+        const int c = s->eoff_host[f];
+        if (c > s->icap) return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_exch_pack: fragment %d: %d images", f, c);
+        counts[f] = c;
+        s->eoff_host[f] = o;
+        o += c;
+    }
+    s->eoff_host[26] = o;
+    CUDA_TRY(cudaMemcpyAsync(s->eoff_dev, s->eoff_host, sizeof(int) * 27, cudaMemcpyHostToDevice, st));
+    k_images_pack<<<ceil_div(nvt, 256), 256, 0, st>>>(nvt, s->emask, s->erank, s->eoff_dev, s->mpos[0], s->mvel[0],
+                                                       s->isend, s->ividx, 26 * s->icap, dev_err_ptr());
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(st));    // eoff_host is read by the transport's views
+    return CTC_OK;
+}
+
+// fsi_bulk + fsi_halo (src/sim/objinter/imp/main.h:42-92): the local vertices
+// and the images received from the neighbours (rcounts [host, 26]) against the
+// local solvent, in the subdomain's cells only; the reactions go to the solvent
+// forces, the images' forces to the back bags (kind 5).  Call after
+// ctc_sub_exch_pack (it clears the forces) and before ctc_sub_halo_update.
+extern "C" int ctc_sub_mem_fsi(ctc_sub *s, const int *rcounts, void *stream) {
+    if (!s || !rcounts) return fail(CTC_ERR_ARG, "ctc_sub_mem_fsi: bad arguments");
+    if (!s->mnv) return CTC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool stable = s->cfg.sim.rng == CTC_RNG_STABLE;
+    // fsi_bulk draws one seed, fsi_halo one (src/fsi/imp/{bulk,halo}.h); the
+    // stable keys use the first draw of rank 0's trunk for both
+    Kiss &tr = stable ? s->fsi_trunk0 : s->fsi_trunk;
+    s->fseed[0] = kiss_get(&tr);
+    s->fseed[1] = kiss_get(&tr);
+    const float sb = s->fseed[0], sh = stable ? s->fseed[0] : s->fseed[1];
+    DpdPar P;
+    P.a = s->fsi.a; P.g = s->fsi.g; P.s = s->fsi.s; P.spow = s->fsi.spow;
+    FsiArgs A;
+    memset(&A, 0, sizeof(A));
+    A.L = s->L;
+    A.spos = s->pos[0]; A.svel = s->vel[0]; A.starts = s->starts; A.counts = s->counts;
+    A.fs = (float*)s->force; A.sstride = 4;
+    A.par = P;
+    A.err = dev_err_ptr();
+    A.no_wrap = 1;
+    A.vkey_w = stable ? 1 : 0;
+    A.pstride = 4; A.fstride = 4;
+    const int nvt = s->mnc * s->mnv;
+    if (nvt > 0 && s->n > 0) {
+        A.nv = nvt; A.pv = (const float*)s->mpos[0]; A.vv = (const float*)s->mvel[0];
+        A.fv = (float*)s->mforce;
+        A.seed_bulk = sb;
+        CUDA_TRY(fsi_launch(A, s->cfg.sim.rng, st));
+    }
+    ArrivalBags R;
+    long tot = 0;
+    for (int j = 0; j < 26; j++) {
+        if (rcounts[j] < 0 || rcounts[j] > s->icap)
+            return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_fsi: bag %d: %d images", j, rcounts[j]);
+        R.rpre[j] = (int)tot;
+        R.rbase[j] = j * s->icap;
+        s->irn[j] = (int)tot;
+        tot += rcounts[j];
+    }
+    R.rpre[26] = (int)tot;
+    s->irn[26] = (int)tot;
+    if (tot > 0) {
+        k_images_unpack<<<ceil_div(tot, 256), 256, 0, st>>>((int)tot, s->L, s->irecv, R, s->ipos, s->ivel);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemsetAsync(s->iforce, 0, sizeof(float4) * (size_t)tot, st));
+        if (s->n > 0) {
+            A.nv = (int)tot; A.pv = (const float*)s->ipos; A.vv = (const float*)s->ivel;
+            A.fv = (float*)s->iforce;
+            A.seed_bulk = sh;
+            CUDA_TRY(fsi_launch(A, s->cfg.sim.rng, st));
+        }
+    }
+    return CTC_OK;
+}
+
+// unpack_ff of exch_obj and the membranes' own step: the forces on this
+// rank's images, sent back into the back bags (kind 5, the image bags' order),
+// added to the vertices; the internal forces (rbc_force_apply) and the vertex
+// update (scheme_move_apply)
+extern "C" int ctc_sub_mem_update(ctc_sub *s, void *stream) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sub_mem_update: bad arguments");
+    const int nvt = s->mnc * s->mnv;
+    if (nvt == 0) return CTC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int tot = s->eoff_host[26];
+    if (tot > 0) {
+        k_images_back<<<ceil_div(tot, 256), 256, 0, st>>>(tot, s->iback, s->ividx, s->mforce);
+        CUDA_TRY(cudaGetLastError());
+    }
+    int rc = membrane_forces(s->rbc, &s->mpar, s->mnc, (const float*)s->mpos[0], (const float*)s->mvel[0], 4,
+                             (float*)s->mforce, 4, st);
+    if (rc) return rc;
+    const float3 bf = make_float3(s->cfg.sim.bodyf[0], s->cfg.sim.bodyf[1], s->cfg.sim.bodyf[2]);
+    CUDA_TRY(integrate_launch(s->mcount, nvt, s->mpos[0], s->mvel[0], s->mforce, s->cfg.sim.dt, s->mmass, bf, st));
+    return CTC_OK;
+}
+
+// device pointers of the membranes' state (float4 SoA, cell after cell; w of
+// a position: the vertex's global id) and the last step's vertex forces
+extern "C" int ctc_sub_membrane_state(ctc_sub *s, float **pos, float **vel, float **force) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sub_membrane_state: null");
+    if (pos) *pos = (float*)s->mpos[0];
+    if (vel) *vel = (float*)s->mvel[0];
+    if (force) *force = (float*)s->mforce;
+    return CTC_OK;
+}
+
+// the membranes: cells, vertices per cell, and (when the arrays are given)
+// the vertices [host, AoS, nc nv] and the cells' global ids [host, nc].
+// Synchronises.
+extern "C" int ctc_sub_get_membranes(ctc_sub *s, int *nc, int *nv, float *pp, int *cell_ids, void *stream) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sub_get_membranes: null");
+    if (nc) *nc = s->mnc;
+    if (nv) *nv = s->mnv;
+    const int nvt = s->mnc * s->mnv;
+    if ((!pp && !cell_ids) || nvt == 0) return CTC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<float4> p(nvt), v(nvt);
+    CUDA_TRY(cudaMemcpyAsync(p.data(), s->mpos[0], sizeof(float4) * nvt, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(v.data(), s->mvel[0], sizeof(float4) * nvt, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (int i = 0; i < nvt; i++) {
+        if (pp) {
+            float *o = pp + 6 * (size_t)i;
+            o[0] = p[i].x; o[1] = p[i].y; o[2] = p[i].z;
+            o[3] = v[i].x; o[4] = v[i].y; o[5] = v[i].z;
+        }
+        if (cell_ids && i % s->mnv == 0) {
+            int id;
+            memcpy(&id, &p[i].w, sizeof(int));
+            cell_ids[i / s->mnv] = id / s->mnv;
+        }
+    }
+    return CTC_OK;
+}
+
 // the exchange buffers for the transport, all device addresses: kind 0 the
 // migration bags (records of 2 float4), 1 the halo particle bags (records of
 // 2 float4), 2 the halo fragment-cell start bags (ints, ncell(f) + 1 each,
@@ -570,8 +1045,27 @@ extern "C" int ctc_sub_halo_update(ctc_sub *s, const int *rcounts, void *stream)
 // left it; recv[f]: where the bag from direction f goes; cap[f]: its
 // capacity (elements)
 extern "C" int ctc_sub_bags(const ctc_sub *s, int kind, void **send, void **recv, int *cap) {
-    if (!s || !send || !recv || !cap || kind < 0 || kind > 2) return fail(CTC_ERR_ARG, "ctc_sub_bags: bad arguments");
+    if (!s || !send || !recv || !cap || kind < 0 || kind > 5) return fail(CTC_ERR_ARG, "ctc_sub_bags: bad arguments");
+    if (kind >= 3 && !s->mnv) return fail(CTC_ERR_ARG, "ctc_sub_bags: no membranes");
     for (int f = 0; f < 26; f++) {
+        if (kind == 3) {
+            send[f] = s->csend + 2 * (size_t)s->csend_off[f] * s->mnv;
+            recv[f] = s->crecv + 2 * (size_t)f * s->ccap * s->mnv;
+            cap[f] = s->ccap;
+            continue;
+        }
+        if (kind == 4) {
+            send[f] = s->isend + 2 * (size_t)s->eoff_host[f];
+            recv[f] = s->irecv + 2 * (size_t)f * s->icap;
+            cap[f] = s->icap;
+            continue;
+        }
+        if (kind == 5) {
+            send[f] = s->iforce + (size_t)s->irn[f];
+            recv[f] = s->iback + (size_t)s->eoff_host[f];
+            cap[f] = s->icap;
+            continue;
+        }
         if (kind == 0) {
             send[f] = s->dsend + 2 * (size_t)s->dsend_off[f];
             recv[f] = s->drecv + 2 * (size_t)s->dbase[f];

@@ -381,7 +381,8 @@ __device__ __forceinline__ void fsi_q_block(const FsiArgs &A, const int bid) {
             const float4 b = __ldg(A.spos + j);
             float rnd;
             if (RNG == 0) rnd = mean0var1uu(halo ? seed_halo : seed_bulk, halo ? rec.z : (unsigned)vk, (unsigned)(j - sk));
-            else rnd = mean0var1uu(seed_bulk, (unsigned)vk, (unsigned)__float_as_int(b.w));
+            else rnd = mean0var1uu(seed_bulk, A.vkey_w ? (unsigned)__float_as_int(a.w) : (unsigned)vk,
+                                   (unsigned)__float_as_int(b.w));
             float3 f;
             if (dpd_force(P, a, va, b, __ldg(A.svel + j), rnd, f)) {
                 red3(A.fv, A.fstride, v, 1.0f, f);

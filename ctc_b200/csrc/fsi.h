@@ -37,6 +37,9 @@ struct FsiArgs {
     // src/fsi/dev/map/bulk.h): the pair pass of ctc_fsi_pairs over vertices or
     // over images the caller lists
     int no_wrap;
+    // stable keys: the vertex's id from the w of its position (float4 SoA)
+    // instead of its index -- vertices of a subdomain keep their global ids
+    int vkey_w;
 };
 
 // ints of the count buffer of fsi_images_launch: 26 per box with B.nbox > 0;

@@ -173,6 +173,104 @@ class SubDomain:
         ids = p[:, 3].copy().view(np.int32)
         return np.concatenate([p[:, :3], v[:, :3]], axis=1), ids
 
+    # -- membranes ---------------------------------------------------------------
+    def set_membranes(self, pv, cell_ids, tri, nv, params, fsi, maxc, mass=0.5):
+        """Cells of one template in this subdomain: pv (nc*nv, 6) in subdomain
+        coordinates, cell_ids (nc,) their global ids, tri (nt, 3), room for
+        maxc cells; params a dict of RbcParams fields, fsi a DpdParams."""
+        import torch
+        pv = np.ascontiguousarray(pv, np.float32).reshape(-1, 6)
+        tri = np.ascontiguousarray(tri, np.int32).reshape(-1, 3)
+        cell_ids = np.ascontiguousarray(cell_ids, np.int32)
+        self.mnv = int(nv)
+        with torch.cuda.device(self.device):
+            check(lib().ctc_sub_set_membranes(self.h, len(cell_ids), self.mnv, len(tri), tri.ctypes.data_as(C.c_void_p),
+                                              pv.ctypes.data_as(C.c_void_p), cell_ids.ctypes.data_as(C.c_void_p),
+                                              int(maxc), C.byref(_lib.RbcParams(**params)), C.byref(fsi),
+                                              float(mass)))
+        self.maxc = int(maxc)
+        self._mbase = {}
+        for kind in (3, 4, 5):
+            send, recv, cap = (C.c_void_p * 26)(), (C.c_void_p * 26)(), (C.c_int * 26)()
+            check(lib().ctc_sub_bags(self.h, kind, send, recv, cap))
+            cap = list(cap)
+            el = {3: self.REC * self.mnv, 4: self.REC, 5: 4}[kind]
+            tot = el * sum(cap)
+            # the cells leaving in one step fit the maxc cells' send buffer
+            stot = el * self.maxc if kind == 3 else tot
+            self._mbase[kind] = (_view(send[0], stot, torch.float32, self.device),
+                                 _view(recv[0], tot, torch.float32, self.device), cap, el)
+
+    def membrane_forces(self):
+        """The last step's vertex forces (nc*nv, 3) and their global vertex ids [host]."""
+        import torch
+        nc, nv = C.c_int(), C.c_int()
+        check(lib().ctc_sub_get_membranes(self.h, C.byref(nc), C.byref(nv), None, None, self._stream()))
+        n = nc.value * nv.value
+        pos, frc = C.c_void_p(), C.c_void_p()
+        check(lib().ctc_sub_membrane_state(self.h, C.byref(pos), None, C.byref(frc)))
+        torch.cuda.synchronize(self.device)
+        p = _view(pos.value, 4 * n, torch.float32, self.device).view(-1, 4).cpu().numpy()
+        f = _view(frc.value, 4 * n, torch.float32, self.device).view(-1, 4).cpu().numpy()
+        return f[:, :3], p[:, 3].copy().view(np.int32)
+
+    def has_membranes(self):
+        return bool(getattr(self, "mnv", 0))
+
+    def get_membranes(self):
+        """(pv (nc*nv, 6) in subdomain coordinates, cell ids (nc,)) [host]."""
+        nc, nv = C.c_int(), C.c_int()
+        check(lib().ctc_sub_get_membranes(self.h, C.byref(nc), C.byref(nv), None, None, self._stream()))
+        pv = np.zeros((nc.value * nv.value, 6), np.float32)
+        ids = np.zeros(nc.value, np.int32)
+        if nc.value:
+            check(lib().ctc_sub_get_membranes(self.h, None, None, pv.ctypes.data_as(C.c_void_p),
+                                              ids.ctypes.data_as(C.c_void_p), self._stream()))
+        return pv, ids
+
+    def mem_bags(self, kind, counts, rcounts=None):
+        """Send bags (sized by counts) and receive bags of membrane kind 3
+        (cells), 4 (images) or 5 (the images' forces sent back: send bag j
+        holds rcounts[j] of the images received from direction j, receive
+        bag f the forces on this rank's image bag f of counts[f] images)."""
+        sb, rb, cap, el = self._mbase[kind]
+        send, recv = [], []
+        if kind == 5:
+            o = 0
+            for j in range(26):
+                send.append(sb[o:o + el * rcounts[j]])
+                o += el * rcounts[j]
+            o = 0
+            for f in range(26):
+                recv.append(rb[o:o + el * counts[f]])
+                o += el * counts[f]
+            return send, recv, cap
+        o = 0
+        for f in range(26):
+            send.append(sb[o:o + el * counts[f]])
+            o += el * counts[f]
+        recv = [rb[el * cap[0] * f:el * cap[0] * (f + 1)] for f in range(26)]
+        return send, recv, cap
+
+    def mem_distr_pack(self):
+        c = (C.c_int * 26)()
+        check(lib().ctc_sub_mem_distr_pack(self.h, c, self._stream()))
+        return list(c)
+
+    def mem_distr_unpack(self, rcounts):
+        check(lib().ctc_sub_mem_distr_unpack(self.h, (C.c_int * 26)(*rcounts), self._stream()))
+
+    def mem_exch_pack(self):
+        c = (C.c_int * 26)()
+        check(lib().ctc_sub_mem_exch_pack(self.h, c, self._stream()))
+        return list(c)
+
+    def mem_fsi(self, rcounts):
+        check(lib().ctc_sub_mem_fsi(self.h, (C.c_int * 26)(*rcounts), self._stream()))
+
+    def mem_update(self):
+        check(lib().ctc_sub_mem_update(self.h, self._stream()))
+
     def forces(self):
         """The last step's forces (n, 3), cell-sorted [host]."""
         import torch
@@ -349,12 +447,20 @@ def step(subs, transport, marks=None):
             e.record()
             marks.append(e)
     R = SubDomain.REC
+    mem = bool(getattr(subs[0], "mnv", 0))
     for s in subs:
         s.distr_pack()
     counts = [s.distr_counts() for s in subs]
     rcounts = transport.exchange_counts(counts)
     bags = [s.bags(0, c) for s, c in zip(subs, counts)]
     transport.exchange([b[0] for b in bags], [b[1] for b in bags], rcounts, R).wait()
+    if mem:     # whole cells migrate beside the solvent (distr_rbc)
+        ccounts = [s.mem_distr_pack() for s in subs]
+        crc = transport.exchange_counts(ccounts)
+        cb = [s.mem_bags(3, c) for s, c in zip(subs, ccounts)]
+        transport.exchange([b[0] for b in cb], [b[1] for b in cb], crc, R * subs[0].mnv).wait()
+        for s, rc in zip(subs, crc):
+            s.mem_distr_unpack(rc)
     mark()
     for s, rc in zip(subs, rcounts):
         s.distr_unpack(rc)
@@ -371,9 +477,22 @@ def step(subs, transport, marks=None):
     fss = [s.bags(2, None) for s in subs]
     h1 = transport.exchange([b[0] for b in bags], [b[1] for b in bags], rcounts, R)
     h2 = transport.exchange([b[0] for b in fss], [b[1] for b in fss], [b[2] for b in fss], 1)
+    if mem:     # the vertices' images for the neighbours' FSI (exch_obj)
+        icounts = [s.mem_exch_pack() for s in subs]
+        irc = transport.exchange_counts(icounts)
+        ib = [s.mem_bags(4, c) for s, c in zip(subs, icounts)]
+        transport.exchange([b[0] for b in ib], [b[1] for b in ib], irc, R).wait()
     h1.wait()
     h2.wait()
+    if mem:     # FSI of the own vertices and of the images; the images' forces go back
+        for s, rc in zip(subs, irc):
+            s.mem_fsi(rc)
+        fb = [s.mem_bags(5, c, rc) for s, c, rc in zip(subs, icounts, irc)]
+        transport.exchange([b[0] for b in fb], [b[1] for b in fb], icounts, 4).wait()
     mark()
     for s, rc in zip(subs, rcounts):
         s.halo_update(rc)
+    if mem:
+        for s in subs:
+            s.mem_update()
     mark()

@@ -520,10 +520,45 @@ int ctc_sub_bulk(ctc_sub *s, void *stream);
 int ctc_sub_halo_update(ctc_sub *s, const int *rcounts, void *stream);
 /* exchange buffers [device addresses, 26 each]: kind 0 migration records, 1
  * halo records (2 float4 each: position with the id bits in w, velocity), 2
- * halo fragment-cell starts (ints, fixed sizes cap[f]); send[f] the last
- * pack's bag for direction f, recv[f] where the bag from direction f goes,
- * cap[f] its capacity in elements */
+ * halo fragment-cell starts (ints, fixed sizes cap[f]); with membranes 3 the
+ * migrating cells (nv records each), 4 the vertices' images (records), 5 the
+ * forces on the images sent back (float4: send[j] the forces on the images
+ * received from direction j, recv[f] those on this rank's image bag f).
+ * send[f] the last pack's bag for direction f, recv[f] where the bag from
+ * direction f goes, cap[f] its capacity in elements (cells for kind 3) */
 int ctc_sub_bags(const ctc_sub *s, int kind, void **send, void **recv, int *cap);
+/* membranes in the subdomain (src/distr/rbc, src/exch/obj, src/fsi halo):
+ * nc cells of one template (nv, nt, tri [host]), their vertices pp [host,
+ * AoS, subdomain coordinates] and global cell ids [host, nc] (a vertex's id,
+ * the stable keys' id, is cell id * nv + vertex), room for maxc cells; p, fsi
+ * and mass as ctc_sim_set_membranes.  A step with membranes adds, in order:
+ * mem_distr_pack + exchange kind 3 + mem_distr_unpack beside the solvent's
+ * migration; mem_exch_pack + exchange kind 4 beside the halo exchange;
+ * mem_fsi after ctc_sub_bulk; exchange kind 5; mem_update after
+ * ctc_sub_halo_update.  Contact and walls are not in the subdomain step. */
+int ctc_sub_set_membranes(ctc_sub *s, int nc, int nv, int nt, const int *tri, const float *pp, const int *cell_ids,
+                          int maxc, const ctc_rbc_params *p, const ctc_dpd_params *fsi, float mass);
+/* the cells whose bounding-box centre left into the cell bags; counts [host,
+ * 26] in cells; synchronises */
+int ctc_sub_mem_distr_pack(ctc_sub *s, int *counts, void *stream);
+/* the received cells (rcounts [host, 26]) moved in and appended */
+int ctc_sub_mem_distr_unpack(ctc_sub *s, const int *rcounts, void *stream);
+/* the vertices within 1 of a face into the image bags; counts [host, 26];
+ * synchronises */
+int ctc_sub_mem_exch_pack(ctc_sub *s, int *counts, void *stream);
+/* FSI of the local vertices and of the received images (rcounts [host, 26])
+ * against the local solvent: reactions into the solvent forces, the images'
+ * forces into the back bags */
+int ctc_sub_mem_fsi(ctc_sub *s, const int *rcounts, void *stream);
+/* the forces sent back for this rank's images added to its vertices, the
+ * internal membrane forces and the vertex update */
+int ctc_sub_mem_update(ctc_sub *s, void *stream);
+/* cells, vertices per cell, and (if given) the vertices pp [host, AoS] and
+ * global cell ids [host]; synchronises */
+int ctc_sub_get_membranes(ctc_sub *s, int *nc, int *nv, float *pp, int *cell_ids, void *stream);
+/* device pointers of the membranes' state (float4 SoA; w: vertex ids) and of
+ * the last step's vertex forces */
+int ctc_sub_membrane_state(ctc_sub *s, float **pos, float **vel, float **force);
 /* the number of particles (synchronises) */
 int ctc_sub_count(ctc_sub *s, int *n, void *stream);
 /* device pointers of the state: cell-sorted float4 positions (ids in w),

@@ -341,3 +341,163 @@ def test_dist_transport_one_rank_nccl_equals_local():
     finally:
         dist.destroy_process_group()
     assert C.device_error() == 0
+
+
+# -- membranes in the decomposed step ------------------------------------------
+def grid_cells(centres, seed, drift=(0.0, 0.0, 0.0)):
+    """RBCs (642 vertices) around the given centres, randomly rotated, on the
+    2^-12 grid: (pv (nc*642, 6), triangles, parameters)."""
+    from ctc_b200 import mesh
+    X, F = mesh.rbc_template(7.82)
+    rng = np.random.default_rng(seed)
+    r = np.concatenate([X @ mesh.random_rotation(rng).T + np.asarray(c) for c in centres])
+    pv = np.zeros((len(r), 6), np.float32)
+    pv[:, :3] = np.floor(r * 4096.0) / 4096.0
+    pv[:, 3:] = rng.normal(0.0, np.sqrt(systems.KBT / systems.RBC_MASS), (len(r), 3)) + np.asarray(drift)
+    A, V = mesh.area_volume(X, F)
+    return pv, F, systems.rbc_params(A, V)
+
+
+def split_cells(pv, nv, cart, L):
+    """Every rank's cells (the rank whose subdomain holds the centre of the
+    cell's bounding box) in its subdomain's coordinates, and their ids."""
+    Lg = np.array(cart.dims) * np.array(L)
+    lo = systems.box_lo(Lg)
+    r = pv[:, :3].astype(np.float64).reshape(-1, nv, 3)
+    c = 0.5 * (r.min(1) + r.max(1))
+    b = np.floor((c - lo) / np.array(L)).astype(int)
+    out = []
+    for k in range(cart.size):
+        ck = np.array(cart.coords(k))
+        sel = np.flatnonzero((b == ck).all(1))
+        o = lo + (ck + 0.5) * np.array(L)
+        q = pv.reshape(-1, nv, 6)[sel].copy()
+        q[:, :, :3] = (q[:, :, :3].astype(np.float64) - o).astype(np.float32)
+        out.append((q.reshape(-1, 6), sel.astype(np.int32), o))
+    return out
+
+
+def sim_membranes(sim, nvt):
+    """(positions, velocities, forces) of a Sim's vertices, cell after cell."""
+    import ctypes
+    C, _ = mods()
+    from ctc_b200 import _lib
+    p, v, f = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    _lib.check(_lib.lib().ctc_sim_membrane_state(sim.h, ctypes.byref(p), ctypes.byref(v), ctypes.byref(f)))
+    d = torch.device("cuda")
+    get = lambda a: C._wrap_dev(a.value, 4 * nvt, torch.float32, d).reshape(nvt, 4)[:, :3].cpu().numpy()
+    return get(p), get(v), get(f)
+
+
+def _mem_setup(dims, L, centres, seed, dt, bodyf=(0.0, 0.0, 0.0), drift=(0.0, 0.0, 0.0), vstd=None):
+    C, X = mods()
+    cart = X.Cart(dims)
+    Lg = tuple(d * l for d, l in zip(dims, L))
+    pp = grid_solvent(Lg, seed=seed, vstd=vstd)
+    pp[:, 3:] += np.asarray(drift, np.float32)      # the solvent flows with the cells
+    pv, tri, par = grid_cells(centres, seed + 1, drift)
+    nv = 642
+    dpd = C.DpdParams(*systems.dpd_params())
+    fsi = C.DpdParams(*systems.dpd_params())
+    sim = C.Sim(Lg, len(pp), dpd, dt=dt, bodyf=bodyf, rng=C.CTC_RNG_STABLE)
+    sim.set_solvent(pp)
+    sim.set_membranes(pv, tri, nv, par, fsi, mass=systems.RBC_MASS)
+    parts = split(pp, cart, L)
+    cparts = split_cells(pv, nv, cart, L)
+    subs = [X.SubDomain(L, cart, r, len(pp), dpd, dt=dt, bodyf=bodyf, rng=C.CTC_RNG_STABLE, maxd=40.0)
+            for r in range(cart.size)]
+    for s, (q, ids, _), (cq, cids, _) in zip(subs, parts, cparts):
+        s.set_solvent(q, ids)
+        s.set_membranes(cq, cids, tri, nv, par, fsi, maxc=len(centres), mass=systems.RBC_MASS)
+    return cart, pp, pv, sim, subs, parts, cparts
+
+
+def gather_membranes(subs, parts, nvt, nv):
+    """Every rank's vertices by global vertex id: (pv in global coordinates,
+    forces, the rank of each cell)."""
+    pv = np.full((nvt, 6), np.nan)
+    ff = np.full((nvt, 3), np.nan)
+    owner = np.full(nvt // nv, -1)
+    for r, (s, (_, _, o)) in enumerate(zip(subs, parts)):
+        q, cids = s.get_membranes()
+        f, vids = s.membrane_forces()
+        assert np.array_equal(vids, (cids[:, None] * nv + np.arange(nv)).reshape(-1))
+        g = q.astype(np.float64)
+        g[:, :3] += o
+        pv[vids] = g
+        ff[vids] = f
+        assert (owner[cids] == -1).all(), "every cell on exactly one rank"
+        owner[cids] = r
+    assert (owner >= 0).all()
+    return pv, ff, owner
+
+
+@pytest.mark.parametrize("dims,L,centres", [
+    ((2, 1, 1), (16, 16, 16), [(0.3, 0.2, -0.4), (-15.7, 3.1, 2.2), (-8.0, -4.0, 4.5)]),
+    ((2, 2, 1), (16, 16, 16), [(0.3, 0.4, -0.4), (-15.6, -15.7, 2.2), (8.2, -8.0, -6.3), (-7.9, 7.6, 5.1)]),
+])
+def test_ranks_membranes_forces_equal_undivided_box(dims, L, centres):
+    """Cells straddling the faces between ranks (their vertices' images cross
+    for FSI, the forces on the images come back): solvent and vertex forces
+    equal the undivided box's at 1e-5 with stable keys, positions on the
+    2^-12 grid."""
+    C, X = mods()
+    cart, pp, pv, sim, subs, parts, cparts = _mem_setup(dims, L, centres, 51, dt=0.0)
+    n, nv, nvt = len(pp), 642, len(pv)
+    sim.step(1)
+    torch.cuda.synchronize()
+    _, sids, sf = sim_state(sim, n)
+    ref = np.empty((n, 3))
+    ref[sids] = sf
+    _, _, mref = sim_membranes(sim, nvt)
+    X.step(subs, X.LocalTransport(cart))
+    torch.cuda.synchronize()
+    _, ff = gather(subs, parts)
+    _, mf, owner = gather_membranes(subs, parts, nvt, nv)
+    # the FSI reactions reach the solvent on the ranks across the faces
+    assert rel_err(ff, ref).max() < 1e-5
+    assert rel_err(mf, mref).max() < 1e-5
+    assert len(set(owner.tolist())) > 1
+    assert C.device_error() == 0
+
+
+def test_ranks_membranes_migrate_and_follow_undivided_box():
+    """Solvent and cells flowing along x (0.2 per step): a cell crosses the
+    face between the two ranks, another the periodic face, and both change
+    rank; six steps with a body force: every cell on the rank that holds its bounding-box centre, and the
+    vertices and the solvent follow the undivided box's run."""
+    C, X = mods()
+    dims, L = (2, 1, 1), (16, 16, 16)
+    centres = [(-0.45, 0.2, -0.4), (15.55, 3.1, 2.2), (-8.0, -4.0, 4.5)]
+    dt, K = 0.01, 6
+    cart, pp, pv, sim, subs, parts, cparts = _mem_setup(dims, L, centres, 61, dt=dt, bodyf=(0.5, 0.0, 0.0),
+                                                        drift=(20.0, 0.0, 0.0), vstd=1.0)
+    n, nv, nvt = len(pp), 642, len(pv)
+    owners = []
+    T = X.LocalTransport(cart)
+    for k in range(K):
+        X.step(subs, T)
+        torch.cuda.synchronize()
+        owners.append(gather_membranes(subs, parts, nvt, nv)[2])
+    sim.step(K)
+    torch.cuda.synchronize()
+    assert owners[0][0] == 0 and owners[-1][0] == 1, owners
+    assert owners[0][1] == 1 and owners[-1][1] == 0, owners
+    mp, mv, _ = sim_membranes(sim, nvt)
+    got, _, _ = gather_membranes(subs, parts, nvt, nv)
+    Lg = np.array(cart.dims) * np.array(L)
+    dx = got[:, :3] - mp
+    dx -= np.round(dx / Lg) * Lg
+    dx = np.abs(dx).max(1)
+    assert np.quantile(dx, 0.999) < 1e-4 and dx.max() < 2e-3, (np.quantile(dx, 0.999), dx.max())
+    dv = np.abs(got[:, 3:] - mv).max(1)
+    assert np.quantile(dv, 0.99) < 1e-2 and dv.max() < 0.2, (np.quantile(dv, 0.99), dv.max())
+    sp, sids, _ = sim_state(sim, n)
+    ref = np.empty((n, 6))
+    ref[sids] = sp
+    sg, _ = gather(subs, parts)
+    dx = sg[:, :3] - ref[:, :3]
+    dx -= np.round(dx / Lg) * Lg
+    dx = np.abs(dx).max(1)
+    assert np.quantile(dx, 0.999) < 1e-4 and dx.max() < 2e-3, (np.quantile(dx, 0.999), dx.max())
+    assert C.device_error() == 0
