@@ -566,6 +566,10 @@ class Sim:
         """Replay the step as CUDA graphs (captured on first use)."""
         check(lib().ctc_sim_set_graph(self.h, int(bool(enable))))
 
+    def set_fused_count(self, enable=True):
+        """The update counts the next cell-list build's cells (default on)."""
+        check(lib().ctc_sim_set_fused_count(self.h, int(bool(enable))))
+
     def tune(self, reps=3, stream=None):
         """Autotune the pair kernels' launch shapes on the current state (after
         a step); returns (bulk threads, bulk unroll, halo threads, halo unroll,

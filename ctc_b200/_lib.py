@@ -99,6 +99,7 @@ SIGNATURES = {
     "ctc_cnt_apply_seeded": (C.c_int, [vp, C.POINTER(DpdLjParams), C.c_int, vp, C.c_float, C.c_float, vp, vp]),
     "ctc_sim_set_contact": (C.c_int, [vp, C.POINTER(DpdLjParams)]),
     "ctc_sim_set_graph": (C.c_int, [vp, C.c_int]),
+    "ctc_sim_set_fused_count": (C.c_int, [vp, C.c_int]),
     "ctc_mesh_write_ply": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int,
                                      C.c_int]),
     "ctc_sim_set_membrane_noise": (C.c_int, [vp, C.c_int, C.c_uint]),

@@ -336,6 +336,8 @@ struct ctc_sim {
     Off27 off;
     int cur;                               // index of the buffer that holds the state
     bool built;                            // starts/counts describe pos[cur]
+    bool fuse_count;                       // the update counts the next build's cells (no walls)
+    bool counted;                          // counts and w.cidslot hold the count pass of pos[cur]
     Kiss trunk_host[27];                   // host mirror, for ctc_sim_next_seeds
     int prof;                              // record per-phase events each step
     std::vector<cudaEvent_t> ev;           // CTC_SIM_PHASES + 1 events per profiled step
@@ -447,6 +449,8 @@ extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
     s->cur = 0;
     s->n_host = 0;
     s->built = false;
+    s->fuse_count = true;
+    s->counted = false;
     *ps = s;
     return CTC_OK;
 }
@@ -507,6 +511,7 @@ static int sim_set(ctc_sim *s, int n, const float *pp, bool host, cudaStream_t s
     CUDA_TRY(cudaStreamSynchronize(st));
     s->n_host = n;
     s->built = false;
+    s->counted = false;
     return CTC_OK;
 }
 
@@ -706,10 +711,15 @@ extern "C" int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream) {
     return CTC_OK;
 }
 
+// the update fuses the next build's count pass unless bounce-back moves the
+// particles after it
+static bool sim_fuses(const ctc_sim *s) { return s->fuse_count && !s->wall; }
+
 // one step: seeds, wrap + cell lists into the other buffer, forces, update
 // the device work of one step from buffer s->cur (built: the cell lists
-// describe it, so its count is starts[nc]); enqueued on st, capturable
-static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
+// describe it, so its count is starts[nc]; counted: the previous update
+// counted its cells); enqueued on st, capturable
+static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built, bool counted) {
     int src = s->cur, dst = 1 - s->cur;
     int ntr = s->cfg.rng == CTC_RNG_REFERENCE ? 27 : 1;
     sim_mark(s, 0, st);
@@ -718,7 +728,7 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
     // it aside, the build overwrites starts
     if (built) CUDA_TRY(cudaMemcpyAsync(s->count0, s->starts + s->nc, sizeof(int), cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(clist_launch(s->L, s->n_host, s->count0, s->pos[src], s->vel[src], 1, s->counts, s->starts,
-                          s->pos[dst], s->vel[dst], nullptr, s->w, dev_err_ptr(), st));
+                          s->pos[dst], s->vel[dst], nullptr, s->w, dev_err_ptr(), st, Boxes(), 0, counted));
     const int nvt = s->mnc * s->mnv;
     if (nvt > 0) {
         // objects_distribute: whole cells re-enter through a periodic face
@@ -794,8 +804,12 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built) {
         if (rc) return rc;
     }
     sim_mark(s, 7, st);
-    CUDA_TRY(integrate_launch(s->starts + s->nc, s->n_host, s->pos[dst], s->vel[dst], s->force, s->cfg.dt,
-                              s->cfg.mass, bf, st));
+    if (sim_fuses(s))   // the forces' readers of counts have run: the next build's count pass
+        CUDA_TRY(integrate_count_launch(s->starts + s->nc, s->n_host, s->pos[dst], s->vel[dst], s->force, s->cfg.dt,
+                                        s->cfg.mass, bf, s->L, s->counts, s->w, dev_err_ptr(), st));
+    else
+        CUDA_TRY(integrate_launch(s->starts + s->nc, s->n_host, s->pos[dst], s->vel[dst], s->force, s->cfg.dt,
+                                  s->cfg.mass, bf, st));
     sim_mark(s, 8, st);
     if (nvt > 0) {
         // objects_advance: internal forces on top of the FSI ones, then the update
@@ -837,10 +851,11 @@ static void sim_advance(ctc_sim *s) {
     if (s->prof) s->prof_steps++;
     s->cur = 1 - s->cur;
     s->built = true;
+    s->counted = sim_fuses(s);
 }
 
 static int sim_step1(ctc_sim *s, cudaStream_t st) {
-    int rc = sim_enqueue(s, st, s->built);
+    int rc = sim_enqueue(s, st, s->built, s->built && s->counted);
     if (rc) return rc;
     sim_advance(s);
     return CTC_OK;
@@ -863,7 +878,7 @@ static int sim_capture(ctc_sim *s, int k) {
     s->cur = k;
     cudaGraph_t g = nullptr;
     CUDA_TRY(cudaStreamBeginCapture(s->own, cudaStreamCaptureModeThreadLocal));
-    int rc = sim_enqueue(s, s->own, true);
+    int rc = sim_enqueue(s, s->own, true, sim_fuses(s));   // graphs replay the steady state
     cudaError_t e = cudaStreamEndCapture(s->own, &g);
     s->cur = keep;
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -881,7 +896,7 @@ extern "C" int ctc_sim_step(ctc_sim *s, int nsteps, void *stream) {
     // the first step after new state, and profiled steps, run directly
     // (and every step with a time-dependent wall velocity, which a graph would freeze)
     const bool timed_wall = s->wall && s->wall->vel.type == CTC_WVEL_SHEAR_SIN;
-    for (; k < nsteps && (!s->use_graph || s->prof || !s->built || timed_wall); k++) {
+    for (; k < nsteps && (!s->use_graph || s->prof || !s->built || timed_wall || (sim_fuses(s) && !s->counted)); k++) {
         int rc = sim_step1(s, st);
         if (rc) return rc;
     }
@@ -941,6 +956,7 @@ extern "C" int ctc_sim_tune(ctc_sim *s, int reps, int *choice, void *stream) {
     CUDA_TRY(cudaMemcpyAsync(s->count0, s->starts + s->nc, sizeof(int), cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(clist_launch(s->L, s->n_host, s->count0, s->pos[s->cur], s->vel[s->cur], 1, s->counts, s->starts,
                           s->pos[spare], s->vel[spare], nullptr, s->w, dev_err_ptr(), st));
+    s->counted = false;        // the next step counts again
     A.pos = s->pos[spare]; A.vel = s->vel[spare];
     CUDA_TRY(frag_starts_launch(s->L, s->counts, s->fss, s->off, st));
     CUDA_TRY(halo_pack_launch(A, s->off, s->pack, s->pack_off, s->pack_cap, st));
@@ -1014,6 +1030,14 @@ extern "C" int ctc_sim_set_graph(ctc_sim *s, int enable) {
     if (!s) return fail(CTC_ERR_ARG, "ctc_sim_set_graph: null");
     if (!enable) sim_drop_graphs(s);
     s->use_graph = enable != 0;
+    return CTC_OK;
+}
+
+extern "C" int ctc_sim_set_fused_count(ctc_sim *s, int enable) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sim_set_fused_count: null");
+    sim_drop_graphs(s);
+    s->fuse_count = enable != 0;
+    s->counted = false;
     return CTC_OK;
 }
 

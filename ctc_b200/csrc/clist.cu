@@ -48,21 +48,14 @@ __device__ __forceinline__ int cell_of(float4 p, int3 L) {
 // its cells in the concatenated cell arrays)
 // (the kernels' bodies take their thread's global index, so that the
 // persistent step of many boxes runs them too; kernels.cu)
-__device__ __forceinline__ void clist_count_at(int i, int n, const int *__restrict__ nptr,
-                                               const float4 *__restrict__ pos, int3 L, int wrap,
-                                               int2 *__restrict__ cidslot, int *__restrict__ counts, int *err,
-                                               const Boxes &B) {
-    if (nptr) n = min(n, *nptr);
+// the count of one particle whose position p is already loaded (i >= n: no
+// particle, but the thread still takes part in the warp's match); c0 = the
+// offset of its box's cells
+__device__ __forceinline__ void clist_count_val(int i, int n, float4 p, int3 L, int c0, int wrap,
+                                                int2 *__restrict__ cidslot, int *__restrict__ counts, int *err) {
     int cid = -1;
     bool wrapped = false;
     if (i < n) {
-        int c0 = 0;
-        if (B.nbox > 0) {
-            const int box = box_find(B.p0, B.nbox, i);
-            L = box_L(B, box);
-            c0 = __ldg(B.c0 + box);
-        }
-        float4 p = __ldg(pos + i);
         if (wrap) wrap_pos(p, L, wrapped);
         cid = cell_of(p, L);
         if (cid < 0 && wrap) set_error(err, DEV_BAD_PARTICLE);
@@ -81,6 +74,24 @@ __device__ __forceinline__ void clist_count_at(int i, int n, const int *__restri
     } else if (i < n) {
         cidslot[i] = make_int2(-1, 0);
     }
+}
+
+__device__ __forceinline__ void clist_count_at(int i, int n, const int *__restrict__ nptr,
+                                               const float4 *__restrict__ pos, int3 L, int wrap,
+                                               int2 *__restrict__ cidslot, int *__restrict__ counts, int *err,
+                                               const Boxes &B) {
+    if (nptr) n = min(n, *nptr);
+    int c0 = 0;
+    float4 p = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (i < n) {
+        if (B.nbox > 0) {
+            const int box = box_find(B.p0, B.nbox, i);
+            L = box_L(B, box);
+            c0 = __ldg(B.c0 + box);
+        }
+        p = __ldg(pos + i);
+    }
+    clist_count_val(i, n, p, L, c0, wrap, cidslot, counts, err);
 }
 
 __global__ void k_clist_count(int n, const int *__restrict__ nptr, const float4 *__restrict__ pos, int3 L,
@@ -250,11 +261,14 @@ void clist_carve(ClistScratch *w, void *base, int ncells, int maxp) {
 
 cudaError_t clist_launch(int3 L, int n, const int *nptr, const float4 *pos_in, const float4 *vel_in, int wrap,
                          int *counts, int *starts, float4 *pos_out, float4 *vel_out, int *order,
-                         const ClistScratch &w, int *err, cudaStream_t st, const Boxes &B, int nc_boxes) {
+                         const ClistScratch &w, int *err, cudaStream_t st, const Boxes &B, int nc_boxes,
+                         bool counted) {
     int nc = B.nbox > 0 ? nc_boxes : L.x * L.y * L.z;
-    cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nc, st);
     const int T = 256;
-    if (n > 0) k_clist_count<<<ceil_div(n, T), T, 0, st>>>(n, nptr, pos_in, L, wrap, w.cidslot, counts, err, B);
+    if (!counted) {
+        cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)nc, st);
+        if (n > 0) k_clist_count<<<ceil_div(n, T), T, 0, st>>>(n, nptr, pos_in, L, wrap, w.cidslot, counts, err, B);
+    }
     k_scan_tiles<<<w.nsums, SCAN_T, 0, st>>>(nc, counts, starts, w.sums);
     k_scan_sums<<<1, SCAN_T, 0, st>>>(w.nsums, w.sums, starts + nc);
     k_scan_add<<<ceil_div(nc, T), T, 0, st>>>(nc, starts, w.sums);

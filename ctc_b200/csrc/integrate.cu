@@ -9,10 +9,8 @@
 namespace ctc {
 
 // cell-sorted SoA state; the particle count is read on the device
-__device__ __forceinline__ void integrate_at(int i, const int *__restrict__ nptr, float4 *__restrict__ pos,
-                                             float4 *__restrict__ vel, const float4 *__restrict__ force, float dt,
-                                             float mass, float3 a) {
-    if (i >= *nptr) return;
+__device__ __forceinline__ float4 integrate_one(int i, float4 *__restrict__ pos, float4 *__restrict__ vel,
+                                                const float4 *__restrict__ force, float dt, float mass, float3 a) {
     float4 f = force[i], v = vel[i], r = pos[i];
     // f += m*a, then v += f/m*dt, r += v*dt, each a fused multiply-add as compiled
     f.x = __fmaf_rn(mass, a.x, f.x);
@@ -26,6 +24,13 @@ __device__ __forceinline__ void integrate_at(int i, const int *__restrict__ nptr
     r.z = __fmaf_rn(v.z, dt, r.z);
     vel[i] = v;
     pos[i] = r;
+    return r;
+}
+
+__device__ __forceinline__ void integrate_at(int i, const int *__restrict__ nptr, float4 *__restrict__ pos,
+                                             float4 *__restrict__ vel, const float4 *__restrict__ force, float dt,
+                                             float mass, float3 a) {
+    if (i < *nptr) integrate_one(i, pos, vel, force, dt, mass, a);
 }
 
 __global__ void k_integrate(const int *__restrict__ nptr, float4 *__restrict__ pos, float4 *__restrict__ vel,

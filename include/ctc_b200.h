@@ -392,6 +392,11 @@ int ctc_sim_step(ctc_sim *s, int nsteps, void *stream);
  * and before its later work; the first step after new state and profiled
  * steps run directly; 0: direct launches */
 int ctc_sim_set_graph(ctc_sim *s, int enable);
+/* 1 (the default): the update also counts the updated particles into the
+ * next step's cells (the cell-list build's first pass, fused; off while walls
+ * bounce particles after the update); 0: the build counts them itself.  Both
+ * give the same cell lists from the same positions. */
+int ctc_sim_set_fused_count(ctc_sim *s, int enable);
 /* autotuner: times every launch shape of the bulk and halo pair kernels
  * (as ctc_batch_tune, and two variants of the bulk kernel: 1 its candidate
  * rows staged in shared memory by bulk copies (128 threads x 4 or 8 loads),

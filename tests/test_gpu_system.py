@@ -180,3 +180,40 @@ def test_fused_step_forces_vs_modules(case):
     assert _rel_err(fs_step.cpu().numpy(), fs.cpu().numpy()) < 1e-5
     assert _rel_err(fv_step.cpu().numpy(), fv.cpu().numpy()) < 1e-5
     sim.close()
+
+
+def test_fused_count_builds_the_same_cell_lists():
+    """The update that counts the next step's cells (the default) against the
+    cell-list build counting them itself.  Without pair forces the motion is
+    exact arithmetic, so the states agree bit for bit while particles cross
+    cells and periodic faces each step (direct steps, then graph replays, a
+    tuner call in between that recounts); with forces they agree to the
+    float atomics' order."""
+    import ctc_b200 as C
+    L = (16, 12, 8)
+    ps = systems.solvent(L, seed=95)
+    ps[:, 3:] = np.random.default_rng(96).normal(0.0, 3.0, (len(ps), 3)).astype(np.float32)
+    for forces in (False, True):
+        dpd = C.DpdParams(*systems.dpd_params()) if forces else C.DpdParams(0.0, 0.0, 0.0, 0.25)
+        out = []
+        for fused in (True, False):
+            sim = C.Sim(L, len(ps), dpd, mass=1.0, dt=0.01, bodyf=(0.5, -0.25, 0.0))
+            sim.set_fused_count(fused)
+            sim.set_solvent(ps)
+            sim.step(2)
+            sim.set_graph(True)
+            sim.step(3)
+            sim.set_tune((128, 4, 128, 2))
+            if fused:
+                sim.tune(reps=1)
+                sim.set_tune((128, 4, 128, 2))
+            sim.step(3)
+            out.append(sim.get_solvent())
+            sim.close()
+        a, b = out
+        assert a.shape == b.shape == ps.shape
+        if forces:
+            assert np.abs(a - b).max() < 1e-3
+        else:
+            assert np.array_equal(a, b)
+    assert C.device_error() == 0
