@@ -1,11 +1,15 @@
-"""Multi-process host logic of the decomposed solvent (no GPU): 2, 4 and 8
-gloo ranks run the product's step orchestration (``exch.step``), cart
-(``exch.Cart``) and transport (``exch.DistTransport``) over host tensors.
-Each rank's subdomain is a numpy stand-in written here -- the same bins,
-bags, shifts and record layout as the device kernels, with deterministic DPD
-forces (no random term) in float64 -- and after three steps with migration
-the ranks together hold exactly the undivided periodic box's state.  The
-device kernels themselves are tested on the GPU (tests/test_gpu_exch.py)."""
+"""Multi-process host logic of the decomposed solvent and membranes (no
+GPU): 2, 4 and 8 gloo ranks run the product's step orchestration
+(``exch.step``), cart (``exch.Cart``) and transport (``exch.DistTransport``)
+over host tensors.  Each rank's subdomain is a numpy stand-in written here --
+the same bins, bags, shifts and record layout as the device kernels, with
+deterministic DPD forces (no random term) in float64 -- and after three
+steps with migration the ranks together hold exactly the undivided periodic
+box's state.  With membranes the stand-in also migrates whole cells (binned
+by the centre of their bounding box), sends its vertices' images across the
+faces for the solvent-vertex forces and takes the images' forces back, as
+the device path does; the cells' internal forces are springs.  The device
+kernels themselves are tested on the GPU (tests/test_gpu_exch.py)."""
 import os
 import socket
 import sys
@@ -39,6 +43,63 @@ def dpd_forces(pa, va, pb, vb, same):
     ev = (e * (va[:, None, :] - vb[None, :, :])).sum(-1)
     mag = np.where(ok, A * (1.0 - rs) - G * w * w * ev, 0.0)
     return (mag[..., None] * e).sum(1)
+
+
+def pair_matrix(pa, va, pb, vb):
+    """Pairwise forces (na, nb, 3) on the particles a from the particles b."""
+    d = pa[:, None, :] - pb[None, :, :]
+    r = np.sqrt((d * d).sum(-1))
+    ok = (r < 1.0) & (r > 1e-9)
+    rs = np.where(ok, r, 1.0)
+    e = d / rs[..., None]
+    w = np.where(ok, (1.0 - rs) ** SPOW, 0.0)
+    ev = (e * (va[:, None, :] - vb[None, :, :])).sum(-1)
+    mag = np.where(ok, A * (1.0 - rs) - G * w * w * ev, 0.0)
+    return mag[..., None] * e
+
+
+KS, NV = 40.0, 8          # the cells: 8 vertices joined by springs of constant KS
+
+
+def spring_forces(cr, rest):
+    """Internal forces of cells (nc, NV, 3): every vertex pair a spring at its
+    rest length."""
+    d = cr[:, :, None, :] - cr[:, None, :, :]
+    r = np.sqrt((d * d).sum(-1))
+    np.einsum("cii->ci", r)[...] = 1.0
+    mag = -KS * (r - rest[None])
+    np.einsum("cii->ci", mag)[...] = 0.0
+    return (mag[..., None] * d / r[..., None]).sum(2)
+
+
+def undivided_cells(pp, cells, rest, Lg, steps):
+    """The periodic box with solvent and cells: solvent pairs and
+    solvent-vertex pairs by minimum image, springs inside the cells."""
+    r, v = pp[:, :3].copy(), pp[:, 3:].copy()
+    cr, cv = cells[..., :3].copy(), cells[..., 3:].copy()
+    Lg = np.asarray(Lg, float)
+    nc = len(cr)
+    for _ in range(steps):
+        d = r[:, None, :] - r[None, :, :]
+        d -= np.round(d / Lg) * Lg
+        img = r[:, None, :] - d
+        f = np.zeros_like(r)
+        for i in range(len(r)):
+            f[i] = dpd_forces(r[i:i + 1], v[i:i + 1], img[i], v, False)[0]
+        vr, vv = cr.reshape(-1, 3), cv.reshape(-1, 3)
+        dv = vr[:, None, :] - r[None, :, :]
+        dv -= np.round(dv / Lg) * Lg                # solvent b's nearest image seen from vertex k
+        F = np.zeros((len(vr), len(r), 3))
+        for k in range(len(vr)):
+            F[k] = pair_matrix(vr[k:k + 1], vv[k:k + 1], vr[k] - dv[k], v)[0]
+        fv = F.sum(1).reshape(nc, NV, 3) + spring_forces(cr, rest)
+        f -= F.sum(0)
+        v = v + f * DT
+        r = r + v * DT
+        r -= np.floor((r + Lg / 2) / Lg) * Lg
+        cv = cv + fv * DT
+        cr = cr + cv * DT
+    return np.concatenate([r, v], 1), np.concatenate([cr, cv], 2)
 
 
 def undivided(pp, Lg, steps):
@@ -153,7 +214,100 @@ class NumpySub:
         self.r = self.r + self.v * DT
 
 
-def _rank_main(rank, world, port, dims, L, out):
+class NumpySubCells(NumpySub):
+    """The stand-in with whole cells of NV vertices: a cell migrates with its
+    bounding box's centre (records of NV x 8 floats, vertex id = cell id x NV
+    + vertex); a vertex within 1 of a face, or beyond it, sends an image to
+    every fragment of those faces; the forces on the images come back in the
+    order of the image bags."""
+
+    def __init__(self, L, cart, rank, pp, ids, cells, cell_ids, rest):
+        super().__init__(L, cart, rank, pp, ids)
+        self.mnv = NV
+        self.cr, self.cv = cells[..., :3].astype(np.float64), cells[..., 3:].astype(np.float64)
+        self.cids, self.rest = cell_ids.copy(), rest
+        ccap, icap = 16, 1024
+        z = lambda k: [torch.zeros(k, dtype=torch.float64) for _ in range(26)]
+        self.csend, self.crecv = z(self.REC * NV * ccap), z(self.REC * NV * ccap)
+        self.isend, self.irecv = z(self.REC * icap), z(self.REC * icap)
+        self.bsend, self.brecv = z(4 * icap), z(4 * icap)
+        self.caps = {3: ccap, 4: icap, 5: icap}
+
+    def mem_distr_pack(self):
+        b = self._bin(0.5 * (self.cr.min(1) + self.cr.max(1)))
+        counts = []
+        for f in range(26):
+            sel = np.flatnonzero(b == f)
+            rec = np.zeros((len(sel), NV, 8))
+            rec[..., :3], rec[..., 4:7] = self.cr[sel], self.cv[sel]
+            rec[..., 3] = self.cids[sel, None] * NV + np.arange(NV)
+            self.csend[f][:rec.size] = torch.from_numpy(rec.reshape(-1))
+            counts.append(len(sel))
+        keep = b == 26
+        self.cr, self.cv, self.cids = self.cr[keep], self.cv[keep], self.cids[keep]
+        return counts
+
+    def mem_bags(self, kind, counts, rcounts=None):
+        if kind == 3:
+            return [self.csend[f][:self.REC * NV * counts[f]] for f in range(26)], self.crecv, [self.caps[3]] * 26
+        if kind == 4:
+            return [self.isend[f][:self.REC * counts[f]] for f in range(26)], self.irecv, [self.caps[4]] * 26
+        return [self.bsend[j][:4 * rcounts[j]] for j in range(26)], self.brecv, [self.caps[5]] * 26
+
+    def mem_distr_unpack(self, rcounts):
+        for j in range(26):
+            rec = self.crecv[j][:self.REC * NV * rcounts[j]].numpy().reshape(-1, NV, 8)
+            cr = rec[..., :3] + np.array(self.X.FRAG_DIRS[j]) * self.L
+            assert (self._bin(0.5 * (cr.min(1) + cr.max(1))) == 26).all()
+            self.cr = np.concatenate([self.cr, cr])
+            self.cv = np.concatenate([self.cv, rec[..., 4:7]])
+            self.cids = np.concatenate([self.cids, (rec[:, 0, 3] // NV).astype(int)])
+
+    def mem_exch_pack(self):
+        lo = -(self.L // 2)
+        vr, vv = self.cr.reshape(-1, 3), self.cv.reshape(-1, 3)
+        side = np.where(vr < lo + 1, -1, np.where(vr >= lo + self.L - 1, 1, 0))
+        sel = [[] for _ in range(26)]
+        for i, sd in enumerate(side):
+            axes = [k for k in range(3) if sd[k]]
+            for m in range(1, 1 << len(axes)):
+                d = [0, 0, 0]
+                for q, k in enumerate(axes):
+                    if (m >> q) & 1:
+                        d[k] = int(sd[k])
+                sel[self.X.frag_d2i(tuple(d))].append(i)
+        self._ivid = [np.array(x, int) for x in sel]
+        vid = (self.cids[:, None] * NV + np.arange(NV)).reshape(-1)
+        for f in range(26):
+            rec = np.zeros((len(sel[f]), 8))
+            rec[:, :3], rec[:, 3], rec[:, 4:7] = vr[sel[f]], vid[sel[f]], vv[sel[f]]
+            self.isend[f][:rec.size] = torch.from_numpy(rec.reshape(-1))
+        return [len(x) for x in sel]
+
+    def mem_fsi(self, rcounts):
+        vr, vv = self.cr.reshape(-1, 3), self.cv.reshape(-1, 3)
+        F = pair_matrix(vr, vv, self.r, self.v)      # the own vertices, no periodic wrap
+        self.mf = F.sum(1)
+        self.f -= F.sum(0)
+        for j in range(26):
+            rec = self.irecv[j][:self.REC * rcounts[j]].numpy().reshape(-1, 8)
+            out = np.zeros((len(rec), 4))
+            if len(rec):
+                Fj = pair_matrix(rec[:, :3] + np.array(self.X.FRAG_DIRS[j]) * self.L, rec[:, 4:7], self.r, self.v)
+                self.f -= Fj.sum(0)
+                out[:, :3] = Fj.sum(1)
+            self.bsend[j][:out.size] = torch.from_numpy(out.reshape(-1))
+
+    def mem_update(self):
+        for f in range(26):
+            b = self.brecv[f][:4 * len(self._ivid[f])].numpy().reshape(-1, 4)
+            np.add.at(self.mf, self._ivid[f], b[:, :3])
+        fv = self.mf.reshape(-1, NV, 3) + spring_forces(self.cr, self.rest)
+        self.cv = self.cv + fv * DT
+        self.cr = self.cr + self.cv * DT
+
+
+def _rank_main(rank, world, port, dims, L, out, with_cells=False):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     sys.path.insert(0, ROOT)
     import datetime
@@ -162,28 +316,59 @@ def _rank_main(rank, world, port, dims, L, out):
     from ctc_b200 import exch
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     cart = exch.Cart(dims)
-    pp, Lg = _system(dims, L)
+    pp, Lg = _system(dims, L, 2.0 if with_cells else 0.0)
     c = np.floor((pp[:, :3] + np.array(Lg) / 2) / np.array(L)).astype(int)
     me = np.array(cart.coords(rank))
     sel = np.flatnonzero((c == me).all(1))
     o = -np.array(Lg) / 2 + (me + 0.5) * np.array(L)
     q = pp[sel].copy()
     q[:, :3] -= o
-    sub = NumpySub(L, cart, rank, q, sel)
+    if with_cells:
+        cells, rest = _cells(Lg)
+        cc = 0.5 * (cells[..., :3].min(1) + cells[..., :3].max(1))
+        cb = np.floor((cc + np.array(Lg) / 2) / np.array(L)).astype(int)
+        csel = np.flatnonzero((cb == me).all(1))
+        cq = cells[csel].copy()
+        cq[..., :3] -= o
+        sub = NumpySubCells(L, cart, rank, q, sel, cq, csel, rest)
+    else:
+        sub = NumpySub(L, cart, rank, q, sel)
     T = exch.DistTransport(cart, rank)
     for _ in range(3):
         exch.step([sub], T)
     res = np.concatenate([sub.r + o, sub.v], 1)
-    out.put((rank, sub.ids.tolist(), res.tolist()))
+    cres = (sub.cids.tolist(), np.concatenate([sub.cr + o, sub.cv], 2).tolist()) if with_cells else None
+    out.put((rank, sub.ids.tolist(), res.tolist(), cres))
     dist.destroy_process_group()
 
 
-def _system(dims, L):
+def _cells(Lg):
+    """Four cells of NV vertices (a cube of edge 0.7, rotated, perturbed)
+    with their springs' rest lengths; two sit just inside a face (the one
+    between the first two ranks along x, and the periodic one) and drift
+    across it with the solvent."""
+    rng = np.random.default_rng(9)
+    cube = np.array([[x, y, z] for x in (-0.35, 0.35) for y in (-0.35, 0.35) for z in (-0.35, 0.35)])
+    rest = np.sqrt(((cube[:, None] - cube[None]) ** 2).sum(-1))
+    hx = Lg[0] / 2
+    centres = [(-0.02, 0.3, 0.2), (hx - 0.02, -0.9, 0.6), (-hx / 2, Lg[1] / 2 - 0.3, -Lg[2] / 2 + 0.2),
+               (hx / 2, 0.4, -0.5)]
+    cells = []
+    for c in centres:
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        r = cube @ q.T + np.array(c) + rng.normal(0, 0.02, (NV, 3))
+        v = rng.normal(0, 0.3, (NV, 3)) + np.array([2.0, 0.0, 0.0])
+        cells.append(np.concatenate([r, v], 1))
+    return np.array(cells), rest
+
+
+def _system(dims, L, drift=0.0):
     Lg = tuple(d * l for d, l in zip(dims, L))
     rng = np.random.default_rng(7)
     n = 3 * int(np.prod(Lg))
     r = -np.array(Lg) / 2 + rng.random((n, 3)) * np.array(Lg)
     v = rng.normal(0, 1.5, (n, 3))
+    v[:, 0] += drift
     return np.concatenate([r, v], 1), Lg
 
 
@@ -206,7 +391,7 @@ def test_ranks_gloo_equal_undivided_box(dims):
     ref = undivided(pp, Lg, 3)
     got = np.full_like(ref, np.nan)
     seen = np.zeros(len(pp), int)
-    for rank, ids, st in res:
+    for rank, ids, st, _ in res:
         got[ids] = np.array(st).reshape(-1, 6)
         seen[ids] += 1
     assert (seen == 1).all()
@@ -216,8 +401,57 @@ def test_ranks_gloo_equal_undivided_box(dims):
     assert np.abs(got[:, 3:] - ref[:, 3:]).max() < 1e-9
     # some particles changed rank on the way
     moved = sum(int((np.floor((np.array(st).reshape(-1, 6)[:, :3] + np.array(Lg) / 2) / np.array(L)) !=
-                     np.floor((pp[ids, :3] + np.array(Lg) / 2) / np.array(L))).any(1).sum()) for _, ids, st in res)
+                     np.floor((pp[ids, :3] + np.array(Lg) / 2) / np.array(L))).any(1).sum()) for _, ids, st, _ in res)
     assert moved > 0
+
+
+def _run_ranks(dims, L, with_cells):
+    import torch.multiprocessing as mp
+    world = dims[0] * dims[1] * dims[2]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, dims, L, q, with_cells)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=300) for _ in procs]
+    for p in procs:
+        p.join(60)
+        assert p.exitcode == 0
+    return res
+
+
+@pytest.mark.parametrize("dims", [(2, 1, 1), (2, 2, 1), (2, 2, 2)])
+def test_ranks_gloo_cells_equal_undivided_box(dims):
+    """Solvent and cells flowing along x: after three steps the ranks hold
+    exactly the undivided box's solvent and cells (1e-9), every cell on one
+    rank, and the two cells placed just inside a face have changed rank."""
+    L = (4, 4, 4)
+    res = _run_ranks(dims, L, True)
+    pp, Lg = _system(dims, L, 2.0)
+    cells, rest = _cells(Lg)
+    ref, cref = undivided_cells(pp, cells, rest, Lg, 3)
+    Lg = np.array(Lg, float)
+    got = np.full_like(ref, np.nan)
+    cgot = np.full_like(cref, np.nan)
+    owner = np.full(len(cells), -1)
+    for rank, ids, st, (cids, cst) in res:
+        got[ids] = np.array(st).reshape(-1, 6)
+        assert (owner[cids] == -1).all()
+        owner[cids] = rank
+        cgot[cids] = np.array(cst).reshape(-1, NV, 6)
+    assert (owner >= 0).all()
+    d = got[:, :3] - ref[:, :3]
+    d -= np.round(d / Lg) * Lg
+    assert np.abs(d).max() < 1e-9 and np.abs(got[:, 3:] - ref[:, 3:]).max() < 1e-9
+    d = cgot[..., :3] - cref[..., :3]
+    d -= np.round(d / Lg) * Lg
+    assert np.abs(d).max() < 1e-9 and np.abs(cgot[..., 3:] - cref[..., 3:]).max() < 1e-9
+    from ctc_b200 import exch
+    cart = exch.Cart(dims)
+    start = np.floor((0.5 * (cells[..., :3].min(1) + cells[..., :3].max(1)) + Lg / 2) / np.array(L)).astype(int)
+    first = [cart.rank(tuple(c)) for c in start]
+    assert owner[0] != first[0] and owner[1] != first[1], (owner, first)
 
 
 def test_cart_neighbours_are_symmetric():
