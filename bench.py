@@ -66,6 +66,11 @@ CONFIGS = {
     "c2d": dict(decomposed=True, L=(96, 48, 48), dims=(2, 2, 2), bodyf=(0.01, 0.0, 0.0), steps=200,
                 name="C2 192x96x96 rho=10 (17,694,720 particles), body force 0.01 x, decomposed into 2x2x2 "
                      "subdomains of 96x48x48 with migration and halo exchange"),
+    # C3 decomposed the same way: whole cells migrate between ranks and their
+    # vertices' images cross the faces for FSI (src/distr/rbc + src/exch/obj)
+    "c3d": dict(decomposed=True, L=(32, 32, 32), dims=(2, 2, 2), rbc=200, bodyf=(0.0, 0.0, 0.0), steps=100,
+                name="C3 64x64x64 rho=10 + 200 RBC (642 vertices), decomposed into 2x2x2 subdomains of 32x32x32 "
+                     "with cell migration, vertex images and solvent migration and halo exchange"),
     "c5": dict(batch=True, nbox=512, bodyf=(0.0, 0.0, 0.0), steps=100,
                name="C5 512 periodic boxes, edges uniform in 8..24, rho=10, one RBC in every 4th box"),
 }
@@ -458,12 +463,32 @@ def run_decomposed(args, cfg, world, rank, local):
         transport = exch.DistTransport(cart, rank, group, device=dev)
         par = "%dx%dx%d cart, one subdomain per GPU (bags over NCCL)" % dims
     dpd = ctc.DpdParams(*systems.dpd_params())
+    fsi = ctc.DpdParams(0.0, systems.GAMMA, systems.dpd_params()[2], systems.SPOW)   # a = 0, gamma = 8
+    nv = 642
+    cells = {}
+    if cfg.get("rbc"):
+        # cells in the coordinates of the subdomain that holds the centre of
+        # their bounding box, with global cell ids
+        Lg = np.array(dims) * np.array(L) if world == 1 else np.array(L)
+        pv, tri, mpar = systems.rbc_system(tuple(int(x) for x in Lg), cfg["rbc"], seed=3 + rank)
+        lo = systems.box_lo(Lg)
+        rr = pv[:, :3].astype(np.float64).reshape(-1, nv, 3)
+        b = np.floor((0.5 * (rr.min(1) + rr.max(1)) - lo) / np.array(L)).astype(int)
+        for r in mine:
+            cr = np.array(cart.coords(r)) if world == 1 else np.zeros(3, int)
+            sel = np.flatnonzero((b == cr).all(1))
+            q = pv.reshape(-1, nv, 6)[sel].copy()
+            q[:, :, :3] = (q[:, :, :3].astype(np.float64) - (lo + (cr + 0.5) * np.array(L))).astype(np.float32)
+            cells[r] = (q.reshape(-1, 6), (sel + rank * cfg["rbc"]).astype(np.int32))
     subs = []
     for r in mine:
         pp = systems.solvent(L, seed=2 + r)
         n = len(pp)
         sub = exch.SubDomain(L, cart, r, int(1.05 * n) + 4096, dpd, dt=systems.DT, bodyf=cfg["bodyf"], device=dev)
         sub.set_solvent(pp, np.arange(r * n, (r + 1) * n, dtype=np.int32))
+        if cfg.get("rbc"):
+            q, cid = cells[r]
+            sub.set_membranes(q, cid, tri, nv, mpar, fsi, maxc=2 * len(cid) + 16, mass=systems.RBC_MASS)
         subs.append(sub)
     for _ in range(args.warmup):
         exch.step(subs, transport)
@@ -496,15 +521,21 @@ def run_decomposed(args, cfg, world, rank, local):
         ev = [s0] + m
         phase += [ev[k].elapsed_time(ev[k + 1]) for k in range(4)]
     phase /= 3
-    n_all = allsum(world, sum(s.count() for s in subs))
+    nvt = sum(len(s.get_membranes()[1]) * nv for s in subs) if cfg.get("rbc") else 0
+    n_all = allsum(world, sum(s.count() for s in subs) + nvt)
     ms_max = allmax(world, ms)
-    # bytes each step moves between ranks: the last step's migration and halo records
+    # bytes each step moves between ranks: the last step's migration and halo
+    # records; with membranes also the cells that migrate, the vertex images and
+    # the images' forces sent back
     moved = 0
     for s in subs:
         s.distr_pack()
+        if cfg.get("rbc"):
+            moved += 32 * nv * sum(s.mem_distr_pack()) + 48 * sum(s.mem_exch_pack())
         s.exch_pack()
         moved += 32 * (sum(s.distr_counts()) + sum(s.exch_counts()))
     moved = allsum(world, moved)
+    nvt_all = allsum(world, nvt)
     if rank != 0:
         return
     line = {
@@ -513,8 +544,9 @@ def run_decomposed(args, cfg, world, rank, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded uniform solvent, Maxwellian velocities)",
         "config": {"workload": cfg["name"] if world == 1 else
-                   "C2 192x96x96 per GPU decomposed over %d GPUs" % world,
-                   "subdomain": list(L), "dims": list(dims), "particles": int(n_all), "rng": "reference keys",
+                   "%s per GPU decomposed over %d GPUs" % (cfg["name"].split(",")[0], world),
+                   "subdomain": list(L), "dims": list(dims), "particles": int(n_all),
+                   "membrane_vertices": int(nvt_all), "rng": "reference keys",
                    "parallelism": par, "l2": "inputs larger than L2"},
         "host_ms_per_step": 1e3 * wall / args.steps,
         "phase_ms": {"migration": phase[0], "cell_lists": phase[1], "pack_bulk_halo_exchange": phase[2],

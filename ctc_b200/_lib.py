@@ -178,6 +178,7 @@ SIGNATURES = {
     "ctc_sub_bulk": (C.c_int, [vp, vp]),
     "ctc_sub_halo_update": (C.c_int, [vp, ip, vp]),
     "ctc_sub_bags": (C.c_int, [vp, C.c_int, C.POINTER(vp), C.POINTER(vp), ip]),
+    "ctc_bags_copy": (C.c_int, [C.c_int, C.POINTER(vp), C.POINTER(vp), C.POINTER(C.c_longlong), vp]),
     "ctc_sub_count": (C.c_int, [vp, ip, vp]),
     "ctc_sub_set_membranes": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int, C.POINTER(RbcParams),
                                         C.POINTER(DpdParams), C.c_float]),

@@ -264,6 +264,29 @@ __global__ void k_images_back(int total, const float4 *__restrict__ back, const 
     atomicAdd(force + __ldg(vidx + t), make_float4(f.x, f.y, f.z, 0.0f));
 }
 
+// many device-to-device copies in one launch: copy blockIdx.y, its bytes in
+// 16-byte words when both ends are 16-byte aligned, the rest byte by byte
+constexpr int BAGS_COPY_MAX = 128;
+struct BagCopies {
+    const char *src[BAGS_COPY_MAX];
+    char *dst[BAGS_COPY_MAX];
+    long long bytes[BAGS_COPY_MAX];
+};
+
+__global__ void k_bags_copy(const __grid_constant__ BagCopies B) {
+    const int k = blockIdx.y;
+    const char *src = B.src[k];
+    char *dst = B.dst[k];
+    const long long nb = B.bytes[k];
+    const bool wide = (((unsigned long long)src | (unsigned long long)dst) & 15ull) == 0;
+    const long long nw = wide ? nb / 16 : 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += stride)
+        ((int4*)dst)[i] = __ldg((const int4*)src + i);
+    for (long long i = 16 * nw + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += stride)
+        dst[i] = src[i];
+}
+
 // cells of fragment f of an L box (src/frag/imp.cpp ncell)
 static int frag_ncell(int3 L, int f) {
     return (frag_i2dx(f) == 0 ? L.x : 1) * (frag_i2dy(f) == 0 ? L.y : 1) * (frag_i2dz(f) == 0 ? L.z : 1);
@@ -1079,6 +1102,33 @@ extern "C" int ctc_sub_bags(const ctc_sub *s, int kind, void **send, void **recv
             recv[f] = s->xrfss + s->off.d[f];
             cap[f] = s->off.d[f + 1] - s->off.d[f];
         }
+    }
+    return CTC_OK;
+}
+
+// src[k] -> dst[k] (bytes[k]) for k < n, device memory of this device, on
+// stream: a transport whose ranks share a process moves its bags with one
+// launch per 128 copies instead of one copy call per bag
+extern "C" int ctc_bags_copy(int n, void *const *dst, const void *const *src, const long long *bytes,
+                             void *stream) {
+    if (n < 0 || (n > 0 && (!dst || !src || !bytes))) return fail(CTC_ERR_ARG, "ctc_bags_copy: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int k0 = 0; k0 < n; k0 += BAGS_COPY_MAX) {
+        BagCopies B;
+        const int m = std::min(BAGS_COPY_MAX, n - k0);
+        long long most = 0;
+        for (int k = 0; k < m; k++) {
+            if (bytes[k0 + k] < 0 || (bytes[k0 + k] > 0 && (!dst[k0 + k] || !src[k0 + k])))
+                return fail(CTC_ERR_ARG, "ctc_bags_copy: copy %d", k0 + k);
+            B.src[k] = (const char*)src[k0 + k];
+            B.dst[k] = (char*)dst[k0 + k];
+            B.bytes[k] = bytes[k0 + k];
+            most = std::max(most, bytes[k0 + k]);
+        }
+        if (most == 0) continue;
+        const int bx = (int)std::min<long long>(64, (most + 16 * 256 - 1) / (16 * 256));
+        k_bags_copy<<<dim3(bx, m), 256, 0, st>>>(B);
+        CUDA_TRY(cudaGetLastError());
     }
     return CTC_OK;
 }

@@ -136,6 +136,15 @@ class SubDomain:
                 self._fss = ([sb[roff[f]:roff[f + 1]] for f in range(26)],
                              [rb[roff[f]:roff[f + 1]] for f in range(26)], cap)
             self._base.append((sb, [rb[roff[f]:roff[f + 1]] for f in range(26)], cap))
+        # the same bags as device addresses (bag_ptrs): send buffer start,
+        # receive bag addresses, capacities, bytes per counted unit
+        self._ptrs = {}
+        for kind in range(3):
+            sb, recv, cap = self._base[kind]
+            unit = 4 if kind == 2 else 4 * self.REC
+            rp = [r.data_ptr() for r in recv]
+            sp = [b.data_ptr() for b in self._fss[0]] if kind == 2 else sb.data_ptr()
+            self._ptrs[kind] = (sp, rp, list(cap), unit)
 
     def close(self):
         if getattr(self, "h", None) and self.h.value and _lib._lib is not None:
@@ -200,6 +209,8 @@ class SubDomain:
             stot = el * self.maxc if kind == 3 else tot
             self._mbase[kind] = (_view(send[0], stot, torch.float32, self.device),
                                  _view(recv[0], tot, torch.float32, self.device), cap, el)
+            rp = [recv[0] + 4 * el * cap[0] * f for f in range(26)] if kind != 5 else recv[0]
+            self._ptrs[kind] = (send[0], rp, cap, 4 * el)
 
     def membrane_forces(self):
         """The last step's vertex forces (nc*nv, 3) and their global vertex ids [host]."""
@@ -298,6 +309,28 @@ class SubDomain:
             o = e
         return send, recv, cap
 
+    def bag_ptrs(self, kind, counts, rcounts=None):
+        """The bags of bags() (kinds 0-2) and mem_bags() (kinds 3-5) as device
+        addresses, for a transport whose ranks share a process: (send
+        addresses, the units each sends, receive addresses, their capacities
+        in units, bytes per unit).  Kind 2 sends its fixed bags whole; kind 5
+        sends rcounts[j] forces from bag j and receives counts[f] into bag f."""
+        sp, rp, cap, unit = self._ptrs[kind]
+        if kind == 2:
+            return sp, cap, rp, cap, unit
+        sent = rcounts if kind == 5 else counts
+        send, o = [], sp
+        for f in range(26):
+            send.append(o)
+            o += unit * sent[f]
+        if kind == 5:
+            recv, o = [], rp
+            for f in range(26):
+                recv.append(o)
+                o += unit * counts[f]
+            return send, sent, recv, counts, unit
+        return send, sent, rp, cap, unit
+
     # -- the phases of a step ------------------------------------------------
     def distr_pack(self):
         check(lib().ctc_sub_distr_pack(self.h, self._stream()))
@@ -336,26 +369,69 @@ class LocalTransport:
 
     def __init__(self, cart):
         self.cart = cart
+        self.nbr = [cart.neighbours(r) for r in range(cart.size)]
+        self.anti = [frag_anti(f) for f in range(26)]
 
     def exchange_counts(self, counts):
         """counts[r][f] sent by rank r in direction f -> received [r][j]."""
         out = [[0] * 26 for _ in counts]
+        anti = self.anti
         for r, c in enumerate(counts):
-            nbr = self.cart.neighbours(r)
+            nbr = self.nbr[r]
             for f in range(26):
-                out[nbr[f]][frag_anti(f)] = c[f]
+                out[nbr[f]][anti[f]] = c[f]
         return out
 
+    def exchange_ptrs(self, bags, stream):
+        """bags[r] = SubDomain.bag_ptrs(...) of rank r: every send bag copied
+        into its receive bag with one launch (ctc_bags_copy) on stream."""
+        src, dst, nbytes = [], [], []
+        anti = self.anti
+        for r, (sp, sent, _, _, unit) in enumerate(bags):
+            nbr = self.nbr[r]
+            for f in range(26):
+                if sent[f]:
+                    q, j = nbr[f], anti[f]
+                    if sent[f] > bags[q][3][j]:
+                        raise ValueError("bag %d of rank %d: %d units into %d" % (f, r, sent[f], bags[q][3][j]))
+                    src.append(sp[f])
+                    dst.append(bags[q][2][j])
+                    nbytes.append(sent[f] * unit)
+        if src:
+            k = len(src)
+            check(lib().ctc_bags_copy(k, (C.c_void_p * k)(*dst), (C.c_void_p * k)(*src),
+                                      (C.c_longlong * k)(*nbytes), stream))
+        return _Done()
+
     def exchange(self, sends, recvs, rcounts, rec):
-        """sends[r][f] (sized), recvs[r][j] (capacity) device tensors; rcounts[r][j]
-        the elements / rec received in bag j of rank r.  The copies are
-        enqueued on the current stream; the handle's wait() is a no-op."""
+        """sends[r][f] (sized), recvs[r][j] (capacity) tensors; rcounts[r][j]
+        the elements / rec received in bag j of rank r.  Device bags move in
+        one launch (ctc_bags_copy) on the current stream; the handle's wait()
+        is a no-op."""
+        src, dst, nbytes = [], [], []
+        dev = None
         for r, s in enumerate(sends):
             nbr = self.cart.neighbours(r)
             for f in range(26):
                 n = s[f].numel()
-                if n:
-                    recvs[nbr[f]][frag_anti(f)][:n].copy_(s[f])
+                if not n:
+                    continue
+                d = recvs[nbr[f]][frag_anti(f)]
+                if n > d.numel() or d.dtype != s[f].dtype:
+                    raise ValueError("bag %d of rank %d: %d elements into %d" % (f, r, n, d.numel()))
+                if s[f].is_cuda:
+                    dev = s[f].device
+                    src.append(s[f].data_ptr())
+                    dst.append(d.data_ptr())
+                    nbytes.append(n * s[f].element_size())
+                else:
+                    d[:n].copy_(s[f])
+        if src:
+            import torch
+            k = len(src)
+            check(lib().ctc_bags_copy(k, (C.c_void_p * k)(*dst), (C.c_void_p * k)(*src),
+                                      (C.c_longlong * k)(*nbytes),
+                                      C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
         return _Done()
 
 
@@ -448,17 +524,37 @@ def step(subs, transport, marks=None):
             marks.append(e)
     R = SubDomain.REC
     mem = bool(getattr(subs[0], "mnv", 0))
+    direct = hasattr(transport, "exchange_ptrs")    # ranks of one process: bags by address
+
+    def move(kind, counts, rcounts, rec, back=None):
+        """Bags of one kind from every rank to its neighbours; counts the send
+        sizes (kind 5: the forces go back for the images rcounts came from)."""
+        if direct:
+            if kind == 5:
+                ptrs = [s.bag_ptrs(5, c, b) for s, c, b in zip(subs, counts, back)]
+            elif kind == 2:
+                ptrs = [s.bag_ptrs(2, None) for s in subs]
+            else:
+                ptrs = [s.bag_ptrs(kind, c) for s, c in zip(subs, counts)]
+            return transport.exchange_ptrs(ptrs, subs[0]._stream())
+        if kind == 2:
+            bags = [s.bags(2, None) for s in subs]
+            return transport.exchange([b[0] for b in bags], [b[1] for b in bags], [b[2] for b in bags], rec)
+        if kind == 5:
+            bags = [s.mem_bags(5, c, b) for s, c, b in zip(subs, counts, back)]
+        else:
+            bags = [(s.bags if kind < 3 else s.mem_bags)(kind, c) for s, c in zip(subs, counts)]
+        return transport.exchange([b[0] for b in bags], [b[1] for b in bags], rcounts, rec)
+
     for s in subs:
         s.distr_pack()
     counts = [s.distr_counts() for s in subs]
     rcounts = transport.exchange_counts(counts)
-    bags = [s.bags(0, c) for s, c in zip(subs, counts)]
-    transport.exchange([b[0] for b in bags], [b[1] for b in bags], rcounts, R).wait()
+    move(0, counts, rcounts, R).wait()
     if mem:     # whole cells migrate beside the solvent (distr_rbc)
         ccounts = [s.mem_distr_pack() for s in subs]
         crc = transport.exchange_counts(ccounts)
-        cb = [s.mem_bags(3, c) for s, c in zip(subs, ccounts)]
-        transport.exchange([b[0] for b in cb], [b[1] for b in cb], crc, R * subs[0].mnv).wait()
+        move(3, ccounts, crc, R * subs[0].mnv).wait()
         for s, rc in zip(subs, crc):
             s.mem_distr_unpack(rc)
     mark()
@@ -473,22 +569,18 @@ def step(subs, transport, marks=None):
         s.bulk()
     counts = [s.exch_counts() for s in subs]
     rcounts = transport.exchange_counts(counts)
-    bags = [s.bags(1, c) for s, c in zip(subs, counts)]
-    fss = [s.bags(2, None) for s in subs]
-    h1 = transport.exchange([b[0] for b in bags], [b[1] for b in bags], rcounts, R)
-    h2 = transport.exchange([b[0] for b in fss], [b[1] for b in fss], [b[2] for b in fss], 1)
+    h1 = move(1, counts, rcounts, R)
+    h2 = move(2, None, None, 1)
     if mem:     # the vertices' images for the neighbours' FSI (exch_obj)
         icounts = [s.mem_exch_pack() for s in subs]
         irc = transport.exchange_counts(icounts)
-        ib = [s.mem_bags(4, c) for s, c in zip(subs, icounts)]
-        transport.exchange([b[0] for b in ib], [b[1] for b in ib], irc, R).wait()
+        move(4, icounts, irc, R).wait()
     h1.wait()
     h2.wait()
     if mem:     # FSI of the own vertices and of the images; the images' forces go back
         for s, rc in zip(subs, irc):
             s.mem_fsi(rc)
-        fb = [s.mem_bags(5, c, rc) for s, c, rc in zip(subs, icounts, irc)]
-        transport.exchange([b[0] for b in fb], [b[1] for b in fb], icounts, 4).wait()
+        move(5, icounts, icounts, 4, back=irc).wait()
     mark()
     for s, rc in zip(subs, rcounts):
         s.halo_update(rc)

@@ -532,6 +532,10 @@ int ctc_sub_halo_update(ctc_sub *s, const int *rcounts, void *stream);
  * send[f] the last pack's bag for direction f, recv[f] where the bag from
  * direction f goes, cap[f] its capacity in elements (cells for kind 3) */
 int ctc_sub_bags(const ctc_sub *s, int kind, void **send, void **recv, int *cap);
+/* src[k] -> dst[k], bytes[k] bytes, for k < n [host arrays of device
+ * addresses of this device], enqueued on stream as one launch per 128 copies:
+ * the bags of ranks that share a process (exch.LocalTransport) */
+int ctc_bags_copy(int n, void *const *dst, const void *const *src, const long long *bytes, void *stream);
 /* membranes in the subdomain (src/distr/rbc, src/exch/obj, src/fsi halo):
  * nc cells of one template (nv, nt, tri [host]), their vertices pp [host,
  * AoS, subdomain coordinates] and global cell ids [host, nc] (a vertex's id,
