@@ -531,7 +531,9 @@ def run_decomposed(args, cfg, world, rank, local):
     for s in subs:
         s.distr_pack()
         if cfg.get("rbc"):
-            moved += 32 * nv * sum(s.mem_distr_pack()) + 48 * sum(s.mem_exch_pack())
+            s.mem_distr_pack()
+            s.mem_exch_pack()
+            moved += 32 * nv * sum(s.mem_distr_counts()) + 48 * sum(s.mem_exch_counts())
         s.exch_pack()
         moved += 32 * (sum(s.distr_counts()) + sum(s.exch_counts()))
     moved = allsum(world, moved)

@@ -182,9 +182,11 @@ SIGNATURES = {
     "ctc_sub_count": (C.c_int, [vp, ip, vp]),
     "ctc_sub_set_membranes": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, C.c_int, C.POINTER(RbcParams),
                                         C.POINTER(DpdParams), C.c_float]),
-    "ctc_sub_mem_distr_pack": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_mem_distr_pack": (C.c_int, [vp, vp]),
+    "ctc_sub_mem_distr_counts": (C.c_int, [vp, ip]),
     "ctc_sub_mem_distr_unpack": (C.c_int, [vp, ip, vp]),
-    "ctc_sub_mem_exch_pack": (C.c_int, [vp, ip, vp]),
+    "ctc_sub_mem_exch_pack": (C.c_int, [vp, vp]),
+    "ctc_sub_mem_exch_counts": (C.c_int, [vp, ip]),
     "ctc_sub_mem_fsi": (C.c_int, [vp, ip, vp]),
     "ctc_sub_mem_update": (C.c_int, [vp, vp]),
     "ctc_sub_get_membranes": (C.c_int, [vp, ip, ip, vp, vp, vp]),

@@ -191,14 +191,14 @@ __global__ void k_cell_bins(int nv, int3 L, const float4 *__restrict__ pos, int 
     }
 }
 
-// whole cells: cell src[k] of the input into slot dst0 + k of the output,
-// every vertex moved by `shift`; in/out either SoA (pos, vel) or records of
-// two float4 (recs_in / recs_out)
+// whole cells: cell src[k] (src null: cell k) of the input into slot dst0 + k
+// of the output, every vertex moved by `shift`; in/out either SoA (pos, vel)
+// or records of two float4 (recs_in / recs_out)
 __global__ void k_cells_copy(int nv, const int *__restrict__ src, int dst0, const float4 *__restrict__ pin,
                              const float4 *__restrict__ vin, int recs_in, float4 *__restrict__ pout,
                              float4 *__restrict__ vout, int recs_out, float3 shift) {
     const int c = blockIdx.y;
-    const int s = __ldg(src + c);
+    const int s = src ? __ldg(src + c) : c;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
         const size_t i = (size_t)s * nv + v, o = (size_t)(dst0 + c) * nv + v;
         float4 p = __ldg(recs_in ? pin + 2 * i : pin + i);
@@ -214,10 +214,69 @@ __global__ void k_cells_copy(int nv, const int *__restrict__ src, int dst0, cons
     }
 }
 
+// the pack order of the cells: the leaving ones by fragment, then the staying
+// ones (bin 26), each group by cell index; count[27] the cells per bin.  One
+// block: bins counted in shared memory, then one warp places 32 cells at a
+// time, ranked within their bin by a match over the warp
+__global__ void k_cells_order(int nc, const int *__restrict__ bins, int *__restrict__ order,
+                              int *__restrict__ count) {
+    __shared__ int cnt[27], off[27];
+    if (threadIdx.x < 27) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) atomicAdd(&cnt[__ldg(bins + c)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int o = 0;
+        for (int b = 0; b < 27; b++) {
+            off[b] = o;
+            o += cnt[b];
+            count[b] = cnt[b];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+        const int c = c0 + lane;
+        const int b = c < nc ? __ldg(bins + c) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, b);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        if (b >= 0) order[off[b] + rank] = c;
+        __syncwarp();
+        if (b >= 0 && rank == 0) off[b] += __popc(peers);
+        __syncwarp();
+    }
+}
+
+// the cells in pack order (k_cells_order): the first nc - count[26] into the
+// cell bags (records, slot k), the rest into the staying state (slot k -
+// leaving)
+__global__ void k_cells_split(int nv, int nc, const int *__restrict__ order, const int *__restrict__ count,
+                              const float4 *__restrict__ pin, const float4 *__restrict__ vin,
+                              float4 *__restrict__ bags, float4 *__restrict__ pout, float4 *__restrict__ vout) {
+    const int k = blockIdx.y;
+    const int nleave = nc - __ldg(count + 26);
+    const int c = __ldg(order + k);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+        const size_t i = (size_t)c * nv + v;
+        const float4 p = __ldg(pin + i), u = __ldg(vin + i);
+        if (k < nleave) {
+            const size_t o = (size_t)k * nv + v;
+            bags[2 * o] = p;
+            bags[2 * o + 1] = u;
+        } else {
+            const size_t o = (size_t)(k - nleave) * nv + v;
+            pout[o] = p;
+            vout[o] = u;
+        }
+    }
+}
+
 // the vertices' images into the 26 image bags (vertex i, for fragment f of
-// its mask, at its rank there), with the vertex index beside each image
+// its mask, at its rank there; the bags follow one another by the prefix of
+// count[26]), with the vertex index beside each image
 __global__ void k_images_pack(int nv, const unsigned *__restrict__ mask, const int *__restrict__ rank,
-                              const int *__restrict__ boff, const float4 *__restrict__ pos,
+                              const int *__restrict__ count, const float4 *__restrict__ pos,
                               const float4 *__restrict__ vel, float4 *__restrict__ bags, int *__restrict__ vidx,
                               int cap_total, int *err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -225,9 +284,12 @@ __global__ void k_images_pack(int nv, const unsigned *__restrict__ mask, const i
     const unsigned m = __ldg(mask + i);
     if (!m) return;
     const float4 p = __ldg(pos + i), u = __ldg(vel + i);
+    int boff = 0;
     for (int f = 0; f < 26; f++) {
-        if (!((m >> f) & 1u)) continue;
-        const int t = __ldg(boff + f) + __ldg(rank + (size_t)f * nv + i);
+        const int nf = __ldg(count + f);
+        if (!((m >> f) & 1u)) { boff += nf; continue; }
+        const int t = boff + __ldg(rank + (size_t)f * nv + i);
+        boff += nf;
         if (t < 0 || t >= cap_total) { set_error(err, DEV_CELL_OVERFLOW); continue; }
         bags[2 * (size_t)t] = p;
         bags[2 * (size_t)t + 1] = u;
@@ -347,10 +409,13 @@ struct ctc_sub {
     float4 *csend, *crecv;                   // cell bags (kind 3): records, ccap cells per direction
     int csend_off[27];                       // host offsets (cells) of the last pack's bags
     int mstay;                               // cells that stayed
+    int *ccount_dev, *ccount_host;           // cells per bin of the last pack (27; host: pinned)
+    int *ecount_host;                        // images per bag of the last pack (26, pinned)
+    cudaEvent_t ev_cells, ev_images;         // the last packs' counts are on the host
     // vertex images (kind 4) and the forces sent back for them (kind 5)
     unsigned *emask;
     int *erank, *ecount, *eimg;              // fsi_images_launch's buffers
-    int *eoff_dev, *eoff_host;               // image bag offsets of the last pack (27)
+    int *eoff_host;                          // image bag offsets of the last pack (27, pinned)
     int icap;                                // images per bag
     float4 *isend, *irecv, *ipos, *ivel, *iforce, *iback;
     int *ividx;
@@ -385,9 +450,12 @@ extern "C" int ctc_sub_destroy(ctc_sub *s) {
     cudaFree(s->mforce); cudaFree(s->mcount);
     if (s->rbc) ctc_rbc_force_fin(s->rbc);
     cudaFree(s->cbins_dev); cudaFreeHost(s->cbins_host); cudaFree(s->cidx_dev);
+    cudaFree(s->ccount_dev); cudaFreeHost(s->ccount_host); cudaFreeHost(s->ecount_host);
+    for (cudaEvent_t e : {s->ev_cells, s->ev_images})
+        if (e) cudaEventDestroy(e);
     cudaFree(s->csend); cudaFree(s->crecv);
     cudaFree(s->emask); cudaFree(s->erank); cudaFree(s->ecount); cudaFree(s->eimg);
-    cudaFree(s->eoff_dev); cudaFreeHost(s->eoff_host);
+    cudaFreeHost(s->eoff_host);
     cudaFree(s->isend); cudaFree(s->irecv); cudaFree(s->ipos); cudaFree(s->ivel); cudaFree(s->iforce);
     cudaFree(s->iback); cudaFree(s->ividx);
     delete s;
@@ -772,8 +840,14 @@ extern "C" int ctc_sub_set_membranes(ctc_sub *s, int nc, int nv, int nt, const i
     CUDA_TRY(cudaMalloc(&s->erank, sizeof(int) * 26 * nvmax));
     CUDA_TRY(cudaMalloc(&s->ecount, sizeof(int) * fsi_count_ints((int)nvmax, 0)));
     CUDA_TRY(cudaMalloc(&s->eimg, sizeof(int) * 26));
-    CUDA_TRY(cudaMalloc(&s->eoff_dev, sizeof(int) * 27));
     CUDA_TRY(cudaMallocHost(&s->eoff_host, sizeof(int) * 27));
+    CUDA_TRY(cudaMalloc(&s->ccount_dev, sizeof(int) * 27));
+    CUDA_TRY(cudaMallocHost(&s->ccount_host, sizeof(int) * 27));
+    CUDA_TRY(cudaMallocHost(&s->ecount_host, sizeof(int) * 26));
+    memset(s->ccount_host, 0, sizeof(int) * 27);
+    memset(s->ecount_host, 0, sizeof(int) * 26);
+    if (!s->ev_cells) CUDA_TRY(cudaEventCreateWithFlags(&s->ev_cells, cudaEventDisableTiming));
+    if (!s->ev_images) CUDA_TRY(cudaEventCreateWithFlags(&s->ev_images, cudaEventDisableTiming));
     s->icap = (int)nvmax;
     const size_t itot = (size_t)26 * s->icap;
     CUDA_TRY(cudaMalloc(&s->isend, 2 * sizeof(float4) * itot));
@@ -783,7 +857,6 @@ extern "C" int ctc_sub_set_membranes(ctc_sub *s, int nc, int nv, int nt, const i
     CUDA_TRY(cudaMalloc(&s->iforce, sizeof(float4) * itot));
     CUDA_TRY(cudaMalloc(&s->iback, sizeof(float4) * itot));
     CUDA_TRY(cudaMalloc(&s->ividx, sizeof(int) * itot));
-    CUDA_TRY(cudaMemset(s->eoff_dev, 0, sizeof(int) * 27));
     memset(s->eoff_host, 0, sizeof(int) * 27);
     // fsi_ini of this rank (src/fsi/imp/main.h:7); the stable keys draw from
     // rank 0's trunk on every rank, so that a pair's key does not depend on
@@ -825,47 +898,47 @@ extern "C" int ctc_sub_set_membranes(ctc_sub *s, int nc, int nv, int nt, const i
 }
 
 // distr_rbc (src/distr/rbc/imp): the cells whose bounding-box centre left the
-// subdomain into the 26 cell bags (kind 3, nv records each, in cell order),
-// the others kept in order; counts [host, 26] in cells.  Synchronises.
-extern "C" int ctc_sub_mem_distr_pack(ctc_sub *s, int *counts, void *stream) {
-    if (!s || !counts) return fail(CTC_ERR_ARG, "ctc_sub_mem_distr_pack: bad arguments");
-    for (int f = 0; f < 26; f++) counts[f] = 0;
-    for (int f = 0; f < 27; f++) s->csend_off[f] = 0;
-    s->mstay = s->mnc;
-    if (s->mnc == 0) return CTC_OK;
+// subdomain into the 26 cell bags (kind 3, nv records each, by fragment and
+// then by cell index), the others kept in order -- all on the device; the
+// counts follow to the host (ctc_sub_mem_distr_counts)
+extern "C" int ctc_sub_mem_distr_pack(ctc_sub *s, void *stream) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sub_mem_distr_pack: bad arguments");
+    if (!s->mnv) return CTC_OK;
     cudaStream_t st = (cudaStream_t)stream;
     const int nv = s->mnv, nc = s->mnc;
-    k_cell_bins<<<nc, 256, 0, st>>>(nv, s->L, s->mpos[0], s->cbins_dev);
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaMemcpyAsync(s->cbins_host, s->cbins_dev, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<int> order, stay;
-    for (int f = 0; f < 26; f++) {
-        s->csend_off[f] = (int)order.size();
-        for (int c = 0; c < nc; c++)
-            if (s->cbins_host[c] == f) order.push_back(c);
-        counts[f] = (int)order.size() - s->csend_off[f];
-        if (counts[f] > s->ccap)
-            return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_distr_pack: fragment %d: %d cells leaving > capacity %d", f,
-                        counts[f], s->ccap);
+    if (nc > 0) {
+        k_cell_bins<<<nc, 256, 0, st>>>(nv, s->L, s->mpos[0], s->cbins_dev);
+        k_cells_order<<<1, 256, 0, st>>>(nc, s->cbins_dev, s->cidx_dev, s->ccount_dev);
+        k_cells_split<<<dim3(ceil_div(nv, 256), nc), 256, 0, st>>>(nv, nc, s->cidx_dev, s->ccount_dev, s->mpos[0],
+                                                                   s->mvel[0], s->csend, s->mpos[1], s->mvel[1]);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(s->ccount_host, s->ccount_dev, sizeof(int) * 27, cudaMemcpyDeviceToHost, st));
+    } else {
+        memset(s->ccount_host, 0, sizeof(int) * 27);
     }
-    s->csend_off[26] = (int)order.size();
-    for (int c = 0; c < nc; c++)
-        if (s->cbins_host[c] == 26) stay.push_back(c);
-    const int nleave = (int)order.size(), nstay = (int)stay.size();
-    order.insert(order.end(), stay.begin(), stay.end());
-    CUDA_TRY(cudaMemcpyAsync(s->cidx_dev, order.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
-    if (nleave > 0)
-        k_cells_copy<<<dim3(ceil_div(nv, 256), nleave), 256, 0, st>>>(nv, s->cidx_dev, 0, s->mpos[0], s->mvel[0], 0,
-                                                                      s->csend, nullptr, 1, make_float3(0, 0, 0));
-    if (nstay > 0)
-        k_cells_copy<<<dim3(ceil_div(nv, 256), nstay), 256, 0, st>>>(nv, s->cidx_dev + nleave, 0, s->mpos[0],
-                                                                     s->mvel[0], 0, s->mpos[1], s->mvel[1], 0,
-                                                                     make_float3(0, 0, 0));
-    CUDA_TRY(cudaGetLastError());
-    // the order array must stay until the copies have read it
-    CUDA_TRY(cudaStreamSynchronize(st));
-    s->mstay = nstay;
+    CUDA_TRY(cudaEventRecord(s->ev_cells, st));
+    return CTC_OK;
+}
+
+// the last cell pack's counts [host, 26] in cells; waits for that pack only
+extern "C" int ctc_sub_mem_distr_counts(ctc_sub *s, int *counts) {
+    if (!s || !counts) return fail(CTC_ERR_ARG, "ctc_sub_mem_distr_counts: bad arguments");
+    for (int f = 0; f < 26; f++) counts[f] = 0;
+    for (int f = 0; f < 27; f++) s->csend_off[f] = 0;
+    s->mstay = 0;
+    if (!s->mnv) return CTC_OK;
+    CUDA_TRY(cudaEventSynchronize(s->ev_cells));
+    int o = 0;
+    for (int f = 0; f < 26; f++) {
+        counts[f] = s->ccount_host[f];
+        if (counts[f] > s->ccap)
+            return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_distr_counts: fragment %d: %d cells leaving > capacity %d", f,
+                        counts[f], s->ccap);
+        s->csend_off[f] = o;
+        o += counts[f];
+    }
+    s->csend_off[26] = o;
+    s->mstay = s->ccount_host[26];
     return CTC_OK;
 }
 
@@ -884,22 +957,16 @@ extern "C" int ctc_sub_mem_distr_unpack(ctc_sub *s, const int *rcounts, void *st
         total += rcounts[j];
     }
     if (total > s->maxc) return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_distr_unpack: %ld cells > %d", total, s->maxc);
-    std::vector<int> idx(std::max(1, s->ccap));
-    for (int k = 0; k < (int)idx.size(); k++) idx[k] = k;
-    CUDA_TRY(cudaMemcpyAsync(s->cidx_dev + s->maxc, idx.data(), sizeof(int) * std::min(s->ccap, s->maxc),
-                             cudaMemcpyHostToDevice, st));
     int at = s->mstay;
     for (int j = 0; j < 26; j++) {
         if (rcounts[j] == 0) continue;
         const float3 sh = make_float3((float)(frag_i2dx(j) * s->L.x), (float)(frag_i2dy(j) * s->L.y),
                                       (float)(frag_i2dz(j) * s->L.z));
         k_cells_copy<<<dim3(ceil_div(nv, 256), rcounts[j]), 256, 0, st>>>(
-            nv, s->cidx_dev + s->maxc, at, s->crecv + 2 * (size_t)j * s->ccap * nv, nullptr, 1, s->mpos[1],
-            s->mvel[1], 0, sh);
+            nv, nullptr, at, s->crecv + 2 * (size_t)j * s->ccap * nv, nullptr, 1, s->mpos[1], s->mvel[1], 0, sh);
         CUDA_TRY(cudaGetLastError());
         at += rcounts[j];
     }
-    CUDA_TRY(cudaStreamSynchronize(st));   // the index array is a host vector
     std::swap(s->mpos[0], s->mpos[1]);
     std::swap(s->mvel[0], s->mvel[1]);
     s->mnc = at;
@@ -910,32 +977,46 @@ extern "C" int ctc_sub_mem_distr_unpack(ctc_sub *s, const int *rcounts, void *st
 }
 
 // exch_obj's map and pack (src/exch/obj/imp/{map,pack}.h): every vertex
-// within 1 of a face (or beyond it) into the image bag of each fragment it
-// must reach (kind 4, ascending vertex order); counts [host, 26].  Synchronises.
-extern "C" int ctc_sub_mem_exch_pack(ctc_sub *s, int *counts, void *stream) {
-    if (!s || !counts) return fail(CTC_ERR_ARG, "ctc_sub_mem_exch_pack: bad arguments");
+// within 1 of a face, or beyond it, into the image bag of each fragment of
+// those faces (kind 4: the periodic box's image masks, fsi_images_launch; a
+// bag in ascending vertex order, the bags one after another by fragment) --
+// on the device; the counts follow (ctc_sub_mem_exch_counts)
+extern "C" int ctc_sub_mem_exch_pack(ctc_sub *s, void *stream) {
+    if (!s) return fail(CTC_ERR_ARG, "ctc_sub_mem_exch_pack: bad arguments");
+    if (!s->mnv) return CTC_OK;
+    const int nvt = s->mnc * s->mnv;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (nvt > 0) {
+        CUDA_TRY(fsi_images_launch(nvt, s->L, (const float*)s->mpos[0], 4, s->emask, s->erank, s->ecount, s->eimg,
+                                   st));
+        k_images_pack<<<ceil_div(nvt, 256), 256, 0, st>>>(nvt, s->emask, s->erank, s->ecount, s->mpos[0],
+                                                           s->mvel[0], s->isend, s->ividx, 26 * s->icap,
+                                                           dev_err_ptr());
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(s->ecount_host, s->ecount, sizeof(int) * 26, cudaMemcpyDeviceToHost, st));
+    } else {
+        memset(s->ecount_host, 0, sizeof(int) * 26);
+    }
+    CUDA_TRY(cudaEventRecord(s->ev_images, st));
+    return CTC_OK;
+}
+
+// the last image pack's counts [host, 26]; waits for that pack only
+extern "C" int ctc_sub_mem_exch_counts(ctc_sub *s, int *counts) {
+    if (!s || !counts) return fail(CTC_ERR_ARG, "ctc_sub_mem_exch_counts: bad arguments");
     for (int f = 0; f < 26; f++) counts[f] = 0;
     memset(s->eoff_host, 0, sizeof(int) * 27);
-    const int nvt = s->mnc * s->mnv;
-    if (nvt == 0) return CTC_OK;
-    cudaStream_t st = (cudaStream_t)stream;
-    CUDA_TRY(fsi_images_launch(nvt, s->L, (const float*)s->mpos[0], 4, s->emask, s->erank, s->ecount, s->eimg, st));
-    CUDA_TRY(cudaMemcpyAsync(s->eoff_host, s->ecount, sizeof(int) * 26, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    if (!s->mnv) return CTC_OK;
+    CUDA_TRY(cudaEventSynchronize(s->ev_images));
     int o = 0;
     for (int f = 0; f < 26; f++) {
-        const int c = s->eoff_host[f];
-        if (c > s->icap) return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_exch_pack: fragment %d: %d images", f, c);
+        const int c = s->ecount_host[f];
+        if (c > s->icap) return fail(CTC_ERR_CAPACITY, "ctc_sub_mem_exch_counts: fragment %d: %d images", f, c);
         counts[f] = c;
         s->eoff_host[f] = o;
         o += c;
     }
     s->eoff_host[26] = o;
-    CUDA_TRY(cudaMemcpyAsync(s->eoff_dev, s->eoff_host, sizeof(int) * 27, cudaMemcpyHostToDevice, st));
-    k_images_pack<<<ceil_div(nvt, 256), 256, 0, st>>>(nvt, s->emask, s->erank, s->eoff_dev, s->mpos[0], s->mvel[0],
-                                                       s->isend, s->ividx, 26 * s->icap, dev_err_ptr());
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaStreamSynchronize(st));    // eoff_host is read by the transport's views
     return CTC_OK;
 }
 

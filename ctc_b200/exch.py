@@ -264,16 +264,22 @@ class SubDomain:
         return send, recv, cap
 
     def mem_distr_pack(self):
+        check(lib().ctc_sub_mem_distr_pack(self.h, self._stream()))
+
+    def mem_distr_counts(self):
         c = (C.c_int * 26)()
-        check(lib().ctc_sub_mem_distr_pack(self.h, c, self._stream()))
+        check(lib().ctc_sub_mem_distr_counts(self.h, c))
         return list(c)
 
     def mem_distr_unpack(self, rcounts):
         check(lib().ctc_sub_mem_distr_unpack(self.h, (C.c_int * 26)(*rcounts), self._stream()))
 
     def mem_exch_pack(self):
+        check(lib().ctc_sub_mem_exch_pack(self.h, self._stream()))
+
+    def mem_exch_counts(self):
         c = (C.c_int * 26)()
-        check(lib().ctc_sub_mem_exch_pack(self.h, c, self._stream()))
+        check(lib().ctc_sub_mem_exch_counts(self.h, c))
         return list(c)
 
     def mem_fsi(self, rcounts):
@@ -548,11 +554,13 @@ def step(subs, transport, marks=None):
 
     for s in subs:
         s.distr_pack()
+        if mem:     # whole cells migrate beside the solvent (distr_rbc)
+            s.mem_distr_pack()
     counts = [s.distr_counts() for s in subs]
     rcounts = transport.exchange_counts(counts)
     move(0, counts, rcounts, R).wait()
-    if mem:     # whole cells migrate beside the solvent (distr_rbc)
-        ccounts = [s.mem_distr_pack() for s in subs]
+    if mem:
+        ccounts = [s.mem_distr_counts() for s in subs]
         crc = transport.exchange_counts(ccounts)
         move(3, ccounts, crc, R * subs[0].mnv).wait()
         for s, rc in zip(subs, crc):
@@ -563,6 +571,8 @@ def step(subs, transport, marks=None):
     mark()
     for s in subs:
         s.exch_pack()
+        if mem:     # the vertices' images for the neighbours' FSI (exch_obj)
+            s.mem_exch_pack()
     # the bulk forces run on each subdomain's own stream while the host
     # collects the halo counts and the halo bags travel
     for s in subs:
@@ -571,8 +581,8 @@ def step(subs, transport, marks=None):
     rcounts = transport.exchange_counts(counts)
     h1 = move(1, counts, rcounts, R)
     h2 = move(2, None, None, 1)
-    if mem:     # the vertices' images for the neighbours' FSI (exch_obj)
-        icounts = [s.mem_exch_pack() for s in subs]
+    if mem:
+        icounts = [s.mem_exch_counts() for s in subs]
         irc = transport.exchange_counts(icounts)
         move(4, icounts, irc, R).wait()
     h1.wait()

@@ -541,20 +541,25 @@ int ctc_bags_copy(int n, void *const *dst, const void *const *src, const long lo
  * AoS, subdomain coordinates] and global cell ids [host, nc] (a vertex's id,
  * the stable keys' id, is cell id * nv + vertex), room for maxc cells; p, fsi
  * and mass as ctc_sim_set_membranes.  A step with membranes adds, in order:
- * mem_distr_pack + exchange kind 3 + mem_distr_unpack beside the solvent's
- * migration; mem_exch_pack + exchange kind 4 beside the halo exchange;
+ * mem_distr_pack + mem_distr_counts + exchange kind 3 + mem_distr_unpack
+ * beside the solvent's migration; mem_exch_pack + mem_exch_counts + exchange
+ * kind 4 beside the halo exchange;
  * mem_fsi after ctc_sub_bulk; exchange kind 5; mem_update after
  * ctc_sub_halo_update.  Contact and walls are not in the subdomain step. */
 int ctc_sub_set_membranes(ctc_sub *s, int nc, int nv, int nt, const int *tri, const float *pp, const int *cell_ids,
                           int maxc, const ctc_rbc_params *p, const ctc_dpd_params *fsi, float mass);
-/* the cells whose bounding-box centre left into the cell bags; counts [host,
- * 26] in cells; synchronises */
-int ctc_sub_mem_distr_pack(ctc_sub *s, int *counts, void *stream);
+/* the cells whose bounding-box centre left into the cell bags (on the
+ * device, enqueued on stream) */
+int ctc_sub_mem_distr_pack(ctc_sub *s, void *stream);
+/* the last cell pack's counts [host, 26] in cells (waits for that pack) */
+int ctc_sub_mem_distr_counts(ctc_sub *s, int *counts);
 /* the received cells (rcounts [host, 26]) moved in and appended */
 int ctc_sub_mem_distr_unpack(ctc_sub *s, const int *rcounts, void *stream);
-/* the vertices within 1 of a face into the image bags; counts [host, 26];
- * synchronises */
-int ctc_sub_mem_exch_pack(ctc_sub *s, int *counts, void *stream);
+/* the vertices within 1 of a face into the image bags (on the device,
+ * enqueued on stream) */
+int ctc_sub_mem_exch_pack(ctc_sub *s, void *stream);
+/* the last image pack's counts [host, 26] (waits for that pack) */
+int ctc_sub_mem_exch_counts(ctc_sub *s, int *counts);
 /* FSI of the local vertices and of the received images (rcounts [host, 26])
  * against the local solvent: reactions into the solvent forces, the images'
  * forces into the back bags */

@@ -234,6 +234,12 @@ class NumpySubCells(NumpySub):
         self.caps = {3: ccap, 4: icap, 5: icap}
 
     def mem_distr_pack(self):
+        self._cc = self._mem_distr_pack()
+
+    def mem_distr_counts(self):
+        return self._cc
+
+    def _mem_distr_pack(self):
         b = self._bin(0.5 * (self.cr.min(1) + self.cr.max(1)))
         counts = []
         for f in range(26):
@@ -264,6 +270,12 @@ class NumpySubCells(NumpySub):
             self.cids = np.concatenate([self.cids, (rec[:, 0, 3] // NV).astype(int)])
 
     def mem_exch_pack(self):
+        self._ic = self._mem_exch_pack()
+
+    def mem_exch_counts(self):
+        return self._ic
+
+    def _mem_exch_pack(self):
         lo = -(self.L // 2)
         vr, vv = self.cr.reshape(-1, 3), self.cv.reshape(-1, 3)
         side = np.where(vr < lo + 1, -1, np.where(vr >= lo + self.L - 1, 1, 0))
