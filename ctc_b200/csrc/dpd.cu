@@ -148,10 +148,11 @@ __device__ __forceinline__ void vjp_par(const DpdArgs &A, float da, float dg) {
 // shuffles (the queue only holds the warp's targets), the candidate's
 // position rides in the queue record from the filter; only the candidate's
 // velocity is loaded (one box, forces, reference keys)
-// (the body takes its block's index, so that the persistent step of many
-// boxes runs it too; kernels.cu)
+// (the body takes its warp's first target, so that the persistent step of
+// many boxes runs it warp by warp too; kernels.cu.  Without STAGE a warp
+// depends on no other warp of its block.)
 template <int RNG, bool BATCH, int T, int UNROLL, int MODE = 0, bool STAGE = false, bool REGP = false>
-__device__ __forceinline__ void dpd_bulk_block(const DpdArgs &A, const int bid) {
+__device__ __forceinline__ void dpd_bulk_warp(const DpdArgs &A, const int ia0) {
     constexpr int W = T / 32;
     static_assert(!STAGE || (!BATCH && MODE == 0 && W <= 8), "staging: one box, forces, at most 8 warps");
     static_assert(!REGP || (RNG == 0 && !BATCH && MODE == 0 && !STAGE), "REGP: one box, forces");
@@ -161,7 +162,7 @@ __device__ __forceinline__ void dpd_bulk_block(const DpdArgs &A, const int bid) 
     using Rec = typename std::conditional<REGP, BulkRecP, BulkRec<BATCH>>::type;
     __shared__ Rec queue[W][RQ];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ia = bid * T + threadIdx.x;
+    const int ia = ia0 + lane;
     int3 L = A.L;
     const int *starts = A.starts;
     int n, box = 0;
@@ -183,7 +184,6 @@ __device__ __forceinline__ void dpd_bulk_block(const DpdArgs &A, const int bid) 
     float acc_a = 0.0f, acc_g = 0.0f;               // MODE 1: parameter cotangents
 
     float4 pa = make_float4(0, 0, 0, 0), va = make_float4(0, 0, 0, 0);
-    const int ia0 = bid * T + warp * 32;            // the warp's first target
     int cx = 0, cy = 0, cz = 0;
     if (act) {
         pa = __ldg(A.pos + ia);
@@ -381,6 +381,12 @@ __device__ __forceinline__ void dpd_bulk_block(const DpdArgs &A, const int bid) 
         // a block whose wait gave up keeps its shared memory until the copies land
         if (stage_mem.ok && !staged) mbar_wait_bounded(&stage_mem.bar, 1u << 22);
     }
+}
+
+// block bid of T threads: its warps take the targets bid * T + 32 w ...
+template <int RNG, bool BATCH, int T, int UNROLL, int MODE = 0, bool STAGE = false, bool REGP = false>
+__device__ __forceinline__ void dpd_bulk_block(const DpdArgs &A, const int bid) {
+    dpd_bulk_warp<RNG, BATCH, T, UNROLL, MODE, STAGE, REGP>(A, bid * T + (threadIdx.x >> 5) * 32);
 }
 
 template <int RNG, bool BATCH, int T, int UNROLL, int MODE = 0, bool STAGE = false, bool REGP = false>
