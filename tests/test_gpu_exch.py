@@ -501,3 +501,110 @@ def test_ranks_membranes_migrate_and_follow_undivided_box():
     dx = np.abs(dx).max(1)
     assert np.quantile(dx, 0.999) < 1e-4 and dx.max() < 2e-3, (np.quantile(dx, 0.999), dx.max())
     assert C.device_error() == 0
+
+
+def test_rank_without_cells_takes_images_and_a_cell():
+    """Every cell starts on rank 0 of a 2 x 1 x 1 cart: rank 1 holds none, yet
+    evaluates FSI for the images that cross to it and sends their forces
+    back (forces equal to the undivided box's at dt = 0); then, flowing along
+    x, a cell migrates into the empty rank."""
+    C, X = mods()
+    dims, L = (2, 1, 1), (16, 16, 16)
+    centres = [(-0.3, 0.2, -0.4), (-8.0, -4.0, 4.5)]
+    cart, pp, pv, sim, subs, parts, cparts = _mem_setup(dims, L, centres, 71, dt=0.0)
+    assert len(cparts[1][1]) == 0 and len(cparts[0][1]) == 2
+    n, nv, nvt = len(pp), 642, len(pv)
+    sim.step(1)
+    torch.cuda.synchronize()
+    _, sids, sf = sim_state(sim, n)
+    ref = np.empty((n, 3))
+    ref[sids] = sf
+    _, _, mref = sim_membranes(sim, nvt)
+    X.step(subs, X.LocalTransport(cart))
+    torch.cuda.synchronize()
+    _, ff = gather(subs, parts)
+    _, mf, owner = gather_membranes(subs, parts, nvt, nv)
+    assert (owner == 0).all()
+    assert rel_err(ff, ref).max() < 1e-5
+    assert rel_err(mf, mref).max() < 1e-5
+    # the flow carries the first cell across x = 0 into rank 1
+    cart, pp, pv, sim, subs, parts, cparts = _mem_setup(dims, L, centres, 71, dt=0.01, drift=(20.0, 0.0, 0.0),
+                                                        vstd=1.0)
+    T = X.LocalTransport(cart)
+    for _ in range(4):
+        X.step(subs, T)
+    torch.cuda.synchronize()
+    _, _, owner = gather_membranes(subs, parts, nvt, nv)
+    assert owner[0] == 1 and owner[1] == 0, owner
+    assert C.device_error() == 0
+
+
+def test_membrane_bag_capacity_overflow_is_an_error():
+    """More cells leaving through one face than a cell bag holds (a quarter
+    of maxc, at least 4) is CTC_ERR_CAPACITY at the counts, before any
+    exchange."""
+    C, X = mods()
+    from ctc_b200._lib import CtcError
+    dims, L = (2, 1, 1), (24, 24, 24)
+    # six cells just inside the +x face, moved beyond it
+    centres = [(-0.2, y, z) for y in (-8.0, 0.0, 8.0) for z in (-6.0, 6.0)]
+    Lg = (48, 24, 24)
+    pv, tri, par = grid_cells(centres, 81)
+    nv = 642
+    cartX = X.Cart(dims)
+    cp = split_cells(pv, nv, cartX, L)
+    assert len(cp[0][1]) == 6
+    pp = grid_solvent(Lg, seed=81)
+    parts = split(pp, cartX, L)
+    dpd = C.DpdParams(*systems.dpd_params())
+    sub = X.SubDomain(L, cartX, 0, len(pp), dpd, dt=0.0)
+    sub.set_solvent(parts[0][0], parts[0][1])
+    q = cp[0][0].copy()
+    q[:, 0] += 0.5                  # every centre now beyond the face
+    sub.set_membranes(q, cp[0][1], tri, nv, par, C.DpdParams(*systems.dpd_params()), maxc=6,
+                      mass=systems.RBC_MASS)
+    sub.mem_distr_pack()
+    with pytest.raises(CtcError, match="capacity"):
+        sub.mem_distr_counts()
+    assert C.device_error() == 0
+
+
+def test_dist_transport_one_rank_nccl_with_cells_equals_local():
+    """The NCCL transport of a one-rank cart with cells (they leave and
+    re-enter through the periodic faces, their images come back to the rank
+    itself) steps as the in-process transport does."""
+    import datetime
+    import socket
+
+    import torch.distributed as dist
+    C, X = mods()
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        L = (16, 16, 16)
+        cart = X.Cart((1, 1, 1))
+        pp = grid_solvent(L, seed=91, vstd=1.0)
+        pp[:, 3] += 20.0
+        pv, tri, par = grid_cells([(7.9, 0.1, 0.2), (-3.0, 4.0, -7.5)], 92, drift=(20.0, 0.0, 0.0))
+        dpd = C.DpdParams(*systems.dpd_params())
+        out = []
+        for T in (X.LocalTransport(cart), X.DistTransport(cart, 0, device=torch.device("cuda"))):
+            sub = X.SubDomain(L, cart, 0, len(pp) + 64, dpd, dt=0.01)
+            sub.set_solvent(pp)
+            sub.set_membranes(pv, np.arange(2, dtype=np.int32), tri, 642, par, C.DpdParams(*systems.dpd_params()),
+                              maxc=4, mass=systems.RBC_MASS)
+            for _ in range(4):
+                X.step([sub], T)
+            torch.cuda.synchronize()
+            out.append((sub.get_solvent(), sub.get_membranes()))
+        (s0, m0), (s1, m1) = out
+        assert np.array_equal(s0[1], s1[1]) and np.array_equal(m0[1], m1[1])
+        assert np.abs(s0[0][:, :3] - s1[0][:, :3]).max() < 1e-5
+        assert np.abs(m0[0][:, :3] - m1[0][:, :3]).max() < 1e-5
+        assert np.abs(m0[0][:, 3:] - m1[0][:, 3:]).max() < 1e-2
+    finally:
+        dist.destroy_process_group()
+    assert C.device_error() == 0
