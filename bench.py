@@ -603,10 +603,10 @@ def run_batch(args, cfg, world, rank, local):
 
     # the same steps as ONE persistent launch each (grid-wide barriers between
     # the stages), replayed as a graph of that one launch; the kernel built for
-    # 3 and for 2 blocks per SM; then its stages as block 0 saw them
+    # 3, 2 and 4 blocks per SM; then its stages as block 0 saw them
     pers = {}
-    for occ in (3, 2):
-        b.set_persistent(1 if occ == 3 else 2)
+    for occ in (3, 2, 4):
+        b.set_persistent(occ)
         b.step(2)
         torch.cuda.synchronize()
         e0.record(stream)
@@ -616,7 +616,7 @@ def run_batch(args, cfg, world, rank, local):
         assert ctc.device_error() == 0, "device error during the persistent steps"
         pers[occ] = (allmax(world, e0.elapsed_time(e1)), b.persistent_grid())
     occ = min(pers, key=lambda k: pers[k][0])
-    b.set_persistent(1 if occ == 3 else 2)
+    b.set_persistent(occ)
     b.persistent_stages(True)
     b.step(2)
     stage_ms = b.persistent_stages(False)

@@ -758,8 +758,9 @@ class Batch:
 
     def set_persistent(self, enable=True):
         """Each step as one persistent cooperative launch (grid-wide barriers
-        between its stages) instead of one launch per stage; enable = 2 builds
-        the launch for 2 blocks per SM (more registers) instead of 3."""
+        between its stages) instead of one launch per stage; enable = 2, 3 or
+        4 takes the kernel built for that many blocks per SM (128, 80 or 64
+        registers; True: 4, the fastest measured)."""
         check(lib().ctc_batch_set_persistent(self.h, int(enable)))
 
     def persistent_check(self, barrier, stream=None):

@@ -132,7 +132,7 @@ __device__ __forceinline__ void persist_scan_sums(int nb, int *__restrict__ sums
 }
 
 // MINB blocks of PERSIST_T threads per SM: 3 caps the registers at 80 (a few
-// spill), 2 at 128 (none)
+// spill), 2 at 128 (none), 4 at 64
 template <int RNG, int U, int HU, int MINB>
 __global__ void __launch_bounds__(PERSIST_T, MINB) k_batch_persistent(const __grid_constant__ PersistArgs P) {
     __shared__ int flag;
@@ -253,7 +253,7 @@ using PersistKernel = void (*)(PersistArgs);
 
 // the co-resident blocks of the kernel on the current device (cached per device)
 static int persist_grid(PersistKernel k, int which) {
-    static int grid[64][4];
+    static int grid[64][6];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
     if (grid[dev][which] == 0) {
@@ -266,10 +266,13 @@ static int persist_grid(PersistKernel k, int which) {
 }
 
 cudaError_t batch_persistent_launch(const PersistArgs &P, cudaStream_t st, int *grid_out) {
-    const bool st3 = P.occupancy != 2;
-    const PersistKernel k = P.rng == CTC_RNG_STABLE ? (st3 ? k_batch_persistent<1, 2, 2, 3> : k_batch_persistent<1, 2, 2, 2>)
-                                                    : (st3 ? k_batch_persistent<0, 2, 2, 3> : k_batch_persistent<0, 2, 2, 2>);
-    const int grid = persist_grid(k, (P.rng == CTC_RNG_STABLE) + 2 * !st3);
+    const int v = P.occupancy == 2 ? 1 : (P.occupancy == 4 ? 2 : 0);     // 3, 2 or 4 blocks per SM
+    static const PersistKernel ks[2][3] = {
+        {k_batch_persistent<0, 2, 2, 3>, k_batch_persistent<0, 2, 2, 2>, k_batch_persistent<0, 2, 2, 4>},
+        {k_batch_persistent<1, 2, 2, 3>, k_batch_persistent<1, 2, 2, 2>, k_batch_persistent<1, 2, 2, 4>}};
+    const int r = P.rng == CTC_RNG_STABLE;
+    const PersistKernel k = ks[r][v];
+    const int grid = persist_grid(k, r + 2 * v);
     if (grid <= 0) return cudaErrorInvalidConfiguration;
     if (grid_out) *grid_out = grid;
     void *args[] = {(void*)&P};

@@ -49,7 +49,7 @@ struct PersistArgs {
     float dt, mass, mmass;
     float3 bodyf;
     int rng;                        // CTC_RNG_REFERENCE or CTC_RNG_STABLE
-    int occupancy;                  // blocks per SM the kernel is built for: 3 (80 registers) or 2 (128)
+    int occupancy;                  // blocks per SM the kernel is built for: 3 (80 registers), 2 (128) or 4 (64)
     GridBar *bar;
     int *err;
     int hold;                       // test hook: block 0 stops before barrier `hold` (-1: never)

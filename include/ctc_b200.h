@@ -622,9 +622,10 @@ int ctc_batch_set_graph(ctc_batch *b, int enable);
  * (2, 4) (may be NULL) */
 int ctc_batch_tune(ctc_batch *b, int reps, int *choice, void *stream);
 int ctc_batch_set_tune(ctc_batch *b, const int *choice);
-/* the step as ONE persistent cooperative launch (1: the kernel built for 3
- * blocks of 256 threads per SM, 80 registers; 2: for 2 blocks, 128
- * registers) instead of one launch per stage (0): the same stages in one
+/* the step as ONE persistent cooperative launch (1 or 4: the kernel built
+ * for 4 blocks of 256 threads per SM, 64 registers; 3: for 3 blocks, 80
+ * registers; 2: for 2 blocks, 128 registers) instead of one launch per stage
+ * (0): the same stages in one
  * kernel whose co-resident blocks meet
  * at grid-wide barriers between dependent stages (bulk 256 threads x 2
  * loads, halo 256 x 2; the tuner's shapes are not used); every wait at a

@@ -155,6 +155,31 @@ def test_persistent_step_matches_launch_per_stage(graph):
         assert np.abs(v0[:, 3:] - v1[:, 3:]).max() < VEL_TOL
 
 
+@pytest.mark.parametrize("build", [2, 3, 4])
+def test_persistent_builds_match_launch_per_stage(build):
+    """Each build of the persistent kernel (2, 3 or 4 blocks per SM: 128, 80
+    or 64 registers) steps as the launch per stage does."""
+    import ctc_b200 as C
+    L, solv, cells, mem, tri, par = _boxes(seed=17)
+    dpd = systems.dpd_params()
+    fsi = (0.0, 8.0, dpd[2], 0.25)
+    out = []
+    for persistent in (0, build):
+        b = _new_batch(L, solv, cells, mem, tri, par, dpd, fsi, (0.01, 0.0, 0.0))
+        b.set_persistent(persistent)
+        b.step(2)
+        out.append((b.get_solvent(), b.get_membranes()))
+        if persistent:
+            assert b.persistent_grid() >= 148 * min(build, 2)
+        b.close()
+    (s0, v0), (s1, v1) = out
+    assert np.abs(s0[:, :3] - s1[:, :3]).max() < 2 * POS_TOL
+    assert np.abs(s0[:, 3:] - s1[:, 3:]).max() < VEL_TOL
+    assert np.abs(v0[:, :3] - v1[:, :3]).max() < 2 * POS_TOL
+    assert np.abs(v0[:, 3:] - v1[:, 3:]).max() < VEL_TOL
+    assert C.device_error() == 0
+
+
 def test_persistent_step_stable_keys():
     """The same with the stable keys (a second instantiation of the kernel)."""
     import ctc_b200 as C
