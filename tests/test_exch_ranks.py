@@ -475,3 +475,112 @@ def test_cart_neighbours_are_symmetric():
             assert cart.rank(cart.coords(r)) == r
             for f in range(26):
                 assert cart.neighbours(nb[f])[exch.frag_anti(f)] == r
+
+
+# -- ranks of one process: bags moved by address ---------------------------------
+class _HostCopies:
+    """Stands in for the library's ctc_bags_copy on host memory."""
+
+    def __init__(self):
+        self.launches = 0
+
+    def ctc_bags_copy(self, n, dst, src, nbytes, stream):
+        import ctypes
+        self.launches += 1
+        for k in range(n):
+            ctypes.memmove(dst[k], src[k], nbytes[k])
+        return 0
+
+
+class PtrSubCells(NumpySubCells):
+    """The numpy stand-in with its bags as addresses (SubDomain.bag_ptrs'
+    contract: send addresses, units sent, receive addresses, capacities,
+    bytes per unit), for LocalTransport.exchange_ptrs."""
+
+    def _stream(self):
+        return None
+
+    def bag_ptrs(self, kind, counts, rcounts=None):
+        rec = 8 * self.REC
+        if kind == 0 or kind == 1:
+            return ([t.data_ptr() for t in self.send], counts, [t.data_ptr() for t in self.recv],
+                    [4096] * 26, rec)
+        if kind == 2:
+            return ([t.data_ptr() for t in self.fsend], [4] * 26, [t.data_ptr() for t in self.frecv], [4] * 26, 4)
+        if kind == 3:
+            return ([t.data_ptr() for t in self.csend], counts, [t.data_ptr() for t in self.crecv],
+                    [self.caps[3]] * 26, rec * NV)
+        if kind == 4:
+            return ([t.data_ptr() for t in self.isend], counts, [t.data_ptr() for t in self.irecv],
+                    [self.caps[4]] * 26, rec)
+        return ([t.data_ptr() for t in self.bsend], rcounts, [t.data_ptr() for t in self.brecv],
+                counts, 32)
+
+
+@pytest.mark.parametrize("dims", [(2, 1, 1), (2, 2, 1)])
+def test_local_transport_by_address_equals_undivided_box(dims, monkeypatch):
+    """All ranks in one process (LocalTransport): exch.step moves every bag
+    by address, one copy call per exchange, and after three steps of solvent
+    and cells flowing across the faces the ranks hold exactly the undivided
+    box's state."""
+    from ctc_b200 import exch
+    fake = _HostCopies()
+    monkeypatch.setattr(exch, "lib", lambda: fake)
+    L = (4, 4, 4)
+    cart = exch.Cart(dims)
+    pp, Lg = _system(dims, L, 2.0)
+    cells, rest = _cells(Lg)
+    c = np.floor((pp[:, :3] + np.array(Lg) / 2) / np.array(L)).astype(int)
+    cc = 0.5 * (cells[..., :3].min(1) + cells[..., :3].max(1))
+    cb = np.floor((cc + np.array(Lg) / 2) / np.array(L)).astype(int)
+    subs, origins = [], []
+    for r in range(cart.size):
+        me = np.array(cart.coords(r))
+        o = -np.array(Lg) / 2 + (me + 0.5) * np.array(L)
+        sel = np.flatnonzero((c == me).all(1))
+        q = pp[sel].copy()
+        q[:, :3] -= o
+        csel = np.flatnonzero((cb == me).all(1))
+        cq = cells[csel].copy()
+        cq[..., :3] -= o
+        subs.append(PtrSubCells(L, cart, r, q, sel, cq, csel, rest))
+        origins.append(o)
+    T = exch.LocalTransport(cart)
+    for _ in range(3):
+        exch.step(subs, T)
+    assert 3 * 3 <= fake.launches <= 3 * 6      # one copy call per exchange that moves anything
+    ref, cref = undivided_cells(pp, cells, rest, Lg, 3)
+    Lg = np.array(Lg, float)
+    got = np.full_like(ref, np.nan)
+    cgot = np.full_like(cref, np.nan)
+    for s, o in zip(subs, origins):
+        got[s.ids] = np.concatenate([s.r + o, s.v], 1)
+        cgot[s.cids] = np.concatenate([s.cr + o, s.cv], 2)
+    d = got[:, :3] - ref[:, :3]
+    d -= np.round(d / Lg) * Lg
+    assert np.abs(d).max() < 1e-9 and np.abs(got[:, 3:] - ref[:, 3:]).max() < 1e-9
+    d = cgot[..., :3] - cref[..., :3]
+    d -= np.round(d / Lg) * Lg
+    assert np.abs(d).max() < 1e-9 and np.abs(cgot[..., 3:] - cref[..., 3:]).max() < 1e-9
+
+
+def test_subdomain_bag_addresses():
+    """SubDomain.bag_ptrs: send bags one after another by the counts (kind 5:
+    by the images received), receive bags at their fixed places (kind 5: by
+    this rank's image counts), fixed bags for kind 2."""
+    from ctc_b200 import exch
+
+    class Fake:
+        _ptrs = {0: (1000, [5000 + 64 * f for f in range(26)], [2] * 26, 32),
+                 2: ([100 + f for f in range(26)], [200 + f for f in range(26)], [3] * 26, 4),
+                 5: (7000, 9000, [8] * 26, 16)}
+    counts = list(range(26))
+    send, sent, recv, cap, unit = exch.SubDomain.bag_ptrs(Fake(), 0, counts)
+    assert send[0] == 1000 and send[3] == 1000 + 32 * (0 + 1 + 2) and sent == counts
+    assert recv[5] == 5000 + 64 * 5 and cap == [2] * 26 and unit == 32
+    send, sent, recv, cap, unit = exch.SubDomain.bag_ptrs(Fake(), 2, None)
+    assert send[4] == 104 and recv[4] == 204 and sent == [3] * 26 and unit == 4
+    back = [2 * f for f in range(26)]
+    send, sent, recv, cap, unit = exch.SubDomain.bag_ptrs(Fake(), 5, counts, back)
+    assert sent == back and cap == counts and unit == 16
+    assert send[2] == 7000 + 16 * (0 + 2) and recv[3] == 9000 + 16 * (0 + 1 + 2)
