@@ -376,6 +376,9 @@ struct ctc_sim {
     cudaGraphExec_t gexec[2];
     cudaStream_t own;
     cudaEvent_t ev_in, ev_out;
+    // the halo pairs on a second stream beside the bulk pairs (not in profiled steps)
+    cudaStream_t side;
+    cudaEvent_t ev_fork, ev_join;
 };
 
 // the contact's vertex cell list for the current membranes
@@ -451,6 +454,9 @@ extern "C" int ctc_sim_create(const ctc_sim_config *cfg, ctc_sim **ps) {
     s->built = false;
     s->fuse_count = true;
     s->counted = false;
+    CUDA_TRY(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
     *ps = s;
     return CTC_OK;
 }
@@ -463,6 +469,9 @@ extern "C" int ctc_sim_destroy(ctc_sim *s) {
     if (s->own) cudaStreamDestroy(s->own);
     if (s->ev_in) cudaEventDestroy(s->ev_in);
     if (s->ev_out) cudaEventDestroy(s->ev_out);
+    if (s->side) cudaStreamDestroy(s->side);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
     for (int b = 0; b < 2; b++) { cudaFree(s->pos[b]); cudaFree(s->vel[b]); }
     cudaFree(s->force); cudaFree(s->counts); cudaFree(s->starts); cudaFree(s->count0); cudaFree(s->fss);
     if (s->wall) ctc_wall_fin(s->wall);
@@ -756,10 +765,20 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built, bool counted) {
     CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n_host, st));
     if (nvt > 0) CUDA_TRY(cudaMemsetAsync(s->mforce, 0, sizeof(float4) * (size_t)nvt, st));
     sim_mark(s, 2, st);
+    // the halo pairs run beside the bulk pairs on the second stream (both only
+    // add to the forces); profiled steps run them one after the other
+    const bool overlap = !s->prof;
     A.which = 1;
+    if (overlap) {
+        CUDA_TRY(cudaEventRecord(s->ev_fork, st));
+        CUDA_TRY(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
+        CUDA_TRY(halo_packed_launch(A, s->pack, s->pack_off, s->pack_cap, s->cfg.rng, s->side, 26, s->tune));
+        CUDA_TRY(cudaEventRecord(s->ev_join, s->side));
+    }
     CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st, s->tune));
     sim_mark(s, 3, st);
-    CUDA_TRY(halo_packed_launch(A, s->pack, s->pack_off, s->pack_cap, s->cfg.rng, st, 26, s->tune));
+    if (overlap) CUDA_TRY(cudaStreamWaitEvent(st, s->ev_join, 0));
+    else CUDA_TRY(halo_packed_launch(A, s->pack, s->pack_off, s->pack_cap, s->cfg.rng, st, 26, s->tune));
     sim_mark(s, 4, st);
     WvelView wstep;
     if (s->wall) {
