@@ -407,6 +407,8 @@ def run_ours(args, cfg, world, rank, local):
                    "l2": "inputs larger than L2 (state %.2f GB per buffer)" % (32e-9 * n)},
         "gpu_launches": launches * args.steps,
         "phase_ms": phases,
+        "phase_note": "direct launches with events between the phases (the halo after the bulk); the timed "
+                      "steps run the halo beside the bulk on a second stream",
         "roofline": {"bound": "hbm", "kernel": "k_dpd_bulk", "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic * n if traffic else None,
