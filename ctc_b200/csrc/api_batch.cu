@@ -49,6 +49,7 @@ struct ctc_batch {
     float *seeds = nullptr, *fseeds = nullptr;      // 27 per box; FSI: 2 per box
     int cur = 0;
     bool loaded = false;
+    bool counted = false;          // counts and w.cidslot hold the count pass of pos[cur] (the last update's)
     // membranes: mnc cells of mnv vertices, grouped by box (B.v0)
     int mnc = 0, mnv = 0;
     ctc_rbc_force *rbc = nullptr;
@@ -66,6 +67,9 @@ struct ctc_batch {
     cudaStream_t own = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};   // one step from buffer 0, one from buffer 1
+    // the halo and FSI pairs on a second stream beside the bulk pairs
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // the step as one persistent launch (ctc_batch_set_persistent)
     bool persistent = false;
     int occupancy = 4;                               // of the persistent kernel: 4, 3 or 2 blocks per SM
@@ -103,6 +107,9 @@ extern "C" int ctc_batch_destroy(ctc_batch *b) {
     if (b->ev_in) cudaEventDestroy(b->ev_in);
     if (b->ev_out) cudaEventDestroy(b->ev_out);
     if (b->own) cudaStreamDestroy(b->own);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->side) cudaStreamDestroy(b->side);
     delete b;
     return CTC_OK;
 }
@@ -217,6 +224,9 @@ extern "C" int ctc_batch_create(const ctc_batch_config *cfg, ctc_batch **pb) {
     }
     cu(cudaMemcpy(b->trunk, tr.data(), sizeof(Kiss) * tr.size(), cudaMemcpyHostToDevice), "trunks");
     cu(cudaMemcpy(b->ftrunk, ft.data(), sizeof(Kiss) * ft.size(), cudaMemcpyHostToDevice), "trunks");
+    cu(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking), "streams");
+    cu(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "events");
+    cu(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming), "events");
     if (rc) { ctc_batch_destroy(b); return rc; }
     *pb = b;
     return CTC_OK;
@@ -240,6 +250,7 @@ extern "C" int ctc_batch_set_solvent(ctc_batch *b, const float *pp, void *stream
     CUDA_TRY(cudaStreamSynchronize(st));
     b->cur = 0;
     b->loaded = true;
+    b->counted = false;
     return CTC_OK;
 }
 
@@ -367,13 +378,15 @@ static int batch_step_persistent(ctc_batch *b, cudaStream_t st, int hold) {
     return CTC_OK;
 }
 
-// one step of every box, the order of ctc_sim_step
-static int batch_step1(ctc_batch *b, cudaStream_t st) {
+// one step of every box, the order of ctc_sim_step (counted: the last update
+// counted the cells of pos[cur]; the update of this step counts the next
+// build's cells)
+static int batch_step1(ctc_batch *b, cudaStream_t st, bool counted) {
     if (b->persistent) return batch_step_persistent(b, st, -1);
     const int src = b->cur, dst = 1 - b->cur;
     CUDA_TRY(draw_seeds_launch(b->trunk, 27 * b->nbox, b->seeds, st));
     CUDA_TRY(clist_launch(make_int3(1, 1, 1), b->ntot, nullptr, b->pos[src], b->vel[src], 1, b->counts, b->starts,
-                          b->pos[dst], b->vel[dst], nullptr, b->w, dev_err_ptr(), st, b->B, b->nctot));
+                          b->pos[dst], b->vel[dst], nullptr, b->w, dev_err_ptr(), st, b->B, b->nctot, counted));
     const int nvt = b->mnc * b->mnv;
     if (nvt > 0) {
         CUDA_TRY(rbc_wrap_launch(b->mnc, b->mnv, make_int3(1, 1, 1), b->mpos, st, b->B));
@@ -390,19 +403,28 @@ static int batch_step1(ctc_batch *b, cudaStream_t st) {
     CUDA_TRY(frag_starts_boxes_launch(b->B, b->counts, b->fss, st));
     CUDA_TRY(halo_pack_boxes_launch(A, b->coff, 26 * b->nbox, b->ncells_frag, b->pack, b->pack_off, b->pack_cap, st));
     CUDA_TRY(cudaMemsetAsync(b->force, 0, sizeof(float4) * (size_t)b->ntot, st));
+    if (nvt > 0) CUDA_TRY(cudaMemsetAsync(b->mforce, 0, sizeof(float4) * (size_t)nvt, st));
     A.which = 1;
-    CUDA_TRY(dpd_launch(A, b->ntot, b->rng, st, b->tune));
-    CUDA_TRY(halo_packed_launch(A, b->pack, b->pack_off, b->pack_cap, b->rng, st, 26 * b->nbox, b->tune));
+    // the halo and the solvent-membrane pairs run on the second stream beside
+    // the bulk pairs (all of them only add to the forces)
+    cudaStream_t s2 = b->side;
+    CUDA_TRY(cudaEventRecord(b->ev_fork, st));
+    CUDA_TRY(cudaStreamWaitEvent(s2, b->ev_fork, 0));
+    CUDA_TRY(halo_packed_launch(A, b->pack, b->pack_off, b->pack_cap, b->rng, s2, 26 * b->nbox, b->tune));
     if (nvt > 0) {
-        CUDA_TRY(cudaMemsetAsync(b->mforce, 0, sizeof(float4) * (size_t)nvt, st));
         DpdPar F;
         F.a = b->fsi.a; F.g = b->fsi.g; F.s = b->fsi.s; F.spow = b->fsi.spow;
         int rc = fsi_forces(make_int3(1, 1, 1), F, nvt, (const float*)b->mpos, (const float*)b->mvel, 4, b->pos[dst],
                             b->vel[dst], b->starts, b->counts, (float*)b->mforce, 4, (float*)b->force, 4, 0.0f, 0.0f,
-                            b->fseeds, b->rng, b->fmask, b->frank, b->fcount, b->fimg, st, b->B, b->vperm, b->mnv);
+                            b->fseeds, b->rng, b->fmask, b->frank, b->fcount, b->fimg, s2, b->B, b->vperm, b->mnv);
         if (rc) return rc;
     }
-    CUDA_TRY(integrate_launch(b->ntot_dev, b->ntot, b->pos[dst], b->vel[dst], b->force, b->dt, b->mass, b->bodyf, st));
+    CUDA_TRY(cudaEventRecord(b->ev_join, s2));
+    CUDA_TRY(dpd_launch(A, b->ntot, b->rng, st, b->tune));
+    CUDA_TRY(cudaStreamWaitEvent(st, b->ev_join, 0));
+    CUDA_TRY(integrate_count_launch(b->ntot_dev, b->ntot, b->pos[dst], b->vel[dst], b->force, b->dt, b->mass,
+                                    b->bodyf, make_int3(1, 1, 1), b->counts, b->w, dev_err_ptr(), st, b->B,
+                                    b->nctot));
     if (nvt > 0) {
         int rc = membrane_forces(b->rbc, &b->mpar, b->mnc, (const float*)b->mpos, (const float*)b->mvel, 4,
                                  (float*)b->mforce, 4, st);
@@ -420,7 +442,7 @@ static int batch_capture(ctc_batch *b, int k) {
     cudaGraph_t g = nullptr;
     if (!dev_err_ptr()) return fail(CTC_ERR_CUDA, "ctc_batch_step: device error word unavailable");
     CUDA_TRY(cudaStreamBeginCapture(b->own, cudaStreamCaptureModeThreadLocal));
-    int rc = batch_step1(b, b->own);
+    int rc = batch_step1(b, b->own, true);     // graphs replay the steady state
     cudaError_t e = cudaStreamEndCapture(b->own, &g);
     b->cur = keep;
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -437,8 +459,9 @@ extern "C" int ctc_batch_step(ctc_batch *b, int nsteps, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     if (!b->use_graph) {
         for (int s = 0; s < nsteps; s++) {
-            int rc = batch_step1(b, st);
+            int rc = batch_step1(b, st, b->counted);
             if (rc) return rc;
+            b->counted = !b->persistent;
         }
         return CTC_OK;
     }
@@ -446,22 +469,29 @@ extern "C" int ctc_batch_step(ctc_batch *b, int nsteps, void *stream) {
     CUDA_TRY(cudaEventRecord(b->ev_in, st));
     CUDA_TRY(cudaStreamWaitEvent(b->own, b->ev_in, 0));
     for (int s = 0; s < nsteps; s++) {
+        if (!b->persistent && !b->counted) {     // the first step after new state counts its cells itself
+            int rc = batch_step1(b, b->own, false);
+            if (rc) return rc;
+            b->counted = true;
+            continue;
+        }
         if (!b->exec[b->cur]) {
             int rc = batch_capture(b, b->cur);
             if (rc) return rc;
         }
         CUDA_TRY(cudaGraphLaunch(b->exec[b->cur], b->own));
         b->cur = 1 - b->cur;
+        b->counted = !b->persistent;
     }
     CUDA_TRY(cudaEventRecord(b->ev_out, b->own));
     CUDA_TRY(cudaStreamWaitEvent(st, b->ev_out, 0));
     return CTC_OK;
 }
 
-// the step as one persistent cooperative launch (1: its kernel built for 3
-// blocks of 256 threads per SM; 2: for 2, more registers) or as one launch
-// per stage (0); the membranes' bending must be Kantor or none, without their
-// random force
+// the step as one persistent cooperative launch (1 or 4: its kernel built for
+// 4 blocks of 256 threads per SM; 3: for 3; 2: for 2, more registers) or as
+// one launch per stage (0); the membranes' bending must be Kantor or none,
+// without their random force
 extern "C" int ctc_batch_set_persistent(ctc_batch *b, int enable) {
     if (!b || enable < 0 || enable > 4) return fail(CTC_ERR_ARG, "ctc_batch_set_persistent: bad arguments");
     if (enable && b->rbc) {
@@ -478,6 +508,7 @@ extern "C" int ctc_batch_set_persistent(ctc_batch *b, int enable) {
     }
     drop_graphs(b);
     b->persistent = enable != 0;
+    b->counted = false;
     b->occupancy = enable == 1 ? 4 : enable;                // 1: the fastest measured build
     return CTC_OK;
 }
@@ -550,6 +581,7 @@ extern "C" int ctc_batch_tune(ctc_batch *b, int reps, int *choice, void *stream)
     CUDA_TRY(draw_seeds_launch(b->trunk, 27 * b->nbox, b->seeds, st));
     CUDA_TRY(clist_launch(make_int3(1, 1, 1), b->ntot, nullptr, b->pos[src], b->vel[src], 1, b->counts, b->starts,
                           b->pos[dst], b->vel[dst], nullptr, b->w, dev_err_ptr(), st, b->B, b->nctot));
+    b->counted = false;        // the next step counts again
     CUDA_TRY(frag_starts_boxes_launch(b->B, b->counts, b->fss, st));
     DpdArgs A;
     dpd_args_common(&A, make_int3(1, 1, 1), &b->dpd);

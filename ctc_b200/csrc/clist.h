@@ -29,9 +29,10 @@ cudaError_t clist_launch(int3 L, int n, const int *nptr, const float4 *pos_in, c
 // the update of a cell-sorted state (integrate_launch) with the count pass of
 // the next cell-list build fused: the new positions, still in registers, are
 // wrapped and counted into counts (ncells, cleared here first) and w.cidslot
+// (with B.nbox > 0: the boxes' cells, nc_boxes in all, L ignored)
 cudaError_t integrate_count_launch(const int *nptr, int nmax, float4 *pos, float4 *vel, const float4 *force,
                                    float dt, float mass, float3 a, int3 L, int *counts, const ClistScratch &w,
-                                   int *err, cudaStream_t st);
+                                   int *err, cudaStream_t st, const Boxes &B = Boxes(), int nc_boxes = 0);
 
 // exclusive scan: starts[0..nc) of counts, starts[nc] = total; sums holds
 // scan_sums_ints(nc) ints

@@ -24,21 +24,31 @@ namespace ctc {
 // goes from the update's registers to the cell and slot
 __global__ void k_integrate_count(const int *__restrict__ nptr, float4 *__restrict__ pos, float4 *__restrict__ vel,
                                   const float4 *__restrict__ force, float dt, float mass, float3 a, int3 L,
-                                  int2 *__restrict__ cidslot, int *__restrict__ counts, int *err) {
+                                  int2 *__restrict__ cidslot, int *__restrict__ counts, int *err,
+                                  const __grid_constant__ Boxes B) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, n = *nptr;
     float4 r = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (i < n) r = integrate_one(i, pos, vel, force, dt, mass, a);
-    clist_count_val(i, n, r, L, 0, 1, cidslot, counts, err);
+    int c0 = 0;
+    if (i < n) {
+        r = integrate_one(i, pos, vel, force, dt, mass, a);
+        if (B.nbox > 0) {       // the particle's box: its edges and the offset of its cells
+            const int box = box_find(B.p0, B.nbox, i);
+            L = box_L(B, box);
+            c0 = __ldg(B.c0 + box);
+        }
+    }
+    clist_count_val(i, n, r, L, c0, 1, cidslot, counts, err);
 }
 
 cudaError_t integrate_count_launch(const int *nptr, int nmax, float4 *pos, float4 *vel, const float4 *force,
                                    float dt, float mass, float3 a, int3 L, int *counts, const ClistScratch &w,
-                                   int *err, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * (size_t)L.x * L.y * L.z, st);
+                                   int *err, cudaStream_t st, const Boxes &B, int nc_boxes) {
+    const size_t nc = B.nbox > 0 ? (size_t)nc_boxes : (size_t)L.x * L.y * L.z;
+    cudaError_t e = cudaMemsetAsync(counts, 0, sizeof(int) * nc, st);
     if (e != cudaSuccess) return e;
     if (nmax > 0)
         k_integrate_count<<<ceil_div(nmax, 256), 256, 0, st>>>(nptr, pos, vel, force, dt, mass, a, L, w.cidslot,
-                                                                counts, err);
+                                                                counts, err, B);
     return cudaGetLastError();
 }
 

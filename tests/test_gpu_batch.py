@@ -222,3 +222,42 @@ def test_persistent_barrier_wait_gives_up():
     torch.cuda.synchronize()
     assert C.device_error() == 0
     b.close()
+
+
+def test_fused_count_bookkeeping_across_modes():
+    """The update counts the next step's cells; every way of stepping keeps
+    that right: direct steps, graph replays, a tuner call (which recounts), a
+    persistent step (which counts itself) and back.  Without pair forces the
+    motion is exact arithmetic (the membranes' internal forces are summed
+    per vertex in a fixed order), so the states equal a run of direct steps
+    bit for bit while particles and cells cross the boxes' faces."""
+    import ctc_b200 as C
+    L, solv, cells, mem, tri, par = _boxes(seed=19)
+    rng = np.random.default_rng(20)
+    solv = [p.copy() for p in solv]
+    for p in solv:
+        p[:, 3:] = rng.normal(0.0, 3.0, (len(p), 3)).astype(np.float32)
+    zero = (0.0, 0.0, 0.0, 0.25)
+    out = []
+    for mixed in (False, True):
+        b = _new_batch(L, solv, cells, mem, tri, par, zero, zero, (0.5, 0.0, 0.0))
+        b.set_tune((128, 4, 128, 2))
+        if not mixed:
+            b.step(9)
+        else:
+            b.step(2)
+            b.set_graph(True)
+            b.step(2)
+            b.tune(reps=1)
+            b.set_tune((128, 4, 128, 2))
+            b.step(2)
+            b.set_persistent(True)
+            b.step(1)
+            b.set_persistent(False)
+            b.step(2)
+        out.append((b.get_solvent(), b.get_membranes()))
+        b.close()
+    (s0, v0), (s1, v1) = out
+    assert np.array_equal(s0, s1)
+    assert np.array_equal(v0, v1)
+    assert C.device_error() == 0
