@@ -720,6 +720,9 @@ extern "C" int ctc_sim_get_membranes(ctc_sim *s, float *pp, void *stream) {
     return CTC_OK;
 }
 
+// particles from which the halo pairs run beside the bulk pairs
+constexpr int SIM_OVERLAP_MIN = 1 << 18;
+
 // the update fuses the next build's count pass unless bounce-back moves the
 // particles after it
 static bool sim_fuses(const ctc_sim *s) { return s->fuse_count && !s->wall; }
@@ -766,8 +769,10 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built, bool counted) {
     if (nvt > 0) CUDA_TRY(cudaMemsetAsync(s->mforce, 0, sizeof(float4) * (size_t)nvt, st));
     sim_mark(s, 2, st);
     // the halo pairs run beside the bulk pairs on the second stream (both only
-    // add to the forces); profiled steps run them one after the other
-    const bool overlap = !s->prof;
+    // add to the forces) in boxes large enough for the bulk kernel to leave
+    // issue slots; small boxes are launch-bound, and there the fork and join
+    // cost more than they hide.  Profiled steps run the two one after the other.
+    const bool overlap = !s->prof && s->n_host >= SIM_OVERLAP_MIN;
     A.which = 1;
     if (overlap) {
         CUDA_TRY(cudaEventRecord(s->ev_fork, st));
