@@ -567,10 +567,12 @@ def run_decomposed(args, cfg, world, rank, local):
 # single-box system per box stepped one after another
 # ---------------------------------------------------------------------------
 def run_batch(args, cfg, world, rank, local):
+    import ctypes as C
+
     import torch
 
     import ctc_b200 as ctc
-    from ctc_b200 import systems
+    from ctc_b200 import _lib, systems
     torch.cuda.set_device(local)
     nbox = args.nbox or cfg["nbox"]
     L, n, pp, cells, pv, tri, par = systems.batch_system(nbox=nbox, seed=5 + rank)
@@ -625,15 +627,21 @@ def run_batch(args, cfg, world, rank, local):
     p_ms, p_blocks = pers[occ]
     b.set_persistent(False)
 
-    # end to end through the public API: host state in, K steps, host state out
+    # end to end through the public API: the state in from pinned host memory
+    # (solvent and membranes), K steps, the state out into pinned host memory
+    host_in = torch.from_numpy(np.ascontiguousarray(pp, np.float32)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    m_in = torch.from_numpy(np.ascontiguousarray(pv, np.float32)).pin_memory()
+    m_out = torch.empty_like(m_in).pin_memory()
+    st = C.c_void_p(stream.cuda_stream)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    b.set_solvent(pp)
-    b.set_membranes(cells, pv, tri, 642, par, fsi, mass=systems.RBC_MASS)
+    _lib.check(_lib.lib().ctc_batch_set_solvent(b.h, C.c_void_p(host_in.data_ptr()), st))
+    b.set_membranes(cells, m_in.numpy(), tri, 642, par, fsi, mass=systems.RBC_MASS)
     b.step(args.steps)
-    b.get_solvent()
-    b.get_membranes()
+    _lib.check(_lib.lib().ctc_batch_get_solvent(b.h, C.c_void_p(host_out.data_ptr()), st))
+    _lib.check(_lib.lib().ctc_batch_get_membranes(b.h, C.c_void_p(m_out.data_ptr()), st))
     torch.cuda.synchronize()
     e2e_s = allmax(world, time.perf_counter() - t0)
     b.close()

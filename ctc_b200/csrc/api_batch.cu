@@ -241,10 +241,7 @@ extern "C" int ctc_batch_set_solvent(ctc_batch *b, const float *pp, void *stream
     if (b->ntot > 0) {
         CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(float) * 6 * (size_t)b->ntot, st));
         CUDA_TRY(cudaMemcpyAsync(tmp, pp, sizeof(float) * 6 * (size_t)b->ntot, cudaMemcpyHostToDevice, st));
-        for (int k = 0; k < b->nbox; k++) {
-            const int o = b->p0h[k], n = b->p0h[k + 1] - o;
-            CUDA_TRY(aos_to_soa(n, tmp + 6 * (size_t)o, b->pos[0] + o, b->vel[0] + o, st));
-        }
+        CUDA_TRY(aos_to_soa_boxes(b->ntot, tmp, b->pos[0], b->vel[0], b->B, st));
         CUDA_TRY(cudaFreeAsync(tmp, st));
     }
     CUDA_TRY(cudaStreamSynchronize(st));

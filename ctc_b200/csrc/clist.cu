@@ -227,6 +227,18 @@ __global__ void k_aos_to_soa(int n, const float *__restrict__ pp, float4 *__rest
     vel[i] = make_float4(q[3], q[4], q[5], 0.0f);
 }
 
+// the same over the concatenated particles of many boxes: w = the index
+// inside the particle's box
+__global__ void k_aos_to_soa_boxes(int n, const float *__restrict__ pp, float4 *__restrict__ pos,
+                                   float4 *__restrict__ vel, const __grid_constant__ Boxes B) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k = i - __ldg(B.p0 + box_find(B.p0, B.nbox, i));
+    const float *q = pp + 6 * (size_t)i;
+    pos[i] = make_float4(q[0], q[1], q[2], __int_as_float(k));
+    vel[i] = make_float4(q[3], q[4], q[5], 0.0f);
+}
+
 __global__ void k_soa_to_aos(const int *__restrict__ nptr, int nfix, const float4 *__restrict__ pos,
                              const float4 *__restrict__ vel, float *__restrict__ pp) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -292,6 +304,11 @@ cudaError_t scan_launch(int nc, const int *counts, int *starts, int *sums, cudaS
 
 cudaError_t aos_to_soa(int n, const float *pp, float4 *pos, float4 *vel, cudaStream_t st) {
     if (n > 0) k_aos_to_soa<<<ceil_div(n, 256), 256, 0, st>>>(n, pp, pos, vel);
+    return cudaGetLastError();
+}
+
+cudaError_t aos_to_soa_boxes(int n, const float *pp, float4 *pos, float4 *vel, const Boxes &B, cudaStream_t st) {
+    if (n > 0) k_aos_to_soa_boxes<<<ceil_div(n, 256), 256, 0, st>>>(n, pp, pos, vel, B);
     return cudaGetLastError();
 }
 

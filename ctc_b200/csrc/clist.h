@@ -40,6 +40,8 @@ size_t scan_sums_ints(int nc);
 cudaError_t scan_launch(int nc, const int *counts, int *starts, int *sums, cudaStream_t st);
 
 cudaError_t aos_to_soa(int n, const float *pp, float4 *pos, float4 *vel, cudaStream_t st);
+// many boxes' particles concatenated (B.p0): w = the index inside the box
+cudaError_t aos_to_soa_boxes(int n, const float *pp, float4 *pos, float4 *vel, const Boxes &B, cudaStream_t st);
 cudaError_t soa_to_aos(const int *nptr, int nmax, const float4 *pos, const float4 *vel, float *pp,
                        cudaStream_t st);
 
