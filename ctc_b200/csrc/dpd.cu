@@ -45,7 +45,7 @@ __device__ __forceinline__ int frag_index(int3 L, const int *fss_fid, int fid, i
 
 // ---------------------------------------------------------------------------
 // 1-D bulk copies global -> this CTA's shared memory, completed on an mbarrier
-// (cp.async.bulk, no multicast: the source is this GPU's own memory)
+// (cp.async.bulk into this CTA alone; the source is this GPU's own memory)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
