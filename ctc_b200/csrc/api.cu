@@ -768,16 +768,30 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built, bool counted) {
     CUDA_TRY(cudaMemsetAsync(s->force, 0, sizeof(float4) * (size_t)s->n_host, st));
     if (nvt > 0) CUDA_TRY(cudaMemsetAsync(s->mforce, 0, sizeof(float4) * (size_t)nvt, st));
     sim_mark(s, 2, st);
-    // the halo pairs run beside the bulk pairs on the second stream (both only
-    // add to the forces) in boxes large enough for the bulk kernel to leave
-    // issue slots; small boxes are launch-bound, and there the fork and join
-    // cost more than they hide.  Profiled steps run the two one after the other.
+    // the halo and solvent-membrane pairs run beside the bulk pairs on the
+    // second stream (all only add to the forces) in boxes large enough for the
+    // bulk kernel to leave issue slots; small boxes are launch-bound, and there
+    // the fork and join cost more than they hide.  Profiled steps run them one
+    // after the other.
     const bool overlap = !s->prof && s->n_host >= SIM_OVERLAP_MIN;
+    // solvent-membrane forces into the vertex forces and, as reactions, the solvent ones
+    auto fsi = [&](cudaStream_t q) -> int {
+        DpdPar F;
+        F.a = s->fsi.a; F.g = s->fsi.g; F.s = s->fsi.s; F.spow = s->fsi.spow;
+        return fsi_forces(s->L, F, nvt, (const float*)s->mpos, (const float*)s->mvel, 4, s->pos[dst], s->vel[dst],
+                          s->starts, s->counts, (float*)s->mforce, 4, (float*)s->force, 4, 0.0f, 0.0f,
+                          s->seeds_dev + 27, s->cfg.rng, s->fmask, s->frank, s->fcount, s->fimg_start, q, Boxes(),
+                          s->vperm, s->mnv);
+    };
     A.which = 1;
-    if (overlap) {
+    if (overlap) {      // the halo pairs, then the solvent-membrane pairs, beside the bulk pairs
         CUDA_TRY(cudaEventRecord(s->ev_fork, st));
         CUDA_TRY(cudaStreamWaitEvent(s->side, s->ev_fork, 0));
         CUDA_TRY(halo_packed_launch(A, s->pack, s->pack_off, s->pack_cap, s->cfg.rng, s->side, 26, s->tune));
+        if (nvt > 0) {
+            int rc = fsi(s->side);
+            if (rc) return rc;
+        }
         CUDA_TRY(cudaEventRecord(s->ev_join, s->side));
     }
     CUDA_TRY(dpd_launch(A, s->n_host, s->cfg.rng, st, s->tune));
@@ -806,14 +820,8 @@ static int sim_enqueue(ctc_sim *s, cudaStream_t st, bool built, bool counted) {
     }
     sim_mark(s, 5, st);
     const float3 bf = make_float3(s->cfg.bodyf[0], s->cfg.bodyf[1], s->cfg.bodyf[2]);
-    if (nvt > 0) {
-        // solvent-membrane forces into the vertex forces and, as reactions, the solvent ones
-        DpdPar F;
-        F.a = s->fsi.a; F.g = s->fsi.g; F.s = s->fsi.s; F.spow = s->fsi.spow;
-        int rc = fsi_forces(s->L, F, nvt, (const float*)s->mpos, (const float*)s->mvel, 4, s->pos[dst], s->vel[dst],
-                            s->starts, s->counts, (float*)s->mforce, 4, (float*)s->force, 4, 0.0f, 0.0f,
-                            s->seeds_dev + 27, s->cfg.rng, s->fmask, s->frank, s->fcount, s->fimg_start, st,
-                            Boxes(), s->vperm, s->mnv);
+    if (nvt > 0 && !overlap) {
+        int rc = fsi(st);
         if (rc) return rc;
     }
     sim_mark(s, 6, st);
