@@ -477,6 +477,9 @@ extern "C" int ctc_sub_create(const ctc_sub_config *cfg, ctc_sub **ps) {
     if (rc) return rc;
     ctc_sub *s = new ctc_sub();
     s->cfg = *cfg;
+    // the bulk pairs with reference keys take the variant that reads the
+    // target's data from its lane (the faster one on a large box)
+    if (cfg->sim.rng == CTC_RNG_REFERENCE) s->tune.bulk_stage = 2;
     s->L = make_int3(cfg->sim.LX, cfg->sim.LY, cfg->sim.LZ);
     s->nc = cfg->sim.LX * cfg->sim.LY * cfg->sim.LZ;
     s->maxp = cfg->sim.maxp;
