@@ -702,10 +702,10 @@ def run_batch(args, cfg, world, rank, local):
                    "tuned_shape": {"bulk_threads": tune[0], "bulk_unroll": tune[1], "halo_threads": tune[2],
                                    "halo_unroll": tune[3]},
                    "graph": True, "l2": "inputs larger than L2 (%.2f GB of state)" % (32e-9 * ntot)},
-        # seeds, 6 cell-list kernels, cell wrap, FSI seeds, fragment starts, 2 halo packing kernels, bulk,
-        # halo, 3 image-list kernels, FSI, update, area/volume, membrane forces, vertex update: each once
-        # for all boxes
-        "gpu_launches": 22 * args.steps,
+        # seeds, 5 cell-list kernels, cell wrap, FSI seeds, fragment starts, 2 halo packing kernels, bulk,
+        # halo, 3 image-list kernels, FSI, the update with the next build's count pass, area/volume,
+        # membrane forces, vertex update: each once for all boxes (profiles/launches_c5.md)
+        "gpu_launches": 21 * args.steps,
         "per_box": {"value": pb_value, "unit": "particle-steps/s", "steps": pb_steps,
                     "ms_per_step": pb_ms_step, "graph_launches_per_step": int(len(n)),
                     "note": "one single-box system per box, stepped box after box on one stream, each "
