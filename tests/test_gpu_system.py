@@ -105,20 +105,23 @@ def _rel_err(f, ref):
     return float((np.abs(f - ref).max(1) / np.maximum(mag, floor)).max())
 
 
+@pytest.mark.parametrize("edge", [16, 32])
 @pytest.mark.parametrize("case", ["membranes", "contact", "walls"])
-def test_fused_step_forces_vs_modules(case):
+def test_fused_step_forces_vs_modules(case, edge):
     """The force arrays of one fused step -- the solvent's (bulk + halo pairs,
     wall forces, FSI reactions) and the vertices' (wall forces and repulsion,
     FSI, contact, internal membrane forces on top) -- against the module entry
     points composed in the reference's order on the same state and seeds
     (each module held to the reference's own kernels at 1e-5): within 1e-5
     relative, max-norm per particle, so that no force term of the fused step
-    can be dropped or doubled unseen."""
+    can be dropped or doubled unseen.  The 32^3 box (327,680 particles) is
+    large enough for the step to run the halo and solvent-membrane pairs on
+    its second stream beside the bulk pairs; the 16^3 box runs them after."""
     import os
 
     import ctc_b200 as C
     from .test_gpu_wall import SDF
-    L = (16, 16, 16)
+    L = (edge, edge, edge)
     dpd = systems.dpd_params()
     fsi = C.DpdParams(0.0, 8.0, dpd[2], 0.25)
     cnt = C.DpdLjParams(2.6666667, 8.0, dpd[2], 0.25, 0.3, 0.44)
@@ -138,7 +141,7 @@ def test_fused_step_forces_vs_modules(case):
         X, F = mesh.rbc_template()                        # one cell in the channel, near a plate
         pv = np.zeros((len(X), 6), np.float32)
         pv[:, :3] = X
-        pv[:, 2] += 4.2
+        pv[:, 2] += 4.2 * edge / 16                      # the plates scale with the box
         pv[:, 3:] = np.random.default_rng(103).normal(0, 0.3, (len(X), 3))
         tri, nv = F, len(X)
         A, V = mesh.area_volume(X, F)
