@@ -385,7 +385,10 @@ int ctc_sim_set_solvent(ctc_sim *s, int n, const float *pp, void *stream);
 /* same from a device AoS array */
 int ctc_sim_set_solvent_dev(ctc_sim *s, int n, const float *pp, void *stream);
 /* advance nsteps steps: wrap + cell lists, bulk + halo DPD, body force,
- * update -- the reference's step order (src/sim/imp/run.h:8-68) */
+ * update -- the reference's step order (src/sim/imp/run.h:8-68).  In boxes of
+ * 2^18 particles or more the halo and solvent-membrane pairs run on the
+ * object's own second stream beside the bulk pairs, forked from and joined
+ * back into `stream` by events, so the work stays ordered on `stream`. */
 int ctc_sim_step(ctc_sim *s, int nsteps, void *stream);
 /* 1: steps replay CUDA graphs captured on first use (one per ping-pong
  * buffer) on the object's own stream, ordered after the caller's stream work
