@@ -1,5 +1,5 @@
 """Multi-process host logic of the decomposed solvent and membranes (no
-GPU): 2, 4 and 8 gloo ranks run the product's step orchestration
+GPU): 2, 3, 4 and 8 gloo ranks run the product's step orchestration
 (``exch.step``), cart (``exch.Cart``) and transport (``exch.DistTransport``)
 over host tensors.  Each rank's subdomain is a numpy stand-in written here --
 the same bins, bags, shifts and record layout as the device kernels, with
@@ -336,7 +336,7 @@ def _rank_main(rank, world, port, dims, L, out, with_cells=False):
     q = pp[sel].copy()
     q[:, :3] -= o
     if with_cells:
-        cells, rest = _cells(Lg)
+        cells, rest = _cells(Lg, L)
         cc = 0.5 * (cells[..., :3].min(1) + cells[..., :3].max(1))
         cb = np.floor((cc + np.array(Lg) / 2) / np.array(L)).astype(int)
         csel = np.flatnonzero((cb == me).all(1))
@@ -354,7 +354,7 @@ def _rank_main(rank, world, port, dims, L, out, with_cells=False):
     dist.destroy_process_group()
 
 
-def _cells(Lg):
+def _cells(Lg, L):
     """Four cells of NV vertices (a cube of edge 0.7, rotated, perturbed)
     with their springs' rest lengths; two sit just inside a face (the one
     between the first two ranks along x, and the periodic one) and drift
@@ -363,7 +363,8 @@ def _cells(Lg):
     cube = np.array([[x, y, z] for x in (-0.35, 0.35) for y in (-0.35, 0.35) for z in (-0.35, 0.35)])
     rest = np.sqrt(((cube[:, None] - cube[None]) ** 2).sum(-1))
     hx = Lg[0] / 2
-    centres = [(-0.02, 0.3, 0.2), (hx - 0.02, -0.9, 0.6), (-hx / 2, Lg[1] / 2 - 0.3, -Lg[2] / 2 + 0.2),
+    face = -hx + L[0]                       # between the first two ranks along x
+    centres = [(face - 0.02, 0.3, 0.2), (hx - 0.02, -0.9, 0.6), (-hx / 2, Lg[1] / 2 - 0.3, -Lg[2] / 2 + 0.2),
                (hx / 2, 0.4, -0.5)]
     cells = []
     for c in centres:
@@ -433,7 +434,7 @@ def _run_ranks(dims, L, with_cells):
     return res
 
 
-@pytest.mark.parametrize("dims", [(2, 1, 1), (2, 2, 1), (2, 2, 2)])
+@pytest.mark.parametrize("dims", [(3, 1, 1), (2, 1, 1), (2, 2, 1), (2, 2, 2)])
 def test_ranks_gloo_cells_equal_undivided_box(dims):
     """Solvent and cells flowing along x: after three steps the ranks hold
     exactly the undivided box's solvent and cells (1e-9), every cell on one
@@ -441,7 +442,7 @@ def test_ranks_gloo_cells_equal_undivided_box(dims):
     L = (4, 4, 4)
     res = _run_ranks(dims, L, True)
     pp, Lg = _system(dims, L, 2.0)
-    cells, rest = _cells(Lg)
+    cells, rest = _cells(Lg, L)
     ref, cref = undivided_cells(pp, cells, rest, Lg, 3)
     Lg = np.array(Lg, float)
     got = np.full_like(ref, np.nan)
@@ -517,7 +518,7 @@ class PtrSubCells(NumpySubCells):
                 counts, 32)
 
 
-@pytest.mark.parametrize("dims", [(2, 1, 1), (2, 2, 1)])
+@pytest.mark.parametrize("dims", [(3, 1, 1), (2, 1, 1), (2, 2, 1)])
 def test_local_transport_by_address_equals_undivided_box(dims, monkeypatch):
     """All ranks in one process (LocalTransport): exch.step moves every bag
     by address, one copy call per exchange, and after three steps of solvent
@@ -529,7 +530,7 @@ def test_local_transport_by_address_equals_undivided_box(dims, monkeypatch):
     L = (4, 4, 4)
     cart = exch.Cart(dims)
     pp, Lg = _system(dims, L, 2.0)
-    cells, rest = _cells(Lg)
+    cells, rest = _cells(Lg, L)
     c = np.floor((pp[:, :3] + np.array(Lg) / 2) / np.array(L)).astype(int)
     cc = 0.5 * (cells[..., :3].min(1) + cells[..., :3].max(1))
     cb = np.floor((cc + np.array(Lg) / 2) / np.array(L)).astype(int)
