@@ -245,6 +245,8 @@ def cpu_sample_box(L, target_s=3.0):
 def cpu_steps(L, nsteps, bodyf):
     import oracle
     from ctc_b200 import systems
+    # every host core this process may run on (torchrun sets OMP_NUM_THREADS=1)
+    oracle.set_num_threads(len(os.sched_getaffinity(0)))
     pp = systems.solvent(L, seed=2)
     dpd = systems.dpd_params()
     k0 = oracle.Kiss(0, 0, 0, 0)

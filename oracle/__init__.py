@@ -105,6 +105,7 @@ def lib():
             "orc_diag": (None, [C.c_int, f32p, C.c_double, f64p]),
             "orc_read_floats": (C.c_int, [C.c_char_p, f32p, C.c_int]),
             "orc_num_threads": (C.c_int, []),
+            "orc_set_num_threads": (None, [C.c_int]),
             "orc_dpd_step": (C.c_int, [C.c_int] * 4 + [f32p, f32p, Dpd, f32p, C.c_float, C.c_void_p, C.c_float]),
             "orc_sdf_tex_size": (None, [i32p, i32p]),
             "orc_sdf_resample": (None, [i32p, f32p, f32p, i32p, i32p, f32p, f32p, f32p, f32p]),
@@ -410,6 +411,10 @@ def read_floats(path, cap=1 << 24):
 
 def num_threads():
     return lib().orc_num_threads()
+
+
+def set_num_threads(n):
+    lib().orc_set_num_threads(int(n))
 
 
 def dpd_step(L, pp, dpd, seeds, mass, bodyf, dt):

@@ -37,6 +37,16 @@ int orc_num_threads(void) {
 #endif
 }
 
+/* the threads the timed CPU steps use (a launcher may have set
+ * OMP_NUM_THREADS=1 for its ranks); n <= 0 leaves the setting as it is */
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
 /* bulk pair loop of src/fluforces/bulk/dev/main.h:23-97 for the particles
  * [i0, i1); the reactions land at most one z-layer below the particle's own
  * layer, so slabs of two cell layers of one colour never write the same
