@@ -44,31 +44,38 @@ def test_rbc_system_steps_vs_oracle(bodyf):
     assert C.device_error() == 0
 
 
-def test_sim_graph_replay_matches_direct_launches():
+@pytest.mark.parametrize("edge", [12, 32])
+def test_sim_graph_replay_matches_direct_launches(edge):
     """The step replayed as CUDA graphs gives the direct launches' result and
-    advances the host mirrors of the trunks alike (membranes and contact on)."""
+    advances the host mirrors of the trunks alike (membranes and contact on).
+    In the 32^3 box (327,680 particles) both run the halo and solvent-membrane
+    pairs on the second stream beside the bulk pairs; a third run, profiled,
+    runs them one after the other, and all three agree."""
     import ctc_b200 as C
-    L = (12, 12, 12)
+    L = (edge, edge, edge)
     ps = systems.solvent(L, seed=91)
     pv, tri, par = systems.rbc_system(L, 1, seed=92)
     dpd = systems.dpd_params()
     fsi = C.DpdParams(0.0, 8.0, dpd[2], 0.25)
     cnt = C.DpdLjParams(2.6666667, 8.0, dpd[2], 0.25, 0.3, 0.44)
     out = []
-    for graph in (False, True):
+    for graph, prof in ((False, False), (True, False), (False, True)):
         sim = C.Sim(L, len(ps), C.DpdParams(*dpd), mass=1.0, dt=systems.DT, bodyf=(0.01, 0.0, 0.0))
         sim.set_solvent(ps)
         sim.set_membranes(pv, tri, len(pv), par, fsi, mass=systems.RBC_MASS)
         sim.set_contact(cnt)
         sim.set_graph(graph)
+        sim.profile(prof)
         sim.step(4)
+        sim.profile(False)
         seeds = sim.next_seeds()
         out.append((sim.get_solvent(), sim.get_membranes(), seeds))
         sim.close()
-    (s0, v0, k0), (s1, v1, k1) = out
-    assert np.array_equal(k0, k1)
-    assert s0.shape == s1.shape
-    assert np.abs(s0 - s1).max() < 1e-4 and np.abs(v0 - v1).max() < 1e-4
+    (s0, v0, k0) = out[2]
+    for s1, v1, k1 in out[:2]:
+        assert np.array_equal(k0, k1)
+        assert s0.shape == s1.shape
+        assert np.abs(s0 - s1).max() < 1e-4 and np.abs(v0 - v1).max() < 1e-4
     assert C.device_error() == 0
 
 
